@@ -1,0 +1,273 @@
+"""ORACLE — test infrastructure only.
+
+ctypes binding of the CPU restatement in this folder (``_build/liboracle.so``).
+Only the tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+it; the product path never imports it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+P = (1 << 31) - 1
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", _HERE, "-j8"])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+U32P = C.POINTER(C.c_uint32)
+U8P = C.POINTER(C.c_uint8)
+PP = C.POINTER(U32P)
+
+
+def _declare(L):
+    def f(name, res, *args):
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = list(args)
+
+    f("oracle_set_threads", None, C.c_int)
+    f("oracle_max_threads", C.c_int)
+    f("oracle_m31_reduce", C.c_uint32, C.c_uint64)
+    f("oracle_m31_partial_reduce", C.c_uint32, C.c_uint32)
+    f("oracle_m31_mul", C.c_uint32, C.c_uint32, C.c_uint32)
+    f("oracle_m31_inv", C.c_uint32, C.c_uint32)
+    f("oracle_qm31_mul", None, U32P, U32P, U32P)
+    f("oracle_qm31_inv", None, U32P, U32P)
+    f("oracle_index_to_point", None, C.c_uint64, U32P)
+    f("oracle_secure_gen_mul", None, C.c_uint64, C.c_uint64, U32P)
+    f("oracle_blake2s", None, U8P, C.c_size_t, U8P)
+    f("oracle_twiddles_half_odds", None, C.c_uint32, U32P, U32P)
+    f("oracle_interpolate", None, U32P, C.c_uint32, C.c_uint32)
+    f("oracle_interpolate_columns", None, PP, C.c_uint32, C.c_uint32, C.c_uint32)
+    f("oracle_evaluate", None, U32P, C.c_size_t, C.c_uint32, C.c_uint32, U32P)
+    f("oracle_evaluate_columns", None, PP, C.c_uint32, C.c_size_t, C.c_uint32, C.c_uint32, PP)
+    f("oracle_bit_reverse", None, U32P, C.c_uint32)
+    f("oracle_commit_on_layer", None, C.c_uint32, U8P, C.c_uint32, PP, U8P)
+    f("oracle_merkle_root", None, C.c_uint32, PP, U32P, U8P)
+    f("oracle_channel_mix_u32s", None, U32P, C.c_size_t, U8P)
+    f("oracle_channel_mix_u64", None, C.c_uint64, U8P)
+    f("oracle_channel_draw_secure_felts", C.c_uint32, U8P, C.c_size_t, U32P)
+    f("oracle_grind", C.c_uint64, U8P, C.c_uint32)
+    f("oracle_verify_pow", C.c_int, U8P, C.c_uint32, C.c_uint64)
+    f("oracle_fold_line", None, PP, C.c_uint32, U32P, PP)
+    f("oracle_fold_circle_into_line", None, PP, PP, C.c_uint32, U32P)
+    f("oracle_accumulate_numerators", None, C.c_uint32, C.c_uint32, PP, U32P, C.c_uint32, U32P, U32P, U32P, PP, U32P)
+    f("oracle_compute_quotients_and_combine", None, C.c_uint32, PP, U32P, U32P, U32P, C.c_uint32, PP)
+    f("oracle_lift_and_accumulate", None, C.c_uint32, PP, U32P, PP)
+    f("oracle_eval_at_point", None, U32P, C.c_uint32, U32P, U32P)
+    if hasattr(L, "oracle_prove"):
+        f("oracle_prove", C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32,
+          C.c_uint32, C.c_uint32, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t))
+        f("oracle_verify", C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_size_t)
+
+
+# ---------------------------------------------------------------- helpers
+def u32(a):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    return a, a.ctypes.data_as(U32P)
+
+
+def ptr_array(arrays):
+    arr = (U32P * len(arrays))(*[a.ctypes.data_as(U32P) for a in arrays])
+    return C.cast(arr, PP), arr
+
+
+def planes(q):
+    """(n,4) uint32 array -> list of 4 contiguous planes."""
+    return [np.ascontiguousarray(q[:, i]) for i in range(4)]
+
+
+def unplanes(ps):
+    return np.stack(ps, axis=1)
+
+
+def set_threads(n):
+    lib().oracle_set_threads(n)
+
+
+def max_threads():
+    return lib().oracle_max_threads()
+
+
+def blake2s(data: bytes) -> bytes:
+    buf = (C.c_uint8 * max(len(data), 1)).from_buffer_copy(data or b"\0")
+    out = (C.c_uint8 * 32)()
+    lib().oracle_blake2s(buf, len(data), out)
+    return bytes(out)
+
+
+def twiddles_half_odds(log_size):
+    n = 1 << log_size
+    tw = np.zeros(n, np.uint32)
+    itw = np.zeros(n, np.uint32)
+    lib().oracle_twiddles_half_odds(log_size, tw.ctypes.data_as(U32P), itw.ctypes.data_as(U32P))
+    return tw, itw
+
+
+def interpolate(values, log_n, root_log=None):
+    v = np.array(values, dtype=np.uint32)
+    lib().oracle_interpolate(v.ctypes.data_as(U32P), log_n, root_log if root_log is not None else max(log_n - 1, 1))
+    return v
+
+
+def interpolate_columns(cols, log_n, root_log=None):
+    cols = [np.array(c, dtype=np.uint32) for c in cols]
+    pp, keep = ptr_array(cols)
+    lib().oracle_interpolate_columns(pp, len(cols), log_n, root_log if root_log is not None else max(log_n - 1, 1))
+    return cols
+
+
+def evaluate(coeffs, log_n, root_log=None):
+    c, cp = u32(coeffs)
+    out = np.zeros(1 << log_n, np.uint32)
+    lib().oracle_evaluate(cp, len(c), log_n, root_log if root_log is not None else max(log_n - 1, 1), out.ctypes.data_as(U32P))
+    return out
+
+
+def evaluate_columns(cols, log_n, root_log=None):
+    cols = [np.ascontiguousarray(c, dtype=np.uint32) for c in cols]
+    outs = [np.zeros(1 << log_n, np.uint32) for _ in cols]
+    ip, k1 = ptr_array(cols)
+    op, k2 = ptr_array(outs)
+    lib().oracle_evaluate_columns(ip, len(cols), len(cols[0]), log_n,
+                                  root_log if root_log is not None else max(log_n - 1, 1), op)
+    return outs
+
+
+def bit_reverse(values):
+    v = np.array(values, dtype=np.uint32)
+    lib().oracle_bit_reverse(v.ctypes.data_as(U32P), int(len(v)).bit_length() - 1)
+    return v
+
+
+def commit_on_layer(log_size, prev, cols):
+    cols = [np.ascontiguousarray(c, dtype=np.uint32) for c in cols]
+    out = np.zeros((1 << log_size) * 32, np.uint8)
+    pp, keep = ptr_array(cols) if cols else (C.cast(None, PP), None)
+    prev_p = None
+    if prev is not None:
+        prev = np.ascontiguousarray(prev, dtype=np.uint8)
+        prev_p = prev.ctypes.data_as(U8P)
+    lib().oracle_commit_on_layer(log_size, prev_p, len(cols), pp, out.ctypes.data_as(U8P))
+    return out.reshape(-1, 32)
+
+
+def merkle_root(cols):
+    cols = [np.ascontiguousarray(c, dtype=np.uint32) for c in cols]
+    logs = np.array([int(len(c)).bit_length() - 1 for c in cols], np.uint32)
+    pp, keep = ptr_array(cols) if cols else (C.cast(None, PP), None)
+    out = (C.c_uint8 * 32)()
+    lib().oracle_merkle_root(len(cols), pp, logs.ctypes.data_as(U32P), out)
+    return bytes(out)
+
+
+def channel_mix_u32s(words):
+    w, wp = u32(words)
+    out = (C.c_uint8 * 32)()
+    lib().oracle_channel_mix_u32s(wp, len(w), out)
+    return bytes(out)
+
+
+def channel_mix_u64(v):
+    out = (C.c_uint8 * 32)()
+    lib().oracle_channel_mix_u64(v, out)
+    return bytes(out)
+
+
+def grind(digest: bytes, pow_bits):
+    d = (C.c_uint8 * 32).from_buffer_copy(digest)
+    return lib().oracle_grind(d, pow_bits)
+
+
+def verify_pow(digest: bytes, pow_bits, nonce):
+    d = (C.c_uint8 * 32).from_buffer_copy(digest)
+    return bool(lib().oracle_verify_pow(d, pow_bits, nonce))
+
+
+def fold_line(eval_q, log_n, alpha):
+    ps = planes(eval_q)
+    outs = [np.zeros(1 << (log_n - 1), np.uint32) for _ in range(4)]
+    ip, k1 = ptr_array(ps)
+    op, k2 = ptr_array(outs)
+    a, ap = u32(alpha)
+    lib().oracle_fold_line(ip, log_n, ap, op)
+    return unplanes(outs)
+
+
+def fold_circle_into_line(dst_q, src_q, log_n, alpha):
+    dps = planes(dst_q)
+    sps = planes(src_q)
+    dp, k1 = ptr_array(dps)
+    sp, k2 = ptr_array(sps)
+    a, ap = u32(alpha)
+    lib().oracle_fold_circle_into_line(dp, sp, log_n, ap)
+    return unplanes(dps)
+
+
+def accumulate_numerators(cols, log_size, point8, col_idx, values4, rand4):
+    cols = [np.ascontiguousarray(c, dtype=np.uint32) for c in cols]
+    pp, keep = ptr_array(cols)
+    outs = [np.zeros(1 << log_size, np.uint32) for _ in range(4)]
+    op, k2 = ptr_array(outs)
+    flt = np.zeros(4, np.uint32)
+    pt, ptp = u32(point8)
+    ci, cip = u32(col_idx)
+    v, vp = u32(np.asarray(values4).reshape(-1))
+    r, rp = u32(np.asarray(rand4).reshape(-1))
+    lib().oracle_accumulate_numerators(log_size, len(cols), pp, ptp, len(ci), cip, vp, rp, op, flt.ctypes.data_as(U32P))
+    return unplanes(outs), flt
+
+
+def compute_quotients_and_combine(partials, first_linear4, points8, lifting_log_size):
+    all_planes = []
+    logs = []
+    for p in partials:
+        all_planes += planes(p)
+        logs.append(int(len(p)).bit_length() - 1)
+    pp, keep = ptr_array(all_planes)
+    lg, lgp = u32(logs)
+    fl, flp = u32(np.asarray(first_linear4).reshape(-1))
+    pt, ptp = u32(np.asarray(points8).reshape(-1))
+    outs = [np.zeros(1 << lifting_log_size, np.uint32) for _ in range(4)]
+    op, k2 = ptr_array(outs)
+    lib().oracle_compute_quotients_and_combine(len(partials), pp, lgp, flp, ptp, lifting_log_size, op)
+    return unplanes(outs)
+
+
+def lift_and_accumulate(cols_q):
+    all_planes = []
+    logs = []
+    for p in cols_q:
+        all_planes += planes(p)
+        logs.append(int(len(p)).bit_length() - 1)
+    pp, keep = ptr_array(all_planes)
+    lg, lgp = u32(logs)
+    outs = [np.zeros(len(cols_q[-1]), np.uint32) for _ in range(4)]
+    op, k2 = ptr_array(outs)
+    lib().oracle_lift_and_accumulate(len(cols_q), pp, lgp, op)
+    return unplanes(outs)
+
+
+def eval_at_point(coeffs, point8):
+    c, cp = u32(coeffs)
+    pt, ptp = u32(point8)
+    out = np.zeros(4, np.uint32)
+    lib().oracle_eval_at_point(cp, int(len(c)).bit_length() - 1, ptp, out.ctypes.data_as(U32P))
+    return out

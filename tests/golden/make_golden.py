@@ -1,0 +1,76 @@
+"""Extracts the reference's known-answer vectors for the prover hot path into
+``reference_vectors.json``.
+
+The reference is a Rust crate that cannot be built in this container, so its
+own test files are read as text and the literal expected values are copied
+out. Run from the repository root, in the container that holds the reference:
+
+    python tests/golden/make_golden.py /root/reference
+
+Sources (paths inside the reference checkout):
+  crates/stwo/src/core/vcs/blake2_hash.rs      single_hash_test   (Blake2s of b"a")
+  crates/stwo/src/core/channel/blake2s.rs      test_mix_u64, test_mix_u32s (channel digests)
+  crates/stwo/src/core/fields/m31.rs           doc-tests of partial_reduce / reduce
+  crates/stwo/src/core/circle.rs               M31_CIRCLE_GEN, SECURE_FIELD_CIRCLE_GEN,
+                                               test_secure_field_circle_gen prime factors
+"""
+import json
+import os
+import re
+import sys
+
+
+def _read(root, rel):
+    with open(os.path.join(root, rel)) as f:
+        return f.read()
+
+
+def _byte_array_after(text, marker):
+    # the expected digest is the first bracketed list of hex bytes after `marker`
+    i = text.index(marker)
+    m = re.search(r"\[\s*0x", text[i:])
+    j = i + m.start()
+    block = text[j:text.index("]", j) + 1]
+    return [int(x, 16) for x in re.findall(r"0x([0-9a-fA-F]+)", block)]
+
+
+def main(root):
+    out = {}
+    bh = _read(root, "crates/stwo/src/core/vcs/blake2_hash.rs")
+    m = re.search(r'Blake2sHasher::hash\(b"a"\);\s*assert_eq!\(\s*hash_a\.to_string\(\),\s*"([0-9a-f]{64})"', bh)
+    out["blake2s_a"] = m.group(1)
+
+    ch = _read(root, "crates/stwo/src/core/channel/blake2s.rs")
+    out["channel_mix_u64"] = {
+        "value": int(re.search(r"mix_u64\((0x[0-9a-fA-F]+)\)", ch).group(1), 16),
+        "digest": _byte_array_after(ch, "let digest_bytes: [u8; 32] = digest_64.into();"),
+        "u32s": [int(x, 16) for x in re.search(r"mix_u32s\(&\[(0x[0-9a-fA-F]+),\s*(0x[0-9a-fA-F]+)\]\)", ch).groups()],
+    }
+    m = re.search(r"pub fn test_mix_u32s.*?mix_u32s\(&\[([0-9,\s]+)\]\)", ch, re.S)
+    out["channel_mix_u32s"] = {
+        "words": [int(x) for x in m.group(1).split(",") if x.strip()],
+        "digest": _byte_array_after(ch, "pub fn test_mix_u32s"),
+    }
+
+    m31 = _read(root, "crates/stwo/src/core/fields/m31.rs")
+    out["m31_partial_reduce"] = {"input_expr": "2*P-19", "expected_expr": "P-19",
+                                 "found": "let val = 2 * P - 19;" in m31}
+    out["m31_reduce"] = {"input_expr": "P^2-19", "expected_expr": "P-19",
+                         "found": "let val = (P as u64).pow(2) - 19;" in m31}
+
+    circ = _read(root, "crates/stwo/src/core/circle.rs")
+    g = re.search(r"M31_CIRCLE_GEN: CirclePoint<M31> = CirclePoint \{\s*x: M31::from_u32_unchecked\((\d+)\),\s*y: M31::from_u32_unchecked\((\d+)\)", circ)
+    out["m31_circle_gen"] = [int(g.group(1)), int(g.group(2))]
+    sg = re.search(r"SECURE_FIELD_CIRCLE_GEN: CirclePoint<SecureField> = CirclePoint \{\s*x: SecureField::from_u32_unchecked\(([\d,\s]+)\),\s*y: SecureField::from_u32_unchecked\(([\d,\s]+)\)", circ)
+    out["secure_circle_gen"] = [[int(v) for v in sg.group(1).split(",")], [int(v) for v in sg.group(2).split(",")]]
+    pf = re.search(r"let prime_factors = \[(.*?)\];", circ, re.S).group(1)
+    out["secure_circle_order_factors"] = [[int(a), int(b)] for a, b in re.findall(r"\((\d+),\s*(\d+)\)", pf)]
+
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_vectors.json")
+    with open(dst, "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", dst)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

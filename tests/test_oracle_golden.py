@@ -1,0 +1,178 @@
+"""Pins the CPU oracle against the reference's known-answer vectors and against
+independent definitions (hashlib's Blake2s, the circle-polynomial basis)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as O
+
+P = O.P
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_vectors.json")))
+
+
+def test_blake2s_known_answer():
+    # crates/stwo/src/core/vcs/blake2_hash.rs single_hash_test
+    assert O.blake2s(b"a").hex() == GOLDEN["blake2s_a"]
+
+
+@pytest.mark.parametrize("n", [0, 1, 3, 31, 32, 33, 63, 64, 65, 100, 127, 128, 129, 400, 632, 1000])
+def test_blake2s_matches_rfc7693(n):
+    rng = np.random.default_rng(n)
+    data = rng.integers(0, 256, n, dtype=np.uint8).tobytes()
+    assert O.blake2s(data) == hashlib.blake2s(data, digest_size=32).digest()
+
+
+def test_channel_known_answers():
+    # crates/stwo/src/core/channel/blake2s.rs test_mix_u64 / test_mix_u32s
+    g = GOLDEN["channel_mix_u64"]
+    assert O.channel_mix_u64(g["value"]) == bytes(g["digest"])
+    assert O.channel_mix_u32s(g["u32s"]) == bytes(g["digest"])
+    g = GOLDEN["channel_mix_u32s"]
+    assert O.channel_mix_u32s(g["words"]) == bytes(g["digest"])
+
+
+def test_m31_doc_vectors():
+    L = O.lib()
+    assert GOLDEN["m31_partial_reduce"]["found"] and GOLDEN["m31_reduce"]["found"]
+    assert L.oracle_m31_partial_reduce(2 * P - 19) == P - 19
+    assert L.oracle_m31_reduce(P * P - 19) == P - 19
+    rng = np.random.default_rng(1)
+    for _ in range(200):
+        a, b = (int(x) for x in rng.integers(0, P, 2))
+        assert L.oracle_m31_mul(a, b) == a * b % P
+        if a:
+            assert L.oracle_m31_mul(L.oracle_m31_inv(a), a) == 1
+
+
+def test_qm31_inverse():
+    rng = np.random.default_rng(2)
+    for _ in range(50):
+        a = rng.integers(0, P, 4).astype(np.uint32)
+        ai = np.zeros(4, np.uint32)
+        O.lib().oracle_qm31_inv(O.u32(a)[1], ai.ctypes.data_as(O.U32P))
+        r = np.zeros(4, np.uint32)
+        O.lib().oracle_qm31_mul(O.u32(a)[1], O.u32(ai)[1], r.ctypes.data_as(O.U32P))
+        assert list(r) == [1, 0, 0, 0]
+
+
+def test_circle_generators():
+    # crates/stwo/src/core/circle.rs: M31_CIRCLE_GEN has order 2^31.
+    xy = np.zeros(2, np.uint32)
+    O.lib().oracle_index_to_point(1, xy.ctypes.data_as(O.U32P))
+    assert list(xy) == GOLDEN["m31_circle_gen"]
+    O.lib().oracle_index_to_point(1 << 30, xy.ctypes.data_as(O.U32P))
+    assert list(xy) == [P - 1, 0]
+    # test_secure_field_circle_gen: GEN^(P^4-1) = identity, GEN^((P^4-1)/p) != identity.
+    order = P ** 4 - 1
+    prod = 1
+    for p, e in GOLDEN["secure_circle_order_factors"]:
+        prod *= p ** e
+    assert prod == order
+    out = np.zeros(8, np.uint32)
+
+    def gen_mul(s):
+        O.lib().oracle_secure_gen_mul(s & (2 ** 64 - 1), s >> 64, out.ctypes.data_as(O.U32P))
+        return list(out)
+
+    assert gen_mul(1) == GOLDEN["secure_circle_gen"][0] + GOLDEN["secure_circle_gen"][1]
+    assert gen_mul(order) == [1, 0, 0, 0, 0, 0, 0, 0]
+    for p, _ in GOLDEN["secure_circle_order_factors"]:
+        assert gen_mul(order // p) != [1, 0, 0, 0, 0, 0, 0, 0]
+
+
+def _domain_points(log_n):
+    """Canonic circle domain points in natural order, by index arithmetic."""
+    pts = []
+    half = 1 << (log_n - 1)
+    init = 1 << (31 - (log_n + 1))       # half_odds(log_n - 1).initial_index
+    step = 1 << (31 - (log_n - 1))
+    xy = np.zeros(2, np.uint32)
+    for i in range(1 << log_n):
+        idx = (init + step * i) % (1 << 31) if i < half else (-(init + step * (i - half))) % (1 << 31)
+        O.lib().oracle_index_to_point(idx, xy.ctypes.data_as(O.U32P))
+        pts.append((int(xy[0]), int(xy[1])))
+    return pts
+
+
+def _bitrev(i, n):
+    return int(format(i, "0{}b".format(n))[::-1], 2) if n else i
+
+
+@pytest.mark.parametrize("log_n", [1, 2, 3, 4, 5, 7])
+def test_fft_matches_basis_definition(log_n):
+    """evaluate() at bit-reversed position i equals the coefficient polynomial
+    folded at domain point i (the circle-FFT basis, cpu/circle.rs:82-98)."""
+    rng = np.random.default_rng(log_n)
+    coeffs = rng.integers(0, P, 1 << log_n).astype(np.uint32)
+    evals = O.evaluate(coeffs, log_n)
+    pts = _domain_points(log_n)
+    for i in range(1 << log_n):
+        x, y = pts[i]
+        v = O.eval_at_point(coeffs, [x, 0, 0, 0, y, 0, 0, 0])
+        assert list(v) == [int(evals[_bitrev(i, log_n)]), 0, 0, 0]
+    back = O.interpolate(evals, log_n)
+    assert np.array_equal(back, coeffs)
+
+
+@pytest.mark.parametrize("log_n", [8, 12, 16])
+def test_fft_roundtrip_and_lde(log_n):
+    rng = np.random.default_rng(log_n)
+    coeffs = rng.integers(0, P, 1 << log_n).astype(np.uint32)
+    ev = O.evaluate(coeffs, log_n, root_log=log_n + 1)
+    assert np.array_equal(O.interpolate(ev, log_n, root_log=log_n + 1), coeffs)
+    lde = O.evaluate(coeffs, log_n + 1, root_log=log_n + 1)
+    back = O.interpolate(lde, log_n + 1, root_log=log_n + 1)
+    assert np.array_equal(back[: 1 << log_n], coeffs) and not back[1 << log_n:].any()
+
+
+def test_merkle_layer_is_blake2s_of_bytes():
+    rng = np.random.default_rng(3)
+    cols = [rng.integers(0, P, 8).astype(np.uint32) for _ in range(5)]
+    leaves = O.commit_on_layer(3, None, cols)
+    for i in range(8):
+        data = b"".join(int(c[i]).to_bytes(4, "little") for c in cols)
+        assert bytes(leaves[i]) == hashlib.blake2s(data, digest_size=32).digest()
+    nodes = O.commit_on_layer(2, leaves.reshape(-1), cols[:2])
+    for i in range(4):
+        data = bytes(leaves[2 * i]) + bytes(leaves[2 * i + 1]) + b"".join(int(c[i]).to_bytes(4, "little") for c in cols[:2])
+        assert bytes(nodes[i]) == hashlib.blake2s(data, digest_size=32).digest()
+    # an empty tree is the hash of the empty string (prover.rs:23-27)
+    assert O.merkle_root([]) == hashlib.blake2s(b"", digest_size=32).digest()
+
+
+def test_grind_is_smallest_nonce():
+    digest = hashlib.blake2s(b"grind", digest_size=32).digest()
+    nonce = O.grind(digest, 8)
+    assert O.verify_pow(digest, 8, nonce)
+    assert not any(O.verify_pow(digest, 8, n) for n in range(nonce))
+
+
+def _qm(a):
+    return [int(v) for v in a]
+
+
+def test_fold_line_formula():
+    """fold_line: f0,f1 = ibutterfly(f(x), f(-x), 1/x); out = f0 + alpha f1."""
+    rng = np.random.default_rng(4)
+    log_n = 4
+    ev = rng.integers(0, P, (1 << log_n, 4)).astype(np.uint32)
+    alpha = rng.integers(0, P, 4).astype(np.uint32)
+    out = O.fold_line(ev, log_n, alpha)
+    # LineDomain(half_odds(4)): x of coset points; bit-reversed pair index.
+    init = 1 << (31 - (log_n + 2))
+    step = 1 << (31 - log_n)
+    xy = np.zeros(2, np.uint32)
+    L = O.lib()
+    for i in range(1 << (log_n - 1)):
+        j = _bitrev(i << 1, log_n)
+        L.oracle_index_to_point((init + step * j) % (1 << 31), xy.ctypes.data_as(O.U32P))
+        xinv = L.oracle_m31_inv(int(xy[0]))
+        f0 = [(int(a) + int(b)) % P for a, b in zip(ev[2 * i], ev[2 * i + 1])]
+        f1 = [((int(a) - int(b)) % P) * xinv % P for a, b in zip(ev[2 * i], ev[2 * i + 1])]
+        r = np.zeros(4, np.uint32)
+        L.oracle_qm31_mul(O.u32(alpha)[1], O.u32(np.array(f1, np.uint32))[1], r.ctypes.data_as(O.U32P))
+        expect = [(a + int(b)) % P for a, b in zip(f0, r)]
+        assert _qm(out[i]) == expect
