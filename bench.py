@@ -1,0 +1,435 @@
+#!/usr/bin/env python
+"""Benchmark driver: prints ONE JSON line (rank 0).
+
+Workloads
+  kernels   the kernel-level sweep: circle-FFT evaluate + interpolate of one
+            M31 column at log sizes 16..26, Blake2s Merkle commit (leaves +
+            all node layers) of 64 M31 columns at log size 20, and a QM31
+            fold_line of a 2^22 line evaluation. metric: algorithmic GB/s.
+  poseidon  (default once the prover is built) full Poseidon2 proof, 2^18
+            instances; metric: proof ms.
+
+Multi-GPU: every rank runs the same workload on its own GPU (independent
+replicas, no collective on the data path); value = work of all ranks / the
+slowest rank's time ("scaling": "weak").
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "nitroozk-stwo_b200"))
+
+import numpy as np  # noqa: E402
+
+P = (1 << 31) - 1
+L2_BYTES = 126 * (1 << 20)
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ distributed
+def dist_setup(args, backend):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world, device=None):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------ kernel sweep
+FFT_LOGS = list(range(16, 27))
+MERKLE_LOG, MERKLE_COLS = 20, 64
+FOLD_LOG = 22
+
+
+def sweep_bytes():
+    fft = {n: 16 * (1 << n) for n in FFT_LOGS}            # evaluate 8*2^n + interpolate 8*2^n
+    merkle_leaf = (4 * MERKLE_COLS + 32) * (1 << MERKLE_LOG)
+    merkle_nodes = sum(96 * (1 << L) for L in range(MERKLE_LOG))
+    fold = 24 * (1 << FOLD_LOG)
+    return fft, merkle_leaf, merkle_nodes, fold
+
+
+class KernelSweep:
+    def __init__(self, seed):
+        import torch
+        from gpustark.backend import GpuBackend, to_device, Context
+        self.torch = torch
+        self.B = GpuBackend
+        self.stream = torch.cuda.current_stream()
+        self.ctx = Context(self.stream)
+        rng = np.random.default_rng(seed)
+        self.tw = self.B.precompute_twiddles(max(FFT_LOGS), ctx=self.ctx)
+        self.tw_fold = self.B.precompute_twiddles(FOLD_LOG + 1, ctx=self.ctx)
+        self.host_fft = {n: rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32) for n in FFT_LOGS}
+        self.fft_in = {n: to_device(self.host_fft[n]) for n in FFT_LOGS}
+        self.fft_buf = {n: torch.empty(1 << n, dtype=torch.int32, device="cuda") for n in FFT_LOGS}
+        self.host_cols = [rng.integers(0, P, 1 << MERKLE_LOG, dtype=np.int64).astype(np.uint32) for _ in range(MERKLE_COLS)]
+        self.cols = [to_device(c) for c in self.host_cols]
+        self.layers = [torch.empty((1 << L) * 8, dtype=torch.int32, device="cuda") for L in range(MERKLE_LOG + 1)]
+        self.host_fold = rng.integers(0, P, (1 << FOLD_LOG, 4), dtype=np.int64).astype(np.uint32)
+        self.fold_in = [to_device(self.host_fold[:, i].copy()) for i in range(4)]
+        self.alpha = rng.integers(0, P, 4).tolist()
+        self.flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
+        self.groups = ["fft%d" % n for n in FFT_LOGS] + ["merkle_leaf", "merkle_nodes", "fold_line"]
+        self.times = {g: [] for g in self.groups}
+
+    def flush_l2(self):
+        self.flush.zero_()
+
+    def step(self, record=True):
+        torch = self.torch
+        ev = {}
+
+        def mark(name):
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(self.stream)
+            ev[name] = e
+
+        for n in FFT_LOGS:
+            mark("fft%d_s" % n)
+            self.B.evaluate_polynomials([self.fft_in[n]], n, self.tw, out=[self.fft_buf[n]], ctx=self.ctx)
+            self.B.interpolate_columns([self.fft_buf[n]], n, self.tw, ctx=self.ctx)
+            mark("fft%d_e" % n)
+        mark("merkle_leaf_s")
+        self.B.commit_on_layer(MERKLE_LOG, None, self.cols, ctx=self.ctx, out=self.layers[MERKLE_LOG])
+        mark("merkle_leaf_e")
+        mark("merkle_nodes_s")
+        for L in range(MERKLE_LOG - 1, -1, -1):
+            self.B.commit_on_layer(L, self.layers[L + 1], [], ctx=self.ctx, out=self.layers[L])
+        mark("merkle_nodes_e")
+        mark("fold_line_s")
+        self.B.fold_line(self.fold_in, FOLD_LOG, self.alpha, self.tw_fold, ctx=self.ctx)
+        mark("fold_line_e")
+        if record:
+            self.stream.synchronize()
+            for g in self.groups:
+                self.times[g].append(ev[g + "_s"].elapsed_time(ev[g + "_e"]))
+        return ev
+
+    def e2e_step(self, pinned):
+        """The same work through the C ABI with host buffers: inputs copied from
+        pinned host memory, results (FFT outputs, root, fold) copied back."""
+        torch = self.torch
+        h2d = d2h = 0
+        for n in FFT_LOGS:
+            self.fft_in[n].copy_(pinned["fft%d" % n], non_blocking=True)
+            h2d += 4 << n
+        for i, c in enumerate(self.cols):
+            c.copy_(pinned["col%d" % i], non_blocking=True)
+            h2d += 4 << MERKLE_LOG
+        for i in range(4):
+            self.fold_in[i].copy_(pinned["fold%d" % i], non_blocking=True)
+            h2d += 4 << FOLD_LOG
+        self.step(record=False)
+        for n in FFT_LOGS:
+            pinned["out%d" % n].copy_(self.fft_buf[n], non_blocking=True)
+            d2h += 4 << n
+        pinned["root"].copy_(self.layers[0], non_blocking=True)
+        d2h += 32
+        return h2d, d2h
+
+
+def cpu_sweep_sample(threads):
+    """Oracle (CPU restatement) on a bounded sample of the sweep: FFT log 20,
+    Merkle 64 x 2^16, fold 2^20. Returns (GB/s, seconds, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    O.set_threads(threads)
+    rng = np.random.default_rng(5)
+    n = 20
+    c = rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32)
+    cols = [rng.integers(0, P, 1 << 16, dtype=np.int64).astype(np.uint32) for _ in range(64)]
+    ev = rng.integers(0, P, (1 << 20, 4), dtype=np.int64).astype(np.uint32)
+    alpha = [1, 2, 3, 4]
+    t0 = time.perf_counter()
+    reps = 0
+    total = 0
+    while True:
+        e = O.evaluate(c, n, root_log=n)
+        O.interpolate(e, n, root_log=n)
+        total += 16 * (1 << n)
+        O.merkle_root(cols)
+        total += (4 * 64 + 32) * (1 << 16) + 96 * (1 << 16)
+        O.fold_line(ev, 20, alpha)
+        total += 24 * (1 << 20)
+        reps += 1
+        if time.perf_counter() - t0 > 10 or reps >= 20:
+            break
+    dt = time.perf_counter() - t0
+    return total / dt / 1e9, dt, "oracle: FFT 2^20 eval+interp, Merkle 64x2^16, fold_line 2^20; %d reps" % reps
+
+
+def run_kernels(args, world, rank, local):
+    import torch
+    from gpustark import lib as gslib
+    torch.cuda.set_device(local)
+    hbm_peak, peak_kind = load_peaks()
+    sw = KernelSweep(seed=1234 + rank)
+    fft_b, leaf_b, node_b, fold_b = sweep_bytes()
+    bytes_per_step = sum(fft_b.values()) + leaf_b + node_b + fold_b
+    for _ in range(args.warmup):
+        sw.step(record=False)
+        sw.flush_l2()
+    torch.cuda.synchronize()
+    for g in sw.groups:
+        sw.times[g].clear()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = gslib().gs_launch_count()
+    barrier(world)
+    torch.cuda.synchronize()
+    step_ms = []
+    for _ in range(args.steps):
+        sw.flush_l2()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(sw.stream)
+        sw.step(record=False)
+        ev1.record(sw.stream)
+        sw.stream.synchronize()
+        step_ms.append(ev0.elapsed_time(ev1))
+    torch.cuda.synchronize()
+    barrier(world)
+    launches = gslib().gs_launch_count() - l0
+    clk = clocks.stop()
+    # per-group timing pass (separate, with events between groups)
+    for _ in range(max(2, min(args.steps, 5))):
+        sw.flush_l2()
+        sw.step(record=True)
+    total_ms = max_over_ranks(sum(step_ms), world, "cuda")
+    ms_per_step = total_ms / args.steps
+    value = world * bytes_per_step * args.steps / (total_ms / 1e3) / 1e9
+    # dominant kernel (op) and its roofline
+    avg = {g: statistics.mean(sw.times[g]) for g in sw.groups}
+    dom = max(avg, key=avg.get)
+    alg = {**{"fft%d" % n: fft_b[n] for n in FFT_LOGS}, "merkle_leaf": leaf_b, "merkle_nodes": node_b, "fold_line": fold_b}
+    achieved = alg[dom] / (avg[dom] / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(dom)
+        except Exception:
+            traffic = None
+    # end-to-end through the C ABI with host buffers
+    pinned = {}
+    for n in FFT_LOGS:
+        pinned["fft%d" % n] = torch.from_numpy(sw.host_fft[n].view(np.int32)).pin_memory()
+        pinned["out%d" % n] = torch.empty(1 << n, dtype=torch.int32).pin_memory()
+    for i, c in enumerate(sw.host_cols):
+        pinned["col%d" % i] = torch.from_numpy(c.view(np.int32)).pin_memory()
+    for i in range(4):
+        pinned["fold%d" % i] = torch.from_numpy(sw.host_fold[:, i].copy().view(np.int32)).pin_memory()
+    pinned["root"] = torch.empty(8, dtype=torch.int32).pin_memory()
+    e2e_steps = max(1, min(args.steps, 5))
+    sw.e2e_step(pinned)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(sw.stream)
+    for _ in range(e2e_steps):
+        h2d, d2h = sw.e2e_step(pinned)
+    e1.record(sw.stream)
+    sw.stream.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
+    e2e_value = world * bytes_per_step * e2e_steps / (e2e_ms / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        gbs, secs, desc = cpu_sweep_sample(threads)
+        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc,
+               "seconds": round(secs, 2)}
+    out = {
+        "metric": "FFT/Merkle HBM GB/s (kernel sweep: circle FFT 2^16..2^26, Merkle 64x2^20, fold 2^22)",
+        "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic: seeded uniform M31",
+        "config": {"workload": "kernel sweep (configs[1]): circle-FFT evaluate+interpolate log 16..26, "
+                               "Blake2s Merkle commit 64 cols x 2^20, QM31 fold_line 2^22",
+                   "l2": "flushed between timed steps (write of 2x L2)",
+                   "parallelism": "replicas x%d" % world},
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                     "traffic": traffic, "algorithmic_bytes": alg[dom], "avg_ms": round(avg[dom], 4)},
+        "per_op_ms": {g: round(v, 4) for g, v in avg.items()},
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if cpu:
+        out["cpu_baseline"] = cpu
+    return out
+
+
+def run_reference(args, world, rank):
+    """The reference arm: the CPU implementation of the path (the oracle port,
+    the reference's Rust prover cannot be built here) on all host threads."""
+    if rank != 0:
+        return None
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(args.warmup):
+        cpu_sweep_sample(threads)
+    t_all = 0.0
+    desc = ""
+    for _ in range(args.steps):
+        gbs, secs, desc = cpu_sweep_sample(threads)
+        vals.append(gbs)
+        t_all += secs
+    v = statistics.mean(vals)
+    return {
+        "impl": "reference",
+        "metric": "FFT/Merkle HBM GB/s (kernel sweep: circle FFT 2^16..2^26, Merkle 64x2^20, fold 2^22)",
+        "value": round(v, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * t_all / max(args.steps, 1), 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic: seeded uniform M31",
+        "config": {"workload": "kernel sweep (configs[1]), bounded CPU sample", "parallelism": "cpu threads"},
+        "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def run_case(args):
+    """One op on a small case, for ncu captures: `--case fft:26`, `--case merkle:20:64`, `--case fold:22`."""
+    import torch
+    from gpustark.backend import GpuBackend as B, to_device, Context
+    kind, *params = args.case.split(":")
+    rng = np.random.default_rng(7)
+    ctx = Context(torch.cuda.current_stream())
+    if kind == "fft":
+        n = int(params[0])
+        tw = B.precompute_twiddles(n, ctx=ctx)
+        x = to_device(rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32))
+        y = torch.empty_like(x)
+        work = lambda: (B.evaluate_polynomials([x], n, tw, out=[y], ctx=ctx), B.interpolate_columns([y], n, tw, ctx=ctx))
+    elif kind == "merkle":
+        n, k = int(params[0]), int(params[1])
+        cols = [to_device(rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32)) for _ in range(k)]
+        out = torch.empty((1 << n) * 8, dtype=torch.int32, device="cuda")
+        work = lambda: B.commit_on_layer(n, None, cols, ctx=ctx, out=out)
+    elif kind == "fold":
+        n = int(params[0])
+        tw = B.precompute_twiddles(n + 1, ctx=ctx)
+        ev = [to_device(rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32)) for _ in range(4)]
+        work = lambda: B.fold_line(ev, n, [1, 2, 3, 4], tw, ctx=ctx)
+    else:
+        raise SystemExit("unknown case " + args.case)
+    for _ in range(args.warmup + args.steps):
+        work()
+    torch.cuda.synchronize()
+    print("case done:", args.case)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpustark", choices=["gpustark", "reference"])
+    ap.add_argument("--workload", default="kernels", choices=["kernels"])
+    ap.add_argument("--case", default=None,
+                    help="profiling case: fft:<log>, merkle:<log>:<cols>, fold:<log> (one op, no JSON contract)")
+    args = ap.parse_args()
+    if args.case:
+        run_case(args)
+        return
+    if args.impl == "reference":
+        world, rank, _ = dist_setup(args, "gloo")
+        out = run_reference(args, world, rank)
+    else:
+        world, rank, local = dist_setup(args, "nccl")
+        out = run_kernels(args, world, rank, local)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

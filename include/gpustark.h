@@ -1,0 +1,122 @@
+/*
+ * gpustark — C ABI of the B200 Circle-STARK proving backend.
+ *
+ * Every entry point mirrors one operation of the reference's CUDA FFI
+ * (crates/stwo/src/stwo_cuda/bindings.rs) or one backend-trait method of the
+ * reference prover; the citation next to each declaration names the
+ * reference interface it replaces. Differences from the reference ABI, all
+ * deliberate:
+ *   - every call takes an execution context (one CUDA stream) and returns a
+ *     status code instead of calling exit(); gs_last_error() explains a
+ *     non-zero status (thread-local);
+ *   - column lists are HOST arrays of DEVICE pointers (the library stages
+ *     them), QM31 columns are 4 device coordinate planes;
+ *   - work is stream-ordered on the context's stream; only the calls that
+ *     return host values (roots, nonces, proofs) synchronise.
+ * Field values are canonical M31 words (< 2^31 - 1). Hashes are 32 bytes
+ * (8 little-endian uint32 words) and hash buffers must be 16-byte aligned.
+ */
+#ifndef GPUSTARK_H
+#define GPUSTARK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS_OK 0
+#define GS_ERR_INVALID 1
+#define GS_ERR_CUDA 2
+#define GS_ERR_OOM 3
+#define GS_ERR_UNSUPPORTED 4
+#define GS_ERR_PROOF 5
+#define GS_ERR_TIMEOUT 6
+
+typedef struct gs_ctx gs_ctx;
+
+/* CudaSecureField (bindings.rs:9-15): QM31 (a + b i) + (c + d i) u. */
+typedef struct { uint32_t a, b, c, d; } gs_qm31;
+/* CirclePointSecureField (bindings.rs:68-80). */
+typedef struct { gs_qm31 x, y; } gs_point_qm31;
+
+/* ---------------------------------------------------------------- context */
+const char* gs_last_error(void);
+/* cuda_stream: a cudaStream_t to run on, or NULL for a private stream. */
+int gs_ctx_create(void* cuda_stream, gs_ctx** out);
+int gs_ctx_destroy(gs_ctx* ctx);
+int gs_ctx_synchronize(gs_ctx* ctx);
+void* gs_ctx_stream(gs_ctx* ctx);
+/* Number of kernels this library has launched in this process (no reference
+ * counterpart; used to account device launches in benchmarks). */
+unsigned long long gs_launch_count(void);
+
+/* ----------------------------------------------------------------- memory
+ * cuda_malloc_uint32_t / cuda_alloc_zeroes_uint32_t / cuda_free_memory /
+ * copy_uint32_t_vec_from_host_to_device / ..._device_to_host
+ * (bindings.rs:84-131). Allocation is stream ordered (memory pool). */
+int gs_malloc(gs_ctx* ctx, size_t bytes, void** out);
+int gs_free(gs_ctx* ctx, void* ptr);
+int gs_memset_zero(gs_ctx* ctx, void* dst, size_t bytes);
+int gs_memcpy_h2d(gs_ctx* ctx, void* dst, const void* src, size_t bytes);
+int gs_memcpy_d2h(gs_ctx* ctx, void* dst, const void* src, size_t bytes); /* synchronises */
+int gs_memcpy_d2d(gs_ctx* ctx, void* dst, const void* src, size_t bytes);
+
+/* -------------------------------------------------------------- ColumnOps */
+/* bit_reverse_base_field (bindings.rs:133); ColumnOps::bit_reverse_column. */
+int gs_bit_reverse_base_field(gs_ctx* ctx, uint32_t* col, uint32_t log_size);
+/* bit_reverse_secure_field (bindings.rs:135). */
+int gs_bit_reverse_secure_field(gs_ctx* ctx, uint32_t* const planes[4], uint32_t log_size);
+/* batch_inverse_base_field (bindings.rs:137). */
+int gs_batch_inverse_base_field(gs_ctx* ctx, const uint32_t* src, uint32_t* dst, size_t n);
+
+/* ---------------------------------------------------------------- PolyOps */
+/* precompute_twiddles (bindings.rs:165) + batch_inverse: twiddle tree of the
+ * coset (initial_index, step_index, log_size) given as circle indices; writes
+ * 2^log_size twiddles and, if itwiddles != NULL, their inverses.
+ * PolyOps::precompute_twiddles (prover/poly/circle/ops.rs:123). */
+int gs_precompute_twiddles(gs_ctx* ctx, uint32_t initial_index, uint32_t step_index, uint32_t log_size,
+                           uint32_t* twiddles, uint32_t* itwiddles);
+/* ntt_b2n_column (bindings.rs:503-510); PolyOps::interpolate_columns
+ * (ops.rs:28-39): in place, bit-reversed evaluations on CanonicCoset(log_size)
+ * -> coefficients. The twiddle tree is that of half_odds(twiddles_log_size). */
+int gs_interpolate_columns(gs_ctx* ctx, uint32_t* const* cols, uint32_t n_cols, uint32_t log_size,
+                           const uint32_t* itwiddles, uint32_t twiddles_log_size);
+/* ntt_n2b_columns (bindings.rs:512-519); PolyOps::evaluate_polynomials /
+ * extend + evaluate (ops.rs:88-120): 2^coeffs_log_size coefficients per
+ * column -> bit-reversed evaluations on CanonicCoset(log_size), written to
+ * evals (distinct buffers of 2^log_size words). */
+int gs_evaluate_columns(gs_ctx* ctx, const uint32_t* const* coeffs, uint32_t coeffs_log_size, uint32_t* const* evals,
+                        uint32_t n_cols, uint32_t log_size, const uint32_t* twiddles, uint32_t twiddles_log_size);
+
+/* -------------------------------------------------------------- MerkleOps */
+/* commit_on_first_layer / commit_on_layer_with_previous (bindings.rs:262-275);
+ * MerkleOps<Blake2sMerkleHasher>::commit_on_layer (prover/vcs/ops.rs:24-28).
+ * prev_layer: 2^(log_size+1) hashes or NULL; out: 2^log_size hashes. */
+int gs_commit_on_layer(gs_ctx* ctx, uint32_t log_size, const uint32_t* prev_layer, uint32_t n_cols,
+                       const uint32_t* const* cols, uint32_t* out);
+
+/* ---------------------------------------------------------------- FriOps */
+/* fold_line (bindings.rs:196-203); FriOps::fold_line (prover/fri.rs:39-44),
+ * fold_step 1: line evaluation on half_odds(log_size) -> 2^(log_size-1).
+ * leaf_hashes: optional (NULL) output of the next layer's Merkle leaves. */
+int gs_fold_line(gs_ctx* ctx, const uint32_t* const src[4], uint32_t log_size, gs_qm31 alpha, uint32_t* const dst[4],
+                 const uint32_t* itwiddles, uint32_t twiddles_log_size, uint32_t* leaf_hashes);
+/* fold_circle_into_line (bindings.rs:205-212); FriOps::fold_circle_into_line
+ * (prover/fri.rs:61-66): dst = dst * alpha^2 + fold(src), src on
+ * CanonicCoset(log_size), dst of size 2^(log_size-1). */
+int gs_fold_circle_into_line(gs_ctx* ctx, const uint32_t* const src[4], uint32_t log_size, gs_qm31 alpha,
+                             uint32_t* const dst[4], const uint32_t* itwiddles, uint32_t twiddles_log_size,
+                             uint32_t* leaf_hashes);
+
+/* --------------------------------------------------------------- GrindOps */
+/* grind_blake2s (bindings.rs:615); GrindOps<Blake2sChannel>::grind
+ * (core/proof_of_work.rs): prefixed_digest = H(POW_PREFIX, 0^12, digest,
+ * pow_bits) as 8 LE words; returns the smallest valid nonce. Synchronises. */
+int gs_grind_blake2s(gs_ctx* ctx, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint64_t* nonce);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUSTARK_H */

@@ -1,0 +1,203 @@
+// C ABI (include/gpustark.h) over the internal launch interface.
+#include "../../include/gpustark.h"
+#include "runtime.cuh"
+
+struct gs_ctx {
+  gs::Context c;
+};
+
+using namespace gs;
+
+namespace gs {
+int fold_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itw,
+                    uint32_t tw_log, uint32_t* leaf_out);
+int fold_circle_into_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
+                                const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out);
+}
+
+#define CTX_REQUIRED(ctx) GS_REQUIRE((ctx) != nullptr, "null context")
+
+static qm31 to_qm(gs_qm31 v) { return qm_make(v.a, v.b, v.c, v.d); }
+
+extern "C" {
+
+const char* gs_last_error(void) { return last_error(); }
+
+int gs_ctx_create(void* cuda_stream, gs_ctx** out) {
+  GS_REQUIRE(out != nullptr, "null output");
+  gs_ctx* c = new gs_ctx();
+  int s = c->c.init(cuda_stream);
+  if (s != OK) {
+    c->c.destroy();
+    delete c;
+    return s;
+  }
+  *out = c;
+  return OK;
+}
+
+int gs_ctx_destroy(gs_ctx* ctx) {
+  if (!ctx) return OK;
+  ctx->c.destroy();
+  delete ctx;
+  return OK;
+}
+
+int gs_ctx_synchronize(gs_ctx* ctx) {
+  CTX_REQUIRED(ctx);
+  return ctx->c.sync();
+}
+
+void* gs_ctx_stream(gs_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+
+unsigned long long gs_launch_count(void) { return launch_count(); }
+
+int gs_malloc(gs_ctx* ctx, size_t bytes, void** out) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(out != nullptr, "null output");
+  cudaError_t e = cudaMallocAsync(out, bytes ? bytes : 16, ctx->c.stream);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? ERR_OOM : ERR_CUDA;
+  }
+  return OK;
+}
+
+int gs_free(gs_ctx* ctx, void* ptr) {
+  CTX_REQUIRED(ctx);
+  if (!ptr) return OK;
+  GS_CUDA_TRY(cudaFreeAsync(ptr, ctx->c.stream));
+  return OK;
+}
+
+int gs_memset_zero(gs_ctx* ctx, void* dst, size_t bytes) {
+  CTX_REQUIRED(ctx);
+  GS_CUDA_TRY(cudaMemsetAsync(dst, 0, bytes, ctx->c.stream));
+  return OK;
+}
+
+int gs_memcpy_h2d(gs_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  CTX_REQUIRED(ctx);
+  GS_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->c.stream));
+  return OK;
+}
+
+int gs_memcpy_d2h(gs_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  CTX_REQUIRED(ctx);
+  GS_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->c.stream));
+  GS_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+  return OK;
+}
+
+int gs_memcpy_d2d(gs_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  CTX_REQUIRED(ctx);
+  GS_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->c.stream));
+  return OK;
+}
+
+int gs_bit_reverse_base_field(gs_ctx* ctx, uint32_t* col, uint32_t log_size) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(col != nullptr, "null column");
+  return bit_reverse(ctx->c.stream, col, log_size);
+}
+
+int gs_bit_reverse_secure_field(gs_ctx* ctx, uint32_t* const planes[4], uint32_t log_size) {
+  CTX_REQUIRED(ctx);
+  for (int i = 0; i < 4; i++) {
+    GS_REQUIRE(planes[i] != nullptr, "null plane");
+    GS_TRY(bit_reverse(ctx->c.stream, planes[i], log_size));
+  }
+  return OK;
+}
+
+int gs_batch_inverse_base_field(gs_ctx* ctx, const uint32_t* src, uint32_t* dst, size_t n) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(n == 0 || (src && dst), "null buffer");
+  return batch_inverse(ctx->c.stream, src, dst, n);
+}
+
+int gs_precompute_twiddles(gs_ctx* ctx, uint32_t initial_index, uint32_t step_index, uint32_t log_size,
+                           uint32_t* twiddles, uint32_t* itwiddles) {
+  CTX_REQUIRED(ctx);
+  return precompute_twiddles(ctx->c.stream, initial_index, step_index, log_size, twiddles, itwiddles);
+}
+
+int gs_interpolate_columns(gs_ctx* ctx, uint32_t* const* cols, uint32_t n_cols, uint32_t log_size,
+                           const uint32_t* itwiddles, uint32_t twiddles_log_size) {
+  CTX_REQUIRED(ctx);
+  if (n_cols == 0) return OK;
+  GS_REQUIRE(cols != nullptr, "null column list");
+  for (uint32_t i = 0; i < n_cols; i++) GS_REQUIRE(cols[i] != nullptr, "null column");
+  GS_REQUIRE(log_size <= 2 || itwiddles != nullptr, "null itwiddles");
+  const void* const* d = nullptr;
+  GS_TRY(ctx->c.stage_ptrs((const void* const*)cols, n_cols, &d));
+  return interpolate_columns(ctx->c.stream, (uint32_t* const*)d, n_cols, log_size, itwiddles, twiddles_log_size);
+}
+
+int gs_evaluate_columns(gs_ctx* ctx, const uint32_t* const* coeffs, uint32_t coeffs_log_size, uint32_t* const* evals,
+                        uint32_t n_cols, uint32_t log_size, const uint32_t* twiddles, uint32_t twiddles_log_size) {
+  CTX_REQUIRED(ctx);
+  if (n_cols == 0) return OK;
+  GS_REQUIRE(coeffs != nullptr && evals != nullptr, "null column list");
+  for (uint32_t i = 0; i < n_cols; i++) GS_REQUIRE(coeffs[i] && evals[i] && coeffs[i] != evals[i], "bad column pair");
+  GS_REQUIRE(log_size <= 2 || twiddles != nullptr, "null twiddles");
+  const void* const* ds = nullptr;
+  const void* const* dd = nullptr;
+  GS_TRY(ctx->c.stage_ptrs((const void* const*)coeffs, n_cols, &ds));
+  GS_TRY(ctx->c.stage_ptrs((const void* const*)evals, n_cols, &dd));
+  return evaluate_columns(ctx->c.stream, (const uint32_t* const*)ds, coeffs_log_size, (uint32_t* const*)dd, n_cols,
+                          log_size, twiddles, twiddles_log_size);
+}
+
+int gs_commit_on_layer(gs_ctx* ctx, uint32_t log_size, const uint32_t* prev_layer, uint32_t n_cols,
+                       const uint32_t* const* cols, uint32_t* out) {
+  CTX_REQUIRED(ctx);
+  const void* const* d = nullptr;
+  if (n_cols) {
+    GS_REQUIRE(cols != nullptr, "null column list");
+    for (uint32_t i = 0; i < n_cols; i++) GS_REQUIRE(cols[i] != nullptr, "null column");
+    GS_TRY(ctx->c.stage_ptrs((const void* const*)cols, n_cols, &d));
+  }
+  return commit_on_layer(ctx->c.stream, log_size, prev_layer, (const uint32_t* const*)d, n_cols, out);
+}
+
+int gs_fold_line(gs_ctx* ctx, const uint32_t* const src[4], uint32_t log_size, gs_qm31 alpha, uint32_t* const dst[4],
+                 const uint32_t* itwiddles, uint32_t twiddles_log_size, uint32_t* leaf_hashes) {
+  CTX_REQUIRED(ctx);
+  CPlanes s;
+  Planes d;
+  for (int i = 0; i < 4; i++) {
+    GS_REQUIRE(src[i] && dst[i], "null plane");
+    GS_REQUIRE(((uintptr_t)src[i] & 7) == 0, "source planes must be 8-byte aligned");
+    s.p[i] = src[i];
+    d.p[i] = dst[i];
+  }
+  GS_REQUIRE(itwiddles != nullptr, "null itwiddles");
+  return fold_line_fused(ctx->c.stream, s, log_size, to_qm(alpha), d, itwiddles, twiddles_log_size, leaf_hashes);
+}
+
+int gs_fold_circle_into_line(gs_ctx* ctx, const uint32_t* const src[4], uint32_t log_size, gs_qm31 alpha,
+                             uint32_t* const dst[4], const uint32_t* itwiddles, uint32_t twiddles_log_size,
+                             uint32_t* leaf_hashes) {
+  CTX_REQUIRED(ctx);
+  CPlanes s;
+  Planes d;
+  for (int i = 0; i < 4; i++) {
+    GS_REQUIRE(src[i] && dst[i], "null plane");
+    GS_REQUIRE(((uintptr_t)src[i] & 7) == 0, "source planes must be 8-byte aligned");
+    s.p[i] = src[i];
+    d.p[i] = dst[i];
+  }
+  GS_REQUIRE(itwiddles != nullptr || log_size < 3, "null itwiddles");
+  return fold_circle_into_line_fused(ctx->c.stream, s, log_size, to_qm(alpha), d, itwiddles, twiddles_log_size,
+                                     leaf_hashes);
+}
+
+int gs_grind_blake2s(gs_ctx* ctx, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint64_t* nonce) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(prefixed_digest != nullptr, "null digest");
+  return grind_blake2s(ctx->c.stream, prefixed_digest, pow_bits, (uint32_t*)ctx->c.d_small, nonce);
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+// FRI folds over QM31 columns stored as 4 coordinate planes.
+//
+// fold_line (crates/stwo/src/prover/backend/cpu/fri.rs:64-86):
+//   for pair i of a line evaluation on half_odds(n) in bit-reversed order,
+//   f0 = f(x) + f(-x), f1 = (f(x) - f(-x)) / x, out[i] = f0 + alpha f1,
+//   with 1/x read from the itwiddle level of half_odds(n) (offset L - 2^n).
+// fold_circle_into_line (cpu/fri.rs:88-113):
+//   f0 = f(p) + f(-p), f1 = (f(p) - f(-p)) / p.y,
+//   dst[i] = dst[i] alpha^2 + f0 + alpha f1,
+//   with 1/p.y the circle-layer itwiddle of the domain (the same derivation
+//   the interpolation's first layer uses).
+//
+// Fusion: when `leaf_out` is given, the thread that produced element i also
+// hashes it as the Merkle leaf of the next FRI layer (Blake2s of the 4
+// coordinates, one compression), so the folded layer is not read again for
+// its leaf hashes.
+#include "runtime.cuh"
+#include "blake2s.cuh"
+
+namespace gs {
+
+__device__ __forceinline__ void leaf_hash4(uint32_t* leaf_out, size_t i, qm31 v) {
+  uint32_t h[8], m[16];
+  blake2s_init(h);
+  m[0] = v.x.a; m[1] = v.x.b; m[2] = v.y.a; m[3] = v.y.b;
+#pragma unroll
+  for (int j = 4; j < 16; j++) m[j] = 0;
+  blake2s_compress(h, m, 16, true);
+  uint4* o = reinterpret_cast<uint4*>(leaf_out + 8 * i);
+  o[0] = make_uint4(h[0], h[1], h[2], h[3]);
+  o[1] = make_uint4(h[4], h[5], h[6], h[7]);
+}
+
+__device__ __forceinline__ void load_pair(CPlanes s, size_t i, qm31& a, qm31& b) {
+  uint2 p0 = __ldg(reinterpret_cast<const uint2*>(s.p[0]) + i);
+  uint2 p1 = __ldg(reinterpret_cast<const uint2*>(s.p[1]) + i);
+  uint2 p2 = __ldg(reinterpret_cast<const uint2*>(s.p[2]) + i);
+  uint2 p3 = __ldg(reinterpret_cast<const uint2*>(s.p[3]) + i);
+  a = qm_make(p0.x, p1.x, p2.x, p3.x);
+  b = qm_make(p0.y, p1.y, p2.y, p3.y);
+}
+
+__global__ void fold_line_kernel(CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* __restrict__ itw,
+                                 uint32_t tw_len, uint32_t* leaf_out) {
+  const size_t half = (size_t)1 << (log_n - 1);
+  const uint32_t* lvl = itw + (tw_len - (1u << log_n));
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < half; i += (size_t)gridDim.x * blockDim.x) {
+    qm31 fx, fnx;
+    load_pair(src, i, fx, fnx);
+    uint32_t xinv = __ldg(lvl + i);
+    qm31 f0 = qm_add(fx, fnx);
+    qm31 f1 = qm_mul_m31(qm_sub(fx, fnx), xinv);
+    qm31 r = qm_add(f0, qm_mul(alpha, f1));
+    dst.p[0][i] = r.x.a; dst.p[1][i] = r.x.b; dst.p[2][i] = r.y.a; dst.p[3][i] = r.y.b;
+    if (leaf_out) leaf_hash4(leaf_out, i, r);
+  }
+}
+
+struct SmallInvY { uint32_t v[2]; };
+
+__global__ void fold_circle_kernel(CPlanes src, uint32_t log_n, qm31 alpha, qm31 alpha_sq, Planes dst,
+                                   const uint32_t* __restrict__ itw, uint32_t tw_len, SmallInvY small,
+                                   uint32_t* leaf_out) {
+  const size_t half = (size_t)1 << (log_n - 1);
+  const uint32_t* t0 = log_n >= 3 ? itw + (tw_len - (1u << (log_n - 1))) : nullptr;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < half; i += (size_t)gridDim.x * blockDim.x) {
+    qm31 fp, fnp;
+    load_pair(src, i, fp, fnp);
+    uint32_t yinv;
+    if (t0) {
+      uint32_t q = (uint32_t)(i >> 2), r = (uint32_t)(i & 3);
+      uint32_t x = __ldg(t0 + 2 * q + (r < 2 ? 1u : 0u));
+      yinv = (r == 1 || r == 2) ? neg(x) : x;
+    } else {
+      yinv = small.v[i];
+    }
+    qm31 f0 = qm_add(fp, fnp);
+    qm31 f1 = qm_mul_m31(qm_sub(fp, fnp), yinv);
+    qm31 fprime = qm_add(qm_mul(alpha, f1), f0);
+    qm31 d = qm_make(dst.p[0][i], dst.p[1][i], dst.p[2][i], dst.p[3][i]);
+    qm31 r = qm_add(qm_mul(d, alpha_sq), fprime);
+    dst.p[0][i] = r.x.a; dst.p[1][i] = r.x.b; dst.p[2][i] = r.y.a; dst.p[3][i] = r.y.b;
+    if (leaf_out) leaf_hash4(leaf_out, i, r);
+  }
+}
+
+static unsigned grid_for(size_t n, int threads) {
+  size_t b = (n + threads - 1) / threads;
+  size_t cap = (size_t)num_sms() * 16;
+  return (unsigned)(b < cap ? (b ? b : 1) : cap);
+}
+
+int fold_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itw,
+                    uint32_t tw_log, uint32_t* leaf_out) {
+  GS_REQUIRE(log_n >= 1 && log_n <= tw_log, "fold_line: line domain must fit the twiddle tree");
+  size_t half = (size_t)1 << (log_n - 1);
+  fold_line_kernel<<<grid_for(half, 256), 256, 0, st>>>(src, log_n, alpha, dst, d_itw, 1u << tw_log, leaf_out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+static pt31 host_point(uint32_t k) {
+  pt31 r = {1u, 0u}, cur = {2u, 1268011823u};
+  for (int b = 0; b < 31; b++) {
+    if ((k >> b) & 1u) r = pt_add(r, cur);
+    cur = pt_add(cur, cur);
+  }
+  return r;
+}
+
+int fold_circle_into_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
+                                const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out) {
+  GS_REQUIRE(log_n >= 1 && log_n <= tw_log + 1, "fold_circle_into_line: domain must fit the twiddle tree");
+  SmallInvY small{{0, 0}};
+  if (log_n < 3) {
+    // CanonicCoset(n) half coset: initial index 2^(31-(n+1)), step 2^(31-(n-1)).
+    uint32_t init = 1u << (31 - (log_n + 1)), step = log_n >= 2 ? 1u << (31 - (log_n - 1)) : 0u;
+    for (uint32_t i = 0; i < (1u << (log_n - 1)); i++) {
+      uint32_t j = (log_n - 1) ? ((i & 1) ? 1u : 0u) : 0u;  // bit-reverse over n-1 <= 1 bits
+      pt31 p = host_point((init + j * step) & 0x7fffffffu);
+      small.v[i] = inv(p.y);
+    }
+  }
+  qm31 alpha_sq = qm_mul(alpha, alpha);
+  size_t half = (size_t)1 << (log_n - 1);
+  fold_circle_kernel<<<grid_for(half, 256), 256, 0, st>>>(src, log_n, alpha, alpha_sq, dst, d_itw, 1u << tw_log, small,
+                                                          leaf_out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+int fold_line(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itwiddles,
+              uint32_t tw_log) {
+  return fold_line_fused(st, src, log_n, alpha, dst, d_itwiddles, tw_log, nullptr);
+}
+int fold_circle_into_line(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
+                          const uint32_t* d_itwiddles, uint32_t tw_log) {
+  return fold_circle_into_line_fused(st, src, log_n, alpha, dst, d_itwiddles, tw_log, nullptr);
+}
+
+}  // namespace gs

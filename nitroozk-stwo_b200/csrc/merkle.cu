@@ -1,0 +1,81 @@
+// Blake2s Merkle layer: MerkleOps<Blake2sMerkleHasher>::commit_on_layer.
+//
+// Node i of a layer of log size L is
+//   Blake2s-256( prev[2i] || prev[2i+1] || col_0[i] || ... || col_{k-1}[i] )
+// with the children only when a previous (larger) layer exists and each
+// column value as 4 little-endian bytes (crates/stwo/src/core/vcs/
+// blake2_merkle.rs:18-39, cpu/blake2s.rs:13-26).
+//
+// One thread hashes one node: its message block is built directly in
+// registers from coalesced column reads (consecutive threads read
+// consecutive rows of a column) and compressed in place; the children are
+// read as 4 x 16-byte vector loads. No byte-wise buffering.
+#include "runtime.cuh"
+#include "blake2s.cuh"
+
+namespace gs {
+
+__device__ __forceinline__ void store_hash(uint32_t* out, size_t i, const uint32_t h[8]) {
+  uint4* o = reinterpret_cast<uint4*>(out + 8 * i);
+  o[0] = make_uint4(h[0], h[1], h[2], h[3]);
+  o[1] = make_uint4(h[4], h[5], h[6], h[7]);
+}
+
+__global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, const uint32_t* __restrict__ prev,
+                                                           const uint32_t* const* __restrict__ cols, uint32_t n_cols,
+                                                           uint32_t* __restrict__ out) {
+  const size_t n = (size_t)1 << log_size;
+  const uint32_t prev_words = prev ? 16u : 0u;
+  const uint32_t total_words = prev_words + n_cols;
+  const uint32_t total_bytes = 4u * total_words;
+  const uint32_t n_blocks = total_words == 0 ? 1u : (total_words + 15u) / 16u;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t h[8];
+    blake2s_init(h);
+    uint32_t m[16];
+    uint32_t blk = 0;
+    uint32_t col = 0;
+    if (prev) {
+      const uint4* p = reinterpret_cast<const uint4*>(prev + 16 * i);
+      uint4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+      m[0] = a.x; m[1] = a.y; m[2] = a.z; m[3] = a.w;
+      m[4] = b.x; m[5] = b.y; m[6] = b.z; m[7] = b.w;
+      m[8] = c.x; m[9] = c.y; m[10] = c.z; m[11] = c.w;
+      m[12] = d.x; m[13] = d.y; m[14] = d.z; m[15] = d.w;
+      blk = 1;
+      uint32_t t = total_bytes < 64u ? total_bytes : 64u;
+      blake2s_compress(h, m, t, n_blocks == 1);
+    }
+    for (; blk < n_blocks; blk++) {
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        uint32_t c = col + j;
+        m[j] = c < n_cols ? __ldg(cols[c] + i) : 0u;
+      }
+      col += 16;
+      uint32_t t = 64u * (blk + 1);
+      if (t > total_bytes) t = total_bytes;
+      blake2s_compress(h, m, t, blk + 1 == n_blocks);
+    }
+    store_hash(out, i, h);
+  }
+}
+
+int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, const uint32_t* const* d_cols,
+                    uint32_t n_cols, uint32_t* d_out) {
+  GS_REQUIRE(log_size <= 30, "layer log size out of range");
+  GS_REQUIRE(d_out != nullptr, "null output");
+  GS_REQUIRE(n_cols == 0 || d_cols != nullptr, "null column table");
+  GS_REQUIRE(((uintptr_t)d_out & 15) == 0 && ((uintptr_t)d_prev & 15) == 0, "hash buffers must be 16-byte aligned");
+  size_t n = (size_t)1 << log_size;
+  int threads = 256;
+  size_t blocks = (n + threads - 1) / threads;
+  size_t cap = (size_t)num_sms() * 8;
+  if (blocks > cap) blocks = cap;
+  merkle_layer_kernel<<<(unsigned)blocks, threads, 0, st>>>(log_size, d_prev, d_cols, n_cols, d_out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+}  // namespace gs

@@ -1,0 +1,81 @@
+// gpustark runtime: context, error state, pointer-table staging.
+#include "runtime.cuh"
+#include <cstring>
+#include <mutex>
+#include <atomic>
+
+namespace gs {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+
+static std::atomic<unsigned long long> g_launches{0};
+void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+int num_sms() {
+  static int cached[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (!cached[dev]) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cached[dev] = n;
+  }
+  return cached[dev];
+}
+
+int Context::init(void* user_stream) {
+  GS_CUDA_TRY(cudaGetDevice(&device));
+  if (user_stream) {
+    stream = (cudaStream_t)user_stream;
+    own_stream = false;
+  } else {
+    GS_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    own_stream = true;
+  }
+  ring_cap = 1 << 20;
+  ring_off = 0;
+  GS_CUDA_TRY(cudaMallocHost((void**)&h_ring, ring_cap));
+  GS_CUDA_TRY(cudaMalloc((void**)&d_ring, ring_cap));
+  small_cap = 4096;
+  GS_CUDA_TRY(cudaMalloc((void**)&d_small, small_cap));
+  GS_CUDA_TRY(cudaMallocHost((void**)&h_small, small_cap));
+  return OK;
+}
+
+void Context::destroy() {
+  if (stream) cudaStreamSynchronize(stream);
+  if (h_ring) cudaFreeHost(h_ring);
+  if (d_ring) cudaFree(d_ring);
+  if (d_small) cudaFree(d_small);
+  if (h_small) cudaFreeHost(h_small);
+  if (own_stream && stream) cudaStreamDestroy(stream);
+  h_ring = d_ring = d_small = h_small = nullptr;
+  stream = nullptr;
+}
+
+int Context::stage_ptrs(const void* const* host_ptrs, size_t n, const void* const** out) {
+  size_t bytes = (n * sizeof(void*) + 255) & ~(size_t)255;
+  GS_REQUIRE(bytes <= ring_cap, "too many column pointers for one call");
+  if (ring_off + bytes > ring_cap) {
+    // Wrap: earlier copies out of the pinned ring must have completed before
+    // their slots are rewritten.
+    GS_CUDA_TRY(cudaStreamSynchronize(stream));
+    ring_off = 0;
+  }
+  memcpy(h_ring + ring_off, host_ptrs, n * sizeof(void*));
+  GS_CUDA_TRY(cudaMemcpyAsync(d_ring + ring_off, h_ring + ring_off, n * sizeof(void*), cudaMemcpyHostToDevice, stream));
+  *out = (const void* const*)(d_ring + ring_off);
+  ring_off += bytes;
+  return OK;
+}
+
+int Context::sync() {
+  GS_CUDA_TRY(cudaStreamSynchronize(stream));
+  return OK;
+}
+
+}  // namespace gs

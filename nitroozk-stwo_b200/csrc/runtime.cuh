@@ -1,0 +1,110 @@
+// gpustark runtime: execution context, error reporting and the internal
+// (C++) launch interface shared by the kernels, the C ABI and the host prover.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+#include "m31.cuh"
+
+namespace gs {
+
+enum Status : int {
+  OK = 0,
+  ERR_INVALID = 1,    // bad argument (size, alignment, null pointer)
+  ERR_CUDA = 2,       // CUDA runtime / launch failure
+  ERR_OOM = 3,        // device allocation failed
+  ERR_UNSUPPORTED = 4,
+  ERR_PROOF = 5,      // proving failed (constraints not satisfied)
+  ERR_TIMEOUT = 6,    // a bounded device wait ran out
+};
+
+void set_error(const std::string& msg);
+const char* last_error();
+
+#define GS_CUDA_TRY(expr)                                                                 \
+  do {                                                                                    \
+    cudaError_t _e = (expr);                                                              \
+    if (_e != cudaSuccess) {                                                              \
+      ::gs::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e) + " @" __FILE__); \
+      return ::gs::ERR_CUDA;                                                              \
+    }                                                                                     \
+  } while (0)
+#define GS_REQUIRE(cond, msg)                     \
+  do {                                            \
+    if (!(cond)) {                                \
+      ::gs::set_error(std::string("invalid: ") + (msg)); \
+      return ::gs::ERR_INVALID;                   \
+    }                                             \
+  } while (0)
+#define GS_TRY(expr)                      \
+  do {                                    \
+    int _s = (expr);                      \
+    if (_s != ::gs::OK) return _s;        \
+  } while (0)
+
+// A QM31 column as 4 coordinate planes, passed by value to kernels.
+struct Planes { uint32_t* p[4]; };
+struct CPlanes { const uint32_t* p[4]; };
+
+// Count of kernel launches issued by this library (for launch accounting).
+void note_launch(unsigned n = 1);
+unsigned long long launch_count();
+
+// Number of SMs of the current device (cached).
+int num_sms();
+
+// Execution context: one CUDA stream plus a device-side ring for the column
+// pointer tables that the C ABI receives as host arrays.
+struct Context {
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  // pointer-table staging: pinned host ring -> device ring, stream ordered
+  uint8_t* h_ring = nullptr;
+  uint8_t* d_ring = nullptr;
+  size_t ring_cap = 0, ring_off = 0;
+  // small device scratch for results (grind, reductions)
+  uint8_t* d_small = nullptr;
+  uint8_t* h_small = nullptr;  // pinned mirror
+  size_t small_cap = 0;
+
+  int init(void* user_stream);
+  void destroy();
+  // Copies `n` host pointers into device memory usable by kernels launched on
+  // `stream` after this call; returns the device address.
+  int stage_ptrs(const void* const* host_ptrs, size_t n, const void* const** out);
+  int sync();
+};
+
+// ------------------------------------------------------------ launch API
+// All functions enqueue work on `st` and return a Status.
+
+// twiddles.cu
+int precompute_twiddles(cudaStream_t st, uint32_t initial_index, uint32_t step_index, uint32_t log_size,
+                        uint32_t* d_twiddles, uint32_t* d_itwiddles);
+int batch_inverse(cudaStream_t st, const uint32_t* d_in, uint32_t* d_out, size_t n);
+
+// fft.cu (columns given by a device table of pointers)
+int interpolate_columns(cudaStream_t st, uint32_t* const* d_cols, uint32_t n_cols, uint32_t log_n,
+                        const uint32_t* d_itwiddles, uint32_t tw_log);
+int evaluate_columns(cudaStream_t st, const uint32_t* const* d_src, uint32_t coeff_log, uint32_t* const* d_dst,
+                     uint32_t n_cols, uint32_t log_n, const uint32_t* d_twiddles, uint32_t tw_log);
+int bit_reverse(cudaStream_t st, uint32_t* d, uint32_t log_n);
+
+// merkle.cu
+int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, const uint32_t* const* d_cols,
+                    uint32_t n_cols, uint32_t* d_out);
+
+// fri.cu
+int fold_line(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itwiddles,
+              uint32_t tw_log);
+int fold_circle_into_line(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
+                          const uint32_t* d_itwiddles, uint32_t tw_log);
+
+// grind.cu
+int grind_blake2s(cudaStream_t st, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint32_t* d_scratch,
+                  uint64_t* nonce_out);
+
+}  // namespace gs

@@ -1,0 +1,181 @@
+"""GpuBackend: the reference's backend traits over the gpustark C ABI.
+
+Method names and argument meaning follow the reference's traits
+(crates/stwo/src/prover/backend/mod.rs:20-92, prover/poly/circle/ops.rs,
+prover/vcs/ops.rs, prover/fri.rs:28-49, core/proof_of_work.rs) so that a
+caller of those traits finds the same operations here. Device columns are
+torch CUDA tensors of dtype int32 holding M31 words bit-for-bit; QM31 columns
+are lists of 4 such tensors (coordinate planes); a hash layer is an int32
+tensor of 8 words per node. Every call enqueues on the context's stream,
+which is torch's current stream unless another is given.
+"""
+import ctypes as C
+import hashlib
+import struct
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+P = (1 << 31) - 1
+POW_PREFIX = 0x12345678
+
+
+class Context:
+    """One gs_ctx bound to a CUDA stream (default: torch's current stream)."""
+
+    def __init__(self, stream=None):
+        if not torch.cuda.is_available():
+            raise L.GpuStarkError("gpustark needs a CUDA device")
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        self.stream = stream
+        h = C.c_void_p()
+        L.check(L.lib().gs_ctx_create(C.c_void_p(stream.cuda_stream), C.byref(h)), "gs_ctx_create")
+        self.handle = h
+
+    def synchronize(self):
+        L.check(L.lib().gs_ctx_synchronize(self.handle), "gs_ctx_synchronize")
+
+    def close(self):
+        if self.handle:
+            L.lib().gs_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def default_context():
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context()
+    return _default_ctx
+
+
+def to_device(a, device="cuda"):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    return torch.from_numpy(a.view(np.int32)).to(device)
+
+
+def to_host(t):
+    return t.detach().cpu().numpy().view(np.uint32)
+
+
+def qm31(v):
+    v = [int(x) for x in v]
+    return L.QM31(*v)
+
+
+@dataclass
+class TwiddleTree:
+    """PolyOps::Twiddles for the coset half_odds(root_log) (prover/poly/twiddles.rs:9-14)."""
+    root_log: int
+    twiddles: torch.Tensor
+    itwiddles: torch.Tensor
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class GpuBackend:
+    """Static operations mirroring ColumnOps / PolyOps / MerkleOps / FriOps / GrindOps."""
+
+    # ------------------------------------------------------------ ColumnOps
+    @staticmethod
+    def bit_reverse_column(col, ctx=None):
+        ctx = ctx or default_context()
+        n = col.numel()
+        L.check(L.lib().gs_bit_reverse_base_field(ctx.handle, _p(col), n.bit_length() - 1), "bit_reverse_column")
+
+    # -------------------------------------------------------------- PolyOps
+    @staticmethod
+    def precompute_twiddles(root_log, ctx=None) -> TwiddleTree:
+        """Twiddle tree of Coset::half_odds(root_log) (ops.rs:123)."""
+        ctx = ctx or default_context()
+        n = 1 << root_log
+        tw = torch.empty(n, dtype=torch.int32, device="cuda")
+        itw = torch.empty(n, dtype=torch.int32, device="cuda")
+        initial = 1 << (31 - (root_log + 2))
+        step = 1 << (31 - root_log)
+        L.check(L.lib().gs_precompute_twiddles(ctx.handle, initial, step, root_log, _p(tw), _p(itw)),
+                "precompute_twiddles")
+        return TwiddleTree(root_log, tw, itw)
+
+    @staticmethod
+    def interpolate_columns(columns, log_size, twiddles: TwiddleTree, ctx=None):
+        """In place: bit-reversed evaluations on CanonicCoset(log_size) -> coefficients (ops.rs:28-39)."""
+        ctx = ctx or default_context()
+        pp, keep = L.ptr_array([c.data_ptr() for c in columns])
+        L.check(L.lib().gs_interpolate_columns(ctx.handle, pp, len(columns), log_size, _p(twiddles.itwiddles),
+                                               twiddles.root_log), "interpolate_columns")
+        return columns
+
+    @staticmethod
+    def evaluate_polynomials(coeffs, log_size, twiddles: TwiddleTree, out=None, ctx=None):
+        """Coefficients -> bit-reversed evaluations on CanonicCoset(log_size) (ops.rs:88-120)."""
+        ctx = ctx or default_context()
+        if out is None:
+            out = [torch.empty(1 << log_size, dtype=torch.int32, device="cuda") for _ in coeffs]
+        coeff_log = coeffs[0].numel().bit_length() - 1
+        sp, k1 = L.ptr_array([c.data_ptr() for c in coeffs])
+        dp, k2 = L.ptr_array([c.data_ptr() for c in out])
+        L.check(L.lib().gs_evaluate_columns(ctx.handle, sp, coeff_log, dp, len(coeffs), log_size,
+                                            _p(twiddles.twiddles), twiddles.root_log), "evaluate_polynomials")
+        return out
+
+    # ------------------------------------------------------------ MerkleOps
+    @staticmethod
+    def commit_on_layer(log_size, prev_layer, columns, ctx=None, out=None):
+        """One Blake2s Merkle layer (prover/vcs/ops.rs:24-28); returns 2^log_size x 8 words."""
+        ctx = ctx or default_context()
+        if out is None:
+            out = torch.empty((1 << log_size) * 8, dtype=torch.int32, device="cuda")
+        pp, keep = L.ptr_array([c.data_ptr() for c in columns])
+        L.check(L.lib().gs_commit_on_layer(ctx.handle, log_size, _p(prev_layer), len(columns), pp, _p(out)),
+                "commit_on_layer")
+        return out
+
+    # --------------------------------------------------------------- FriOps
+    @staticmethod
+    def fold_line(eval_planes, log_size, alpha, twiddles: TwiddleTree, ctx=None, leaf_hashes=None):
+        """FriOps::fold_line with fold_step 1 (prover/fri.rs:39-44)."""
+        ctx = ctx or default_context()
+        out = [torch.empty(1 << (log_size - 1), dtype=torch.int32, device="cuda") for _ in range(4)]
+        sp, k1 = L.ptr_array([t.data_ptr() for t in eval_planes])
+        dp, k2 = L.ptr_array([t.data_ptr() for t in out])
+        L.check(L.lib().gs_fold_line(ctx.handle, sp, log_size, qm31(alpha), dp, _p(twiddles.itwiddles),
+                                     twiddles.root_log, _p(leaf_hashes)), "fold_line")
+        return out
+
+    @staticmethod
+    def fold_circle_into_line(dst_planes, src_planes, log_size, alpha, twiddles: TwiddleTree, ctx=None,
+                              leaf_hashes=None):
+        """FriOps::fold_circle_into_line (prover/fri.rs:61-66); dst updated in place."""
+        ctx = ctx or default_context()
+        sp, k1 = L.ptr_array([t.data_ptr() for t in src_planes])
+        dp, k2 = L.ptr_array([t.data_ptr() for t in dst_planes])
+        L.check(L.lib().gs_fold_circle_into_line(ctx.handle, sp, log_size, qm31(alpha), dp, _p(twiddles.itwiddles),
+                                                 twiddles.root_log, _p(leaf_hashes)), "fold_circle_into_line")
+        return dst_planes
+
+    # ------------------------------------------------------------- GrindOps
+    @staticmethod
+    def grind(digest: bytes, pow_bits, ctx=None):
+        """GrindOps<Blake2sChannel>::grind: smallest nonce for the channel digest."""
+        ctx = ctx or default_context()
+        pre = hashlib.blake2s(struct.pack("<I", POW_PREFIX) + bytes(12) + digest + struct.pack("<I", pow_bits),
+                              digest_size=32).digest()
+        words = (C.c_uint32 * 8)(*struct.unpack("<8I", pre))
+        nonce = C.c_uint64()
+        L.check(L.lib().gs_grind_blake2s(ctx.handle, words, pow_bits, C.byref(nonce)), "grind")
+        return nonce.value

@@ -1,0 +1,40 @@
+"""The C-ABI library loads without a GPU and exports every symbol that
+include/gpustark.h declares (no compute calls here)."""
+import ctypes
+import os
+import re
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "gpustark.h")
+LIB = os.path.join(ROOT, "nitroozk-stwo_b200", "gpustark", "libgpustark.so")
+
+
+def declared():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(gs_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    assert "gs_ctx_create" in names and "gs_commit_on_layer" in names
+    assert len(names) >= 15
+
+
+def test_library_exports_every_declared_symbol():
+    if not os.path.exists(LIB):
+        import subprocess
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "nitroozk-stwo_b200"), "-j8"])
+    lib = ctypes.CDLL(LIB)
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_declares_only_exported_symbols():
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "nitroozk-stwo_b200"))
+    import gpustark
+    lib = ctypes.CDLL(LIB)
+    for n in gpustark.declared_symbols():
+        assert hasattr(lib, n), n
+    assert set(gpustark.declared_symbols()) <= set(declared())

@@ -1,0 +1,179 @@
+"""Kernel parity: each CUDA op through the C ABI vs the CPU oracle, bit-exact,
+on seeded inputs; at the sweep's full sizes, size-independent properties."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import pyoracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+P = O.P
+
+
+@pytest.fixture(scope="module")
+def B():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from gpustark.backend import GpuBackend
+    return GpuBackend
+
+
+def dev(a):
+    from gpustark.backend import to_device
+    return to_device(a)
+
+
+def host(t):
+    from gpustark.backend import to_host
+    return to_host(t)
+
+
+def rand_m31(rng, *shape):
+    return rng.integers(0, P, shape, dtype=np.int64).astype(np.uint32)
+
+
+@pytest.mark.parametrize("root_log", [1, 2, 3, 5, 8, 13, 17])
+def test_twiddles(B, root_log):
+    t = B.precompute_twiddles(root_log)
+    tw, itw = O.twiddles_half_odds(root_log)
+    assert np.array_equal(host(t.twiddles), tw)
+    assert np.array_equal(host(t.itwiddles), itw)
+
+
+@pytest.mark.parametrize("log_n", [1, 2, 3, 4, 5, 8, 11, 12, 13, 14, 16, 17, 20])
+def test_interpolate_matches_oracle(B, log_n):
+    rng = np.random.default_rng(100 + log_n)
+    n_cols = 3 if log_n > 14 else 5
+    cols = [rand_m31(rng, 1 << log_n) for _ in range(n_cols)]
+    root = max(log_n - 1, 1) + (1 if log_n % 2 else 0)  # also exercise a larger tree
+    tw = B.precompute_twiddles(root)
+    d = [dev(c) for c in cols]
+    B.interpolate_columns(d, log_n, tw)
+    expect = O.interpolate_columns(cols, log_n, root_log=root)
+    for g, e in zip(d, expect):
+        assert np.array_equal(host(g), e)
+
+
+@pytest.mark.parametrize("coeff_log,log_n", [(1, 1), (2, 2), (1, 3), (3, 3), (4, 5), (8, 9), (10, 12), (12, 12),
+                                              (13, 14), (15, 16), (16, 17), (18, 19), (19, 20)])
+def test_evaluate_matches_oracle(B, coeff_log, log_n):
+    rng = np.random.default_rng(200 + coeff_log * 31 + log_n)
+    cols = [rand_m31(rng, 1 << coeff_log) for _ in range(3)]
+    tw = B.precompute_twiddles(max(log_n - 1, 1))
+    out = B.evaluate_polynomials([dev(c) for c in cols], log_n, tw)
+    expect = O.evaluate_columns(cols, log_n, root_log=max(log_n - 1, 1))
+    for g, e in zip(out, expect):
+        assert np.array_equal(host(g), e)
+
+
+def test_bit_reverse(B):
+    rng = np.random.default_rng(7)
+    for log_n in (0, 1, 5, 16):
+        a = rand_m31(rng, 1 << log_n)
+        d = dev(a)
+        B.bit_reverse_column(d)
+        assert np.array_equal(host(d), O.bit_reverse(a))
+
+
+@pytest.mark.parametrize("n_cols", [0, 1, 4, 15, 16, 17, 100, 158])
+@pytest.mark.parametrize("with_prev", [False, True])
+def test_commit_on_layer(B, n_cols, with_prev):
+    rng = np.random.default_rng(300 + n_cols * 2 + with_prev)
+    log_size = 9
+    cols = [rand_m31(rng, 1 << log_size) for _ in range(n_cols)]
+    prev = rng.integers(0, 256, (1 << (log_size + 1)) * 32, dtype=np.uint8) if with_prev else None
+    prev_d = dev(prev.view(np.uint32)) if with_prev else None
+    out = B.commit_on_layer(log_size, prev_d, [dev(c) for c in cols])
+    expect = O.commit_on_layer(log_size, prev, cols)
+    assert np.array_equal(host(out).view(np.uint8).reshape(-1, 32), expect)
+
+
+def test_merkle_root_of_mixed_sizes(B):
+    """Full commit with columns injected at their own layer (prover/vcs/prover.rs:22-48)."""
+    rng = np.random.default_rng(9)
+    sizes = [10, 10, 9, 7, 7, 7, 3, 1]
+    cols = [rand_m31(rng, 1 << s) for s in sizes]
+    prev = None
+    for ls in range(max(sizes), -1, -1):
+        layer_cols = [dev(c) for c, s in zip(cols, sizes) if s == ls]
+        prev = B.commit_on_layer(ls, prev, layer_cols)
+    root = host(prev).view(np.uint8).tobytes()
+    assert root == O.merkle_root(cols)
+
+
+def qm_rand(rng, n):
+    return rand_m31(rng, n, 4)
+
+
+@pytest.mark.parametrize("log_n", [1, 2, 3, 6, 12, 16])
+def test_fold_line(B, log_n):
+    rng = np.random.default_rng(400 + log_n)
+    ev = qm_rand(rng, 1 << log_n)
+    alpha = rand_m31(rng, 4)
+    tw = B.precompute_twiddles(log_n + 1)
+    leaves = __import__("torch").empty((1 << (log_n - 1)) * 8, dtype=__import__("torch").int32, device="cuda")
+    out = B.fold_line([dev(ev[:, i].copy()) for i in range(4)], log_n, alpha, tw, leaf_hashes=leaves)
+    got = np.stack([host(t) for t in out], axis=1)
+    expect = O.fold_line(ev, log_n, alpha)
+    assert np.array_equal(got, expect)
+    # fused leaf hashes = Merkle leaf layer of the folded planes
+    exp_leaves = O.commit_on_layer(log_n - 1, None, [expect[:, i].copy() for i in range(4)])
+    assert np.array_equal(host(leaves).view(np.uint8).reshape(-1, 32), exp_leaves)
+
+
+@pytest.mark.parametrize("log_n", [1, 2, 3, 4, 7, 13, 17])
+def test_fold_circle_into_line(B, log_n):
+    rng = np.random.default_rng(500 + log_n)
+    src = qm_rand(rng, 1 << log_n)
+    dst = qm_rand(rng, 1 << (log_n - 1))
+    alpha = rand_m31(rng, 4)
+    tw = B.precompute_twiddles(max(log_n - 1, 1))
+    d = [dev(dst[:, i].copy()) for i in range(4)]
+    B.fold_circle_into_line(d, [dev(src[:, i].copy()) for i in range(4)], log_n, alpha, tw)
+    got = np.stack([host(t) for t in d], axis=1)
+    expect = O.fold_circle_into_line(dst, src, log_n, alpha)
+    assert np.array_equal(got, expect)
+
+
+@pytest.mark.parametrize("pow_bits", [0, 1, 10, 14])
+def test_grind(B, pow_bits):
+    digest = hashlib.blake2s(b"channel-%d" % pow_bits, digest_size=32).digest()
+    assert B.grind(digest, pow_bits) == O.grind(digest, pow_bits)
+
+
+# ---------------------------------------------------------------- full sizes
+@pytest.mark.parametrize("log_n", [22, 24, 26])
+def test_fft_roundtrip_full_size(B, log_n):
+    """interpolate(evaluate(c)) == c and the LDE restricted to the even rows of
+    CanonicCoset(n+1) ... is checked by sampled points against the oracle."""
+    rng = np.random.default_rng(600 + log_n)
+    c = rand_m31(rng, 1 << log_n)
+    tw = B.precompute_twiddles(log_n)
+    ev = B.evaluate_polynomials([dev(c)], log_n, tw)[0]
+    B.interpolate_columns([ev], log_n, tw)
+    assert np.array_equal(host(ev), c)
+    # sampled evaluation points against the oracle's basis definition
+    lde = B.evaluate_polynomials([dev(c[: 1 << 12].copy())], 13, B.precompute_twiddles(12))[0]
+    assert np.array_equal(host(lde), O.evaluate(c[: 1 << 12], 13, root_log=12))
+
+
+def test_merkle_64x2p20_root(B):
+    rng = np.random.default_rng(700)
+    cols = [rand_m31(rng, 1 << 20) for _ in range(64)]
+    prev = B.commit_on_layer(20, None, [dev(x) for x in cols])
+    for ls in range(19, -1, -1):
+        prev = B.commit_on_layer(ls, prev, [])
+    assert host(prev).view(np.uint8).tobytes() == O.merkle_root(cols)
+
+
+def test_fold_line_2p22(B):
+    rng = np.random.default_rng(800)
+    ev = qm_rand(rng, 1 << 22)
+    alpha = rand_m31(rng, 4)
+    tw = B.precompute_twiddles(23)
+    out = B.fold_line([dev(ev[:, i].copy()) for i in range(4)], 22, alpha, tw)
+    got = np.stack([host(t) for t in out], axis=1)
+    assert np.array_equal(got, O.fold_line(ev, 22, alpha))
