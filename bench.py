@@ -178,8 +178,7 @@ class KernelSweep:
         self.B.commit_on_layer(MERKLE_LOG, None, self.cols, ctx=self.ctx, out=self.layers[MERKLE_LOG])
         mark("merkle_leaf_e")
         mark("merkle_nodes_s")
-        for L in range(MERKLE_LOG - 1, -1, -1):
-            self.B.commit_on_layer(L, self.layers[L + 1], [], ctx=self.ctx, out=self.layers[L])
+        self.B.commit_node_layers(self.layers, ctx=self.ctx)
         mark("merkle_nodes_e")
         mark("fold_line_s")
         self.B.fold_line(self.fold_in, FOLD_LOG, self.alpha, self.tw_fold, ctx=self.ctx)

@@ -43,7 +43,8 @@ typedef struct { gs_qm31 x, y; } gs_point_qm31;
 
 /* ---------------------------------------------------------------- context */
 const char* gs_last_error(void);
-/* cuda_stream: a cudaStream_t to run on, or NULL for a private stream. */
+/* cuda_stream: the cudaStream_t all work of this context is ordered on;
+ * NULL is CUDA's default (legacy) stream. */
 int gs_ctx_create(void* cuda_stream, gs_ctx** out);
 int gs_ctx_destroy(gs_ctx* ctx);
 int gs_ctx_synchronize(gs_ctx* ctx);
@@ -97,6 +98,12 @@ int gs_evaluate_columns(gs_ctx* ctx, const uint32_t* const* coeffs, uint32_t coe
 int gs_commit_on_layer(gs_ctx* ctx, uint32_t log_size, const uint32_t* prev_layer, uint32_t n_cols,
                        const uint32_t* const* cols, uint32_t* out);
 
+/* The node-only part of MerkleProver::commit's layer loop (prover/vcs/
+ * prover.rs:39-48) when no columns are injected below top_log: layers is a
+ * host array of top_log + 1 device buffers, layers[L] holding 2^L hashes;
+ * layers[top_log] is the input, all smaller layers are written. */
+int gs_commit_node_layers(gs_ctx* ctx, uint32_t top_log, uint32_t* const* layers);
+
 /* ---------------------------------------------------------------- FriOps */
 /* fold_line (bindings.rs:196-203); FriOps::fold_line (prover/fri.rs:39-44),
  * fold_step 1: line evaluation on half_odds(log_size) -> 2^(log_size-1).
@@ -109,6 +116,46 @@ int gs_fold_line(gs_ctx* ctx, const uint32_t* const src[4], uint32_t log_size, g
 int gs_fold_circle_into_line(gs_ctx* ctx, const uint32_t* const src[4], uint32_t log_size, gs_qm31 alpha,
                              uint32_t* const dst[4], const uint32_t* itwiddles, uint32_t twiddles_log_size,
                              uint32_t* leaf_hashes);
+
+/* ------------------------------------------------------------ QuotientOps */
+/* accumulate_numerators_batch (bindings.rs:354-365); QuotientOps::
+ * accumulate_numerators (prover/pcs/quotient_ops.rs:27-31) for one sample
+ * batch: out[row] = sum_k c_k * cols[column_indices[k]][row] - sum_k b_k over
+ * columns of 2^log_size rows; b/c are the batch's line coefficients (host). */
+int gs_accumulate_numerators(gs_ctx* ctx, uint32_t log_size, const uint32_t* const* cols, uint32_t n_cols,
+                             const uint32_t* column_indices, const gs_qm31* line_coeffs_b,
+                             const gs_qm31* line_coeffs_c, uint32_t n_coeffs, uint32_t* const out[4]);
+
+/* One accumulated numerator per sample point (AccumulatedNumerators,
+ * prover/pcs/quotient_ops.rs:33-37). */
+typedef struct {
+  const uint32_t* partial[4]; /* 2^log_size QM31 planes (device) */
+  uint32_t log_size;
+  gs_qm31 first_linear_term;
+  gs_point_qm31 sample_point;
+} gs_quotient_acc;
+/* compute_quotients_and_combine (bindings.rs:367-381); QuotientOps::
+ * compute_quotients_and_combine (quotient_ops.rs:39-42): writes the combined
+ * quotient on the bit-reversed CanonicCoset(lifting_log_size). */
+int gs_compute_quotients_and_combine(gs_ctx* ctx, const gs_quotient_acc* accs, uint32_t n_accs,
+                                     uint32_t lifting_log_size, uint32_t* const out[4]);
+
+/* -------------------------------------------------------- AccumulationOps */
+/* lift_and_accumulate (bindings.rs:216-221); AccumulationOps::
+ * lift_and_accumulate (prover/air/accumulation.rs:127-145): columns in
+ * increasing size; planes[4c + k] is coordinate k of column c. out has
+ * 2^out_log_size rows, out_log_size = the largest column's log size. */
+int gs_lift_and_accumulate(gs_ctx* ctx, const uint32_t* const* planes, const uint32_t* log_sizes, uint32_t n_cols,
+                           uint32_t* const out[4], uint32_t out_log_size);
+/* accumulate (bindings.rs:214); AccumulationOps::accumulate: a += b. */
+int gs_accumulate(gs_ctx* ctx, uint32_t* const a[4], const uint32_t* const b[4], size_t n);
+
+/* ----------------------------------------------------- out-of-domain eval */
+/* batch_eval_at_points (bindings.rs:187-194); PolyOps::batch_eval_at_point
+ * (ops.rs:51-59): values of n_polys coefficient polynomials of 2^log_size
+ * coefficients at `point`, written to host memory. Synchronises. */
+int gs_batch_eval_at_point(gs_ctx* ctx, const uint32_t* const* polys, uint32_t n_polys, uint32_t log_size,
+                           gs_point_qm31 point, gs_qm31* out);
 
 /* --------------------------------------------------------------- GrindOps */
 /* grind_blake2s (bindings.rs:615); GrindOps<Blake2sChannel>::grind

@@ -162,6 +162,13 @@ int gs_commit_on_layer(gs_ctx* ctx, uint32_t log_size, const uint32_t* prev_laye
   return commit_on_layer(ctx->c.stream, log_size, prev_layer, (const uint32_t* const*)d, n_cols, out);
 }
 
+int gs_commit_node_layers(gs_ctx* ctx, uint32_t top_log, uint32_t* const* layers) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(layers != nullptr, "null layer list");
+  for (uint32_t k = 0; k <= top_log; k++) GS_REQUIRE(layers[k] != nullptr, "null layer buffer");
+  return commit_node_layers(ctx->c.stream, top_log, layers);
+}
+
 int gs_fold_line(gs_ctx* ctx, const uint32_t* const src[4], uint32_t log_size, gs_qm31 alpha, uint32_t* const dst[4],
                  const uint32_t* itwiddles, uint32_t twiddles_log_size, uint32_t* leaf_hashes) {
   CTX_REQUIRED(ctx);
@@ -192,6 +199,114 @@ int gs_fold_circle_into_line(gs_ctx* ctx, const uint32_t* const src[4], uint32_t
   GS_REQUIRE(itwiddles != nullptr || log_size < 3, "null itwiddles");
   return fold_circle_into_line_fused(ctx->c.stream, s, log_size, to_qm(alpha), d, itwiddles, twiddles_log_size,
                                      leaf_hashes);
+}
+
+int gs_accumulate_numerators(gs_ctx* ctx, uint32_t log_size, const uint32_t* const* cols, uint32_t n_cols,
+                             const uint32_t* column_indices, const gs_qm31* line_coeffs_b,
+                             const gs_qm31* line_coeffs_c, uint32_t n_coeffs, uint32_t* const out[4]) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(n_coeffs == 0 || (cols && column_indices && line_coeffs_b && line_coeffs_c), "null argument");
+  Planes o;
+  for (int i = 0; i < 4; i++) {
+    GS_REQUIRE(out[i] != nullptr, "null output plane");
+    o.p[i] = out[i];
+  }
+  std::vector<NumEntry> entries(n_coeffs);
+  qm31 bsum = qm_zero();
+  for (uint32_t k = 0; k < n_coeffs; k++) {
+    GS_REQUIRE(column_indices[k] < n_cols && cols[column_indices[k]] != nullptr, "column index out of range");
+    entries[k].col = cols[column_indices[k]];
+    entries[k].c[0] = line_coeffs_c[k].a; entries[k].c[1] = line_coeffs_c[k].b;
+    entries[k].c[2] = line_coeffs_c[k].c; entries[k].c[3] = line_coeffs_c[k].d;
+    bsum = qm_add(bsum, to_qm(line_coeffs_b[k]));
+  }
+  const void* d = nullptr;
+  if (n_coeffs) GS_TRY(ctx->c.stage_bytes(entries.data(), entries.size() * sizeof(NumEntry), &d));
+  return accumulate_numerators(ctx->c.stream, d, n_coeffs, bsum, log_size, o);
+}
+
+int gs_compute_quotients_and_combine(gs_ctx* ctx, const gs_quotient_acc* accs, uint32_t n_accs,
+                                     uint32_t lifting_log_size, uint32_t* const out[4]) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(n_accs == 0 || accs != nullptr, "null accumulations");
+  Planes o;
+  for (int i = 0; i < 4; i++) {
+    GS_REQUIRE(out[i] != nullptr, "null output plane");
+    o.p[i] = out[i];
+  }
+  std::vector<QuotAcc> qa(n_accs);
+  for (uint32_t a = 0; a < n_accs; a++) {
+    GS_REQUIRE(accs[a].log_size <= lifting_log_size && accs[a].log_size >= 1, "accumulation larger than lifting domain");
+    for (int i = 0; i < 4; i++) {
+      GS_REQUIRE(accs[a].partial[i] != nullptr, "null partial plane");
+      qa[a].p[i] = accs[a].partial[i];
+    }
+    qa[a].log_size = accs[a].log_size;
+    qa[a].pad = 0;
+    qa[a].first_linear = to_qm(accs[a].first_linear_term);
+    qm31 px = to_qm(accs[a].sample_point.x), py = to_qm(accs[a].sample_point.y);
+    qa[a].prx = px.x; qa[a].pix = px.y; qa[a].pry = py.x; qa[a].piy = py.y;
+  }
+  DomainTables dt;
+  GS_TRY(ctx->c.domain_tables(lifting_log_size, &dt));
+  const void* d = nullptr;
+  if (n_accs) GS_TRY(ctx->c.stage_bytes(qa.data(), qa.size() * sizeof(QuotAcc), &d));
+  return compute_quotients_and_combine(ctx->c.stream, d, n_accs, dt, o);
+}
+
+int gs_lift_and_accumulate(gs_ctx* ctx, const uint32_t* const* planes, const uint32_t* log_sizes, uint32_t n_cols,
+                           uint32_t* const out[4], uint32_t out_log_size) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(n_cols > 0 && planes && log_sizes, "empty accumulation");
+  Planes o;
+  for (int i = 0; i < 4; i++) {
+    GS_REQUIRE(out[i] != nullptr, "null output plane");
+    o.p[i] = out[i];
+  }
+  std::vector<LiftCol> lc(n_cols);
+  for (uint32_t c = 0; c < n_cols; c++) {
+    GS_REQUIRE(log_sizes[c] >= 1 && log_sizes[c] <= out_log_size, "column larger than the output");
+    for (int i = 0; i < 4; i++) {
+      GS_REQUIRE(planes[4 * c + i] != nullptr, "null plane");
+      lc[c].p[i] = planes[4 * c + i];
+    }
+    lc[c].log_size = log_sizes[c];
+    lc[c].pad = 0;
+  }
+  const void* d = nullptr;
+  GS_TRY(ctx->c.stage_bytes(lc.data(), lc.size() * sizeof(LiftCol), &d));
+  return lift_and_accumulate(ctx->c.stream, d, n_cols, out_log_size, o);
+}
+
+int gs_accumulate(gs_ctx* ctx, uint32_t* const a[4], const uint32_t* const b[4], size_t n) {
+  CTX_REQUIRED(ctx);
+  Planes pa;
+  CPlanes pb;
+  for (int i = 0; i < 4; i++) {
+    GS_REQUIRE(a[i] && b[i], "null plane");
+    pa.p[i] = a[i];
+    pb.p[i] = b[i];
+  }
+  return accumulate(ctx->c.stream, pa, pb, n);
+}
+
+int gs_batch_eval_at_point(gs_ctx* ctx, const uint32_t* const* polys, uint32_t n_polys, uint32_t log_size,
+                           gs_point_qm31 point, gs_qm31* out) {
+  CTX_REQUIRED(ctx);
+  if (n_polys == 0) return OK;
+  GS_REQUIRE(polys && out, "null argument");
+  for (uint32_t i = 0; i < n_polys; i++) GS_REQUIRE(polys[i] != nullptr, "null polynomial");
+  size_t need = eval_at_point_scratch_bytes(n_polys, log_size) + 16 * (size_t)n_polys;
+  void* scratch = nullptr;
+  GS_TRY(ctx->c.get_scratch(need, &scratch));
+  const void* const* d = nullptr;
+  GS_TRY(ctx->c.stage_ptrs((const void* const*)polys, n_polys, &d));
+  uint32_t* d_out = (uint32_t*)((uint8_t*)scratch + eval_at_point_scratch_bytes(n_polys, log_size));
+  ptq p = {to_qm(point.x), to_qm(point.y)};
+  GS_TRY(batch_eval_at_point(ctx->c.stream, (const uint32_t* const*)d, n_polys, log_size, p, d_out, (uint32_t*)scratch));
+  GS_CUDA_TRY(cudaMemcpyAsync(out, d_out, 16 * (size_t)n_polys, cudaMemcpyDeviceToHost, ctx->c.stream));
+  GS_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+  return OK;
 }
 
 int gs_grind_blake2s(gs_ctx* ctx, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint64_t* nonce) {

@@ -10,17 +10,22 @@
 // twiddle buffer length. Interpolation runs layers 0..n-1 then scales by
 // 1/2^n; evaluation runs layers n-1..0.
 //
-// Kernel design: a pass loads a tile of 2^(cnt+c) elements into shared
-// memory, runs `cnt` consecutive layers there and writes the tile back. A
-// tile keeps the c lowest index bits contiguous (64-byte runs with c = 4) so
-// that strided passes still read whole DRAM sectors. Columns of one size are
-// batched in a single launch (grid.y = column). The 1/2^n scale is fused
-// into the store of the last interpolation pass.
+// Kernel design (radix-2^R in registers): a pass covers L consecutive layers
+// on tiles of 2^t = 2^(c+L) elements. Each thread holds 2^R elements (R = 5:
+// 32 registers) whose tile indices differ in an R-bit window and runs up to R
+// layers on them with compile-time indexing; stages exchange data through
+// shared memory with an XOR swizzle (bank = e[0:5] ^ e[5:10]) that keeps
+// every access pattern bank-conflict free. The twiddles a thread needs for
+// one layer are consecutive and aligned in the tree, so they arrive as a few
+// 16-byte loads. A tile keeps its c lowest index bits contiguous in global
+// memory (64-byte runs with c = 4) so strided passes read whole sectors.
+// Columns of one size are batched in one launch (grid.y = column). The 1/2^n
+// scale is fused into the final store of the interpolation.
 //
 // Low-degree extension (evaluate 2^m coefficients on a 2^n domain): the top
 // n-m layers of the zero-padded forward FFT only copy (butterfly with a zero
 // partner), so the first pass reads src[v mod 2^m] and only layers m-1..0
-// are computed — the zero-extension pass of the reference disappears.
+// are computed — no zero-extension pass.
 #include "runtime.cuh"
 #include <algorithm>
 #include <cstdlib>
@@ -28,74 +33,171 @@
 namespace gs {
 
 struct FftPass {
-  uint32_t n;         // domain log size
-  uint32_t lo, cnt;   // layers [lo, lo + cnt)
-  uint32_t c;         // contiguous low index bits kept per tile (c <= lo)
-  uint32_t src_mask;  // read src[v & src_mask] (LDE replication)
-  uint32_t tw_len;    // twiddle buffer length
-  uint32_t scale;     // multiply by scale on store when has_scale
+  uint32_t n;           // domain log size
+  uint32_t lo, L;       // layers [lo, lo + L)
+  uint32_t c;           // contiguous low index bits kept per tile (c <= lo)
+  uint32_t t;           // tile log size = c + L
+  uint32_t K;           // register stages
+  uint32_t tile_shift;  // log2(tiles per block)
+  uint32_t src_mask;    // read src[v & src_mask] (LDE replication)
+  uint32_t tw_len;      // twiddle buffer length
+  uint32_t scale;       // multiply by scale on the final store when has_scale
   uint32_t has_scale;
 };
 
-__device__ __forceinline__ uint32_t fft_twiddle(const uint32_t* __restrict__ tw, uint32_t tw_len, uint32_t n,
-                                                uint32_t i, uint32_t h) {
-  if (i >= 1) return __ldg(tw + (tw_len - (1u << (n - i)) + h));
+__device__ __forceinline__ uint32_t circle_twiddle(const uint32_t* __restrict__ tw, uint32_t tw_len, uint32_t n,
+                                                   uint32_t h) {
   uint32_t base = tw_len - (1u << (n - 1));
   uint32_t q = h >> 2, r = h & 3u;
   uint32_t x = __ldg(tw + base + 2 * q + (r < 2 ? 1u : 0u));
   return (r == 1 || r == 2) ? neg(x) : x;
 }
 
+// COUNT consecutive twiddles of layer i starting at group hth (aligned to COUNT).
+template <int COUNT>
+__device__ __forceinline__ void load_twiddles(uint32_t* w, const uint32_t* __restrict__ tw, uint32_t tw_len,
+                                              uint32_t n, uint32_t i, uint32_t hth) {
+  if (i >= 1) {
+    const uint32_t* p = tw + (tw_len - (1u << (n - i)) + hth);
+    if (COUNT >= 4) {
+#pragma unroll
+      for (int g = 0; g < COUNT / 4; g++) {
+        uint4 v = __ldg(reinterpret_cast<const uint4*>(p) + g);
+        w[4 * g] = v.x; w[4 * g + 1] = v.y; w[4 * g + 2] = v.z; w[4 * g + 3] = v.w;
+      }
+    } else if (COUNT == 2) {
+      uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+      w[0] = v.x; w[1] = v.y;
+    } else {
+      w[0] = __ldg(p);
+    }
+  } else {
+    if (COUNT >= 4) {
+      const uint32_t* t0 = tw + (tw_len - (1u << (n - 1)));
+#pragma unroll
+      for (int g = 0; g < COUNT / 4; g++) {
+        uint2 xy = __ldg(reinterpret_cast<const uint2*>(t0) + (hth >> 2) + g);
+        w[4 * g] = xy.y; w[4 * g + 1] = neg(xy.y); w[4 * g + 2] = neg(xy.x); w[4 * g + 3] = xy.x;
+      }
+    } else {
+#pragma unroll
+      for (int g = 0; g < COUNT; g++) w[g] = circle_twiddle(tw, tw_len, n, hth + g);
+    }
+  }
+}
+
 template <bool INV>
-__global__ void __launch_bounds__(512) fft_pass_kernel(const uint32_t* const* __restrict__ src_tab,
+__device__ __forceinline__ void bfly(uint32_t& a, uint32_t& b, uint32_t w) {
+  if (INV) {
+    uint32_t t0 = a;
+    a = add(t0, b);
+    b = mul(sub(t0, b), w);
+  } else {
+    uint32_t t0 = mul(b, w);
+    b = sub(a, t0);
+    a = add(a, t0);
+  }
+}
+
+__device__ __forceinline__ uint32_t swz(uint32_t e) { return e ^ ((e >> 5) & 31u); }
+
+template <bool INV, int R>
+__global__ void __launch_bounds__(256) fft_pass_kernel(const uint32_t* const* __restrict__ src_tab,
                                                        uint32_t* const* __restrict__ dst_tab,
                                                        const uint32_t* __restrict__ tw, FftPass a) {
   extern __shared__ uint32_t sm[];
+  constexpr int NQ = 1 << R;
   const uint32_t col = blockIdx.y;
   const uint32_t* __restrict__ src = src_tab[col];
   uint32_t* __restrict__ dst = dst_tab[col];
-  const uint32_t t = a.cnt + a.c;
-  const uint32_t tile = 1u << t;
-  const uint32_t ml_bits = a.lo - a.c;
-  const uint32_t midlow = blockIdx.x & ((1u << ml_bits) - 1u);
-  const uint32_t hi = blockIdx.x >> ml_bits;
+  const uint32_t tpt_log = a.t - R;
+  const uint32_t ltid = threadIdx.x & ((1u << tpt_log) - 1u);
+  const uint32_t sub_tile = threadIdx.x >> tpt_log;
+  const uint32_t tile = (blockIdx.x << a.tile_shift) | sub_tile;
+  uint32_t* smt = sm + (sub_tile << a.t);
+  const uint32_t ml = a.lo - a.c;
+  const uint32_t midlow = tile & ((1u << ml) - 1u);
+  const uint32_t hi = tile >> ml;
   const uint32_t cmask = (1u << a.c) - 1u;
-  const uint32_t base = (hi << (a.lo + a.cnt)) | (midlow << a.c);
+  const uint32_t basev = (hi << (a.lo + a.L)) | (midlow << a.c);
+  uint32_t x[NQ];
 
-  for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
-    uint32_t v = base | ((e >> a.c) << a.lo) | (e & cmask);
-    sm[e] = src[v & a.src_mask];
-  }
-  __syncthreads();
-
-  for (uint32_t k = 0; k < a.cnt; k++) {
-    const uint32_t li = INV ? k : (a.cnt - 1 - k);
-    const uint32_t i = a.lo + li;
-    const uint32_t s = li + a.c;
-    const uint32_t smask = (1u << s) - 1u;
-    for (uint32_t b = threadIdx.x; b < (tile >> 1); b += blockDim.x) {
-      uint32_t e0 = ((b & ~smask) << 1) | (b & smask);
-      uint32_t e1 = e0 | (1u << s);
-      uint32_t v0 = base | ((e0 >> a.c) << a.lo) | (e0 & cmask);
-      uint32_t w = fft_twiddle(tw, a.tw_len, a.n, i, v0 >> (i + 1));
-      uint32_t x0 = sm[e0], x1 = sm[e1];
-      if (INV) {
-        sm[e0] = add(x0, x1);
-        sm[e1] = mul(sub(x0, x1), w);
+  for (uint32_t k = 0; k < a.K; k++) {
+    uint32_t s0, ja, jb;
+    if (INV) {
+      if (k + 1 < a.K) { s0 = a.c + k * R; ja = 0; jb = R; }
+      else { s0 = a.t - R; ja = a.c + k * R - s0; jb = R; }
+    } else {
+      if (k + 1 < a.K) { s0 = a.t - (k + 1) * R; ja = 0; jb = R; }
+      else { s0 = a.c; ja = 0; jb = a.t - k * R - a.c; }
+    }
+    const uint32_t ebase = ((ltid >> s0) << (s0 + R)) | (ltid & ((1u << s0) - 1u));
+    if (k == 0) {
+      if (s0 == 0 && a.c == 0 && a.src_mask == 0xffffffffu && NQ >= 4) {
+        const uint4* p = reinterpret_cast<const uint4*>(src + (basev | ebase));
+#pragma unroll
+        for (int g = 0; g < NQ / 4; g++) {
+          uint4 v = __ldg(p + g);
+          x[4 * g] = v.x; x[4 * g + 1] = v.y; x[4 * g + 2] = v.z; x[4 * g + 3] = v.w;
+        }
       } else {
-        uint32_t tmp = mul(x1, w);
-        sm[e0] = add(x0, tmp);
-        sm[e1] = sub(x0, tmp);
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+          uint32_t e = ebase | ((uint32_t)q << s0);
+          uint32_t v = basev | ((e >> a.c) << a.lo) | (e & cmask);
+          x[q] = __ldg(src + (v & a.src_mask));
+        }
+      }
+    } else {
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < NQ; q++) x[q] = smt[swz(ebase | ((uint32_t)q << s0))];
+      __syncthreads();
+    }
+    const uint32_t vth = basev | ((ebase >> a.c) << a.lo) | (ebase & cmask);
+#pragma unroll
+    for (int jj = 0; jj < R; jj++) {
+      const int j = INV ? jj : (R - 1 - jj);
+      if ((uint32_t)j < ja || (uint32_t)j >= jb) continue;
+      const uint32_t i = a.lo + s0 + (uint32_t)j - a.c;
+      const uint32_t hth = vth >> (i + 1);
+      constexpr int MAXW = NQ / 2;
+      uint32_t w[MAXW];
+      // COUNT = 2^(R-1-j), resolved at compile time after unrolling
+      switch (R - 1 - j) {
+        case 0: load_twiddles<1>(w, tw, a.tw_len, a.n, i, hth); break;
+        case 1: load_twiddles<2>(w, tw, a.tw_len, a.n, i, hth); break;
+        case 2: load_twiddles<4>(w, tw, a.tw_len, a.n, i, hth); break;
+        case 3: load_twiddles<8>(w, tw, a.tw_len, a.n, i, hth); break;
+        default: load_twiddles<16>(w, tw, a.tw_len, a.n, i, hth); break;
+      }
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        if (q & (1 << j)) continue;
+        bfly<INV>(x[q], x[q | (1 << j)], w[q >> (j + 1)]);
       }
     }
-    __syncthreads();
-  }
-
-  for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
-    uint32_t v = base | ((e >> a.c) << a.lo) | (e & cmask);
-    uint32_t x = sm[e];
-    if (a.has_scale) x = mul(x, a.scale);
-    dst[v] = x;
+    if (k + 1 < a.K) {
+#pragma unroll
+      for (int q = 0; q < NQ; q++) smt[swz(ebase | ((uint32_t)q << s0))] = x[q];
+    } else {
+      if (a.has_scale) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) x[q] = mul(x[q], a.scale);
+      }
+      if (s0 == 0 && a.c == 0 && NQ >= 4) {
+        uint4* p = reinterpret_cast<uint4*>(dst + (basev | ebase));
+#pragma unroll
+        for (int g = 0; g < NQ / 4; g++) p[g] = make_uint4(x[4 * g], x[4 * g + 1], x[4 * g + 2], x[4 * g + 3]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+          uint32_t e = ebase | ((uint32_t)q << s0);
+          uint32_t v = basev | ((e >> a.c) << a.lo) | (e & cmask);
+          dst[v] = x[q];
+        }
+      }
+    }
   }
 }
 
@@ -189,22 +291,35 @@ static int launch_small(cudaStream_t st, const uint32_t* const* src, uint32_t* c
 }
 
 struct FftTuning {
-  uint32_t tile_log = 12;      // log2 of shared-memory tile (elements)
+  uint32_t tile_log = 13;      // log2 of the shared-memory tile (elements), <= 13
   uint32_t coalesce_bits = 4;  // contiguous low bits per strided tile row
 };
 static FftTuning g_fft_tuning;
 
+// Splits layers [0, layers) into balanced passes (lo, L): the first pass has
+// the whole tile for layers, later ones reserve `coalesce_bits` of it.
 static void fft_partition(uint32_t layers, std::vector<std::pair<uint32_t, uint32_t>>& parts) {
-  // Splits layers [0, layers) into passes (lo, cnt): the first pass keeps the
-  // whole tile for layers; later ones reserve `coalesce_bits` of the tile.
   const uint32_t T = g_fft_tuning.tile_log, C = g_fft_tuning.coalesce_bits;
-  uint32_t lo = 0;
-  while (lo < layers) {
-    uint32_t c = std::min(C, lo);
-    uint32_t cnt = std::min(layers - lo, T - c);
-    parts.push_back({lo, cnt});
-    lo += cnt;
+  if (layers <= T) {
+    parts.push_back({0, layers});
+    return;
   }
+  uint32_t np = 1 + (layers - T + (T - C) - 1) / (T - C);
+  uint32_t lr = std::min(T - C, (layers + np - 1) / np);
+  uint32_t l0 = layers - lr * (np - 1);
+  parts.push_back({0, l0});
+  uint32_t lo = l0;
+  for (uint32_t p = 1; p < np; p++) {
+    parts.push_back({lo, lr});
+    lo += lr;
+  }
+}
+
+template <bool INV, int R>
+static void launch_pass(cudaStream_t st, dim3 grid, uint32_t threads, size_t smem, const uint32_t* const* s,
+                        uint32_t* const* d, const uint32_t* tw, const FftPass& a) {
+  fft_pass_kernel<INV, R><<<grid, threads, smem, st>>>(s, d, tw, a);
+  note_launch();
 }
 
 template <bool INV>
@@ -217,20 +332,31 @@ static int run_passes(cudaStream_t st, const uint32_t* const* src, uint32_t* con
     FftPass a{};
     a.n = n;
     a.lo = parts[p].first;
-    a.cnt = parts[p].second;
+    a.L = parts[p].second;
     a.c = std::min(g_fft_tuning.coalesce_bits, a.lo);
+    a.t = a.c + a.L;
+    const uint32_t R = std::min<uint32_t>(5, a.L);
+    a.K = (a.L + R - 1) / R;
     a.src_mask = (p == 0) ? src_mask : 0xffffffffu;
     a.tw_len = tw_len;
     a.has_scale = (INV && p + 1 == parts.size()) ? 1u : 0u;
     a.scale = a.has_scale ? inv(1u << n) : 1u;
-    uint32_t t = a.cnt + a.c;
-    uint32_t tiles = 1u << (n - t);
-    uint32_t threads = std::min<uint32_t>(512, std::max<uint32_t>(32, 1u << (t - 1)));
-    size_t smem = sizeof(uint32_t) << t;
-    dim3 grid(tiles, n_cols);
+    const uint32_t tpt_log = a.t - R;
+    const uint32_t tiles_log = n - a.t;
+    uint32_t tile_shift = tpt_log < 7 ? 7 - tpt_log : 0;
+    if (tile_shift > tiles_log) tile_shift = tiles_log;
+    a.tile_shift = tile_shift;
+    const uint32_t threads = 1u << (tpt_log + tile_shift);
+    const size_t smem = (size_t)4 << (a.t + tile_shift);
+    dim3 grid(1u << (tiles_log - tile_shift), n_cols);
     const uint32_t* const* s = (p == 0) ? src : (const uint32_t* const*)dst;
-    fft_pass_kernel<INV><<<grid, threads, smem, st>>>(s, dst, tw, a);
-    note_launch();
+    switch (R) {
+      case 1: launch_pass<INV, 1>(st, grid, threads, smem, s, dst, tw, a); break;
+      case 2: launch_pass<INV, 2>(st, grid, threads, smem, s, dst, tw, a); break;
+      case 3: launch_pass<INV, 3>(st, grid, threads, smem, s, dst, tw, a); break;
+      case 4: launch_pass<INV, 4>(st, grid, threads, smem, s, dst, tw, a); break;
+      default: launch_pass<INV, 5>(st, grid, threads, smem, s, dst, tw, a); break;
+    }
     GS_CUDA_TRY(cudaGetLastError());
   }
   return OK;
@@ -260,8 +386,8 @@ int evaluate_columns(cudaStream_t st, const uint32_t* const* d_src, uint32_t coe
 }
 
 void set_fft_tuning(uint32_t tile_log, uint32_t coalesce_bits) {
-  if (tile_log >= 4 && tile_log <= 13) g_fft_tuning.tile_log = tile_log;
-  if (coalesce_bits <= 6 && coalesce_bits + 2 <= g_fft_tuning.tile_log) g_fft_tuning.coalesce_bits = coalesce_bits;
+  if (tile_log >= 6 && tile_log <= 13) g_fft_tuning.tile_log = tile_log;
+  if (coalesce_bits <= 5 && coalesce_bits + 5 <= g_fft_tuning.tile_log) g_fft_tuning.coalesce_bits = coalesce_bits;
 }
 
 // In-place bit reversal of one column (ColumnOps::bit_reverse_column).

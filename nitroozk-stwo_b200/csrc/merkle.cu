@@ -78,4 +78,49 @@ int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, 
   return OK;
 }
 
+// Node-only layers of a small subtree in one block: starting from the layer
+// of log size `top_log` (<= 11, already in memory), computes every layer
+// down to the root, each node = Blake2s(left || right) (no columns injected
+// at these layers). Layer L is written to layers.p[L]; one launch replaces
+// top_log launches of the per-layer kernel.
+struct LayerPtrs { uint32_t* p[12]; };
+
+__global__ void __launch_bounds__(1024) merkle_tail_kernel(uint32_t top_log, LayerPtrs layers) {
+  for (int L = (int)top_log - 1; L >= 0; L--) {
+    const uint32_t* prev = layers.p[L + 1];
+    uint32_t* out = layers.p[L];
+    for (uint32_t i = threadIdx.x; i < (1u << L); i += blockDim.x) {
+      uint32_t h[8], m[16];
+      blake2s_init(h);
+      const uint4* pp = reinterpret_cast<const uint4*>(prev + 16 * i);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        uint4 v = pp[q];  // written by this block in the previous iteration: plain loads
+        m[4 * q] = v.x; m[4 * q + 1] = v.y; m[4 * q + 2] = v.z; m[4 * q + 3] = v.w;
+      }
+      blake2s_compress(h, m, 64, true);
+      store_hash(out, i, h);
+    }
+    __syncthreads();
+  }
+}
+
+int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers) {
+  GS_REQUIRE(top_log <= 30, "layer log size out of range");
+  // per-layer kernel down to 2^11 nodes, then one block for the rest
+  int L = (int)top_log - 1;
+  for (; L >= 11; L--) GS_TRY(commit_on_layer(st, (uint32_t)L, layers[L + 1], nullptr, 0, layers[L]));
+  uint32_t tail_top = (uint32_t)(L + 1);
+  if (tail_top == 0) return OK;
+  LayerPtrs lp{};
+  for (uint32_t k = 0; k <= tail_top && k < 12; k++) {
+    GS_REQUIRE(((uintptr_t)layers[k] & 15) == 0, "hash buffers must be 16-byte aligned");
+    lp.p[k] = layers[k];
+  }
+  merkle_tail_kernel<<<1, 1024, 0, st>>>(tail_top, lp);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
 }  // namespace gs

@@ -1,0 +1,250 @@
+// DEEP quotients and lifted accumulation (QuotientOps / AccumulationOps).
+//
+// accumulate_numerators (crates/stwo/src/prover/backend/cpu/quotients.rs:21-45,
+// core/pcs/quotients.rs:206-219): for one sample batch over columns of one
+// log size,  partial[row] = sum_k c_k * col_k[row] - sum_k b_k   (QM31)
+// with (a_k, b_k, c_k) the complex-conjugate line coefficients. The products
+// c_k * v are accumulated lazily in 64-bit per coordinate and folded every
+// two terms, so a term costs one wide multiply-add per coordinate.
+//
+// compute_quotients_and_combine (cpu/quotients.rs:47-75): for every row of
+// the lifting domain (bit-reversed CanonicCoset(lift)),
+//   q[row] = sum_a (partial_a[lift_idx_a(row)] - A_a * y) * den_a^-1,
+//   den_a = (Re p_a.x - x) Im p_a.y - (Re p_a.y - y) Im p_a.x   (CM31)
+// The CM31 denominators of R rows x K points of a thread are inverted with
+// one field inversion (Montgomery's trick), instead of one inversion each.
+//
+// lift_and_accumulate (cpu/accumulation.rs:27-47): the chain of lifted adds
+// collapses to res[i] = sum_c col_c[lift(i, L - L_c)] because lifted indices
+// compose; one pass reads each column once.
+#include "runtime.cuh"
+
+namespace gs {
+
+__device__ __forceinline__ pt31 ld_pt(const pt31* p) {
+  uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+  return {v.x, v.y};
+}
+
+__device__ __forceinline__ pt31 domain_point_bitrev(const DomainTables& t, uint32_t row) {
+  uint32_t j = __brev(row) >> (32 - t.lift);
+  uint32_t half = 1u << (t.lift - 1);
+  bool second = j >= half;
+  if (second) j -= half;
+  pt31 p = pt_add(ld_pt(t.hi + (j >> t.s)), ld_pt(t.lo + (j & ((1u << t.s) - 1))));
+  return second ? pt_conj(p) : p;
+}
+
+// ------------------------------------------------------------ numerators
+__device__ __forceinline__ uint64_t fold64(uint64_t x) { return (x & P) + (x >> 31); }
+
+__global__ void accumulate_numerators_kernel(const NumEntry* __restrict__ entries, uint32_t n_entries, qm31 b_sum,
+                                             uint32_t log_size, Planes out) {
+  const size_t n = (size_t)1 << log_size;
+  for (size_t row = blockIdx.x * (size_t)blockDim.x + threadIdx.x; row < n; row += (size_t)gridDim.x * blockDim.x) {
+    uint64_t acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
+    uint32_t k = 0;
+    for (; k + 1 < n_entries; k += 2) {
+      const NumEntry e0 = entries[k], e1 = entries[k + 1];
+      uint32_t v0 = __ldg(e0.col + row), v1 = __ldg(e1.col + row);
+      acc0 += (uint64_t)e0.c[0] * v0 + (uint64_t)e1.c[0] * v1;
+      acc1 += (uint64_t)e0.c[1] * v0 + (uint64_t)e1.c[1] * v1;
+      acc2 += (uint64_t)e0.c[2] * v0 + (uint64_t)e1.c[2] * v1;
+      acc3 += (uint64_t)e0.c[3] * v0 + (uint64_t)e1.c[3] * v1;
+      acc0 = fold64(acc0); acc1 = fold64(acc1); acc2 = fold64(acc2); acc3 = fold64(acc3);
+    }
+    if (k < n_entries) {
+      const NumEntry e0 = entries[k];
+      uint32_t v0 = __ldg(e0.col + row);
+      acc0 += (uint64_t)e0.c[0] * v0;
+      acc1 += (uint64_t)e0.c[1] * v0;
+      acc2 += (uint64_t)e0.c[2] * v0;
+      acc3 += (uint64_t)e0.c[3] * v0;
+    }
+    out.p[0][row] = sub(reduce64(acc0), b_sum.x.a);
+    out.p[1][row] = sub(reduce64(acc1), b_sum.x.b);
+    out.p[2][row] = sub(reduce64(acc2), b_sum.y.a);
+    out.p[3][row] = sub(reduce64(acc3), b_sum.y.b);
+  }
+}
+
+int accumulate_numerators(cudaStream_t st, const void* d_entries, uint32_t n_entries, qm31 b_sum, uint32_t log_size,
+                          Planes out) {
+  GS_REQUIRE(log_size <= 30, "log size out of range");
+  size_t n = (size_t)1 << log_size;
+  int threads = 256;
+  size_t blocks = (n + threads - 1) / threads;
+  size_t cap = (size_t)num_sms() * 16;
+  if (blocks > cap) blocks = cap;
+  accumulate_numerators_kernel<<<(unsigned)blocks, threads, 0, st>>>((const NumEntry*)d_entries, n_entries, b_sum,
+                                                                      log_size, out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+// ------------------------------------------------------------ quotients
+constexpr int QUOT_ROWS = 2;   // rows per thread sharing one inversion
+constexpr int QUOT_MAXK = 4;   // sample points per inversion chunk
+
+__global__ void __launch_bounds__(128) quotients_kernel(const QuotAcc* __restrict__ accs, uint32_t n_accs,
+                                                        DomainTables dt, Planes out) {
+  const size_t n = (size_t)1 << dt.lift;
+  const size_t n_groups = n / QUOT_ROWS;
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < n_groups; g += (size_t)gridDim.x * blockDim.x) {
+    // Rows g, g + n/R, ...: consecutive threads touch consecutive rows.
+    pt31 dp[QUOT_ROWS];
+    qm31 q[QUOT_ROWS];
+#pragma unroll
+    for (int r = 0; r < QUOT_ROWS; r++) {
+      dp[r] = domain_point_bitrev(dt, (uint32_t)(g + r * n_groups));
+      q[r] = qm_zero();
+    }
+    for (uint32_t a0 = 0; a0 < n_accs; a0 += QUOT_MAXK) {
+      const uint32_t kc = n_accs - a0 < (uint32_t)QUOT_MAXK ? n_accs - a0 : (uint32_t)QUOT_MAXK;
+      cm31 den[QUOT_ROWS][QUOT_MAXK];
+      cm31 pref[QUOT_ROWS][QUOT_MAXK];
+      cm31 run = {1, 0};
+#pragma unroll
+      for (int r = 0; r < QUOT_ROWS; r++) {
+#pragma unroll
+        for (int k = 0; k < QUOT_MAXK; k++) {
+          if ((uint32_t)k < kc) {
+            const QuotAcc& A = accs[a0 + k];
+            cm31 d = cm_sub(cm_mul(cm_sub(A.prx, cm31{dp[r].x, 0}), A.piy),
+                            cm_mul(cm_sub(A.pry, cm31{dp[r].y, 0}), A.pix));
+            den[r][k] = d;
+            pref[r][k] = run;
+            run = cm_mul(run, d);
+          }
+        }
+      }
+      cm31 inv_run = cm_inv(run);
+#pragma unroll
+      for (int r = QUOT_ROWS - 1; r >= 0; r--) {
+#pragma unroll
+        for (int k = QUOT_MAXK - 1; k >= 0; k--) {
+          if ((uint32_t)k < kc) {
+            cm31 dinv = cm_mul(inv_run, pref[r][k]);
+            inv_run = cm_mul(inv_run, den[r][k]);
+            const QuotAcc& A = accs[a0 + k];
+            uint32_t row = (uint32_t)(g + r * n_groups);
+            uint32_t log_ratio = dt.lift - A.log_size;
+            uint32_t li = ((row >> (log_ratio + 1)) << 1) + (row & 1u);
+            qm31 pn = qm_make(__ldg(A.p[0] + li), __ldg(A.p[1] + li), __ldg(A.p[2] + li), __ldg(A.p[3] + li));
+            qm31 full = qm_sub(pn, qm_mul_m31(A.first_linear, dp[r].y));
+            q[r] = qm_add(q[r], qm_mul_cm31(full, dinv));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < QUOT_ROWS; r++) {
+      size_t row = g + r * n_groups;
+      out.p[0][row] = q[r].x.a; out.p[1][row] = q[r].x.b; out.p[2][row] = q[r].y.a; out.p[3][row] = q[r].y.b;
+    }
+  }
+}
+
+// Point tables for the canonic half coset of log size lift-1:
+// initial index 2^(31-(lift+1)), step 2^(31-(lift-1)).
+__global__ void domain_tables_kernel(pt31* hi, pt31* lo, uint32_t s, uint32_t n_hi, uint32_t init, uint32_t step) {
+  // circle generator powers, recomputed per thread (tiny tables)
+  uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t n_lo = 1u << s;
+  if (idx >= n_hi + n_lo) return;
+  uint32_t k;
+  if (idx < n_hi) k = (init + (uint32_t)(((uint64_t)idx << s) * step & 0x7fffffffu)) & 0x7fffffffu;
+  else k = (uint32_t)(((uint64_t)(idx - n_hi) * step) & 0x7fffffffu);
+  pt31 r = {1u, 0u}, cur = {2u, 1268011823u};
+  for (int b = 0; b < 31; b++) {
+    if ((k >> b) & 1u) r = pt_add(r, cur);
+    cur = pt_add(cur, cur);
+  }
+  if (idx < n_hi) hi[idx] = r;
+  else lo[idx - n_hi] = r;
+}
+
+int make_domain_tables(cudaStream_t st, uint32_t lift, pt31* d_buf /* n_hi + n_lo entries */, DomainTables* out) {
+  GS_REQUIRE(lift >= 2 && lift <= 30, "lifting log size out of range");
+  uint32_t half_log = lift - 1;
+  uint32_t s = half_log / 2;
+  uint32_t n_hi = 1u << (half_log - s), n_lo = 1u << s;
+  uint32_t init = 1u << (31 - (lift + 1)), step = 1u << (31 - (lift - 1));
+  uint32_t total = n_hi + n_lo;
+  domain_tables_kernel<<<(total + 127) / 128, 128, 0, st>>>(d_buf, d_buf + n_hi, s, n_hi, init, step);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  *out = DomainTables{d_buf, d_buf + n_hi, s, lift};
+  return OK;
+}
+size_t domain_tables_len(uint32_t lift) {
+  uint32_t half_log = lift - 1, s = half_log / 2;
+  return (size_t)(1u << (half_log - s)) + (1u << s);
+}
+
+int compute_quotients_and_combine(cudaStream_t st, const void* d_accs, uint32_t n_accs, const DomainTables& dt,
+                                  Planes out) {
+  size_t n = (size_t)1 << dt.lift;
+  GS_REQUIRE(n >= QUOT_ROWS, "lifting domain too small");
+  size_t groups = n / QUOT_ROWS;
+  int threads = 128;
+  size_t blocks = (groups + threads - 1) / threads;
+  size_t cap = (size_t)num_sms() * 16;
+  if (blocks > cap) blocks = cap;
+  quotients_kernel<<<(unsigned)blocks, threads, 0, st>>>((const QuotAcc*)d_accs, n_accs, dt, out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+// ------------------------------------------------------------ accumulation
+__global__ void lift_and_accumulate_kernel(const LiftCol* __restrict__ cols, uint32_t n_cols, uint32_t log_size,
+                                           Planes out) {
+  const size_t n = (size_t)1 << log_size;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (uint32_t c = 0; c < n_cols; c++) {
+      const LiftCol& C = cols[c];
+      uint32_t r = log_size - C.log_size;
+      size_t li = ((i >> (r + 1)) << 1) + (i & 1);
+      a0 = add(a0, __ldg(C.p[0] + li));
+      a1 = add(a1, __ldg(C.p[1] + li));
+      a2 = add(a2, __ldg(C.p[2] + li));
+      a3 = add(a3, __ldg(C.p[3] + li));
+    }
+    out.p[0][i] = a0; out.p[1][i] = a1; out.p[2][i] = a2; out.p[3][i] = a3;
+  }
+}
+
+int lift_and_accumulate(cudaStream_t st, const void* d_cols, uint32_t n_cols, uint32_t log_size, Planes out) {
+  GS_REQUIRE(log_size >= 1 && log_size <= 30, "log size out of range");
+  size_t n = (size_t)1 << log_size;
+  size_t blocks = (n + 255) / 256;
+  size_t cap = (size_t)num_sms() * 16;
+  if (blocks > cap) blocks = cap;
+  lift_and_accumulate_kernel<<<(unsigned)blocks, 256, 0, st>>>((const LiftCol*)d_cols, n_cols, log_size, out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+__global__ void accumulate_kernel(Planes a, CPlanes b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) a.p[c][i] = add(a.p[c][i], __ldg(b.p[c] + i));
+  }
+}
+
+int accumulate(cudaStream_t st, Planes a, CPlanes b, size_t n) {
+  size_t blocks = (n + 255) / 256;
+  size_t cap = (size_t)num_sms() * 16;
+  if (blocks > cap) blocks = cap;
+  if (blocks == 0) return OK;
+  accumulate_kernel<<<(unsigned)blocks, 256, 0, st>>>(a, b, n);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+}  // namespace gs

@@ -29,13 +29,10 @@ int num_sms() {
 
 int Context::init(void* user_stream) {
   GS_CUDA_TRY(cudaGetDevice(&device));
-  if (user_stream) {
-    stream = (cudaStream_t)user_stream;
-    own_stream = false;
-  } else {
-    GS_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    own_stream = true;
-  }
+  // The given stream is always used as is; NULL is CUDA's default stream
+  // (the stream torch reports as 0), so work stays ordered with the caller's.
+  stream = (cudaStream_t)user_stream;
+  own_stream = false;
   ring_cap = 1 << 20;
   ring_off = 0;
   GS_CUDA_TRY(cudaMallocHost((void**)&h_ring, ring_cap));
@@ -48,6 +45,12 @@ int Context::init(void* user_stream) {
 
 void Context::destroy() {
   if (stream) cudaStreamSynchronize(stream);
+  if (scratch) cudaFree(scratch);
+  scratch = nullptr;
+  for (int i = 0; i < 31; i++) {
+    if (dom_buf[i]) cudaFree(dom_buf[i]);
+    dom_buf[i] = nullptr;
+  }
   if (h_ring) cudaFreeHost(h_ring);
   if (d_ring) cudaFree(d_ring);
   if (d_small) cudaFree(d_small);
@@ -57,19 +60,56 @@ void Context::destroy() {
   stream = nullptr;
 }
 
-int Context::stage_ptrs(const void* const* host_ptrs, size_t n, const void* const** out) {
-  size_t bytes = (n * sizeof(void*) + 255) & ~(size_t)255;
-  GS_REQUIRE(bytes <= ring_cap, "too many column pointers for one call");
+int Context::stage_bytes(const void* host, size_t len, const void** out) {
+  size_t bytes = (len + 255) & ~(size_t)255;
+  GS_REQUIRE(bytes <= ring_cap, "staged argument block too large");
   if (ring_off + bytes > ring_cap) {
     // Wrap: earlier copies out of the pinned ring must have completed before
     // their slots are rewritten.
     GS_CUDA_TRY(cudaStreamSynchronize(stream));
     ring_off = 0;
   }
-  memcpy(h_ring + ring_off, host_ptrs, n * sizeof(void*));
-  GS_CUDA_TRY(cudaMemcpyAsync(d_ring + ring_off, h_ring + ring_off, n * sizeof(void*), cudaMemcpyHostToDevice, stream));
-  *out = (const void* const*)(d_ring + ring_off);
+  memcpy(h_ring + ring_off, host, len);
+  GS_CUDA_TRY(cudaMemcpyAsync(d_ring + ring_off, h_ring + ring_off, len, cudaMemcpyHostToDevice, stream));
+  *out = (const void*)(d_ring + ring_off);
   ring_off += bytes;
+  return OK;
+}
+
+int Context::stage_ptrs(const void* const* host_ptrs, size_t n, const void* const** out) {
+  const void* d = nullptr;
+  GS_TRY(stage_bytes(host_ptrs, n * sizeof(void*), &d));
+  *out = (const void* const*)d;
+  return OK;
+}
+
+int Context::get_scratch(size_t bytes, void** out) {
+  if (bytes > scratch_cap) {
+    if (scratch) GS_CUDA_TRY(cudaFreeAsync(scratch, stream));
+    scratch = nullptr;
+    size_t cap = bytes < (1u << 20) ? (1u << 20) : bytes;
+    cudaError_t e = cudaMallocAsync(&scratch, cap, stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      scratch_cap = 0;
+      set_error("scratch allocation failed");
+      return ERR_OOM;
+    }
+    scratch_cap = cap;
+  }
+  *out = scratch;
+  return OK;
+}
+
+int Context::domain_tables(uint32_t lift, DomainTables* out) {
+  GS_REQUIRE(lift >= 2 && lift <= 30, "lifting log size out of range");
+  if (!dom_buf[lift]) {
+    void* buf = nullptr;
+    GS_CUDA_TRY(cudaMalloc(&buf, domain_tables_len(lift) * sizeof(pt31)));
+    GS_TRY(make_domain_tables(stream, lift, (pt31*)buf, &dom[lift]));
+    dom_buf[lift] = buf;
+  }
+  *out = dom[lift];
   return OK;
 }
 

@@ -52,6 +52,16 @@ struct CPlanes { const uint32_t* p[4]; };
 void note_launch(unsigned n = 1);
 unsigned long long launch_count();
 
+// Point tables of a canonic circle domain of log size `lift`: natural-order
+// half-coset point j is hi[j >> s] + lo[j & (2^s - 1)]; the other half are the
+// conjugates (used to get domain points from bit-reversed row indices).
+struct DomainTables {
+  const pt31* hi;
+  const pt31* lo;
+  uint32_t s;
+  uint32_t lift;
+};
+
 // Number of SMs of the current device (cached).
 int num_sms();
 
@@ -70,7 +80,17 @@ struct Context {
   uint8_t* h_small = nullptr;  // pinned mirror
   size_t small_cap = 0;
 
+  // growable device scratch (stream ordered)
+  void* scratch = nullptr;
+  size_t scratch_cap = 0;
+  // cached domain point tables per lifting log size
+  void* dom_buf[31] = {nullptr};
+  DomainTables dom[31];
+
   int init(void* user_stream);
+  int stage_bytes(const void* host, size_t bytes, const void** out);
+  int get_scratch(size_t bytes, void** out);
+  int domain_tables(uint32_t lift, DomainTables* out);
   void destroy();
   // Copies `n` host pointers into device memory usable by kernels launched on
   // `stream` after this call; returns the device address.
@@ -96,12 +116,39 @@ int bit_reverse(cudaStream_t st, uint32_t* d, uint32_t log_n);
 // merkle.cu
 int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, const uint32_t* const* d_cols,
                     uint32_t n_cols, uint32_t* d_out);
+// All node-only layers below `top_log` (layers[L] has 2^L hashes, layers[top_log] given).
+int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers);
 
 // fri.cu
 int fold_line(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itwiddles,
               uint32_t tw_log);
 int fold_circle_into_line(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
                           const uint32_t* d_itwiddles, uint32_t tw_log);
+
+// quotients.cu
+int accumulate_numerators(cudaStream_t st, const void* d_entries, uint32_t n_entries, qm31 b_sum, uint32_t log_size,
+                          Planes out);
+int compute_quotients_and_combine(cudaStream_t st, const void* d_accs, uint32_t n_accs, const DomainTables& dt,
+                                  Planes out);
+int lift_and_accumulate(cudaStream_t st, const void* d_cols, uint32_t n_cols, uint32_t log_size, Planes out);
+int accumulate(cudaStream_t st, Planes a, CPlanes b, size_t n);
+int make_domain_tables(cudaStream_t st, uint32_t lift, pt31* d_buf, DomainTables* out);
+size_t domain_tables_len(uint32_t lift);
+// entry layouts shared with the host side
+struct NumEntry { const uint32_t* col; uint32_t c[4]; };
+struct QuotAcc {
+  const uint32_t* p[4];
+  uint32_t log_size;
+  uint32_t pad;
+  qm31 first_linear;
+  cm31 prx, pry, pix, piy;
+};
+struct LiftCol { const uint32_t* p[4]; uint32_t log_size; uint32_t pad; };
+
+// eval_at_point.cu
+size_t eval_at_point_scratch_bytes(uint32_t n_polys, uint32_t log_n);
+int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_t n_polys, uint32_t log_n, ptq point,
+                        uint32_t* d_out, uint32_t* d_scratch);
 
 // grind.cu
 int grind_blake2s(cudaStream_t st, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint32_t* d_scratch,

@@ -21,6 +21,11 @@ class PointQM31(C.Structure):
     _fields_ = [("x", QM31), ("y", QM31)]
 
 
+class QuotientAcc(C.Structure):
+    _fields_ = [("partial", C.c_void_p * 4), ("log_size", C.c_uint32), ("first_linear_term", QM31),
+                ("sample_point", PointQM31)]
+
+
 class GpuStarkError(RuntimeError):
     pass
 
@@ -45,9 +50,16 @@ _PROTOS = {
     "gs_interpolate_columns": [C.c_void_p, VPP, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32],
     "gs_evaluate_columns": [C.c_void_p, VPP, C.c_uint32, VPP, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32],
     "gs_commit_on_layer": [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, VPP, C.c_void_p],
+    "gs_commit_node_layers": [C.c_void_p, C.c_uint32, VPP],
     "gs_fold_line": [C.c_void_p, VPP, C.c_uint32, QM31, VPP, C.c_void_p, C.c_uint32, C.c_void_p],
     "gs_fold_circle_into_line": [C.c_void_p, VPP, C.c_uint32, QM31, VPP, C.c_void_p, C.c_uint32, C.c_void_p],
     "gs_grind_blake2s": [C.c_void_p, U32P, C.c_uint32, C.POINTER(C.c_uint64)],
+    "gs_accumulate_numerators": [C.c_void_p, C.c_uint32, VPP, C.c_uint32, U32P, C.c_void_p, C.c_void_p, C.c_uint32,
+                                 VPP],
+    "gs_compute_quotients_and_combine": [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, VPP],
+    "gs_lift_and_accumulate": [C.c_void_p, VPP, U32P, C.c_uint32, VPP, C.c_uint32],
+    "gs_accumulate": [C.c_void_p, VPP, VPP, C.c_size_t],
+    "gs_batch_eval_at_point": [C.c_void_p, VPP, C.c_uint32, C.c_uint32, PointQM31, C.c_void_p],
 }
 _RESTYPE = {"gs_last_error": C.c_char_p, "gs_ctx_stream": C.c_void_p, "gs_launch_count": C.c_ulonglong}
 _OPTIONAL = set()

@@ -145,6 +145,14 @@ class GpuBackend:
                 "commit_on_layer")
         return out
 
+    @staticmethod
+    def commit_node_layers(layers, ctx=None):
+        """Fills layers[L] (2^L hashes) for L < len(layers)-1 from the top layer (node-only layers)."""
+        ctx = ctx or default_context()
+        pp, keep = L.ptr_array([t.data_ptr() for t in layers])
+        L.check(L.lib().gs_commit_node_layers(ctx.handle, len(layers) - 1, pp), "commit_node_layers")
+        return layers
+
     # --------------------------------------------------------------- FriOps
     @staticmethod
     def fold_line(eval_planes, log_size, alpha, twiddles: TwiddleTree, ctx=None, leaf_hashes=None):
@@ -167,6 +175,65 @@ class GpuBackend:
         L.check(L.lib().gs_fold_circle_into_line(ctx.handle, sp, log_size, qm31(alpha), dp, _p(twiddles.itwiddles),
                                                  twiddles.root_log, _p(leaf_hashes)), "fold_circle_into_line")
         return dst_planes
+
+    # ---------------------------------------------------------- QuotientOps
+    @staticmethod
+    def accumulate_numerators(columns, log_size, column_indices, line_coeffs_b, line_coeffs_c, ctx=None):
+        """QuotientOps::accumulate_numerators for one sample batch (quotient_ops.rs:27-31).
+        line_coeffs_*: sequences of QM31 (4 ints). Returns 4 planes of 2^log_size."""
+        ctx = ctx or default_context()
+        out = [torch.empty(1 << log_size, dtype=torch.int32, device="cuda") for _ in range(4)]
+        cp, k1 = L.ptr_array([c.data_ptr() for c in columns])
+        n = len(column_indices)
+        idx = (C.c_uint32 * max(n, 1))(*[int(i) for i in column_indices])
+        bs = (L.QM31 * max(n, 1))(*[qm31(b) for b in line_coeffs_b])
+        cs = (L.QM31 * max(n, 1))(*[qm31(c) for c in line_coeffs_c])
+        op, k2 = L.ptr_array([t.data_ptr() for t in out])
+        L.check(L.lib().gs_accumulate_numerators(ctx.handle, log_size, cp, len(columns), idx, bs, cs, n, op),
+                "accumulate_numerators")
+        return out
+
+    @staticmethod
+    def compute_quotients_and_combine(accs, lifting_log_size, ctx=None):
+        """accs: list of (partial_planes, log_size, first_linear_term(4), point(8)) (quotient_ops.rs:39-42)."""
+        ctx = ctx or default_context()
+        arr = (L.QuotientAcc * max(len(accs), 1))()
+        for a, (planes_, log_size, flt, pt) in enumerate(accs):
+            for i in range(4):
+                arr[a].partial[i] = planes_[i].data_ptr()
+            arr[a].log_size = log_size
+            arr[a].first_linear_term = qm31(flt)
+            arr[a].sample_point = L.PointQM31(qm31(pt[:4]), qm31(pt[4:]))
+        out = [torch.empty(1 << lifting_log_size, dtype=torch.int32, device="cuda") for _ in range(4)]
+        op, k = L.ptr_array([t.data_ptr() for t in out])
+        L.check(L.lib().gs_compute_quotients_and_combine(ctx.handle, arr, len(accs), lifting_log_size, op),
+                "compute_quotients_and_combine")
+        return out
+
+    # ------------------------------------------------------ AccumulationOps
+    @staticmethod
+    def lift_and_accumulate(cols, ctx=None):
+        """cols: list of 4-plane QM31 columns in increasing size (accumulation.rs:127-145)."""
+        ctx = ctx or default_context()
+        logs = [c[0].numel().bit_length() - 1 for c in cols]
+        out_log = max(logs)
+        out = [torch.empty(1 << out_log, dtype=torch.int32, device="cuda") for _ in range(4)]
+        pp, k1 = L.ptr_array([t.data_ptr() for c in cols for t in c])
+        ls = (C.c_uint32 * len(logs))(*logs)
+        op, k2 = L.ptr_array([t.data_ptr() for t in out])
+        L.check(L.lib().gs_lift_and_accumulate(ctx.handle, pp, ls, len(cols), op, out_log), "lift_and_accumulate")
+        return out
+
+    @staticmethod
+    def batch_eval_at_point(polys, point, ctx=None):
+        """Values of coefficient polynomials at a QM31 circle point (ops.rs:51-59)."""
+        ctx = ctx or default_context()
+        log_size = polys[0].numel().bit_length() - 1
+        pp, k = L.ptr_array([p.data_ptr() for p in polys])
+        out = (L.QM31 * len(polys))()
+        pt = L.PointQM31(qm31(point[:4]), qm31(point[4:]))
+        L.check(L.lib().gs_batch_eval_at_point(ctx.handle, pp, len(polys), log_size, pt, out), "batch_eval_at_point")
+        return [[o.a, o.b, o.c, o.d] for o in out]
 
     # ------------------------------------------------------------- GrindOps
     @staticmethod

@@ -169,6 +169,21 @@ def test_merkle_64x2p20_root(B):
     assert host(prev).view(np.uint8).tobytes() == O.merkle_root(cols)
 
 
+@pytest.mark.parametrize("top", [1, 5, 11, 12, 15])
+def test_commit_node_layers_fused(B, top):
+    """The fused node-only layers equal per-layer commit_on_layer calls."""
+    rng = np.random.default_rng(900 + top)
+    leaves = rng.integers(0, 256, (1 << top) * 32, dtype=np.uint8)
+    layers = [__import__("torch").empty((1 << L) * 8, dtype=__import__("torch").int32, device="cuda")
+              for L in range(top + 1)]
+    layers[top].copy_(dev(leaves.view(np.uint32)))
+    B.commit_node_layers(layers)
+    prev = leaves
+    for L in range(top - 1, -1, -1):
+        prev = O.commit_on_layer(L, prev.reshape(-1), [])
+        assert np.array_equal(host(layers[L]).view(np.uint8).reshape(-1, 32), prev), L
+
+
 def test_fold_line_2p22(B):
     rng = np.random.default_rng(800)
     ev = qm_rand(rng, 1 << 22)
