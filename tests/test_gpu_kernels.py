@@ -43,10 +43,10 @@ def test_twiddles(B, root_log):
     assert np.array_equal(host(t.itwiddles), itw)
 
 
-@pytest.mark.parametrize("log_n", [1, 2, 3, 4, 5, 8, 11, 12, 13, 14, 16, 17, 20])
+@pytest.mark.parametrize("log_n", [1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 20, 21, 22])
 def test_interpolate_matches_oracle(B, log_n):
     rng = np.random.default_rng(100 + log_n)
-    n_cols = 3 if log_n > 14 else 5
+    n_cols = 1 if log_n > 20 else (3 if log_n > 14 else 5)
     cols = [rand_m31(rng, 1 << log_n) for _ in range(n_cols)]
     root = max(log_n - 1, 1) + (1 if log_n % 2 else 0)  # also exercise a larger tree
     tw = B.precompute_twiddles(root)
@@ -58,10 +58,11 @@ def test_interpolate_matches_oracle(B, log_n):
 
 
 @pytest.mark.parametrize("coeff_log,log_n", [(1, 1), (2, 2), (1, 3), (3, 3), (4, 5), (8, 9), (10, 12), (12, 12),
-                                              (13, 14), (15, 16), (16, 17), (18, 19), (19, 20)])
+                                              (13, 14), (15, 16), (16, 17), (18, 19), (19, 20), (5, 18), (20, 22), (22, 22),
+                                              (23, 24)])
 def test_evaluate_matches_oracle(B, coeff_log, log_n):
     rng = np.random.default_rng(200 + coeff_log * 31 + log_n)
-    cols = [rand_m31(rng, 1 << coeff_log) for _ in range(3)]
+    cols = [rand_m31(rng, 1 << coeff_log) for _ in range(1 if log_n > 20 else 3)]
     tw = B.precompute_twiddles(max(log_n - 1, 1))
     out = B.evaluate_polynomials([dev(c) for c in cols], log_n, tw)
     expect = O.evaluate_columns(cols, log_n, root_log=max(log_n - 1, 1))
