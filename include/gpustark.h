@@ -163,6 +163,45 @@ int gs_batch_eval_at_point(gs_ctx* ctx, const uint32_t* const* polys, uint32_t n
  * pow_bits) as 8 LE words; returns the smallest valid nonce. Synchronises. */
 int gs_grind_blake2s(gs_ctx* ctx, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint64_t* nonce);
 
+/* ------------------------------------------------------------------ prove */
+/* PcsConfig (core/pcs/mod.rs:31-36) with FriConfig (core/fri.rs:32-37);
+ * lifting_log_size is None. line_fold_step must be 1 (as the reference's CUDA
+ * FRI, prover/backend/cuda/fri.rs:23). */
+typedef struct {
+  uint32_t pow_bits;
+  uint32_t log_blowup_factor;
+  uint32_t log_last_layer_degree_bound;
+  uint32_t n_queries;
+  uint32_t line_fold_step;
+} gs_pcs_config;
+
+/* Input rule of a proof's trace: the reference examples' inputs, seeded
+ * uniform M31, or columns supplied by the caller from host memory. */
+#define GS_INPUT_REFERENCE 0
+#define GS_INPUT_SEEDED 1
+#define GS_INPUT_HOST 2
+
+/* cuda_prove_wide_fibonacci (crates/examples/src/wide_fibonacci/mod.rs:140-184)
+ * driving prove() (crates/stwo/src/prover/mod.rs:28-150): 2^log_n_rows rows
+ * of n_columns. GS_INPUT_HOST: host_inputs holds columns 0 and 1 (2 x 2^log
+ * words). Writes the serialised StarkProof to proof (capacity bytes); returns
+ * GS_ERR_PROOF when the composition sanity check fails, GS_ERR_INVALID with
+ * *proof_len set when the buffer is too small. Synchronises. */
+int gs_prove_wide_fibonacci(gs_ctx* ctx, uint32_t log_n_rows, uint32_t n_columns, uint64_t seed, uint32_t input_mode,
+                            const uint32_t* host_inputs, const gs_pcs_config* config, uint8_t* proof,
+                            size_t capacity, size_t* proof_len);
+/* cuda_prove_poseidon (crates/examples/src/poseidon/mod.rs:617-700): one
+ * Poseidon2 instance per row, 2^log_n_instances rows. GS_INPUT_HOST:
+ * host_inputs holds the 16 initial-state columns (16 x 2^log words).
+ * composition_log_split = 1 is the reference's fixed split of the composition
+ * polynomial (core/verifier.rs:17), with which the reference's own prove()
+ * returns ConstraintsNotSatisfied for this component (LOG_EXPAND = 2);
+ * composition_log_split = 2 splits it into 4 parts so every committed tree has
+ * the trace's size, which yields a consistent proof. */
+int gs_prove_poseidon(gs_ctx* ctx, uint32_t log_n_instances, uint64_t seed, uint32_t input_mode,
+                      const uint32_t* host_inputs, uint32_t composition_log_split, const gs_pcs_config* config,
+                      uint8_t* proof, size_t capacity, size_t* proof_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,363 @@
+// AIR kernels for the two benchmark components: trace generation, the
+// Poseidon2 logup interaction column and the constraint quotients over the
+// evaluation domain.
+//
+// Semantics follow the reference:
+//   crates/examples/src/wide_fibonacci/mod.rs:48-58,86-130  (WideFibonacciEval, cuda trace: a=1, b=row)
+//   crates/examples/src/poseidon/mod.rs:79-220,222-330      (Poseidon2 rounds, constraints, lookups, trace)
+//   crates/constraint-framework/src/prover/component_prover.rs:177-280 (row_res * denom_inv[row >> trace_log])
+//   crates/constraint-framework/src/prover/cpu_domain.rs:57-92 (offset rows, constraint powers)
+//   crates/constraint-framework/src/lib.rs:218-262          (finalize_logup_in_pairs: one batch)
+//   crates/constraint-framework/src/prover/logup.rs:100-140 (claimed sum, shifted prefix sum)
+//   crates/stwo/src/prover/backend/simd/prefix_sum.rs:123-140 (prefix sum in coset order)
+//
+// Layout: a tree's columns are one contiguous buffer, column c at base + c * 2^log.
+// Constraint values of the base-field constraints are accumulated as
+// sum_k p_k * c_k with p_k in QM31 and c_k in M31: four wide products per term,
+// folded every two terms (lazy reduction), one reduction per row.
+#include "runtime.cuh"
+#include "air.cuh"
+#include <cub/device/device_scan.cuh>
+
+namespace gs {
+
+// ------------------------------------------------------------ seeded input
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+// Uniform M31 for (seed, column, row): the first of mix64(seed ^ mix64(col *
+// 0x100000001B3 + (row << 8) + k)) & (2^31 - 1), k = 0, 1, ..., below P.
+__host__ __device__ __forceinline__ uint32_t seeded_m31(uint64_t seed, uint64_t col, uint64_t row) {
+  for (uint64_t k = 0; k < 256; k++) {
+    uint32_t v = (uint32_t)mix64(seed ^ mix64(col * 0x100000001B3ull + (row << 8) + k)) & 0x7fffffffu;
+    if (v != P) return v;
+  }
+  return 0;  // unreachable in practice: 256 consecutive rejections of one value in 2^31
+}
+
+// ------------------------------------------------------------ wide fibonacci
+__global__ void wf_trace_kernel(uint32_t* cols, uint32_t log_n, uint32_t n_cols, uint64_t seed, uint32_t mode) {
+  const size_t n = (size_t)1 << log_n;
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+    // mode 0: the reference's inputs (a = 1, b = row); 1: seeded; 2: preloaded columns 0-1
+    uint32_t a = mode == 2 ? cols[r] : (mode ? seeded_m31(seed, 0, r) : 1u);
+    uint32_t b = mode == 2 ? cols[n + r] : (mode ? seeded_m31(seed, 1, r) : (uint32_t)(r % P));
+    cols[r] = a;
+    cols[n + r] = b;
+    for (uint32_t k = 2; k < n_cols; k++) {
+      uint32_t c = add(sqr(a), sqr(b));
+      cols[(size_t)k * n + r] = c;
+      a = b;
+      b = c;
+    }
+  }
+}
+
+__device__ __forceinline__ uint64_t fold64a(uint64_t x) { return (x & P) + (x >> 31); }
+
+__global__ void __launch_bounds__(256) wf_constraints_kernel(const uint32_t* __restrict__ cols, uint32_t n_cols,
+                                                             uint32_t eval_log, uint32_t trace_log, ConstraintParams prm,
+                                                             Planes out) {
+  const size_t n = (size_t)1 << eval_log;
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+    uint32_t a = __ldg(cols + r), b = __ldg(cols + n + r);
+    uint64_t acc[4] = {0, 0, 0, 0};
+    for (uint32_t k = 2; k < n_cols; k++) {
+      uint32_t c = __ldg(cols + (size_t)k * n + r);
+      uint32_t cons = sub(c, add(sqr(a), sqr(b)));
+      const uint32_t* p = prm.powers + 4 * (k - 2);
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[q] = fold64a(acc[q] + (uint64_t)p[q] * cons);
+      a = b;
+      b = c;
+    }
+    uint32_t dinv = prm.denom_inv[r >> trace_log];
+#pragma unroll
+    for (int q = 0; q < 4; q++) out.p[q][r] = mul(reduce64(acc[q]), dinv);
+  }
+}
+
+// ------------------------------------------------------------ poseidon2
+constexpr uint32_t PN_RC = 1234;  // the reference's placeholder round constants (poseidon/mod.rs:48-51)
+
+__host__ __device__ __forceinline__ void p2_m4(uint32_t* x) {
+  uint32_t t0 = add(x[0], x[1]);
+  uint32_t t02 = add(t0, t0);
+  uint32_t t1 = add(x[2], x[3]);
+  uint32_t t12 = add(t1, t1);
+  uint32_t t2 = add(add(x[1], x[1]), t1);
+  uint32_t t3 = add(add(x[3], x[3]), t0);
+  uint32_t t4 = add(add(t12, t12), t3);
+  uint32_t t5 = add(add(t02, t02), t2);
+  x[0] = add(t3, t5);
+  x[1] = t5;
+  x[2] = add(t2, t4);
+  x[3] = t4;
+}
+__host__ __device__ __forceinline__ void p2_external(uint32_t* s) {
+#pragma unroll
+  for (int i = 0; i < 4; i++) p2_m4(s + 4 * i);
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    uint32_t t = add(add(s[j], s[j + 4]), add(s[j + 8], s[j + 12]));
+#pragma unroll
+    for (int i = 0; i < 4; i++) s[4 * i + j] = add(s[4 * i + j], t);
+  }
+}
+__host__ __device__ __forceinline__ void p2_internal(uint32_t* s) {
+  uint32_t sum = s[0];
+#pragma unroll
+  for (int i = 1; i < 16; i++) sum = add(sum, s[i]);
+#pragma unroll
+  for (int i = 0; i < 16; i++) s[i] = add(mul(s[i], 1u << (i + 1)), sum);
+}
+__host__ __device__ __forceinline__ uint32_t pow5(uint32_t x) { uint32_t x2 = sqr(x); return mul(sqr(x2), x); }
+
+__global__ void poseidon_trace_kernel(uint32_t* cols, uint32_t log_n, uint64_t seed, uint32_t mode) {
+  const size_t n = (size_t)1 << log_n;
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+    uint32_t s[16];
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      // mode 0: the reference's inputs (row + i); 1: seeded; 2: preloaded columns 0-15
+      s[i] = mode == 2 ? cols[(size_t)i * n + r] : (mode ? seeded_m31(seed, i, r) : (uint32_t)((r + i) % P));
+      cols[(size_t)(c++) * n + r] = s[i];
+    }
+    for (int round = 0; round < 4; round++) {
+#pragma unroll
+      for (int i = 0; i < 16; i++) s[i] = add(s[i], PN_RC);
+      p2_external(s);
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        s[i] = pow5(s[i]);
+        cols[(size_t)(c++) * n + r] = s[i];
+      }
+    }
+    for (int round = 0; round < 14; round++) {
+      s[0] = add(s[0], PN_RC);
+      p2_internal(s);
+      s[0] = pow5(s[0]);
+      cols[(size_t)(c++) * n + r] = s[0];
+    }
+    for (int round = 0; round < 4; round++) {
+#pragma unroll
+      for (int i = 0; i < 16; i++) s[i] = add(s[i], PN_RC);
+      p2_external(s);
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        s[i] = pow5(s[i]);
+        cols[(size_t)(c++) * n + r] = s[i];
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ qm31 combine16(const LookupParams& lp, const uint32_t* v, size_t stride, size_t r) {
+  uint64_t acc[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+    uint32_t x = __ldg(v + (size_t)i * stride + r);
+    const uint32_t* a = lp.alpha_pow + 4 * i;
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[q] = fold64a(acc[q] + (uint64_t)a[q] * x);
+  }
+  qm31 s = qm_make(reduce64(acc[0]), reduce64(acc[1]), reduce64(acc[2]), reduce64(acc[3]));
+  return qm_sub(s, qm_make(lp.z[0], lp.z[1], lp.z[2], lp.z[3]));
+}
+
+__device__ __forceinline__ uint32_t coset_index(uint32_t i, uint32_t log_n) {
+  uint32_t n = 1u << log_n;
+  uint32_t j = log_n ? (__brev(i) >> (32 - log_n)) : 0u;
+  return j < n / 2 ? 2 * j : 2 * (n - 1 - j) + 1;
+}
+
+// Per row: (1/d0 - 1/d1) written at its coset-order position.
+__global__ void logup_fraction_kernel(const uint32_t* __restrict__ cols, uint32_t log_n, LookupParams lp,
+                                      uint4* __restrict__ coset_vals) {
+  const size_t n = (size_t)1 << log_n;
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+    qm31 d0 = combine16(lp, cols, n, r);
+    qm31 d1 = combine16(lp, cols + (size_t)(158 - 16) * n, n, r);
+    qm31 v = qm_mul(qm_sub(d1, d0), qm_inv(qm_mul(d0, d1)));
+    coset_vals[coset_index((uint32_t)r, log_n)] = make_uint4(v.x.a, v.x.b, v.y.a, v.y.b);
+  }
+}
+
+struct AddQM {
+  __device__ __forceinline__ uint4 operator()(const uint4& a, const uint4& b) const {
+    return make_uint4(add(a.x, b.x), add(a.y, b.y), add(a.z, b.z), add(a.w, b.w));
+  }
+};
+
+// out_c[i] = S_c[k] - (k + 1) * shift_c at k = coset position of storage row i.
+__global__ void logup_finalize_kernel(const uint4* __restrict__ scan, uint32_t log_n, qm31 shift, uint32_t* out) {
+  const size_t n = (size_t)1 << log_n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t k = coset_index((uint32_t)i, log_n);
+    uint4 s = scan[k];
+    uint32_t m = (k + 1) % P;
+    out[i] = sub(s.x, mul(shift.x.a, m));
+    out[n + i] = sub(s.y, mul(shift.x.b, m));
+    out[2 * n + i] = sub(s.z, mul(shift.y.a, m));
+    out[3 * n + i] = sub(s.w, mul(shift.y.b, m));
+  }
+}
+
+// offset_bit_reversed_circle_domain_index(i, trace_log, eval_log, -1)
+// (crates/stwo/src/core/utils.rs).
+__device__ __forceinline__ uint32_t prev_row(uint32_t i, uint32_t trace_log, uint32_t eval_log) {
+  uint32_t idx = __brev(i) >> (32 - eval_log);
+  uint32_t half = 1u << (eval_log - 1);
+  uint32_t step = 1u << (eval_log - trace_log - 1);
+  if (idx < half) idx = (idx + half - step) & (half - 1);
+  else idx = ((idx - half + step) & (half - 1)) + half;
+  return __brev(idx) >> (32 - eval_log);
+}
+
+__global__ void __launch_bounds__(128) poseidon_constraints_kernel(const uint32_t* __restrict__ trace,
+                                                                   const uint32_t* __restrict__ inter, uint32_t eval_log,
+                                                                   uint32_t trace_log, ConstraintParams prm,
+                                                                   LookupParams lp, qm31 cumsum_shift, Planes out) {
+  const size_t n = (size_t)1 << eval_log;
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+    uint64_t acc[4] = {0, 0, 0, 0};
+    uint32_t k = 0;  // constraint index
+    auto add_cons = [&](uint32_t c) {
+      const uint32_t* p = prm.powers + 4 * k;
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[q] = fold64a(acc[q] + (uint64_t)p[q] * c);
+      k++;
+    };
+    uint32_t s[16];
+    uint32_t col = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) s[i] = __ldg(trace + (size_t)(col++) * n + r);
+    for (int round = 0; round < 4; round++) {
+#pragma unroll
+      for (int i = 0; i < 16; i++) s[i] = add(s[i], PN_RC);
+      p2_external(s);
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        uint32_t m = __ldg(trace + (size_t)(col++) * n + r);
+        add_cons(sub(pow5(s[i]), m));
+        s[i] = m;
+      }
+    }
+    for (int round = 0; round < 14; round++) {
+      s[0] = add(s[0], PN_RC);
+      p2_internal(s);
+      uint32_t m = __ldg(trace + (size_t)(col++) * n + r);
+      add_cons(sub(pow5(s[0]), m));
+      s[0] = m;
+    }
+    for (int round = 0; round < 4; round++) {
+#pragma unroll
+      for (int i = 0; i < 16; i++) s[i] = add(s[i], PN_RC);
+      p2_external(s);
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        uint32_t m = __ldg(trace + (size_t)(col++) * n + r);
+        add_cons(sub(pow5(s[i]), m));
+        s[i] = m;
+      }
+    }
+    // logup: frac = 1/d0 - 1/d1 as (d1 - d0) / (d0 d1); constraint
+    // (cur - prev + shift) * d0 d1 - (d1 - d0)
+    qm31 d0 = combine16(lp, trace, n, r);
+    qm31 d1 = combine16(lp, trace + (size_t)(158 - 16) * n, n, r);
+    uint32_t pr = prev_row((uint32_t)r, trace_log, eval_log);
+    qm31 cur = qm_make(__ldg(inter + r), __ldg(inter + n + r), __ldg(inter + 2 * n + r), __ldg(inter + 3 * n + r));
+    qm31 prv = qm_make(__ldg(inter + pr), __ldg(inter + n + pr), __ldg(inter + 2 * n + pr), __ldg(inter + 3 * n + pr));
+    qm31 lc = qm_sub(qm_mul(qm_add(qm_sub(cur, prv), cumsum_shift), qm_mul(d0, d1)), qm_sub(d1, d0));
+    qm31 pl = qm_make(prm.powers[4 * k], prm.powers[4 * k + 1], prm.powers[4 * k + 2], prm.powers[4 * k + 3]);
+    qm31 res = qm_add(qm_make(reduce64(acc[0]), reduce64(acc[1]), reduce64(acc[2]), reduce64(acc[3])), qm_mul(pl, lc));
+    uint32_t dinv = prm.denom_inv[r >> trace_log];
+    out.p[0][r] = mul(res.x.a, dinv);
+    out.p[1][r] = mul(res.x.b, dinv);
+    out.p[2][r] = mul(res.y.a, dinv);
+    out.p[3][r] = mul(res.y.b, dinv);
+  }
+}
+
+static unsigned grid_rows(size_t n, int threads) {
+  size_t b = (n + threads - 1) / threads;
+  size_t cap = (size_t)num_sms() * 32;
+  return (unsigned)(b < cap ? (b ? b : 1) : cap);
+}
+
+int wf_trace(cudaStream_t st, uint32_t* cols, uint32_t log_n, uint32_t n_cols, uint64_t seed, uint32_t mode) {
+  GS_REQUIRE(n_cols >= 2 && log_n <= 28, "bad wide fibonacci shape");
+  wf_trace_kernel<<<grid_rows((size_t)1 << log_n, 256), 256, 0, st>>>(cols, log_n, n_cols, seed, mode);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+int wf_constraints(cudaStream_t st, const uint32_t* cols, uint32_t n_cols, uint32_t eval_log, uint32_t trace_log,
+                   const ConstraintParams& prm, Planes out) {
+  GS_REQUIRE(n_cols >= 3 && n_cols - 2 <= MAX_CONSTRAINTS, "bad wide fibonacci width");
+  wf_constraints_kernel<<<grid_rows((size_t)1 << eval_log, 256), 256, 0, st>>>(cols, n_cols, eval_log, trace_log, prm,
+                                                                                out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+int poseidon_trace(cudaStream_t st, uint32_t* cols, uint32_t log_n, uint64_t seed, uint32_t mode) {
+  GS_REQUIRE(log_n <= 28, "bad poseidon size");
+  poseidon_trace_kernel<<<grid_rows((size_t)1 << log_n, 128), 128, 0, st>>>(cols, log_n, seed, mode);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+size_t logup_scratch_bytes(uint32_t log_n) {
+  size_t n = (size_t)1 << log_n;
+  size_t temp = 0;
+  cub::DeviceScan::InclusiveScan(nullptr, temp, (const uint4*)nullptr, (uint4*)nullptr, AddQM(), (int)n);
+  return 2 * n * sizeof(uint4) + ((temp + 255) & ~(size_t)255);
+}
+
+// Interaction column: writes the 4 coordinate columns (out, 4 x 2^log_n) and
+// the claimed sum (host). scratch: logup_scratch_bytes(log_n).
+int poseidon_interaction(cudaStream_t st, const uint32_t* trace, uint32_t log_n, const LookupParams& lp,
+                         uint32_t* out, void* scratch, qm31* claimed_sum) {
+  size_t n = (size_t)1 << log_n;
+  uint4* vals = (uint4*)scratch;
+  uint4* scan = vals + n;
+  void* temp = (void*)(scan + n);
+  size_t temp_bytes = 0;
+  cub::DeviceScan::InclusiveScan(nullptr, temp_bytes, (const uint4*)nullptr, (uint4*)nullptr, AddQM(), (int)n);
+  logup_fraction_kernel<<<grid_rows(n, 128), 128, 0, st>>>(trace, log_n, lp, vals);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  GS_CUDA_TRY(cub::DeviceScan::InclusiveScan(temp, temp_bytes, (const uint4*)vals, scan, AddQM(), (int)n, st));
+  note_launch();
+  uint4 total;
+  GS_CUDA_TRY(cudaMemcpyAsync(&total, scan + (n - 1), sizeof(uint4), cudaMemcpyDeviceToHost, st));
+  GS_CUDA_TRY(cudaStreamSynchronize(st));
+  qm31 cs = qm_make(total.x, total.y, total.z, total.w);
+  *claimed_sum = cs;
+  qm31 shift = qm_mul_m31(cs, inv((uint32_t)(n % P)));
+  logup_finalize_kernel<<<grid_rows(n, 256), 256, 0, st>>>(scan, log_n, shift, out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+int poseidon_constraints(cudaStream_t st, const uint32_t* trace, const uint32_t* inter, uint32_t eval_log,
+                         uint32_t trace_log, const ConstraintParams& prm, const LookupParams& lp, qm31 cumsum_shift,
+                         Planes out) {
+  GS_REQUIRE(eval_log > trace_log, "poseidon constraints need an extended domain");
+  poseidon_constraints_kernel<<<grid_rows((size_t)1 << eval_log, 128), 128, 0, st>>>(trace, inter, eval_log, trace_log,
+                                                                                      prm, lp, cumsum_shift, out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+}  // namespace gs

@@ -1,0 +1,43 @@
+// Parameters and launch interface of the AIR kernels (air.cu).
+#pragma once
+#include "runtime.cuh"
+
+namespace gs {
+
+constexpr int MAX_CONSTRAINTS = 160;
+
+// Random-coefficient powers in the order the constraints are added
+// (powers[4k..4k+3] = alpha^(n-1-k), the reversed powers of
+// DomainEvaluationAccumulator::columns) and the bit-reversed denominator
+// inverses 1 / vanishing(trace coset, eval_domain.at(i)), i < 2^(eval-trace).
+struct ConstraintParams {
+  uint32_t powers[4 * MAX_CONSTRAINTS];
+  uint32_t denom_inv[8];
+};
+
+// LookupElements<16>: alpha^i (i < 16) and z, as QM31 words.
+struct LookupParams {
+  uint32_t alpha_pow[64];
+  uint32_t z[4];
+};
+
+int wf_trace(cudaStream_t st, uint32_t* cols, uint32_t log_n, uint32_t n_cols, uint64_t seed, uint32_t mode);
+int wf_constraints(cudaStream_t st, const uint32_t* cols, uint32_t n_cols, uint32_t eval_log, uint32_t trace_log,
+                   const ConstraintParams& prm, Planes out);
+int poseidon_trace(cudaStream_t st, uint32_t* cols, uint32_t log_n, uint64_t seed, uint32_t mode);
+size_t logup_scratch_bytes(uint32_t log_n);
+int poseidon_interaction(cudaStream_t st, const uint32_t* trace, uint32_t log_n, const LookupParams& lp,
+                         uint32_t* out, void* scratch, qm31* claimed_sum);
+int poseidon_constraints(cudaStream_t st, const uint32_t* trace, const uint32_t* inter, uint32_t eval_log,
+                         uint32_t trace_log, const ConstraintParams& prm, const LookupParams& lp, qm31 cumsum_shift,
+                         Planes out);
+
+// gather.cu: out[k] = src_k[idx_k] (words) and 8-word hash gathers.
+struct GatherItem {
+  const uint32_t* src;
+  uint64_t idx;
+};
+int gather_words(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out);
+int gather_hashes(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out);
+
+}  // namespace gs

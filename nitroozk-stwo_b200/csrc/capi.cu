@@ -1,6 +1,8 @@
 // C ABI (include/gpustark.h) over the internal launch interface.
 #include "../../include/gpustark.h"
 #include "runtime.cuh"
+#include "prover/prove_api.h"
+#include <cstring>
 
 struct gs_ctx {
   gs::Context c;
@@ -313,6 +315,63 @@ int gs_grind_blake2s(gs_ctx* ctx, const uint32_t prefixed_digest[8], uint32_t po
   CTX_REQUIRED(ctx);
   GS_REQUIRE(prefixed_digest != nullptr, "null digest");
   return grind_blake2s(ctx->c.stream, prefixed_digest, pow_bits, (uint32_t*)ctx->c.d_small, nonce);
+}
+
+static int run_prove(gs_ctx* ctx, prover::ProveRequest& req, const gs_pcs_config* config, uint8_t* proof,
+                     size_t capacity, size_t* proof_len) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(proof_len != nullptr, "null proof length");
+  if (config) {
+    req.cfg.pow_bits = config->pow_bits;
+    req.cfg.log_blowup = config->log_blowup_factor;
+    req.cfg.log_last_layer = config->log_last_layer_degree_bound;
+    req.cfg.n_queries = config->n_queries;
+    req.cfg.fold_step = config->line_fold_step;
+  }
+  GS_REQUIRE(req.input_mode <= 2, "unknown input mode");
+  GS_REQUIRE(req.input_mode != 2 || req.host_inputs != nullptr, "host inputs required");
+  GS_REQUIRE(req.cfg.pow_bits <= 32 && req.cfg.n_queries >= 1 && req.cfg.log_last_layer <= 10, "bad PCS config");
+  std::string bytes;
+  int st = prover::prove_component(ctx->c, req, &bytes, nullptr);
+  *proof_len = bytes.size();
+  if (st != OK) {
+    cudaStreamSynchronize(ctx->c.stream);
+    return st;
+  }
+  if (bytes.size() > capacity || !proof) {
+    set_error("proof buffer too small");
+    return ERR_INVALID;
+  }
+  memcpy(proof, bytes.data(), bytes.size());
+  return OK;
+}
+
+int gs_prove_wide_fibonacci(gs_ctx* ctx, uint32_t log_n_rows, uint32_t n_columns, uint64_t seed, uint32_t input_mode,
+                            const uint32_t* host_inputs, const gs_pcs_config* config, uint8_t* proof,
+                            size_t capacity, size_t* proof_len) {
+  prover::ProveRequest req;
+  req.air = 0;
+  req.log_n = log_n_rows;
+  req.n_cols = n_columns;
+  req.seed = seed;
+  req.input_mode = input_mode;
+  req.host_inputs = host_inputs;
+  req.split_log = 1;
+  GS_REQUIRE(n_columns >= 3 && n_columns <= 160, "wide fibonacci needs 3..160 columns");
+  return run_prove(ctx, req, config, proof, capacity, proof_len);
+}
+
+int gs_prove_poseidon(gs_ctx* ctx, uint32_t log_n_instances, uint64_t seed, uint32_t input_mode,
+                      const uint32_t* host_inputs, uint32_t composition_log_split, const gs_pcs_config* config,
+                      uint8_t* proof, size_t capacity, size_t* proof_len) {
+  prover::ProveRequest req;
+  req.air = 1;
+  req.log_n = log_n_instances;
+  req.seed = seed;
+  req.input_mode = input_mode;
+  req.host_inputs = host_inputs;
+  req.split_log = composition_log_split;
+  return run_prove(ctx, req, config, proof, capacity, proof_len);
 }
 
 }  // extern "C"

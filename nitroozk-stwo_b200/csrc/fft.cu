@@ -99,6 +99,8 @@ __device__ __forceinline__ void bfly(uint32_t& a, uint32_t& b, uint32_t w) {
   }
 }
 
+// XOR swizzle over the block's shared-memory index (tile offset included, so
+// blocks holding several small tiles stay conflict free as well).
 __device__ __forceinline__ uint32_t swz(uint32_t e) { return e ^ ((e >> 5) & 31u); }
 
 template <bool INV, int R>
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const uint32_t* const* __
   const uint32_t ltid = threadIdx.x & ((1u << tpt_log) - 1u);
   const uint32_t sub_tile = threadIdx.x >> tpt_log;
   const uint32_t tile = (blockIdx.x << a.tile_shift) | sub_tile;
-  uint32_t* smt = sm + (sub_tile << a.t);
+  const uint32_t smbase = sub_tile << a.t;  // swizzled together with the tile index
   const uint32_t ml = a.lo - a.c;
   const uint32_t midlow = tile & ((1u << ml) - 1u);
   const uint32_t hi = tile >> ml;
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const uint32_t* const* __
     } else {
       __syncthreads();
 #pragma unroll
-      for (int q = 0; q < NQ; q++) x[q] = smt[swz(ebase | ((uint32_t)q << s0))];
+      for (int q = 0; q < NQ; q++) x[q] = sm[swz(smbase | ebase | ((uint32_t)q << s0))];
       __syncthreads();
     }
     const uint32_t vth = basev | ((ebase >> a.c) << a.lo) | (ebase & cmask);
@@ -179,7 +181,7 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const uint32_t* const* __
     }
     if (k + 1 < a.K) {
 #pragma unroll
-      for (int q = 0; q < NQ; q++) smt[swz(ebase | ((uint32_t)q << s0))] = x[q];
+      for (int q = 0; q < NQ; q++) sm[swz(smbase | ebase | ((uint32_t)q << s0))] = x[q];
     } else {
       if (a.has_scale) {
 #pragma unroll
@@ -371,6 +373,17 @@ int interpolate_columns(cudaStream_t st, uint32_t* const* d_cols, uint32_t n_col
   GS_REQUIRE(tw_log + 1 >= log_n, "twiddle tree too small for the domain");
   return run_passes<true>(st, (const uint32_t* const*)d_cols, d_cols, n_cols, log_n, log_n, 0xffffffffu, d_itwiddles,
                           1u << tw_log);
+}
+
+// Out-of-place interpolation (src and dst tables may differ).
+int interpolate_columns_to(cudaStream_t st, const uint32_t* const* d_src, uint32_t* const* d_dst, uint32_t n_cols,
+                           uint32_t log_n, const uint32_t* d_itwiddles, uint32_t tw_log) {
+  if (n_cols == 0) return OK;
+  GS_REQUIRE(log_n >= 1 && log_n <= 30, "log_n out of range");
+  GS_REQUIRE(n_cols <= 65535, "too many columns in one call");
+  if (log_n <= 2) return launch_small(st, d_src, d_dst, n_cols, log_n, true, 0xffffffffu);
+  GS_REQUIRE(tw_log + 1 >= log_n, "twiddle tree too small for the domain");
+  return run_passes<true>(st, d_src, d_dst, n_cols, log_n, log_n, 0xffffffffu, d_itwiddles, 1u << tw_log);
 }
 
 int evaluate_columns(cudaStream_t st, const uint32_t* const* d_src, uint32_t coeff_log, uint32_t* const* d_dst,

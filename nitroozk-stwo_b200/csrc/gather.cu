@@ -1,0 +1,44 @@
+// Decommitment gathers (Column::batch_at / batch_at_multi, crates/stwo/src/
+// prover/backend/mod.rs:70-86; reference CUDA cuda_batch_gather_multi_uint32,
+// cuda_batch_get_blake_2s_hash): one launch fetches every value and hash a
+// decommitment needs, listed as (buffer, index) items.
+#include "air.cuh"
+
+namespace gs {
+
+__global__ void gather_words_kernel(const GatherItem* __restrict__ items, size_t n, uint32_t* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    GatherItem it = items[i];
+    out[i] = __ldg(it.src + it.idx);
+  }
+}
+
+__global__ void gather_hashes_kernel(const GatherItem* __restrict__ items, size_t n, uint32_t* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    GatherItem it = items[i];
+    const uint4* s = reinterpret_cast<const uint4*>(it.src + 8 * it.idx);
+    uint4* o = reinterpret_cast<uint4*>(out + 8 * i);
+    o[0] = __ldg(s);
+    o[1] = __ldg(s + 1);
+  }
+}
+
+int gather_words(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out) {
+  if (n == 0) return OK;
+  unsigned blocks = (unsigned)((n + 255) / 256);
+  gather_words_kernel<<<blocks, 256, 0, st>>>(d_items, n, d_out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+int gather_hashes(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out) {
+  if (n == 0) return OK;
+  unsigned blocks = (unsigned)((n + 255) / 256);
+  gather_hashes_kernel<<<blocks, 256, 0, st>>>(d_items, n, d_out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+}  // namespace gs

@@ -24,20 +24,46 @@ constexpr uint32_t P = 0x7fffffffu;
 
 GS_HD uint32_t umin32(uint32_t a, uint32_t b) { return a < b ? a : b; }
 
-// a + b for a, b < p: one add and one min (r - p wraps above r when r < p).
-GS_HD uint32_t add(uint32_t a, uint32_t b) { uint32_t r = a + b; return umin32(r, r - P); }
-GS_HD uint32_t sub(uint32_t a, uint32_t b) { uint32_t r = a + (P - b); return umin32(r, r - P); }
+// a + b for a, b < p: with s = a + b - p (mod 2^32), the result is
+// min(s + p, s) (s wraps above s + p exactly when a + b < p). On the device
+// that is one three-input add and one add-then-min (VIADDMNMX).
+GS_HD uint32_t add(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  uint32_t s = a + b - P;
+  return __viaddmin_u32(s, P, s);
+#else
+  uint32_t r = a + b;
+  return umin32(r, r - P);
+#endif
+}
+// a - b: d = a - b (mod 2^32), result min(d, d + p).
+GS_HD uint32_t sub(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  uint32_t d = a - b;
+  return __viaddmin_u32(d, P, d);
+#else
+  uint32_t r = a + (P - b);
+  return umin32(r, r - P);
+#endif
+}
 GS_HD uint32_t neg(uint32_t a) { uint32_t r = P - a; return umin32(r, r - P); }
+GS_HD uint32_t mul(uint32_t a, uint32_t b);
 
 // a * b: 62-bit product folded once (lo 31 bits + hi 31 bits < 2p), then one
 // conditional subtract.
+//
+// Device form: with b2 = 2b < 2^32, the 64-bit product a * b2 = 2(ab) has
+// high word (ab) >> 31 and low word 2((ab) mod 2^31), so one wide multiply
+// and one shift-add (LEA.HI) give r = (ab >> 31) + (ab mod 2^31) < 2p, and
+// an add-then-min finishes the reduction.
+__device__ __forceinline__ uint32_t mul_b2(uint32_t a, uint32_t b2) {
+  uint64_t p = (uint64_t)a * b2;
+  uint32_t r = (uint32_t)(p >> 32) + ((uint32_t)p >> 1);
+  return __viaddmin_u32(r, 0u - P, r);
+}
 GS_HD uint32_t mul(uint32_t a, uint32_t b) {
 #ifdef __CUDA_ARCH__
-  uint32_t lo = a * b;
-  uint32_t hi = __umulhi(a, b);
-  uint32_t h = __funnelshift_l(lo, hi, 1);  // (hi:lo) >> 31
-  uint32_t r = (lo & P) + h;
-  return umin32(r, r - P);
+  return mul_b2(a, b << 1);
 #else
   uint64_t p = (uint64_t)a * b;
   uint32_t r = (uint32_t)(p & P) + (uint32_t)(p >> 31);

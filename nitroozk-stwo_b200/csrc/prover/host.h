@@ -1,0 +1,287 @@
+// Host-side protocol pieces of the GPU prover: Blake2s hashing, the
+// Fiat-Shamir channel, circle points over QM31 and proof serialisation.
+//
+// Semantics follow the reference:
+//   crates/stwo/src/core/channel/blake2s.rs:20-140   (channel: mix, draw, pow prefix)
+//   crates/stwo/src/core/vcs/blake2_merkle.rs:53-58  (mix_root)
+//   crates/stwo/src/core/queries.rs:11-28            (draw_queries)
+//   crates/stwo/src/core/circle.rs:12-214            (points, random point, generators)
+//   crates/stwo/src/core/constraints.rs:12-35        (coset_vanishing)
+//   crates/stwo/src/core/pcs/quotients.rs:29-38, core/fri.rs:363-398 (proof layout)
+#pragma once
+#include <array>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "../blake2s.cuh"
+#include "../m31.cuh"
+
+namespace gs {
+namespace host {
+
+using Hash = std::array<uint8_t, 32>;
+
+// Incremental Blake2s-256 over the shared compression function.
+struct Hasher {
+  uint32_t h[8];
+  uint8_t buf[64];
+  size_t len = 0;
+  uint64_t total = 0;
+  Hasher() { blake2s_init(h); }
+  void compress_buf(bool last) {
+    uint32_t m[16];
+    for (int i = 0; i < 16; i++)
+      m[i] = (uint32_t)buf[4 * i] | ((uint32_t)buf[4 * i + 1] << 8) | ((uint32_t)buf[4 * i + 2] << 16) |
+             ((uint32_t)buf[4 * i + 3] << 24);
+    blake2s_compress(h, m, (uint32_t)total, last);
+  }
+  void update(const void* data, size_t n) {
+    const uint8_t* p = (const uint8_t*)data;
+    while (n) {
+      if (len == 64) {
+        total += 64;
+        compress_buf(false);
+        len = 0;
+      }
+      size_t k = 64 - len < n ? 64 - len : n;
+      memcpy(buf + len, p, k);
+      len += k;
+      p += k;
+      n -= k;
+    }
+  }
+  void u32(uint32_t w) { uint8_t b[4] = {(uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)(w >> 24)}; update(b, 4); }
+  Hash finish() {
+    total += len;
+    memset(buf + len, 0, 64 - len);
+    compress_buf(true);
+    Hash out;
+    for (int i = 0; i < 8; i++)
+      for (int j = 0; j < 4; j++) out[4 * i + j] = (uint8_t)(h[i] >> (8 * j));
+    return out;
+  }
+};
+
+inline Hash hash_bytes(const void* d, size_t n) { Hasher s; s.update(d, n); return s.finish(); }
+inline Hash hash_from_words(const uint32_t w[8]) {
+  Hash h;
+  for (int i = 0; i < 8; i++)
+    for (int j = 0; j < 4; j++) h[4 * i + j] = (uint8_t)(w[i] >> (8 * j));
+  return h;
+}
+inline uint32_t word(const Hash& h, int i) {
+  return (uint32_t)h[4 * i] | ((uint32_t)h[4 * i + 1] << 8) | ((uint32_t)h[4 * i + 2] << 16) | ((uint32_t)h[4 * i + 3] << 24);
+}
+
+struct Channel {
+  Hash digest{};
+  uint32_t n_draws = 0;
+  void set(const Hash& d) { digest = d; n_draws = 0; }
+  void mix_root(const Hash& root) { Hasher s; s.update(digest.data(), 32); s.update(root.data(), 32); set(s.finish()); }
+  void mix_felts(const std::vector<qm31>& f) {
+    Hasher s;
+    s.update(digest.data(), 32);
+    for (auto& q : f) { s.u32(q.x.a); s.u32(q.x.b); s.u32(q.y.a); s.u32(q.y.b); }
+    set(s.finish());
+  }
+  void mix_u64(uint64_t v) {
+    Hasher s;
+    s.update(digest.data(), 32);
+    s.u32((uint32_t)v);
+    s.u32((uint32_t)(v >> 32));
+    set(s.finish());
+  }
+  std::array<uint32_t, 8> draw_u32s() {
+    uint8_t in[37];
+    memcpy(in, digest.data(), 32);
+    for (int i = 0; i < 4; i++) in[32 + i] = (uint8_t)(n_draws >> (8 * i));
+    in[36] = 0;
+    n_draws++;
+    Hash h = hash_bytes(in, 37);
+    std::array<uint32_t, 8> r;
+    for (int i = 0; i < 8; i++) r[i] = word(h, i);
+    return r;
+  }
+  std::array<uint32_t, 8> draw_base() {
+    for (;;) {
+      auto u = draw_u32s();
+      bool ok = true;
+      for (auto x : u) ok = ok && x < 2 * P;
+      if (ok) {
+        for (auto& x : u) x = x >= P ? x - P : x;
+        return u;
+      }
+    }
+  }
+  qm31 draw_felt() { auto f = draw_base(); return qm_make(f[0], f[1], f[2], f[3]); }
+  std::vector<qm31> draw_felts(size_t n) {
+    std::vector<qm31> r;
+    while (r.size() < n) {
+      auto f = draw_base();
+      r.push_back(qm_make(f[0], f[1], f[2], f[3]));
+      if (r.size() < n) r.push_back(qm_make(f[4], f[5], f[6], f[7]));
+    }
+    return r;
+  }
+  // H(POW_PREFIX, 0^12, digest, pow_bits) as 8 words (the grind kernel's input).
+  std::array<uint32_t, 8> pow_prefixed(uint32_t pow_bits) const {
+    Hasher s;
+    s.u32(0x12345678u);
+    uint8_t z[12] = {0};
+    s.update(z, 12);
+    s.update(digest.data(), 32);
+    s.u32(pow_bits);
+    Hash h = s.finish();
+    std::array<uint32_t, 8> w;
+    for (int i = 0; i < 8; i++) w[i] = word(h, i);
+    return w;
+  }
+};
+
+inline std::vector<size_t> draw_queries(Channel& ch, uint32_t log_domain, size_t n) {
+  std::vector<size_t> r;
+  uint32_t mask = (uint32_t)((1ull << log_domain) - 1);
+  while (r.size() < n) {
+    auto w = ch.draw_u32s();
+    for (auto x : w) {
+      if (r.size() < n) r.push_back(x & mask);
+    }
+  }
+  return r;
+}
+
+// --------------------------------------------------------------- circle
+inline pt31 index_point(uint32_t k) {
+  pt31 r = {1u, 0u}, cur = {2u, 1268011823u};
+  for (int b = 0; b < 31; b++) {
+    if ((k >> b) & 1u) r = pt_add(r, cur);
+    cur = pt_add(cur, cur);
+  }
+  return r;
+}
+inline ptq to_ptq(pt31 p) { return {qm_from_m31(p.x), qm_from_m31(p.y)}; }
+inline ptq ptq_double(ptq p) { return ptq_add(p, p); }
+inline ptq ptq_rep_double(ptq p, uint32_t n) { for (uint32_t i = 0; i < n; i++) p = ptq_double(p); return p; }
+inline ptq ptq_conj(ptq p) { return {p.x, qm_neg(p.y)}; }
+
+// CanonicCoset(log): coset odds(log) = initial index 2^(30-log), step 2^(31-log).
+inline uint32_t canonic_initial_index(uint32_t log) { return 1u << (31 - (log + 1)); }
+inline uint32_t canonic_step_index(uint32_t log) { return (uint32_t)((1ull << (31 - log)) & 0x7fffffffu); }
+
+// coset_vanishing(CanonicCoset(log).coset, p) for a QM31 point.
+inline qm31 canonic_vanishing(uint32_t log, ptq p) {
+  pt31 init = index_point(canonic_initial_index(log));
+  pt31 half_step = index_point(canonic_step_index(log) >> 1);
+  p = ptq_add(p, to_ptq(pt_conj(init)));
+  p = ptq_add(p, to_ptq(half_step));
+  qm31 x = p.x;
+  for (uint32_t i = 1; i < log; i++) x = qm_double_x(x);
+  return x;
+}
+inline uint32_t canonic_vanishing_m31(uint32_t log, pt31 p) {
+  pt31 init = index_point(canonic_initial_index(log));
+  pt31 half_step = index_point(canonic_step_index(log) >> 1);
+  p = pt_add(pt_add(p, pt_conj(init)), half_step);
+  uint32_t x = p.x;
+  for (uint32_t i = 1; i < log; i++) x = double_x(x);
+  return x;
+}
+
+inline ptq random_point(Channel& ch) {
+  qm31 t = ch.draw_felt();
+  qm31 t2 = qm_sqr(t);
+  qm31 iv = qm_inv(qm_add(t2, qm_one()));
+  return {qm_mul(qm_sub(qm_one(), t2), iv), qm_mul(qm_add(t, t), iv)};
+}
+
+inline size_t bitrev(size_t i, uint32_t log) {
+  size_t r = 0;
+  for (uint32_t b = 0; b < log; b++) r |= ((i >> b) & 1) << (log - 1 - b);
+  return r;
+}
+
+// ------------------------------------------------------------- proof
+struct Decommitment {
+  std::vector<Hash> hash_witness;
+  std::vector<uint32_t> column_witness;
+};
+struct FriLayerProof {
+  std::vector<qm31> fri_witness;
+  Decommitment decommitment;
+  Hash commitment{};
+};
+struct Proof {
+  uint32_t pow_bits = 10, log_blowup = 1, log_last_layer = 0, n_queries = 70, fold_step = 1;
+  std::vector<Hash> commitments;
+  std::vector<std::vector<std::vector<qm31>>> sampled_values;
+  std::vector<Decommitment> decommitments;
+  std::vector<std::vector<uint32_t>> queried_values;
+  uint64_t proof_of_work = 0;
+  FriLayerProof fri_first;
+  std::vector<FriLayerProof> fri_inner;
+  std::vector<qm31> last_layer;
+  uint32_t last_layer_log = 0;
+};
+
+// bincode-1.x style: little-endian fixed width, u64 sequence lengths,
+// Option as a 1-byte tag, hash = 32 raw bytes, QM31 = 4 x u32; field order of
+// CommitmentSchemeProof (config, commitments, sampled_values, decommitments,
+// queried_values, proof_of_work, fri_proof).
+struct Writer {
+  std::string b;
+  void u8(uint8_t v) { b.push_back((char)v); }
+  void u32(uint32_t v) { for (int i = 0; i < 4; i++) b.push_back((char)(v >> (8 * i))); }
+  void u64(uint64_t v) { for (int i = 0; i < 8; i++) b.push_back((char)(v >> (8 * i))); }
+  void hash(const Hash& h) { b.append((const char*)h.data(), 32); }
+  void qm(const qm31& q) { u32(q.x.a); u32(q.x.b); u32(q.y.a); u32(q.y.b); }
+  void dec(const Decommitment& d) {
+    u64(d.hash_witness.size());
+    for (auto& h : d.hash_witness) hash(h);
+    u64(d.column_witness.size());
+    for (auto v : d.column_witness) u32(v);
+  }
+  void layer(const FriLayerProof& l) {
+    u64(l.fri_witness.size());
+    for (auto& q : l.fri_witness) qm(q);
+    dec(l.decommitment);
+    hash(l.commitment);
+  }
+};
+
+inline std::string serialize(const Proof& p) {
+  Writer w;
+  w.u32(p.pow_bits);
+  w.u32(p.log_blowup);
+  w.u32(p.log_last_layer);
+  w.u64(p.n_queries);
+  w.u32(p.fold_step);
+  w.u8(0);  // lifting_log_size: None
+  w.u64(p.commitments.size());
+  for (auto& h : p.commitments) w.hash(h);
+  w.u64(p.sampled_values.size());
+  for (auto& t : p.sampled_values) {
+    w.u64(t.size());
+    for (auto& c : t) {
+      w.u64(c.size());
+      for (auto& q : c) w.qm(q);
+    }
+  }
+  w.u64(p.decommitments.size());
+  for (auto& d : p.decommitments) w.dec(d);
+  w.u64(p.queried_values.size());
+  for (auto& t : p.queried_values) {
+    w.u64(t.size());
+    for (auto v : t) w.u32(v);
+  }
+  w.u64(p.proof_of_work);
+  w.layer(p.fri_first);
+  w.u64(p.fri_inner.size());
+  for (auto& l : p.fri_inner) w.layer(l);
+  w.u64(p.last_layer.size());
+  for (auto& q : p.last_layer) w.qm(q);
+  w.u32(p.last_layer_log);
+  return w.b;
+}
+
+}  // namespace host
+}  // namespace gs

@@ -1,0 +1,30 @@
+// Request/response of the GPU prover driver.
+#pragma once
+#include <string>
+#include "prover.h"
+
+namespace gs {
+namespace prover {
+
+struct ProveRequest {
+  uint32_t air = 0;          // 0 = wide fibonacci, 1 = poseidon2
+  uint32_t log_n = 0;        // trace rows (log)
+  uint32_t n_cols = 100;     // wide fibonacci width
+  uint64_t seed = 0;
+  uint32_t input_mode = 0;   // 0 reference rule, 1 seeded, 2 host inputs
+  const uint32_t* host_inputs = nullptr;  // mode 2: WF a,b columns; Poseidon 16 state columns
+  uint32_t split_log = 1;    // composition split
+  PcsConfig cfg;
+};
+
+struct ProveStats {
+  double constraint_check = 0;  // 1 if the composition sanity check passed
+};
+
+struct Prover;
+struct AirHost;
+int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_bytes, ProveStats* stats);
+int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_bytes, ProveStats* stats);
+
+}  // namespace prover
+}  // namespace gs

@@ -1,0 +1,270 @@
+// prove_ex after the trace commitments: composition commit, OODS samples,
+// DEEP quotients, FRI, proof of work, decommitment and the composition sanity
+// check (crates/stwo/src/prover/mod.rs:50-150, prover/pcs/mod.rs:151-357).
+#include "prover_impl.h"
+#include "prove_api.h"
+
+namespace gs {
+namespace prover {
+
+int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first, std::vector<FriLayerDev>& inner,
+               std::vector<qm31>& last_coeffs);
+void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::vector<bool>& is_witness);
+
+struct ColSamples {
+  std::vector<ptq> points;
+  std::vector<qm31> values;
+};
+
+int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_bytes, ProveStats* stats) {
+  cudaStream_t st = pv.st;
+  const PcsConfig& cfg = pv.cfg;
+  const uint32_t E = air.max_constraint_log();
+  // composition polynomial and its commitment (split into 2^split parts)
+  qm31 random_coeff = pv.ch.draw_felt();
+  uint32_t* comp[4];
+  GS_TRY(pv.composition(air, random_coeff, comp));
+  {
+    std::vector<const uint32_t*> parts;
+    const uint32_t plog = E - split;
+    for (uint32_t t = 0; t < (1u << split); t++)
+      for (int c = 0; c < 4; c++) parts.push_back(comp[c] + ((size_t)t << plog));
+    GS_TRY(pv.commit_coeffs(parts, plog));
+  }
+  ptq oods = host::random_point(pv.ch);
+  const uint32_t lifting = pv.trees.back().max_log();
+  const uint32_t max_ldb = lifting - cfg.log_blowup;
+  // sample points and values per tree / column
+  const size_t n_trees = pv.trees.size();
+  std::vector<std::vector<ColSamples>> samples(n_trees);
+  pt31 step = host::index_point(host::canonic_step_index(max_ldb));
+  for (size_t t = 0; t < n_trees; t++) {
+    Tree& tr = pv.trees[t];
+    samples[t].resize(tr.n_cols);
+    if (tr.n_cols == 0) continue;
+    std::vector<ptq> pts;  // mask points of every column of this tree
+    if (t + 1 == n_trees || t == 1) pts = {oods};
+    else pts = {ptq_add(oods, host::to_ptq(pt_conj(step))), oods};  // interaction: offsets -1, 0
+    for (auto& p : pts) {
+      std::vector<qm31> vals;
+      GS_TRY(pv.sample_tree(tr, host::ptq_rep_double(p, lifting - tr.eval_log), vals));
+      for (uint32_t c = 0; c < tr.n_cols; c++) {
+        samples[t][c].points.push_back(p);
+        samples[t][c].values.push_back(vals[c]);
+      }
+    }
+  }
+  std::vector<qm31> flat;
+  for (auto& tr : samples)
+    for (auto& c : tr) flat.insert(flat.end(), c.values.begin(), c.values.end());
+  pv.ch.mix_felts(flat);
+  // DEEP quotients: per (column size, point) batches of line-coefficient
+  // terms, lifted per point, combined over the lifting domain.
+  qm31 qrc = pv.ch.draw_felt();
+  struct Batch {
+    ptq point;
+    uint32_t log;
+    std::vector<NumEntry> entries;
+    qm31 b_sum = qm_zero(), a_sum = qm_zero();
+  };
+  std::vector<Batch> batches;
+  qm31 pw = qm_one();
+  pt31 lift_step = host::index_point(host::canonic_step_index(lifting));
+  for (size_t t = 0; t < n_trees; t++) {
+    Tree& tr = pv.trees[t];
+    for (uint32_t c = 0; c < tr.n_cols; c++) {
+      auto& cs = samples[t][c];
+      if (cs.points.empty()) continue;
+      std::vector<std::pair<ptq, qm31>> pv_list;
+      if (cs.points.size() == 2) {
+        pt31 period = lift_step;
+        for (uint32_t k = 0; k < tr.eval_log; k++) period = pt_add(period, period);
+        pv_list.push_back({ptq_add(cs.points[1], host::to_ptq(period)), cs.values[1]});
+      }
+      for (size_t k = 0; k < cs.points.size(); k++) pv_list.push_back({cs.points[k], cs.values[k]});
+      for (auto& [p, v] : pv_list) {
+        qm31 a, b, cc;
+        line_coeffs(p, v, pw, a, b, cc);
+        pw = qm_mul(pw, qrc);
+        Batch* bt = nullptr;
+        for (auto& x : batches)
+          if (x.log == tr.eval_log && pt_eq(x.point, p)) bt = &x;
+        if (!bt) {
+          batches.push_back(Batch{p, tr.eval_log, {}, qm_zero(), qm_zero()});
+          bt = &batches.back();
+        }
+        NumEntry e;
+        e.col = tr.eval_col(c);
+        e.c[0] = cc.x.a; e.c[1] = cc.x.b; e.c[2] = cc.y.a; e.c[3] = cc.y.b;
+        bt->entries.push_back(e);
+        bt->b_sum = qm_add(bt->b_sum, b);
+        bt->a_sum = qm_add(bt->a_sum, a);
+      }
+    }
+  }
+  struct PointAcc2 {
+    ptq point;
+    std::vector<std::pair<uint32_t, uint32_t*>> parts;  // (log, planes base of 4 x 2^log)
+    qm31 flt = qm_zero();
+  };
+  std::vector<PointAcc2> per_point;
+  for (auto& bt : batches) {
+    uint32_t* planes = nullptr;
+    GS_TRY(pv.A.alloc_n((size_t)4 << bt.log, &planes));
+    const void* d_entries = nullptr;
+    GS_TRY(pv.ctx.stage_bytes(bt.entries.data(), bt.entries.size() * sizeof(NumEntry), &d_entries));
+    size_t nn = (size_t)1 << bt.log;
+    GS_TRY(accumulate_numerators(st, d_entries, (uint32_t)bt.entries.size(), bt.b_sum, bt.log,
+                                 Planes{{planes, planes + nn, planes + 2 * nn, planes + 3 * nn}}));
+    PointAcc2* pa = nullptr;
+    for (auto& x : per_point)
+      if (pt_eq(x.point, bt.point)) pa = &x;
+    if (!pa) {
+      per_point.push_back(PointAcc2{bt.point, {}, qm_zero()});
+      pa = &per_point.back();
+    }
+    pa->parts.push_back({bt.log, planes});
+    pa->flt = qm_add(pa->flt, bt.a_sum);
+  }
+  std::vector<QuotAcc> qaccs;
+  for (auto& pa : per_point) {
+    std::sort(pa.parts.begin(), pa.parts.end(), [](auto& x, auto& y) { return x.first < y.first; });
+    uint32_t top = pa.parts.back().first;
+    uint32_t* res = pa.parts.back().second;
+    if (pa.parts.size() > 1) {
+      std::vector<LiftCol> lc;
+      for (auto& [lg, base] : pa.parts) {
+        size_t nn = (size_t)1 << lg;
+        lc.push_back(LiftCol{{base, base + nn, base + 2 * nn, base + 3 * nn}, lg, 0});
+      }
+      GS_TRY(pv.A.alloc_n((size_t)4 << top, &res));
+      const void* d = nullptr;
+      GS_TRY(pv.ctx.stage_bytes(lc.data(), lc.size() * sizeof(LiftCol), &d));
+      size_t nn = (size_t)1 << top;
+      GS_TRY(lift_and_accumulate(st, d, (uint32_t)lc.size(), top, Planes{{res, res + nn, res + 2 * nn, res + 3 * nn}}));
+    }
+    size_t nn = (size_t)1 << top;
+    QuotAcc q;
+    q.p[0] = res; q.p[1] = res + nn; q.p[2] = res + 2 * nn; q.p[3] = res + 3 * nn;
+    q.log_size = top;
+    q.pad = 0;
+    q.first_linear = pa.flt;
+    q.prx = pa.point.x.x; q.pix = pa.point.x.y; q.pry = pa.point.y.x; q.piy = pa.point.y.y;
+    qaccs.push_back(q);
+  }
+  uint32_t* quot[4];
+  for (int c = 0; c < 4; c++) GS_TRY(pv.A.alloc_n((size_t)1 << lifting, &quot[c]));
+  {
+    DomainTables dt;
+    GS_TRY(pv.ctx.domain_tables(lifting, &dt));
+    const void* d = nullptr;
+    GS_TRY(pv.ctx.stage_bytes(qaccs.data(), qaccs.size() * sizeof(QuotAcc), &d));
+    GS_TRY(compute_quotients_and_combine(st, d, (uint32_t)qaccs.size(), dt, Planes{{quot[0], quot[1], quot[2], quot[3]}}));
+  }
+  // FRI commit, proof of work
+  FriLayerDev first;
+  std::vector<FriLayerDev> inner;
+  std::vector<qm31> last;
+  GS_TRY(fri_commit(pv, quot, lifting, first, inner, last));
+  auto pre = pv.ch.pow_prefixed(cfg.pow_bits);
+  uint64_t nonce = 0;
+  GS_TRY(grind_blake2s(st, pre.data(), cfg.pow_bits, (uint32_t*)pv.ctx.d_small, &nonce));
+  pv.ch.mix_u64(nonce);
+  // queries
+  auto raw = host::draw_queries(pv.ch, lifting, cfg.n_queries);
+  std::vector<size_t> queries(raw);
+  std::sort(queries.begin(), queries.end());
+  queries.erase(std::unique(queries.begin(), queries.end()), queries.end());
+  // plan all gathers of the decommitment
+  GatherPlan g;
+  struct FriPlan {
+    std::vector<size_t> pos;
+    std::vector<bool> wit;
+    size_t val_base = 0;
+    MerkleDecommitPlan merkle;
+  };
+  auto plan_fri = [&](FriLayerDev& L, const std::vector<size_t>& q, FriPlan& fp) {
+    fri_positions(q, fp.pos, fp.wit);
+    fp.val_base = g.words.size();
+    for (size_t p : fp.pos)
+      for (int c = 0; c < 4; c++) g.add_word(L.planes[c], p);
+    std::vector<const uint32_t*> cols = {L.planes[0], L.planes[1], L.planes[2], L.planes[3]};
+    fp.merkle.plan(g, L.layers, cols, fp.pos);
+  };
+  FriPlan first_plan;
+  plan_fri(first, queries, first_plan);
+  std::vector<FriPlan> inner_plans(inner.size());
+  std::vector<size_t> lq = queries;
+  for (size_t i = 0; i < inner.size(); i++) {
+    std::vector<size_t> f;
+    for (size_t q : lq)
+      if (f.empty() || f.back() != (q >> 1)) f.push_back(q >> 1);
+    lq = f;
+    plan_fri(inner[i], lq, inner_plans[i]);
+  }
+  std::vector<MerkleDecommitPlan> tree_plans(n_trees);
+  for (size_t t = 0; t < n_trees; t++) {
+    Tree& tr = pv.trees[t];
+    if (tr.n_cols == 0) continue;
+    std::vector<size_t> pos = prepare_positions(queries, lifting, tr.max_log());
+    std::vector<const uint32_t*> cols;
+    for (uint32_t c = 0; c < tr.n_cols; c++) cols.push_back(tr.eval_col(c));
+    tree_plans[t].plan(g, tr.layers, cols, pos);
+  }
+  GS_TRY(g.run(pv.ctx, pv.A));
+  // assemble the proof
+  host::Proof P;
+  P.pow_bits = cfg.pow_bits;
+  P.log_blowup = cfg.log_blowup;
+  P.log_last_layer = cfg.log_last_layer;
+  P.n_queries = cfg.n_queries;
+  P.fold_step = cfg.fold_step;
+  auto fri_layer_proof = [&](const FriPlan& fp, const FriLayerDev& L, host::FriLayerProof& out) {
+    for (size_t k = 0; k < fp.pos.size(); k++)
+      if (fp.wit[k]) {
+        const uint32_t* w = g.word_out.data() + fp.val_base + 4 * k;
+        out.fri_witness.push_back(qm_make(w[0], w[1], w[2], w[3]));
+      }
+    std::vector<uint32_t> unused;
+    fp.merkle.assemble(g, unused, out.decommitment);
+    out.commitment = L.root;
+  };
+  fri_layer_proof(first_plan, first, P.fri_first);
+  P.fri_inner.resize(inner.size());
+  for (size_t i = 0; i < inner.size(); i++) fri_layer_proof(inner_plans[i], inner[i], P.fri_inner[i]);
+  P.last_layer = last;
+  P.last_layer_log = 0;
+  while ((1u << P.last_layer_log) < last.size()) P.last_layer_log++;
+  P.proof_of_work = nonce;
+  P.sampled_values.resize(n_trees);
+  P.decommitments.resize(n_trees);
+  P.queried_values.resize(n_trees);
+  for (size_t t = 0; t < n_trees; t++) {
+    Tree& tr = pv.trees[t];
+    P.commitments.push_back(tr.root);
+    for (auto& cs : samples[t]) P.sampled_values[t].push_back(cs.values);
+    if (tr.n_cols) tree_plans[t].assemble(g, P.queried_values[t], P.decommitments[t]);
+  }
+  // sanity check: composition at the OODS point vs constraints from the mask
+  auto& cv = P.sampled_values.back();
+  qm31 total = qm_zero();
+  for (uint32_t t = 0; t < (1u << split); t++) {
+    qm31 e4[4] = {cv[4 * t][0], cv[4 * t + 1][0], cv[4 * t + 2][0], cv[4 * t + 3][0]};
+    qm31 v = from_partial_evals(e4);
+    for (uint32_t b = 0; b < split; b++)
+      if ((t >> b) & 1) v = qm_mul(v, host::ptq_rep_double(oods, E - split + b - 1).x);
+    total = qm_add(total, v);
+  }
+  qm31 dinv = qm_inv(host::canonic_vanishing(max_ldb, oods));
+  qm31 cons = eval_at_point(air, P.sampled_values, random_coeff, dinv);
+  if (stats) stats->constraint_check = qm_eq(total, cons) ? 1.0 : 0.0;
+  *proof_bytes = host::serialize(P);
+  if (!qm_eq(total, cons)) {
+    set_error("constraints not satisfied: composition OODS value differs from the constraints at the mask");
+    return ERR_PROOF;
+  }
+  return OK;
+}
+
+}  // namespace prover
+}  // namespace gs

@@ -1,0 +1,241 @@
+#pragma once
+// GPU prover (see prover.h): commitment trees, composition polynomial,
+// out-of-domain sampling, DEEP quotients, FRI, proof of work, decommitment.
+#include "prover.h"
+#include "host_air.h"
+#include <algorithm>
+
+namespace gs {
+int fold_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itw,
+                    uint32_t tw_log, uint32_t* leaf_out);
+int fold_circle_into_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
+                                const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out);
+int interpolate_columns_to(cudaStream_t st, const uint32_t* const* d_src, uint32_t* const* d_dst, uint32_t n_cols,
+                           uint32_t log_n, const uint32_t* d_itwiddles, uint32_t tw_log);
+
+namespace prover {
+
+using host::Hash;
+
+struct Prover {
+  Context& ctx;
+  cudaStream_t st;
+  PcsConfig cfg;
+  host::Channel ch;
+  Arena A;
+  std::vector<Tree> trees;
+  const uint32_t* tw = nullptr;
+  const uint32_t* itw = nullptr;
+  uint32_t tw_log = 0;
+
+  Prover(Context& c, const PcsConfig& p) : ctx(c), st(c.stream), cfg(p) { A.st = st; }
+
+  int twiddles_for(uint32_t root_log) {
+    GS_TRY(ctx.twiddles(root_log, &tw, &itw));
+    tw_log = root_log;
+    return OK;
+  }
+
+  int table(const std::vector<const uint32_t*>& ptrs, const uint32_t* const** out) {
+    const void* const* d = nullptr;
+    GS_TRY(ctx.stage_ptrs((const void* const*)ptrs.data(), ptrs.size(), &d));
+    *out = (const uint32_t* const*)d;
+    return OK;
+  }
+
+  int merkle(Tree& t) {
+    t.layers.assign(t.eval_log + 1, nullptr);
+    for (uint32_t L = 0; L <= t.eval_log; L++) GS_TRY(A.alloc_n((size_t)8 << L, &t.layers[L]));
+    std::vector<const uint32_t*> cols;
+    for (uint32_t c = 0; c < t.n_cols; c++) cols.push_back(t.eval_col(c));
+    const uint32_t* const* tab = nullptr;
+    GS_TRY(table(cols, &tab));
+    GS_TRY(commit_on_layer(st, t.eval_log, nullptr, tab, t.n_cols, t.layers[t.eval_log]));
+    GS_TRY(commit_node_layers(st, t.eval_log, t.layers.data()));
+    uint32_t w[8];
+    GS_CUDA_TRY(cudaMemcpyAsync(w, t.layers[0], 32, cudaMemcpyDeviceToHost, st));
+    GS_CUDA_TRY(cudaStreamSynchronize(st));
+    t.root = host::hash_from_words(w);
+    return OK;
+  }
+
+  // TreeBuilder::commit on coefficient columns (given by pointer).
+  int commit_coeffs(const std::vector<const uint32_t*>& coeffs, uint32_t coeff_log) {
+    Tree t;
+    t.n_cols = (uint32_t)coeffs.size();
+    t.coeff_log = coeff_log;
+    t.eval_log = coeff_log + cfg.log_blowup;
+    t.coeff_ptrs = coeffs;
+    GS_TRY(table(coeffs, &t.coeff_tab));
+    GS_TRY(A.alloc_n((size_t)t.n_cols << t.eval_log, &t.evals));
+    std::vector<const uint32_t*> dst;
+    for (uint32_t c = 0; c < t.n_cols; c++) dst.push_back(t.eval_col(c));
+    const uint32_t* const* dtab = nullptr;
+    GS_TRY(table(dst, &dtab));
+    GS_TRY(evaluate_columns(st, t.coeff_tab, coeff_log, (uint32_t* const*)dtab, t.n_cols, t.eval_log, tw, tw_log));
+    GS_TRY(merkle(t));
+    ch.mix_root(t.root);
+    trees.push_back(std::move(t));
+    return OK;
+  }
+
+  // TreeBuilder::extend_evals + commit: contiguous evaluations on
+  // CanonicCoset(log) (bit-reversed) are interpolated into new buffers.
+  int commit_evals(const uint32_t* evals, uint32_t n_cols, uint32_t log) {
+    uint32_t* coeffs = nullptr;
+    GS_TRY(A.alloc_n((size_t)n_cols << log, &coeffs));
+    std::vector<const uint32_t*> src, dst;
+    for (uint32_t c = 0; c < n_cols; c++) {
+      src.push_back(evals + ((size_t)c << log));
+      dst.push_back(coeffs + ((size_t)c << log));
+    }
+    const uint32_t* const* stab = nullptr;
+    const uint32_t* const* dtab = nullptr;
+    GS_TRY(table(src, &stab));
+    GS_TRY(table(dst, &dtab));
+    GS_TRY(interpolate_columns_to(st, stab, (uint32_t* const*)dtab, n_cols, log, itw, tw_log));
+    return commit_coeffs(dst, log);
+  }
+
+  int commit_empty() {
+    Tree t;
+    t.root = host::hash_bytes(nullptr, 0);
+    ch.mix_root(t.root);
+    trees.push_back(std::move(t));
+    return OK;
+  }
+
+  // Composition polynomial coefficients (4 planes of 2^eval_log) for the component.
+  int composition(const AirHost& air, qm31 random_coeff, uint32_t* comp[4]) {
+    const uint32_t E = air.max_constraint_log(), T = air.log_n;
+    // trace columns on the evaluation domain
+    std::vector<const uint32_t*> on_domain(trees.size(), nullptr);
+    for (size_t t = 1; t < trees.size(); t++) {
+      Tree& tr = trees[t];
+      if (tr.eval_log == E) { on_domain[t] = tr.evals; continue; }
+      uint32_t* ext = nullptr;
+      GS_TRY(A.alloc_n((size_t)tr.n_cols << E, &ext));
+      std::vector<const uint32_t*> dst;
+      for (uint32_t c = 0; c < tr.n_cols; c++) dst.push_back(ext + ((size_t)c << E));
+      const uint32_t* const* dtab = nullptr;
+      GS_TRY(table(dst, &dtab));
+      GS_TRY(evaluate_columns(st, tr.coeff_tab, tr.coeff_log, (uint32_t* const*)dtab, tr.n_cols, E, tw, tw_log));
+      on_domain[t] = ext;
+    }
+    ConstraintParams prm;
+    memset(&prm, 0, sizeof(prm));
+    const uint32_t nc = air.n_constraints();
+    GS_REQUIRE(nc <= (uint32_t)MAX_CONSTRAINTS, "too many constraints");
+    qm31 pw = qm_one();
+    for (uint32_t k = 0; k < nc; k++) {  // constraint k gets alpha^(nc-1-k)
+      uint32_t* p = prm.powers + 4 * (nc - 1 - k);
+      p[0] = pw.x.a; p[1] = pw.x.b; p[2] = pw.y.a; p[3] = pw.y.b;
+      pw = qm_mul(pw, random_coeff);
+    }
+    // denominators 1 / vanishing(CanonicCoset(T), eval_domain.at(i)), bit-reversed
+    const uint32_t log_expand = E - T;
+    GS_REQUIRE(log_expand <= 3, "constraint blowup above 8");
+    std::vector<uint32_t> dn(1u << log_expand);
+    for (uint32_t i = 0; i < dn.size(); i++) {
+      // eval_domain = CanonicCoset(E).circle_domain(): half coset half_odds(E-1),
+      // point i (i < half) = index 2^(31-(E+1)) + i * 2^(31-(E-1)).
+      uint32_t idx = (uint32_t)(((1ull << (31 - (E + 1))) + (uint64_t)i * (1ull << (31 - (E - 1)))) & 0x7fffffffu);
+      dn[i] = inv(host::canonic_vanishing_m31(T, host::index_point(idx)));
+    }
+    for (uint32_t i = 0; i < dn.size(); i++) prm.denom_inv[host::bitrev(i, log_expand)] = dn[i];
+    for (int c = 0; c < 4; c++) GS_TRY(A.alloc_n((size_t)1 << E, &comp[c]));
+    Planes out{{comp[0], comp[1], comp[2], comp[3]}};
+    if (air.kind == AirKind::WideFibonacci) {
+      GS_TRY(wf_constraints(st, on_domain[1], air.n_cols, E, T, prm, out));
+    } else {
+      qm31 shift = qm_mul_m31(air.claimed_sum, inv((uint32_t)((1ull << T) % P)));
+      GS_TRY(poseidon_constraints(st, on_domain[1], on_domain[2], E, T, prm, air.lookup, shift, out));
+    }
+    // finalize: interpolate the 4 coordinates on CanonicCoset(E)
+    std::vector<const uint32_t*> cp = {comp[0], comp[1], comp[2], comp[3]};
+    const uint32_t* const* ctab = nullptr;
+    GS_TRY(table(cp, &ctab));
+    GS_TRY(interpolate_columns(st, (uint32_t* const*)ctab, 4, E, itw, tw_log));
+    return OK;
+  }
+
+  // Values of every column of tree t at `pt` (already doubled for the tree).
+  int sample_tree(const Tree& t, const ptq& pt, std::vector<qm31>& out) {
+    out.resize(t.n_cols);
+    if (t.n_cols == 0) return OK;
+    size_t need = eval_at_point_scratch_bytes(t.n_cols, t.coeff_log) + 16 * (size_t)t.n_cols;
+    void* scratch = nullptr;
+    GS_TRY(A.alloc(need, &scratch));
+    uint32_t* d_out = (uint32_t*)((uint8_t*)scratch + eval_at_point_scratch_bytes(t.n_cols, t.coeff_log));
+    GS_TRY(batch_eval_at_point(st, t.coeff_tab, t.n_cols, t.coeff_log, pt, d_out, (uint32_t*)scratch));
+    std::vector<uint32_t> h(4 * (size_t)t.n_cols);
+    GS_CUDA_TRY(cudaMemcpyAsync(h.data(), d_out, h.size() * 4, cudaMemcpyDeviceToHost, st));
+    GS_CUDA_TRY(cudaStreamSynchronize(st));
+    for (uint32_t c = 0; c < t.n_cols; c++) out[c] = qm_make(h[4 * c], h[4 * c + 1], h[4 * c + 2], h[4 * c + 3]);
+    return OK;
+  }
+};
+
+struct Sample {
+  ptq point;
+  qm31 value;
+};
+
+// complex_conjugate_line_coeffs (core/constraints.rs:119-134).
+static void line_coeffs(const ptq& p, qm31 v, qm31 alpha, qm31& a, qm31& b, qm31& c) {
+  qm31 aa = qm_sub(qm_conj(v), v);
+  qm31 cc = qm_sub(qm_conj(p.y), p.y);
+  qm31 bb = qm_sub(qm_mul(v, cc), qm_mul(aa, p.y));
+  a = qm_mul(alpha, aa);
+  b = qm_mul(alpha, bb);
+  c = qm_mul(alpha, cc);
+}
+
+static bool pt_eq(const ptq& a, const ptq& b) { return qm_eq(a.x, b.x) && qm_eq(a.y, b.y); }
+
+// Line interpolation of the last FRI layer (prover/line.rs:45-70) on
+// half_odds(log) from bit-reversed values; returns LinePoly coefficients in
+// the reference's internal order.
+static std::vector<qm31> line_interpolate_host(std::vector<qm31> v, uint32_t log) {
+  size_t n = v.size();
+  std::vector<qm31> t(n);
+  for (size_t i = 0; i < n; i++) t[host::bitrev(i, log)] = v[i];
+  v = t;
+  for (uint32_t l = log; l >= 1; l--) {  // domain half_odds(l) = index 2^(29-l) + i * 2^(31-l)
+    size_t size = (size_t)1 << l;
+    for (size_t c = 0; c < n; c += size)
+      for (size_t i = 0; i < size / 2; i++) {
+        uint32_t idx = (uint32_t)(((1ull << (31 - (l + 2))) + (uint64_t)i * (1ull << (31 - l))) & 0x7fffffffu);
+        uint32_t xinv = inv(host::index_point(idx).x);
+        qm31 a = v[c + i], b = v[c + size / 2 + i];
+        v[c + i] = qm_add(a, b);
+        v[c + size / 2 + i] = qm_mul_m31(qm_sub(a, b), xinv);
+      }
+  }
+  uint32_t ninv = inv((uint32_t)n);
+  for (auto& x : v) x = qm_mul_m31(x, ninv);
+  return v;
+}
+
+// FRI layer data kept for decommitment.
+struct FriLayerDev {
+  uint32_t log = 0;
+  uint32_t* planes[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<uint32_t*> layers;
+  Hash root{};
+};
+
+static std::vector<size_t> prepare_positions(const std::vector<size_t>& q, uint32_t lifting, uint32_t tree_log) {
+  std::vector<size_t> r;
+  if (tree_log == 0) return r;
+  for (size_t pos : q) {
+    if (lifting < tree_log) r.push_back(((pos >> 1) << (tree_log - lifting + 1)) + (pos & 1));
+    else r.push_back(((pos >> (lifting - tree_log + 1)) << 1) + (pos & 1));
+  }
+  std::sort(r.begin(), r.end());
+  r.erase(std::unique(r.begin(), r.end()), r.end());
+  return r;
+}
+
+}  // namespace prover
+}  // namespace gs

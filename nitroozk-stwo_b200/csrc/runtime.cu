@@ -33,7 +33,15 @@ int Context::init(void* user_stream) {
   // (the stream torch reports as 0), so work stays ordered with the caller's.
   stream = (cudaStream_t)user_stream;
   own_stream = false;
-  ring_cap = 1 << 20;
+  {
+    // Stream-ordered allocations stay in the device pool between proofs.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t threshold = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+  }
+  ring_cap = 4 << 20;
   ring_off = 0;
   GS_CUDA_TRY(cudaMallocHost((void**)&h_ring, ring_cap));
   GS_CUDA_TRY(cudaMalloc((void**)&d_ring, ring_cap));
@@ -49,7 +57,10 @@ void Context::destroy() {
   scratch = nullptr;
   for (int i = 0; i < 31; i++) {
     if (dom_buf[i]) cudaFree(dom_buf[i]);
+    if (tw_buf[i]) cudaFree(tw_buf[i]);
+    if (itw_buf[i]) cudaFree(itw_buf[i]);
     dom_buf[i] = nullptr;
+    tw_buf[i] = itw_buf[i] = nullptr;
   }
   if (h_ring) cudaFreeHost(h_ring);
   if (d_ring) cudaFree(d_ring);
@@ -110,6 +121,20 @@ int Context::domain_tables(uint32_t lift, DomainTables* out) {
     dom_buf[lift] = buf;
   }
   *out = dom[lift];
+  return OK;
+}
+
+int Context::twiddles(uint32_t root_log, const uint32_t** tw, const uint32_t** itw) {
+  GS_REQUIRE(root_log >= 1 && root_log <= 29, "twiddle root log size out of range");
+  if (!tw_buf[root_log]) {
+    size_t n = (size_t)1 << root_log;
+    GS_CUDA_TRY(cudaMalloc((void**)&tw_buf[root_log], 4 * n));
+    GS_CUDA_TRY(cudaMalloc((void**)&itw_buf[root_log], 4 * n));
+    uint32_t initial = 1u << (31 - (root_log + 2)), step = 1u << (31 - root_log);
+    GS_TRY(precompute_twiddles(stream, initial, step, root_log, tw_buf[root_log], itw_buf[root_log]));
+  }
+  *tw = tw_buf[root_log];
+  *itw = itw_buf[root_log];
   return OK;
 }
 

@@ -91,6 +91,10 @@ struct Context {
   int stage_bytes(const void* host, size_t bytes, const void** out);
   int get_scratch(size_t bytes, void** out);
   int domain_tables(uint32_t lift, DomainTables* out);
+  // device-resident twiddle trees of half_odds(root_log), kept across calls
+  uint32_t* tw_buf[31] = {nullptr};
+  uint32_t* itw_buf[31] = {nullptr};
+  int twiddles(uint32_t root_log, const uint32_t** tw, const uint32_t** itw);
   void destroy();
   // Copies `n` host pointers into device memory usable by kernels launched on
   // `stream` after this call; returns the device address.

@@ -26,6 +26,12 @@ class QuotientAcc(C.Structure):
                 ("sample_point", PointQM31)]
 
 
+class PcsConfig(C.Structure):
+    _fields_ = [("pow_bits", C.c_uint32), ("log_blowup_factor", C.c_uint32),
+                ("log_last_layer_degree_bound", C.c_uint32), ("n_queries", C.c_uint32),
+                ("line_fold_step", C.c_uint32)]
+
+
 class GpuStarkError(RuntimeError):
     pass
 
@@ -60,6 +66,10 @@ _PROTOS = {
     "gs_lift_and_accumulate": [C.c_void_p, VPP, U32P, C.c_uint32, VPP, C.c_uint32],
     "gs_accumulate": [C.c_void_p, VPP, VPP, C.c_size_t],
     "gs_batch_eval_at_point": [C.c_void_p, VPP, C.c_uint32, C.c_uint32, PointQM31, C.c_void_p],
+    "gs_prove_wide_fibonacci": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, U32P,
+                                C.POINTER(PcsConfig), C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
+    "gs_prove_poseidon": [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint32, U32P, C.c_uint32, C.POINTER(PcsConfig),
+                          C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
 }
 _RESTYPE = {"gs_last_error": C.c_char_p, "gs_ctx_stream": C.c_void_p, "gs_launch_count": C.c_ulonglong}
 _OPTIONAL = set()

@@ -1,0 +1,67 @@
+"""Full proofs of the two benchmark components on the GPU prover (C ABI
+gs_prove_wide_fibonacci / gs_prove_poseidon).
+
+Mirrors the reference's example drivers cuda_prove_wide_fibonacci
+(crates/examples/src/wide_fibonacci/mod.rs:140-184) and cuda_prove_poseidon
+(crates/examples/src/poseidon/mod.rs:617-700), which build the trace and call
+the generic prove(); the result is the serialised StarkProof.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .backend import default_context
+
+INPUT_REFERENCE, INPUT_SEEDED, INPUT_HOST = 0, 1, 2
+GS_ERR_PROOF = 5
+
+
+class ConstraintsNotSatisfied(L.GpuStarkError):
+    """prove_ex's composition sanity check failed (ProvingError::ConstraintsNotSatisfied)."""
+
+
+def pcs_config(pow_bits=10, log_blowup=1, log_last_layer=0, n_queries=70, line_fold_step=1):
+    """PcsConfig { pow_bits, FriConfig::new(log_last_layer, log_blowup, n_queries, line_fold_step) }."""
+    return L.PcsConfig(pow_bits, log_blowup, log_last_layer, n_queries, line_fold_step)
+
+
+def _run(fn, args, ctx, capacity):
+    n = C.c_size_t()
+    buf = (C.c_uint8 * capacity)()
+    st = fn(*args, C.cast(buf, C.c_void_p), capacity, C.byref(n))
+    if st == 1 and n.value > capacity:  # retry with the exact size
+        buf = (C.c_uint8 * n.value)()
+        st = fn(*args, C.cast(buf, C.c_void_p), n.value, C.byref(n))
+    if st == GS_ERR_PROOF:
+        raise ConstraintsNotSatisfied(L.lib().gs_last_error().decode())
+    L.check(st, fn.__name__)
+    return bytes(buf[: n.value])
+
+
+def _inputs(host_inputs):
+    if host_inputs is None:
+        return None, None
+    a = np.ascontiguousarray(host_inputs, dtype=np.uint32)
+    return a, a.ctypes.data_as(L.U32P)
+
+
+def prove_wide_fibonacci(log_n_rows, n_columns=100, seed=0, input_mode=INPUT_REFERENCE, host_inputs=None,
+                         config=None, ctx=None, capacity=1 << 24):
+    """host_inputs (INPUT_HOST): array (2, 2^log_n_rows) of columns 0 and 1."""
+    ctx = ctx or default_context()
+    keep, ptr = _inputs(host_inputs)
+    cfg = config or pcs_config()
+    return _run(L.lib().gs_prove_wide_fibonacci,
+                (ctx.handle, log_n_rows, n_columns, seed, input_mode, ptr, C.byref(cfg)), ctx, capacity)
+
+
+def prove_poseidon(log_n_instances, seed=0, input_mode=INPUT_REFERENCE, host_inputs=None, composition_log_split=2,
+                   config=None, ctx=None, capacity=1 << 24):
+    """host_inputs (INPUT_HOST): array (16, 2^log_n_instances) of initial states."""
+    ctx = ctx or default_context()
+    keep, ptr = _inputs(host_inputs)
+    cfg = config or pcs_config()
+    return _run(L.lib().gs_prove_poseidon,
+                (ctx.handle, log_n_instances, seed, input_mode, ptr, composition_log_split, C.byref(cfg)), ctx,
+                capacity)

@@ -72,10 +72,9 @@ def _declare(L):
     f("oracle_compute_quotients_and_combine", None, C.c_uint32, PP, U32P, U32P, U32P, C.c_uint32, PP)
     f("oracle_lift_and_accumulate", None, C.c_uint32, PP, U32P, PP)
     f("oracle_eval_at_point", None, U32P, C.c_uint32, U32P, U32P)
-    if hasattr(L, "oracle_prove"):
-        f("oracle_prove", C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32,
-          C.c_uint32, C.c_uint32, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t))
-        f("oracle_verify", C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_size_t)
+    f("oracle_prove", C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32,
+      C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t))
+    f("oracle_seeded_m31", C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64)
 
 
 # ---------------------------------------------------------------- helpers
@@ -271,3 +270,34 @@ def eval_at_point(coeffs, point8):
     out = np.zeros(4, np.uint32)
     lib().oracle_eval_at_point(cp, int(len(c)).bit_length() - 1, ptp, out.ctypes.data_as(U32P))
     return out
+
+
+class ConstraintsNotSatisfied(RuntimeError):
+    """prove_ex's composition sanity check failed (the reference's ProvingError)."""
+
+
+def default_split(air):
+    """Composition split: 1 for wide fibonacci (the reference's), 2 = LOG_EXPAND for poseidon."""
+    return 1 if air == "wide_fibonacci" else 2
+
+
+def prove(air, log_n, n_cols=100, seed=0, input_mode=0, pow_bits=10, n_queries=70, log_blowup=1, split_log=None,
+          log_last_layer=0):
+    """Full proof bytes from the CPU restatement; air: 'wide_fibonacci' | 'poseidon'."""
+    if split_log is None:
+        split_log = default_split(air)
+    L = lib()
+    cap = 1 << 26
+    buf = (C.c_uint8 * cap)()
+    n = C.c_size_t()
+    st = L.oracle_prove(0 if air == "wide_fibonacci" else 1, log_n, n_cols, seed, input_mode, pow_bits, n_queries,
+                        log_blowup, log_last_layer, split_log, C.cast(buf, C.c_void_p), cap, C.byref(n))
+    if st == 1:
+        raise ConstraintsNotSatisfied("composition OODS value does not match the constraints")
+    if st != 0:
+        raise RuntimeError(f"oracle prove failed with status {st}")
+    return bytes(buf[: n.value])
+
+
+def seeded_m31(seed, col, row):
+    return lib().oracle_seeded_m31(seed, col, row)

@@ -1,0 +1,72 @@
+"""End-to-end parity: the GPU prover's serialised proof is byte-identical to
+the CPU oracle's for the same AIR, inputs and PcsConfig."""
+import numpy as np
+import pytest
+
+import pyoracle as O
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def G():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from gpustark import prove
+    return prove
+
+
+@pytest.mark.parametrize("log_n,n_cols,mode", [(4, 8, 0), (6, 16, 1), (8, 100, 0), (10, 100, 1), (12, 37, 1)])
+def test_wide_fibonacci_proof_bytes(G, log_n, n_cols, mode):
+    got = G.prove_wide_fibonacci(log_n, n_cols, seed=11, input_mode=mode)
+    exp = O.prove("wide_fibonacci", log_n, n_cols=n_cols, seed=11, input_mode=mode)
+    assert got == exp
+
+
+@pytest.mark.parametrize("log_n,mode", [(4, 0), (6, 0), (8, 1), (10, 0), (12, 1)])
+def test_poseidon_proof_bytes(G, log_n, mode):
+    got = G.prove_poseidon(log_n, seed=5, input_mode=mode)
+    exp = O.prove("poseidon", log_n, seed=5, input_mode=mode)
+    assert got == exp
+
+
+def test_poseidon_reference_split_is_rejected_like_the_reference(G):
+    """With the reference's fixed composition split the lifted protocol cannot
+    prove a LOG_EXPAND = 2 component: both provers report ConstraintsNotSatisfied."""
+    with pytest.raises(G.ConstraintsNotSatisfied):
+        G.prove_poseidon(6, composition_log_split=1)
+    with pytest.raises(O.ConstraintsNotSatisfied):
+        O.prove("poseidon", 6, split_log=1)
+
+
+@pytest.mark.parametrize("blowup,queries,pow_bits,last", [(2, 20, 4, 0), (1, 3, 10, 0), (3, 9, 0, 1)])
+def test_pcs_configs(G, blowup, queries, pow_bits, last):
+    cfg = G.pcs_config(pow_bits=pow_bits, log_blowup=blowup, n_queries=queries, log_last_layer=last)
+    got = G.prove_wide_fibonacci(9, 20, seed=3, input_mode=1, config=cfg)
+    exp = O.prove("wide_fibonacci", 9, n_cols=20, seed=3, input_mode=1, pow_bits=pow_bits, n_queries=queries,
+                  log_blowup=blowup, log_last_layer=last)
+    assert got == exp
+
+
+def test_host_inputs_match_seeded(G):
+    log_n = 8
+    st = np.array([[O.seeded_m31(9, i, r) for r in range(1 << log_n)] for i in range(16)], np.uint32)
+    got = G.prove_poseidon(log_n, input_mode=G.INPUT_HOST, host_inputs=st)
+    assert got == G.prove_poseidon(log_n, seed=9, input_mode=G.INPUT_SEEDED)
+    ab = st[:2]
+    assert G.prove_wide_fibonacci(log_n, 30, input_mode=G.INPUT_HOST, host_inputs=ab) == \
+        G.prove_wide_fibonacci(log_n, 30, seed=9, input_mode=G.INPUT_SEEDED)
+
+
+@pytest.mark.slow
+def test_wide_fibonacci_config_size(G):
+    """Wide-Fibonacci 2^16 rows x 100 columns, seeded inputs (the benchmark configuration)."""
+    assert G.prove_wide_fibonacci(16, 100, seed=0, input_mode=1) == \
+        O.prove("wide_fibonacci", 16, n_cols=100, seed=0, input_mode=1)
+
+
+@pytest.mark.slow
+def test_poseidon_config_size(G):
+    """Poseidon2 2^18 instances, seeded inputs (the benchmark configuration)."""
+    assert G.prove_poseidon(18, seed=0, input_mode=1) == O.prove("poseidon", 18, seed=0, input_mode=1)
