@@ -345,31 +345,221 @@ def run_kernels(args, world, rank, local):
     return out
 
 
+# ------------------------------------------------------------ full proofs
+PROOF_SIZES = {"poseidon": 18, "wide_fibonacci": 16}
+
+
+def proof_metric(workload):
+    if workload == "poseidon":
+        return "Poseidon2 2^18 proof ms"
+    return "Wide-Fibonacci 2^16x100 proof ms"
+
+
+def proof_config(workload, log_n):
+    base = {"pcs": "pow_bits=10, FriConfig(log_last_layer=0, log_blowup=1, n_queries=70, fold_step=1)",
+            "channel": "Blake2s", "inputs": "seeded uniform M31 states (mode 1)",
+            "l2": "each proof streams >1 GB through HBM (inputs larger than L2)"}
+    if workload == "poseidon":
+        base.update({"workload": "Poseidon2 AIR full proof, 2^%d instances (one per row), width 16, 8 full + 14 "
+                                 "partial rounds, logup interaction, composition split 4" % log_n})
+    else:
+        base.update({"workload": "Wide-Fibonacci AIR full proof, 2^%d rows x 100 columns" % log_n})
+    return base
+
+
+def cpu_proof_sample(workload, threads, log_target):
+    """Oracle (CPU restatement, all host threads) on a bounded sample; the
+    time is scaled to the target size by n log n. Returns (ms, desc)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    O.set_threads(threads)
+    log_s = log_target - 2
+    air = "poseidon" if workload == "poseidon" else "wide_fibonacci"
+    t0 = time.perf_counter()
+    O.prove(air, log_s, n_cols=100, seed=0, input_mode=1)
+    dt = time.perf_counter() - t0
+    scale = (2 ** log_target * log_target) / (2 ** log_s * log_s)
+    return 1e3 * dt * scale, "oracle %s proof at 2^%d (%.2f s), scaled x%.2f (n log n) to 2^%d" % (
+        air, log_s, dt, scale, log_target)
+
+
+def run_proof(args, world, rank, local):
+    import torch
+    from gpustark import lib as gslib
+    from gpustark import prove as G
+    from gpustark.backend import Context
+    torch.cuda.set_device(local)
+    wl = args.workload
+    log_n = args.log_n or PROOF_SIZES[wl]
+    ctx = Context(torch.cuda.current_stream())
+    stream = torch.cuda.current_stream()
+
+    def one(mode=G.INPUT_SEEDED, host=None):
+        if wl == "poseidon":
+            return G.prove_poseidon(log_n, seed=rank, input_mode=mode, host_inputs=host, ctx=ctx)
+        return G.prove_wide_fibonacci(log_n, 100, seed=rank, input_mode=mode, host_inputs=host, ctx=ctx)
+
+    for _ in range(args.warmup):
+        proof = one()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = gslib().gs_launch_count()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    lat = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        proof = one()
+        lat.append(1e3 * (time.perf_counter() - t))
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    launches = (gslib().gs_launch_count() - l0) // max(args.steps, 1)
+    clk = clocks.stop()
+    total_ms = max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
+    ms_per_step = total_ms / args.steps
+    value = total_ms / (args.steps * world)     # whole-job ms per proof
+    # end to end through the C ABI with host inputs: H2D of the input columns
+    # and D2H of the proof bytes inside the timed region
+    n = 1 << log_n
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    rng = np.random.default_rng(rank)
+    host_cols = 16 if wl == "poseidon" else 2
+    host = rng.integers(0, P, (host_cols, n), dtype=np.int64).astype(np.uint32)
+    host_t = torch.from_numpy(host.view(np.int32)).pin_memory()
+    host_np = host_t.numpy().view(np.uint32)
+    one(G.INPUT_HOST, host_np)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(args.steps, 5))
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        p2 = one(G.INPUT_HOST, host_np)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, "cuda") / (e2e_steps * world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        ms, desc = cpu_proof_sample(wl, threads, log_n)
+        cpu = {"value": round(ms, 1), "unit": "ms", "cores": threads, "kind": "port", "sample": desc}
+    out = {
+        "metric": proof_metric(wl) if log_n == PROOF_SIZES[wl] else proof_metric(wl).replace(
+            str(PROOF_SIZES[wl]), str(log_n)),
+        "value": round(value, 3), "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_per_step, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 (M31/QM31 integer arithmetic)", "data": "synthetic: seeded uniform M31",
+        "config": dict(proof_config(wl, log_n), parallelism="independent proofs x%d" % world),
+        "proofs_per_s": round(1e3 / value, 2), "proof_bytes": len(proof),
+        "latency_ms": {"p50": round(statistics.median(lat), 3), "max": round(max(lat), 3)},
+        "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(host.nbytes),
+                "d2h_bytes_per_step": len(p2)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if cpu:
+        out["cpu_baseline"] = cpu
+    rl = proof_roofline(args, log_n, wl, ctx)
+    if rl:
+        out["roofline"] = rl
+    return out
+
+
+def proof_roofline(args, log_n, wl, ctx):
+    """Roofline of the proof's dominant kernel, timed live on the proof's shape:
+    the low-degree extension of the committed trace (evaluate_polynomials,
+    CanonicCoset(log_n) coefficients -> 2^(log_n + 2) for Poseidon's constraint
+    domain, 2^(log_n + 1) for Wide-Fibonacci)."""
+    import torch
+    from gpustark.backend import GpuBackend as B
+    hbm_peak, peak_kind = load_peaks()
+    cols = 162 if wl == "poseidon" else 100
+    ext = 2 if wl == "poseidon" else 1
+    target = log_n + ext
+    tw = B.precompute_twiddles(target - 1, ctx=ctx)
+    src = torch.randint(0, P, (cols, 1 << log_n), dtype=torch.int32, device="cuda")
+    dst = torch.empty((cols, 1 << target), dtype=torch.int32, device="cuda")
+    srcs = [src[i] for i in range(cols)]
+    dsts = [dst[i] for i in range(cols)]
+    for _ in range(3):
+        B.evaluate_polynomials(srcs, target, tw, out=dsts, ctx=ctx)
+    st = torch.cuda.current_stream()
+    times = []
+    for _ in range(5):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        B.evaluate_polynomials(srcs, target, tw, out=dsts, ctx=ctx)
+        b.record(st)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    ms = statistics.mean(times)
+    alg = 4 * cols * ((1 << log_n) + (1 << target))   # LDE n -> n+b: 4(2^n + 2^(n+b)) bytes per column
+    achieved = alg / (ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("lde_%s_%d" % (wl, log_n))
+        except Exception:
+            traffic = None
+    return {"kernel": "fft_pass_kernel (LDE %d cols 2^%d -> 2^%d)" % (cols, log_n, target), "bound": "hbm",
+            "achieved": round(achieved, 1), "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "algorithmic_bytes": alg,
+            "avg_ms": round(ms, 4)}
+
+
 def run_reference(args, world, rank):
-    """The reference arm: the CPU implementation of the path (the oracle port,
-    the reference's Rust prover cannot be built here) on all host threads."""
+    """The reference arm: the CPU implementation of the path on the host cores.
+    The reference's Rust prover cannot be built here (no Rust toolchain), so
+    this times the oracle port (a C++ restatement of the reference CPU
+    backend and prover) with all host threads, on the same metric."""
     if rank != 0:
         return None
     threads = os.cpu_count() or 1
-    vals = []
-    for _ in range(args.warmup):
-        cpu_sweep_sample(threads)
-    t_all = 0.0
-    desc = ""
-    for _ in range(args.steps):
-        gbs, secs, desc = cpu_sweep_sample(threads)
-        vals.append(gbs)
-        t_all += secs
+    if args.workload == "kernels":
+        vals, t_all, desc = [], 0.0, ""
+        for _ in range(args.warmup):
+            cpu_sweep_sample(threads)
+        for _ in range(args.steps):
+            gbs, secs, desc = cpu_sweep_sample(threads)
+            vals.append(gbs)
+            t_all += secs
+        v = statistics.mean(vals)
+        return {
+            "impl": "reference",
+            "metric": "FFT/Merkle HBM GB/s (kernel sweep: circle FFT 2^16..2^26, Merkle 64x2^20, fold 2^22)",
+            "value": round(v, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * t_all / max(args.steps, 1), 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic: seeded uniform M31",
+            "config": {"workload": "kernel sweep (configs[1]), bounded CPU sample", "parallelism": "cpu threads"},
+            "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+    log_n = args.log_n or PROOF_SIZES[args.workload]
+    for _ in range(min(args.warmup, 1)):
+        cpu_proof_sample(args.workload, threads, log_n)
+    vals, desc = [], ""
+    steps = max(1, min(args.steps, 3))
+    for _ in range(steps):
+        ms, desc = cpu_proof_sample(args.workload, threads, log_n)
+        vals.append(ms)
     v = statistics.mean(vals)
     return {
-        "impl": "reference",
-        "metric": "FFT/Merkle HBM GB/s (kernel sweep: circle FFT 2^16..2^26, Merkle 64x2^20, fold 2^22)",
-        "value": round(v, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(1e3 * t_all / max(args.steps, 1), 2), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic: seeded uniform M31",
-        "config": {"workload": "kernel sweep (configs[1]), bounded CPU sample", "parallelism": "cpu threads"},
-        "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc},
-        "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "impl": "reference", "metric": proof_metric(args.workload), "value": round(v, 1), "unit": "ms",
+        "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": round(v, 1),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32 (M31/QM31 integer arithmetic)", "data": "synthetic: seeded uniform M31",
+        "config": dict(proof_config(args.workload, log_n), parallelism="cpu threads"),
+        "cpu_baseline": {"value": round(v, 1), "unit": "ms", "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
@@ -410,7 +600,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpustark", choices=["gpustark", "reference"])
-    ap.add_argument("--workload", default="kernels", choices=["kernels"])
+    ap.add_argument("--workload", default="poseidon", choices=["poseidon", "wide_fibonacci", "kernels"])
+    ap.add_argument("--log-n", type=int, default=0, help="override the proof size (log instances / rows)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", default=None,
                     help="profiling case: fft:<log>, merkle:<log>:<cols>, fold:<log> (one op, no JSON contract)")
     args = ap.parse_args()
@@ -422,7 +614,10 @@ def main():
         out = run_reference(args, world, rank)
     else:
         world, rank, local = dist_setup(args, "nccl")
-        out = run_kernels(args, world, rank, local)
+        if args.workload == "kernels":
+            out = run_kernels(args, world, rank, local)
+        else:
+            out = run_proof(args, world, rank, local)
     if rank == 0 and out is not None:
         print(json.dumps(out), flush=True)
     if world > 1:

@@ -11,6 +11,7 @@ struct gs_ctx {
 using namespace gs;
 
 namespace gs {
+void fft_set_columns_aligned(bool aligned);
 int fold_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itw,
                     uint32_t tw_log, uint32_t* leaf_out);
 int fold_circle_into_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
@@ -132,6 +133,9 @@ int gs_interpolate_columns(gs_ctx* ctx, uint32_t* const* cols, uint32_t n_cols, 
   GS_REQUIRE(cols != nullptr, "null column list");
   for (uint32_t i = 0; i < n_cols; i++) GS_REQUIRE(cols[i] != nullptr, "null column");
   GS_REQUIRE(log_size <= 2 || itwiddles != nullptr, "null itwiddles");
+  bool aligned = true;
+  for (uint32_t i = 0; i < n_cols; i++) aligned = aligned && (((uintptr_t)cols[i] & 15) == 0);
+  fft_set_columns_aligned(aligned);
   const void* const* d = nullptr;
   GS_TRY(ctx->c.stage_ptrs((const void* const*)cols, n_cols, &d));
   return interpolate_columns(ctx->c.stream, (uint32_t* const*)d, n_cols, log_size, itwiddles, twiddles_log_size);
@@ -144,6 +148,10 @@ int gs_evaluate_columns(gs_ctx* ctx, const uint32_t* const* coeffs, uint32_t coe
   GS_REQUIRE(coeffs != nullptr && evals != nullptr, "null column list");
   for (uint32_t i = 0; i < n_cols; i++) GS_REQUIRE(coeffs[i] && evals[i] && coeffs[i] != evals[i], "bad column pair");
   GS_REQUIRE(log_size <= 2 || twiddles != nullptr, "null twiddles");
+  bool aligned = true;
+  for (uint32_t i = 0; i < n_cols; i++)
+    aligned = aligned && (((uintptr_t)coeffs[i] & 15) == 0) && (((uintptr_t)evals[i] & 15) == 0);
+  fft_set_columns_aligned(aligned);
   const void* const* ds = nullptr;
   const void* const* dd = nullptr;
   GS_TRY(ctx->c.stage_ptrs((const void* const*)coeffs, n_cols, &ds));

@@ -43,6 +43,7 @@ struct FftPass {
   uint32_t tw_len;      // twiddle buffer length
   uint32_t scale;       // multiply by scale on the final store when has_scale
   uint32_t has_scale;
+  uint32_t vec_ok;      // all column pointers 16-byte aligned: vector loads/stores allowed
 };
 
 __device__ __forceinline__ uint32_t circle_twiddle(const uint32_t* __restrict__ tw, uint32_t tw_len, uint32_t n,
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const uint32_t* const* __
     }
     const uint32_t ebase = ((ltid >> s0) << (s0 + R)) | (ltid & ((1u << s0) - 1u));
     if (k == 0) {
-      if (s0 == 0 && a.c == 0 && a.src_mask == 0xffffffffu && NQ >= 4) {
+      if (a.vec_ok && s0 == 0 && a.c == 0 && a.src_mask == 0xffffffffu && NQ >= 4) {
         const uint4* p = reinterpret_cast<const uint4*>(src + (basev | ebase));
 #pragma unroll
         for (int g = 0; g < NQ / 4; g++) {
@@ -187,7 +188,7 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const uint32_t* const* __
 #pragma unroll
         for (int q = 0; q < NQ; q++) x[q] = mul(x[q], a.scale);
       }
-      if (s0 == 0 && a.c == 0 && NQ >= 4) {
+      if (a.vec_ok && s0 == 0 && a.c == 0 && NQ >= 4) {
         uint4* p = reinterpret_cast<uint4*>(dst + (basev | ebase));
 #pragma unroll
         for (int g = 0; g < NQ / 4; g++) p[g] = make_uint4(x[4 * g], x[4 * g + 1], x[4 * g + 2], x[4 * g + 3]);
@@ -324,6 +325,11 @@ static void launch_pass(cudaStream_t st, dim3 grid, uint32_t threads, size_t sme
   note_launch();
 }
 
+// Column pointers of the current call are 16-byte aligned (checked by the
+// callers that know them on the host; the device tables are opaque here).
+static thread_local bool g_cols_aligned = true;
+void fft_set_columns_aligned(bool aligned) { g_cols_aligned = aligned; }
+
 template <bool INV>
 static int run_passes(cudaStream_t st, const uint32_t* const* src, uint32_t* const* dst, uint32_t n_cols, uint32_t n,
                       uint32_t layers, uint32_t src_mask, const uint32_t* tw, uint32_t tw_len) {
@@ -343,6 +349,7 @@ static int run_passes(cudaStream_t st, const uint32_t* const* src, uint32_t* con
     a.tw_len = tw_len;
     a.has_scale = (INV && p + 1 == parts.size()) ? 1u : 0u;
     a.scale = a.has_scale ? inv(1u << n) : 1u;
+    a.vec_ok = g_cols_aligned ? 1u : 0u;
     const uint32_t tpt_log = a.t - R;
     const uint32_t tiles_log = n - a.t;
     uint32_t tile_shift = tpt_log < 7 ? 7 - tpt_log : 0;

@@ -34,6 +34,7 @@ int gather_words(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t*
 
 int gather_hashes(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out) {
   if (n == 0) return OK;
+  GS_REQUIRE(((uintptr_t)d_out & 15) == 0, "hash gather output must be 16-byte aligned");
   unsigned blocks = (unsigned)((n + 255) / 256);
   gather_hashes_kernel<<<blocks, 256, 0, st>>>(d_items, n, d_out);
   note_launch();

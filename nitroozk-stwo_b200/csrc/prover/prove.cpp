@@ -3,6 +3,7 @@
 #include "prove_api.h"
 
 namespace gs {
+void fft_set_columns_aligned(bool aligned);
 namespace prover {
 
 // FRI commit (prover/fri.rs:99-199) on the combined quotient planes (2^lifting).
@@ -126,6 +127,8 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
   GS_REQUIRE(comp_tree >= cfg.log_last_layer + cfg.log_blowup + 1, "trace too small for the FRI last layer");
   uint32_t root = std::max({air.log_n + cfg.log_blowup, E, comp_tree}) - 1;
   GS_TRY(pv.twiddles_for(root));
+  // every column buffer of the prover starts at a multiple of 4 words
+  fft_set_columns_aligned(true);
   // preprocessed tree (empty)
   GS_TRY(pv.commit_empty());
   // trace

@@ -72,19 +72,22 @@ struct GatherPlan {
     size_t nw = words.size(), nh = hashes.size();
     GatherItem *d_items = nullptr;
     uint32_t* d_out = nullptr;
+    // hashes are written as 16-byte vectors: their region starts at a
+    // multiple of 4 words
+    const size_t hbase = (nw + 3) & ~(size_t)3;
     GS_TRY(A.alloc_n(nw + nh + 1, &d_items));
-    GS_TRY(A.alloc_n(nw + 8 * nh + 1, &d_out));
+    GS_TRY(A.alloc_n(hbase + 8 * nh + 4, &d_out));
     std::vector<GatherItem> all(words);
     all.insert(all.end(), hashes.begin(), hashes.end());
     if (!all.empty())
       GS_CUDA_TRY(cudaMemcpyAsync(d_items, all.data(), all.size() * sizeof(GatherItem), cudaMemcpyHostToDevice, st));
     GS_TRY(gather_words(st, d_items, nw, d_out));
-    GS_TRY(gather_hashes(st, d_items + nw, nh, d_out + nw));
-    std::vector<uint32_t> out(nw + 8 * nh);
+    GS_TRY(gather_hashes(st, d_items + nw, nh, d_out + hbase));
+    std::vector<uint32_t> out(hbase + 8 * nh);
     if (!out.empty()) GS_CUDA_TRY(cudaMemcpyAsync(out.data(), d_out, out.size() * 4, cudaMemcpyDeviceToHost, st));
     GS_CUDA_TRY(cudaStreamSynchronize(st));
     word_out.assign(out.begin(), out.begin() + nw);
-    hash_out.assign(out.begin() + nw, out.end());
+    hash_out.assign(out.begin() + hbase, out.end());
     return OK;
   }
   host::Hash hash(size_t slot) const { return host::hash_from_words(hash_out.data() + 8 * slot); }
