@@ -516,6 +516,99 @@ def proof_roofline(args, log_n, wl, ctx):
             "avg_ms": round(ms, 4)}
 
 
+# ------------------------------------------------------------ batched / served
+def job_mix(kind, seed):
+    """configs 4/5 job lists: (air, log_n, n_cols, seed)."""
+    rng = np.random.default_rng(seed)
+    if kind == "batched":   # 64 independent Wide-Fibonacci proofs, rows 2^10..2^16, 16..100 columns
+        return [(0, int(rng.integers(10, 17)), int(rng.integers(16, 101)), i) for i in range(64)]
+    jobs = []               # served: Poseidon2 2^12..2^18 and Wide-Fibonacci 2^12..2^20 (100 columns)
+    for i in range(48):
+        if rng.random() < 0.5:
+            jobs.append((1, int(rng.integers(12, 19)), 0, i))
+        else:
+            jobs.append((0, int(rng.integers(12, 21)), 100, i))
+    return jobs
+
+
+def run_serving(args, world, rank, local):
+    import torch
+    from gpustark import prove as G
+    from gpustark import serve as S
+    from gpustark.backend import Context
+    torch.cuda.set_device(local)
+    ctx = Context(torch.cuda.current_stream())
+    jobs = job_mix(args.workload, 1 + rank)
+
+    def single(a, n, c, sd):
+        if a == 0:
+            return G.prove_wide_fibonacci(n, c, seed=sd, input_mode=G.INPUT_SEEDED, ctx=ctx)
+        return G.prove_poseidon(n, seed=sd, input_mode=G.INPUT_SEEDED, ctx=ctx)
+
+    for j in jobs[:4]:
+        single(*j)
+    torch.cuda.synchronize()
+    # sequential: one proof at a time on one stream
+    barrier(world)
+    t0 = time.perf_counter()
+    seq_lat = []
+    seq_proofs = []
+    for j in jobs:
+        ts = time.perf_counter()
+        seq_proofs.append(single(*j))
+        seq_lat.append(1e3 * (time.perf_counter() - ts))
+    seq_s = time.perf_counter() - t0
+    workers = args.workers
+    arrivals = None
+    with S.ProofServer(workers, 96 << 30) as sv:
+        for j in jobs[:workers]:          # warm the workers' contexts
+            sv.wait(sv.submit(j[0], j[1], j[2] or 100, j[3]))
+        barrier(world)
+        t0 = time.perf_counter()
+        if args.workload == "batched":
+            ids = [sv.submit(a, n, c or 100, sd) for a, n, c, sd in jobs]
+        else:
+            # Poisson arrivals at `load` x the sequential proof rate (seeded)
+            rate = args.load * len(jobs) / seq_s
+            gaps = np.random.default_rng(7 + rank).exponential(1.0 / rate, len(jobs))
+            arrivals = np.cumsum(gaps)
+            ids = []
+            for (a, n, c, sd), at in zip(jobs, arrivals):
+                now = time.perf_counter() - t0
+                if at > now:
+                    time.sleep(at - now)
+                ids.append(sv.submit(a, n, c or 100, sd))
+        res = [sv.wait(i) for i in ids]
+        srv_s = time.perf_counter() - t0
+    identical = all(p == q for (p, _), q in zip(res, seq_proofs))
+    lat = sorted(l for _, l in res)
+    srv_s = max_over_ranks(srv_s, world, "cuda")
+    seq_s = max_over_ranks(seq_s, world, "cuda")
+    pps = world * len(jobs) / srv_s
+    seq_pps = world * len(jobs) / seq_s
+    q = lambda v, f: float(np.percentile(np.asarray(v), f))
+    out = {
+        "metric": ("batched vs sequential proofs/s (64 Wide-Fibonacci proofs, 2^10..2^16 rows)"
+                   if args.workload == "batched" else
+                   "served proofs/s with p50/p99 latency (Poisson mix of Poseidon2 2^12..2^18, WF 2^12..2^20)"),
+        "value": round(pps, 2), "unit": "proofs/s", "n_gpus": world, "steps": 1, "warmup": 1,
+        "ms_per_step": round(1e3 * srv_s, 2), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32 (M31/QM31 integer arithmetic)", "data": "synthetic: seeded uniform M31",
+        "config": {"workload": "%s: %d jobs, %d workers (one CUDA stream each), admission by HBM footprint"
+                               % (args.workload, len(jobs), workers),
+                   "parallelism": "replicas x%d" % world},
+        "sequential_proofs_per_s": round(seq_pps, 2), "speedup_vs_sequential": round(pps / seq_pps, 2),
+        "latency_ms": {"p50": round(q(lat, 50), 2), "p99": round(q(lat, 99), 2)},
+        "sequential_latency_ms": {"p50": round(q(seq_lat, 50), 2), "p99": round(q(seq_lat, 99), 2)},
+        "proofs_identical_to_sequential": identical,
+        "e2e": {"value": round(pps, 2), "unit": "proofs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(sum(len(p) for p, _ in res))},
+    }
+    if arrivals is not None:
+        out["arrival_rate_per_s"] = round(args.load * len(jobs) / seq_s, 2)
+    return out
+
+
 def run_reference(args, world, rank):
     """The reference arm: the CPU implementation of the path on the host cores.
     The reference's Rust prover cannot be built here (no Rust toolchain), so
@@ -600,7 +693,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpustark", choices=["gpustark", "reference"])
-    ap.add_argument("--workload", default="poseidon", choices=["poseidon", "wide_fibonacci", "kernels"])
+    ap.add_argument("--workload", default="poseidon",
+                    choices=["poseidon", "wide_fibonacci", "kernels", "batched", "served"])
+    ap.add_argument("--workers", type=int, default=8, help="server workers (batched / served)")
+    ap.add_argument("--load", type=float, default=2.0, help="served: arrival rate / sequential proof rate")
     ap.add_argument("--log-n", type=int, default=0, help="override the proof size (log instances / rows)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", default=None,
@@ -616,6 +712,8 @@ def main():
         world, rank, local = dist_setup(args, "nccl")
         if args.workload == "kernels":
             out = run_kernels(args, world, rank, local)
+        elif args.workload in ("batched", "served"):
+            out = run_serving(args, world, rank, local)
         else:
             out = run_proof(args, world, rank, local)
     if rank == 0 and out is not None:

@@ -202,6 +202,23 @@ int gs_prove_poseidon(gs_ctx* ctx, uint32_t log_n_instances, uint64_t seed, uint
                       const uint32_t* host_inputs, uint32_t composition_log_split, const gs_pcs_config* config,
                       uint8_t* proof, size_t capacity, size_t* proof_len);
 
+/* ------------------------------------------------------------- serving */
+/* A proof server (no reference counterpart: the reference proves one proof at
+ * a time on the default stream). n_workers threads, each with its own CUDA
+ * stream, prove queued jobs concurrently; a job is admitted when the
+ * estimated device footprint of the jobs in flight plus its own fits
+ * hbm_budget_bytes. Jobs use seeded inputs (GS_INPUT_SEEDED); air 0 = wide
+ * fibonacci (n_columns), 1 = poseidon2 (composition_log_split as in
+ * gs_prove_poseidon). gs_server_wait blocks until the job is done, copies its
+ * proof and reports the submit-to-done latency. */
+typedef struct gs_server gs_server;
+int gs_server_create(uint32_t n_workers, size_t hbm_budget_bytes, gs_server** out);
+int gs_server_submit(gs_server* server, uint32_t air, uint32_t log_n, uint32_t n_columns, uint64_t seed,
+                     uint32_t composition_log_split, const gs_pcs_config* config, uint64_t* job_id);
+int gs_server_wait(gs_server* server, uint64_t job_id, uint8_t* proof, size_t capacity, size_t* proof_len,
+                   double* latency_ms);
+int gs_server_destroy(gs_server* server);
+
 #ifdef __cplusplus
 }
 #endif

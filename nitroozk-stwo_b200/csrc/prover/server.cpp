@@ -1,0 +1,195 @@
+// Proof server: continuous batching of independent proof jobs on one GPU.
+//
+// Worker threads each own an execution context (a non-blocking CUDA stream);
+// a job is admitted when the estimated device footprint of the jobs in flight
+// plus its own fits the HBM budget. While one proof waits on a host step
+// (Merkle roots into the channel, FRI alphas, the proof of work, the
+// decommitment read-back), the other workers' kernels keep the GPU busy.
+// Every job runs the same prove() as a single proof, so its result is
+// identical alone and in the mix.
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <set>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include "../../../include/gpustark.h"
+#include "prove_api.h"
+
+namespace gs {
+namespace prover {
+
+struct Job {
+  uint64_t id;
+  ProveRequest req;
+  size_t footprint;
+  std::chrono::steady_clock::time_point submitted;
+};
+struct Done {
+  int status = OK;
+  std::string proof, error;
+  double latency_ms = 0, service_ms = 0;
+};
+
+// Device bytes a proof holds at its peak (trace, coefficients, LDEs, the
+// constraint-domain extension, composition, Merkle layers), with headroom.
+size_t proof_footprint(const ProveRequest& r) {
+  const size_t n = (size_t)1 << r.log_n;
+  const size_t b = (size_t)1 << r.cfg.log_blowup;
+  const size_t cols = r.air == 0 ? r.n_cols : 162;
+  const size_t ext = r.air == 0 ? 2 : 4;
+  size_t words = cols * n * (2 + b + ext) + 16 * n * ext + 64 * n * b;
+  return words * 4 + (64u << 20);
+}
+
+struct Server {
+  std::vector<std::thread> workers;
+  std::mutex mu;
+  std::condition_variable cv_jobs, cv_done;
+  std::deque<Job> queue;
+  std::map<uint64_t, Done> done;
+  std::set<uint64_t> fetched;  // results already handed out
+  size_t budget = 0, in_flight = 0;
+  uint64_t next_id = 1;
+  bool stopping = false;
+  int device = 0;
+
+  void worker() {
+    cudaSetDevice(device);
+    cudaStream_t st;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    Context ctx;
+    int init = ctx.init(st);
+    for (;;) {
+      Job job;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_jobs.wait(lk, [&] {
+          return stopping || (!queue.empty() && (in_flight == 0 || in_flight + queue.front().footprint <= budget));
+        });
+        if (stopping && queue.empty()) break;
+        job = std::move(queue.front());
+        queue.pop_front();
+        in_flight += job.footprint;
+      }
+      Done d;
+      auto t0 = std::chrono::steady_clock::now();
+      if (init != OK) {
+        d.status = init;
+        d.error = last_error();
+      } else {
+        d.status = prove_component(ctx, job.req, &d.proof, nullptr);
+        if (d.status != OK) d.error = last_error();
+        cudaStreamSynchronize(st);
+      }
+      auto t1 = std::chrono::steady_clock::now();
+      d.service_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+      d.latency_ms = std::chrono::duration<double, std::milli>(t1 - job.submitted).count();
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        in_flight -= job.footprint;
+        done[job.id] = std::move(d);
+      }
+      cv_done.notify_all();
+      cv_jobs.notify_all();
+    }
+    ctx.destroy();
+    cudaStreamDestroy(st);
+  }
+};
+
+}  // namespace prover
+}  // namespace gs
+
+using namespace gs;
+using namespace gs::prover;
+
+struct gs_server {
+  Server s;
+};
+
+extern "C" {
+
+int gs_server_create(uint32_t n_workers, size_t hbm_budget_bytes, gs_server** out) {
+  GS_REQUIRE(out != nullptr && n_workers >= 1 && n_workers <= 64, "bad server arguments");
+  gs_server* sv = new gs_server();
+  sv->s.budget = hbm_budget_bytes;
+  cudaGetDevice(&sv->s.device);
+  for (uint32_t i = 0; i < n_workers; i++) sv->s.workers.emplace_back([sv] { sv->s.worker(); });
+  *out = sv;
+  return OK;
+}
+
+int gs_server_submit(gs_server* sv, uint32_t air, uint32_t log_n, uint32_t n_columns, uint64_t seed,
+                     uint32_t composition_log_split, const gs_pcs_config* config, uint64_t* job_id) {
+  GS_REQUIRE(sv && job_id, "null argument");
+  GS_REQUIRE(air <= 1, "unknown component");
+  Job j;
+  j.req.air = air;
+  j.req.log_n = log_n;
+  j.req.n_cols = n_columns;
+  j.req.seed = seed;
+  j.req.input_mode = GS_INPUT_SEEDED;
+  j.req.split_log = composition_log_split;
+  if (config) {
+    j.req.cfg.pow_bits = config->pow_bits;
+    j.req.cfg.log_blowup = config->log_blowup_factor;
+    j.req.cfg.log_last_layer = config->log_last_layer_degree_bound;
+    j.req.cfg.n_queries = config->n_queries;
+    j.req.cfg.fold_step = config->line_fold_step;
+  }
+  j.footprint = proof_footprint(j.req);
+  j.submitted = std::chrono::steady_clock::now();
+  {
+    std::lock_guard<std::mutex> lk(sv->s.mu);
+    j.id = sv->s.next_id++;
+    *job_id = j.id;
+    sv->s.queue.push_back(std::move(j));
+  }
+  sv->s.cv_jobs.notify_one();
+  return OK;
+}
+
+int gs_server_wait(gs_server* sv, uint64_t job_id, uint8_t* proof, size_t capacity, size_t* proof_len,
+                   double* latency_ms) {
+  GS_REQUIRE(sv && proof_len, "null argument");
+  std::unique_lock<std::mutex> lk(sv->s.mu);
+  GS_REQUIRE(job_id >= 1 && job_id < sv->s.next_id, "unknown job id");
+  GS_REQUIRE(!sv->s.fetched.count(job_id), "job result already fetched");
+  sv->s.cv_done.wait(lk, [&] { return sv->s.done.count(job_id) != 0; });
+  Done& d = sv->s.done[job_id];
+  *proof_len = d.proof.size();
+  if (latency_ms) *latency_ms = d.latency_ms;
+  if (d.status != OK) {
+    int st = d.status;
+    set_error(d.error);
+    sv->s.done.erase(job_id);
+    sv->s.fetched.insert(job_id);
+    return st;
+  }
+  if (!proof || capacity < d.proof.size()) {  // the result stays available for a retry
+    set_error("proof buffer too small");
+    return ERR_INVALID;
+  }
+  memcpy(proof, d.proof.data(), d.proof.size());
+  sv->s.done.erase(job_id);
+  sv->s.fetched.insert(job_id);
+  return OK;
+}
+
+int gs_server_destroy(gs_server* sv) {
+  if (!sv) return OK;
+  {
+    std::lock_guard<std::mutex> lk(sv->s.mu);
+    sv->s.stopping = true;
+  }
+  sv->s.cv_jobs.notify_all();
+  for (auto& t : sv->s.workers) t.join();
+  delete sv;
+  return OK;
+}
+
+}  // extern "C"

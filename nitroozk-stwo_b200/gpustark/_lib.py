@@ -68,6 +68,12 @@ _PROTOS = {
     "gs_batch_eval_at_point": [C.c_void_p, VPP, C.c_uint32, C.c_uint32, PointQM31, C.c_void_p],
     "gs_prove_wide_fibonacci": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, U32P,
                                 C.POINTER(PcsConfig), C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
+    "gs_server_create": [C.c_uint32, C.c_size_t, C.POINTER(C.c_void_p)],
+    "gs_server_submit": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
+                         C.POINTER(PcsConfig), C.POINTER(C.c_uint64)],
+    "gs_server_wait": [C.c_void_p, C.c_uint64, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t),
+                       C.POINTER(C.c_double)],
+    "gs_server_destroy": [C.c_void_p],
     "gs_prove_poseidon": [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint32, U32P, C.c_uint32, C.POINTER(PcsConfig),
                           C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
 }

@@ -1,0 +1,45 @@
+"""Served/batched proving: every job's proof is identical alone and in the mix,
+under a tight HBM budget (admission control) and with several workers."""
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def mods():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from gpustark import prove, serve
+    return prove, serve
+
+
+JOBS = [(0, 10, 100, 1), (1, 8, 0, 2), (0, 12, 40, 3), (1, 10, 0, 4), (0, 9, 16, 5), (1, 12, 0, 6),
+        (0, 14, 100, 7), (1, 6, 0, 8)]
+
+
+def alone(prove, air, log_n, cols, seed):
+    if air == 0:
+        return prove.prove_wide_fibonacci(log_n, cols, seed=seed, input_mode=prove.INPUT_SEEDED)
+    return prove.prove_poseidon(log_n, seed=seed, input_mode=prove.INPUT_SEEDED)
+
+
+@pytest.mark.parametrize("workers,budget", [(4, 64 << 30), (3, 1 << 20)])
+def test_served_results_match_single_proofs(mods, workers, budget):
+    prove, serve = mods
+    with serve.ProofServer(workers, budget) as sv:
+        ids = [sv.submit(a, n, c or 100, s) for a, n, c, s in JOBS]
+        got = [sv.wait(i) for i in ids]
+    for (a, n, c, s), (proof, lat) in zip(JOBS, got):
+        assert proof == alone(prove, a, n, c or 100, s)
+        assert lat > 0
+
+
+def test_server_reports_errors(mods):
+    prove, serve = mods
+    with serve.ProofServer(2) as sv:
+        bad = sv.submit(serve.POSEIDON, 6, composition_log_split=1)
+        good = sv.submit(serve.WIDE_FIBONACCI, 6, 10, 1)
+        with pytest.raises(prove.ConstraintsNotSatisfied):
+            sv.wait(bad)
+        assert sv.wait(good)[0] == alone(prove, 0, 6, 10, 1)
