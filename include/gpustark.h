@@ -156,6 +156,18 @@ int gs_accumulate(gs_ctx* ctx, uint32_t* const a[4], const uint32_t* const b[4],
  * coefficients at `point`, written to host memory. Synchronises. */
 int gs_batch_eval_at_point(gs_ctx* ctx, const uint32_t* const* polys, uint32_t n_polys, uint32_t log_size,
                            gs_point_qm31 point, gs_qm31* out);
+/* No counterpart in the reference. The same evaluation as
+ * gs_batch_eval_at_point, results identical, but allocating nothing: no
+ * context, no cudaMalloc/cudaFree, no pinned staging. Its device scratch is
+ * one file-scope __device__ array of 4 MiB + 22 KiB per device, whose address
+ * is looked up with cudaGetSymbolAddress on the first call on each device
+ * (make that first call before any stream capture). Limits, checked before
+ * any launch (ERR_INVALID otherwise): n_polys <= 256 and
+ * n_polys * 2^max(log_size - 10, 0) <= 2^18. Runs on `stream` (a
+ * cudaStream_t; NULL = the default stream) and synchronises it. Calls that
+ * overlap in time on one device race on the shared array: serialise them. */
+int gs_batch_eval_at_point_noalloc(void* stream, const uint32_t* const* polys, uint32_t n_polys, uint32_t log_size,
+                                   gs_point_qm31 point, gs_qm31* out);
 
 /* --------------------------------------------------------------- GrindOps */
 /* grind_blake2s (bindings.rs:615); GrindOps<Blake2sChannel>::grind

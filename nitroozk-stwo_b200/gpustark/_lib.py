@@ -66,6 +66,7 @@ _PROTOS = {
     "gs_lift_and_accumulate": [C.c_void_p, VPP, U32P, C.c_uint32, VPP, C.c_uint32],
     "gs_accumulate": [C.c_void_p, VPP, VPP, C.c_size_t],
     "gs_batch_eval_at_point": [C.c_void_p, VPP, C.c_uint32, C.c_uint32, PointQM31, C.c_void_p],
+    "gs_batch_eval_at_point_noalloc": [C.c_void_p, VPP, C.c_uint32, C.c_uint32, PointQM31, C.c_void_p],
     "gs_prove_wide_fibonacci": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, U32P,
                                 C.POINTER(PcsConfig), C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
     "gs_server_create": [C.c_uint32, C.c_size_t, C.POINTER(C.c_void_p)],

@@ -235,6 +235,24 @@ class GpuBackend:
         L.check(L.lib().gs_batch_eval_at_point(ctx.handle, pp, len(polys), log_size, pt, out), "batch_eval_at_point")
         return [[o.a, o.b, o.c, o.d] for o in out]
 
+    @staticmethod
+    def batch_eval_at_point_noalloc(polys, point, log_size=None, stream=None):
+        """batch_eval_at_point with no allocation (static device scratch; at
+        most 256 polynomials and 256 * 2^10 coefficients per polynomial at
+        that count). Runs on `stream` (torch's current stream by default)."""
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream()
+        if log_size is None:
+            log_size = polys[0].numel().bit_length() - 1 if polys else 0
+        pp, k = L.ptr_array([p.data_ptr() for p in polys])
+        out = (L.QM31 * max(len(polys), 1))()
+        pt = L.PointQM31(qm31(point[:4]), qm31(point[4:]))
+        handle = getattr(stream, "cuda_stream", stream)
+        L.check(L.lib().gs_batch_eval_at_point_noalloc(handle, pp, len(polys), log_size, pt, out),
+                "batch_eval_at_point_noalloc")
+        return [[o.a, o.b, o.c, o.d] for o in out[:len(polys)]]
+
     # ------------------------------------------------------------- GrindOps
     @staticmethod
     def grind(digest: bytes, pow_bits, ctx=None):
