@@ -657,7 +657,8 @@ def run_reference(args, world, rank):
 
 
 def run_case(args):
-    """One op on a small case, for ncu captures: `--case fft:26`, `--case merkle:20:64`, `--case fold:22`."""
+    """One op on a small case, for ncu captures: `--case fft:26`, `--case lde:18:162` (blowup-2
+    extension of 162 columns), `--case merkle:20:64`, `--case fold:22`."""
     import torch
     from gpustark.backend import GpuBackend as B, to_device, Context
     kind, *params = args.case.split(":")
@@ -669,6 +670,12 @@ def run_case(args):
         x = to_device(rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32))
         y = torch.empty_like(x)
         work = lambda: (B.evaluate_polynomials([x], n, tw, out=[y], ctx=ctx), B.interpolate_columns([y], n, tw, ctx=ctx))
+    elif kind == "lde":
+        n, k = int(params[0]), int(params[1])
+        tw = B.precompute_twiddles(n + 1, ctx=ctx)
+        cs = [to_device(rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32)) for _ in range(k)]
+        ev = [torch.empty(1 << (n + 1), dtype=torch.int32, device="cuda") for _ in range(k)]
+        work = lambda: B.evaluate_polynomials(cs, n + 1, tw, out=ev, ctx=ctx)
     elif kind == "merkle":
         n, k = int(params[0]), int(params[1])
         cols = [to_device(rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32)) for _ in range(k)]
@@ -700,7 +707,7 @@ def main():
     ap.add_argument("--log-n", type=int, default=0, help="override the proof size (log instances / rows)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", default=None,
-                    help="profiling case: fft:<log>, merkle:<log>:<cols>, fold:<log> (one op, no JSON contract)")
+                    help="profiling case: fft:<log>, lde:<log>:<cols>, merkle:<log>:<cols>, fold:<log> (one op, no JSON contract)")
     args = ap.parse_args()
     if args.case:
         run_case(args)

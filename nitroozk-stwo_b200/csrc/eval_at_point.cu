@@ -18,17 +18,14 @@ constexpr uint32_t EAP_S = 10;                 // low bits per chunk: 1024 coeff
 
 struct Factors { qm31 f[31]; };
 
-// W[j] = prod over set bits b < s of j of F_b, for j < 2^s (one block).
-__global__ void eap_weights_kernel(Factors fs, uint32_t s, uint32_t* w /* 4 planes of 2^s, interleaved as [j][4] */) {
-  extern __shared__ uint32_t sw[];  // 4 * 2^s
-  uint32_t n = 1u << s;
-  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
-    qm31 acc = qm_one();
-    for (uint32_t b = 0; b < s; b++)
-      if ((j >> b) & 1u) acc = qm_mul(acc, fs.f[b]);
-    w[4 * j + 0] = acc.x.a; w[4 * j + 1] = acc.x.b; w[4 * j + 2] = acc.y.a; w[4 * j + 3] = acc.y.b;
-  }
-  (void)sw;
+// W[j] = prod over set bits b < s of j of F_b, for j < 2^s (one thread each).
+__global__ void eap_weights_kernel(Factors fs, uint32_t s, uint32_t* w /* [j][4] */) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= (1u << s)) return;
+  qm31 acc = qm_one();
+  for (uint32_t b = 0; b < s; b++)
+    if ((j >> b) & 1u) acc = qm_mul(acc, fs.f[b]);
+  w[4 * j + 0] = acc.x.a; w[4 * j + 1] = acc.x.b; w[4 * j + 2] = acc.y.a; w[4 * j + 3] = acc.y.b;
 }
 
 __device__ __forceinline__ uint64_t fold64e(uint64_t x) { return (x & P) + (x >> 31); }
@@ -75,15 +72,35 @@ __global__ void __launch_bounds__(256) eap_chunk_kernel(const uint32_t* const* _
   }
 }
 
-__global__ void eap_finalize_kernel(const uint32_t* partials, uint32_t n_chunks, uint32_t n_polys, uint32_t* out) {
-  uint32_t poly = blockIdx.x * blockDim.x + threadIdx.x;
-  if (poly >= n_polys) return;
+// One block of 128 threads per polynomial: strided partial sums, then a
+// shuffle and shared-memory reduction (field additions are exact, so the
+// order does not change the result).
+__global__ void __launch_bounds__(128) eap_finalize_kernel(const uint32_t* partials, uint32_t n_chunks, uint32_t n_polys,
+                                                           uint32_t* out) {
+  __shared__ uint4 red[4];
+  const uint32_t poly = blockIdx.x;
+  const uint4* p = reinterpret_cast<const uint4*>(partials) + (size_t)poly * n_chunks;
   uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-  const uint32_t* p = partials + 4 * (size_t)poly * n_chunks;
-  for (uint32_t k = 0; k < n_chunks; k++) {
-    t0 = add(t0, p[4 * k]); t1 = add(t1, p[4 * k + 1]); t2 = add(t2, p[4 * k + 2]); t3 = add(t3, p[4 * k + 3]);
+  for (uint32_t k = threadIdx.x; k < n_chunks; k += blockDim.x) {
+    uint4 v = p[k];
+    t0 = add(t0, v.x); t1 = add(t1, v.y); t2 = add(t2, v.z); t3 = add(t3, v.w);
   }
-  out[4 * poly] = t0; out[4 * poly + 1] = t1; out[4 * poly + 2] = t2; out[4 * poly + 3] = t3;
+  for (int off = 16; off > 0; off >>= 1) {
+    t0 = add(t0, __shfl_down_sync(0xffffffffu, t0, off));
+    t1 = add(t1, __shfl_down_sync(0xffffffffu, t1, off));
+    t2 = add(t2, __shfl_down_sync(0xffffffffu, t2, off));
+    t3 = add(t3, __shfl_down_sync(0xffffffffu, t3, off));
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = make_uint4(t0, t1, t2, t3);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint4 r = red[0];
+    for (uint32_t wv = 1; wv < blockDim.x / 32; wv++) {
+      r.x = add(r.x, red[wv].x); r.y = add(r.y, red[wv].y); r.z = add(r.z, red[wv].z); r.w = add(r.w, red[wv].w);
+    }
+    out[4 * poly] = r.x; out[4 * poly + 1] = r.y; out[4 * poly + 2] = r.z; out[4 * poly + 3] = r.w;
+  }
+  (void)n_polys;
 }
 
 // Factors F_b for a point (host).
@@ -115,14 +132,14 @@ int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_
   GS_REQUIRE(chunks <= 65535 * 32768u, "too many chunks");
   uint32_t* w = d_scratch;
   uint32_t* partials = d_scratch + 4 * (1u << s);
-  eap_weights_kernel<<<1, 256, 0, st>>>(fs, s, w);
+  eap_weights_kernel<<<((1u << s) + 255) / 256, 256, 0, st>>>(fs, s, w);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   dim3 grid(chunks, n_polys);
   eap_chunk_kernel<<<grid, 256, 0, st>>>(d_polys, log_n, w, fs, partials);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
-  eap_finalize_kernel<<<(n_polys + 127) / 128, 128, 0, st>>>(partials, chunks, n_polys, d_out);
+  eap_finalize_kernel<<<n_polys, 128, 0, st>>>(partials, chunks, n_polys, d_out);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;

@@ -40,9 +40,12 @@ __device__ __forceinline__ void load_pair(CPlanes s, size_t i, qm31& a, qm31& b)
   b = qm_make(p0.y, p1.y, p2.y, p3.y);
 }
 
+// d_alpha (optional): the challenge in device memory (4 words, then alpha^2),
+// written by the device channel; overrides `alpha`.
 __global__ void fold_line_kernel(CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* __restrict__ itw,
-                                 uint32_t tw_len, uint32_t* leaf_out) {
+                                 uint32_t tw_len, uint32_t* leaf_out, const uint32_t* __restrict__ d_alpha) {
   const size_t half = (size_t)1 << (log_n - 1);
+  if (d_alpha) alpha = qm_make(d_alpha[0], d_alpha[1], d_alpha[2], d_alpha[3]);
   const uint32_t* lvl = itw + (tw_len - (1u << log_n));
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < half; i += (size_t)gridDim.x * blockDim.x) {
     qm31 fx, fnx;
@@ -60,8 +63,12 @@ struct SmallInvY { uint32_t v[2]; };
 
 __global__ void fold_circle_kernel(CPlanes src, uint32_t log_n, qm31 alpha, qm31 alpha_sq, Planes dst,
                                    const uint32_t* __restrict__ itw, uint32_t tw_len, SmallInvY small,
-                                   uint32_t* leaf_out) {
+                                   uint32_t* leaf_out, const uint32_t* __restrict__ d_alpha) {
   const size_t half = (size_t)1 << (log_n - 1);
+  if (d_alpha) {
+    alpha = qm_make(d_alpha[0], d_alpha[1], d_alpha[2], d_alpha[3]);
+    alpha_sq = qm_make(d_alpha[4], d_alpha[5], d_alpha[6], d_alpha[7]);
+  }
   const uint32_t* t0 = log_n >= 3 ? itw + (tw_len - (1u << (log_n - 1))) : nullptr;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < half; i += (size_t)gridDim.x * blockDim.x) {
     qm31 fp, fnp;
@@ -90,11 +97,12 @@ static unsigned grid_for(size_t n, int threads) {
   return (unsigned)(b < cap ? (b ? b : 1) : cap);
 }
 
-int fold_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itw,
-                    uint32_t tw_log, uint32_t* leaf_out) {
+static int fold_line_launch(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
+                            const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out, const uint32_t* d_alpha) {
   GS_REQUIRE(log_n >= 1 && log_n <= tw_log, "fold_line: line domain must fit the twiddle tree");
   size_t half = (size_t)1 << (log_n - 1);
-  fold_line_kernel<<<grid_for(half, 256), 256, 0, st>>>(src, log_n, alpha, dst, d_itw, 1u << tw_log, leaf_out);
+  fold_line_kernel<<<grid_for(half, 256), 256, 0, st>>>(src, log_n, alpha, dst, d_itw, 1u << tw_log, leaf_out,
+                                                        d_alpha);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;
@@ -109,8 +117,17 @@ static pt31 host_point(uint32_t k) {
   return r;
 }
 
-int fold_circle_into_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
-                                const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out) {
+int fold_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itw,
+                    uint32_t tw_log, uint32_t* leaf_out) {
+  return fold_line_launch(st, src, log_n, alpha, dst, d_itw, tw_log, leaf_out, nullptr);
+}
+int fold_line_dev_alpha(cudaStream_t st, CPlanes src, uint32_t log_n, const uint32_t* d_alpha, Planes dst,
+                        const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out) {
+  return fold_line_launch(st, src, log_n, qm_zero(), dst, d_itw, tw_log, leaf_out, d_alpha);
+}
+
+static int fold_circle_launch(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
+                              const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out, const uint32_t* d_alpha) {
   GS_REQUIRE(log_n >= 1 && log_n <= tw_log + 1, "fold_circle_into_line: domain must fit the twiddle tree");
   SmallInvY small{{0, 0}};
   if (log_n < 3) {
@@ -125,10 +142,18 @@ int fold_circle_into_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm
   qm31 alpha_sq = qm_mul(alpha, alpha);
   size_t half = (size_t)1 << (log_n - 1);
   fold_circle_kernel<<<grid_for(half, 256), 256, 0, st>>>(src, log_n, alpha, alpha_sq, dst, d_itw, 1u << tw_log, small,
-                                                          leaf_out);
+                                                          leaf_out, d_alpha);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;
+}
+int fold_circle_into_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
+                                const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out) {
+  return fold_circle_launch(st, src, log_n, alpha, dst, d_itw, tw_log, leaf_out, nullptr);
+}
+int fold_circle_into_line_dev_alpha(cudaStream_t st, CPlanes src, uint32_t log_n, const uint32_t* d_alpha, Planes dst,
+                                    const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out) {
+  return fold_circle_launch(st, src, log_n, qm_zero(), dst, d_itw, tw_log, leaf_out, d_alpha);
 }
 
 int fold_line(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itwiddles,

@@ -7,68 +7,114 @@ void fft_set_columns_aligned(bool aligned);
 namespace prover {
 
 // FRI commit (prover/fri.rs:99-199) on the combined quotient planes (2^lifting).
+//
+// The whole phase is enqueued without a host round trip: each layer's Merkle
+// root goes through the device channel (mix_root + draw_secure_felt), whose
+// challenge the next fold reads from device memory. Roots, challenges and the
+// last layer come back in one read at the end; the host replays the channel
+// on the roots and checks every challenge.
 int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first,
                       std::vector<FriLayerDev>& inner, std::vector<qm31>& last_coeffs) {
   cudaStream_t st = pv.st;
-  Arena& A = pv.A;
-  auto alloc_layer = [&](FriLayerDev& L, uint32_t log) -> int {
+  const uint32_t last_log = pv.cfg.log_last_layer + pv.cfg.log_blowup;
+  GS_REQUIRE(lifting >= last_log + 1, "FRI: lifting domain below the last layer");
+  const uint32_t n_roots = lifting - last_log;  // the first layer and the committed line layers
+  // one allocation for every FRI buffer, carved at 256-byte boundaries
+  auto up = [](size_t w) { return (w + 63) & ~(size_t)63; };
+  auto tree_words = [&](uint32_t log) {
+    size_t w = 0;
+    for (uint32_t k = 0; k <= log; k++) w += up((size_t)8 << k);
+    return w;
+  };
+  const size_t ctl_words = up(16 + 16 * (size_t)n_roots);
+  size_t words = ctl_words + tree_words(lifting);
+  for (uint32_t lg = lifting - 1;; lg--) {
+    words += 4 * up((size_t)1 << lg);
+    if (lg > last_log) words += tree_words(lg);
+    if (lg == last_log) break;
+  }
+  uint32_t* block = nullptr;
+  GS_TRY(pv.A.alloc_n(words, &block));
+  uint32_t* carve = block;
+  auto take = [&](size_t w) {
+    uint32_t* p = carve;
+    carve += up(w);
+    return p;
+  };
+  uint32_t* ctl = take(ctl_words);  // [0,16): channel state; then roots, then challenges
+  uint32_t* d_roots = ctl + 16;
+  uint32_t* d_felts = d_roots + 8 * (size_t)n_roots;
+  auto take_tree = [&](FriLayerDev& L) {
+    L.layers.assign(L.log + 1, nullptr);
+    for (uint32_t k = 0; k <= L.log; k++) L.layers[k] = take((size_t)8 << k);
+  };
+  auto take_layer = [&](FriLayerDev& L, uint32_t log) {
     L.log = log;
-    for (int c = 0; c < 4; c++) GS_TRY(A.alloc_n((size_t)1 << log, &L.planes[c]));
-    L.layers.assign(log + 1, nullptr);
-    for (uint32_t k = 0; k <= log; k++) GS_TRY(A.alloc_n((size_t)8 << k, &L.layers[k]));
-    return OK;
+    for (int c = 0; c < 4; c++) L.planes[c] = take((size_t)1 << log);
+    if (log > last_log) take_tree(L);
   };
-  auto root_of = [&](FriLayerDev& L) -> int {
-    GS_TRY(commit_node_layers(st, L.log, L.layers.data()));
-    uint32_t w[8];
-    GS_CUDA_TRY(cudaMemcpyAsync(w, L.layers[0], 32, cudaMemcpyDeviceToHost, st));
-    GS_CUDA_TRY(cudaStreamSynchronize(st));
-    L.root = host::hash_from_words(w);
-    return OK;
-  };
+  {
+    uint32_t h[16] = {0};
+    for (int j = 0; j < 8; j++) h[j] = host::word(pv.ch.digest, j);
+    h[8] = pv.ch.n_draws;
+    const void* d = nullptr;
+    GS_TRY(pv.ctx.stage_bytes(h, sizeof h, &d));
+    GS_CUDA_TRY(cudaMemcpyAsync(ctl, d, sizeof h, cudaMemcpyDeviceToDevice, st));
+  }
   // first layer: the quotient columns themselves
   first.log = lifting;
   for (int c = 0; c < 4; c++) first.planes[c] = quot[c];
-  first.layers.assign(lifting + 1, nullptr);
-  for (uint32_t k = 0; k <= lifting; k++) GS_TRY(A.alloc_n((size_t)8 << k, &first.layers[k]));
+  take_tree(first);
   {
     std::vector<const uint32_t*> cols = {quot[0], quot[1], quot[2], quot[3]};
     const uint32_t* const* tab = nullptr;
     GS_TRY(pv.table(cols, &tab));
     GS_TRY(commit_on_layer(st, lifting, nullptr, tab, 4, first.layers[lifting]));
   }
-  GS_TRY(root_of(first));
-  pv.ch.mix_root(first.root);
-  const uint32_t last_log = pv.cfg.log_last_layer + pv.cfg.log_blowup;
+  GS_TRY(commit_node_layers(st, first.log, first.layers.data()));
+  GS_TRY(channel_mix_root_draw(st, ctl, first.layers[0], d_roots, d_felts));
   // fold the circle evaluation into the first line layer (zero-initialised)
   FriLayerDev cur;
-  GS_TRY(alloc_layer(cur, lifting - 1));
+  take_layer(cur, lifting - 1);
   for (int c = 0; c < 4; c++) GS_CUDA_TRY(cudaMemsetAsync(cur.planes[c], 0, (size_t)4 << cur.log, st));
-  qm31 alpha = pv.ch.draw_felt();
-  GS_TRY(fold_circle_into_line_fused(st, CPlanes{{quot[0], quot[1], quot[2], quot[3]}}, lifting, alpha,
-                                     Planes{{cur.planes[0], cur.planes[1], cur.planes[2], cur.planes[3]}}, pv.itw,
-                                     pv.tw_log, cur.layers[cur.log]));
-  if (cur.log != last_log) {
-    for (;;) {
-      GS_TRY(root_of(cur));
-      pv.ch.mix_root(cur.root);
-      alpha = pv.ch.draw_felt();
-      FriLayerDev next;
-      GS_TRY(alloc_layer(next, cur.log - 1));
-      GS_TRY(fold_line_fused(st, CPlanes{{cur.planes[0], cur.planes[1], cur.planes[2], cur.planes[3]}}, cur.log, alpha,
-                             Planes{{next.planes[0], next.planes[1], next.planes[2], next.planes[3]}}, pv.itw,
-                             pv.tw_log, next.layers[next.log]));
-      inner.push_back(std::move(cur));
-      cur = std::move(next);
-      if (cur.log <= last_log) break;
-    }
+  GS_TRY(fold_circle_into_line_dev_alpha(st, CPlanes{{quot[0], quot[1], quot[2], quot[3]}}, lifting, d_felts,
+                                         Planes{{cur.planes[0], cur.planes[1], cur.planes[2], cur.planes[3]}},
+                                         pv.itw, pv.tw_log, cur.log > last_log ? cur.layers[cur.log] : nullptr));
+  uint32_t k = 1;
+  while (cur.log > last_log) {
+    GS_TRY(commit_node_layers(st, cur.log, cur.layers.data()));
+    GS_TRY(channel_mix_root_draw(st, ctl, cur.layers[0], d_roots + 8 * k, d_felts + 8 * k));
+    FriLayerDev next;
+    take_layer(next, cur.log - 1);
+    GS_TRY(fold_line_dev_alpha(st, CPlanes{{cur.planes[0], cur.planes[1], cur.planes[2], cur.planes[3]}}, cur.log,
+                               d_felts + 8 * k, Planes{{next.planes[0], next.planes[1], next.planes[2], next.planes[3]}},
+                               pv.itw, pv.tw_log, next.log > last_log ? next.layers[next.log] : nullptr));
+    inner.push_back(std::move(cur));
+    cur = std::move(next);
+    k++;
   }
-  // last layer: 2^last_log values -> line polynomial, degree check, mix
+  // one read-back: channel state, roots, challenges, then the last layer
+  std::vector<uint32_t> hc(16 + 16 * (size_t)n_roots);
+  GS_CUDA_TRY(cudaMemcpyAsync(hc.data(), ctl, hc.size() * 4, cudaMemcpyDeviceToHost, st));
   size_t n = (size_t)1 << cur.log;
   std::vector<uint32_t> h(4 * n);
   for (int c = 0; c < 4; c++)
     GS_CUDA_TRY(cudaMemcpyAsync(h.data() + c * n, cur.planes[c], 4 * n, cudaMemcpyDeviceToHost, st));
   GS_CUDA_TRY(cudaStreamSynchronize(st));
+  GS_REQUIRE(hc[9] == 0, "device channel: no challenge within the draw bound");
+  for (uint32_t r = 0; r < n_roots; r++) {
+    host::Hash root = host::hash_from_words(hc.data() + 16 + 8 * r);
+    pv.ch.mix_root(root);
+    qm31 a = pv.ch.draw_felt();
+    const uint32_t* f = hc.data() + 16 + 8 * (size_t)n_roots + 8 * r;
+    if (!qm_eq(a, qm_make(f[0], f[1], f[2], f[3]))) {
+      set_error("device channel diverged from the host channel");
+      return ERR_CUDA;
+    }
+    if (r == 0) first.root = root;
+    else inner[r - 1].root = root;
+  }
+  // last layer: 2^last_log values -> line polynomial, degree check, mix
   std::vector<qm31> vals(n);
   for (size_t i = 0; i < n; i++) vals[i] = qm_make(h[i], h[n + i], h[2 * n + i], h[3 * n + i]);
   std::vector<qm31> coeffs = line_interpolate_host(vals, cur.log);
@@ -111,6 +157,7 @@ void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::
 int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_bytes, ProveStats* stats) {
   PcsConfig cfg = req.cfg;
   Prover pv(ctx, cfg);
+  pv.mark("start");
   cudaStream_t st = ctx.stream;
   AirHost air;
   air.kind = req.air == 0 ? AirKind::WideFibonacci : AirKind::Poseidon;
@@ -127,6 +174,7 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
   GS_REQUIRE(comp_tree >= cfg.log_last_layer + cfg.log_blowup + 1, "trace too small for the FRI last layer");
   uint32_t root = std::max({air.log_n + cfg.log_blowup, E, comp_tree}) - 1;
   GS_TRY(pv.twiddles_for(root));
+  pv.mark("twiddles");
   // every column buffer of the prover starts at a multiple of 4 words
   fft_set_columns_aligned(true);
   // preprocessed tree (empty)
@@ -147,7 +195,9 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
       GS_CUDA_TRY(cudaMemcpyAsync(trace, req.host_inputs, 16 * 4 * n, cudaMemcpyHostToDevice, st));
     GS_TRY(poseidon_trace(st, trace, T, req.seed, req.input_mode));
   }
+  pv.mark("trace");
   GS_TRY(pv.commit_evals(trace, air.n_trace_cols(), T));
+  pv.mark("trace_commit");
   if (air.kind == AirKind::Poseidon) {
     auto z = pv.ch.draw_felts(2);
     qm31 alpha = z[1], cur = qm_one();
@@ -162,9 +212,14 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
     uint32_t* inter = nullptr;
     GS_TRY(pv.A.alloc_n((size_t)4 << T, &inter));
     GS_TRY(poseidon_interaction(st, trace, T, air.lookup, inter, scratch, &air.claimed_sum));
+    pv.mark("interaction");
     GS_TRY(pv.commit_evals(inter, 4, T));
+    pv.mark("interaction_commit");
   }
-  return prove_tail(pv, air, split, proof_bytes, stats);
+  int rc = prove_tail(pv, air, split, proof_bytes, stats);
+  pv.mark("end");
+  pv.phases.report();
+  return rc;
 }
 
 }  // namespace prover

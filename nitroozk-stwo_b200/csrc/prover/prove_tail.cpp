@@ -24,6 +24,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   qm31 random_coeff = pv.ch.draw_felt();
   uint32_t* comp[4];
   GS_TRY(pv.composition(air, random_coeff, comp));
+  pv.mark("composition");
   {
     std::vector<const uint32_t*> parts;
     const uint32_t plog = E - split;
@@ -31,6 +32,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
       for (int c = 0; c < 4; c++) parts.push_back(comp[c] + ((size_t)t << plog));
     GS_TRY(pv.commit_coeffs(parts, plog));
   }
+  pv.mark("composition_commit");
   ptq oods = host::random_point(pv.ch);
   const uint32_t lifting = pv.trees.back().max_log();
   const uint32_t max_ldb = lifting - cfg.log_blowup;
@@ -38,6 +40,14 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   const size_t n_trees = pv.trees.size();
   std::vector<std::vector<ColSamples>> samples(n_trees);
   pt31 step = host::index_point(host::canonic_step_index(max_ldb));
+  // every (tree, mask point) evaluation is enqueued, then read back once
+  struct SampleReq {
+    size_t t;
+    ptq p;
+    size_t slot;
+  };
+  std::vector<SampleReq> reqs;
+  size_t n_vals = 0, scratch_bytes = 0;
   for (size_t t = 0; t < n_trees; t++) {
     Tree& tr = pv.trees[t];
     samples[t].resize(tr.n_cols);
@@ -46,11 +56,31 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     if (t + 1 == n_trees || t == 1) pts = {oods};
     else pts = {ptq_add(oods, host::to_ptq(pt_conj(step))), oods};  // interaction: offsets -1, 0
     for (auto& p : pts) {
-      std::vector<qm31> vals;
-      GS_TRY(pv.sample_tree(tr, host::ptq_rep_double(p, lifting - tr.eval_log), vals));
+      reqs.push_back({t, p, n_vals});
+      n_vals += tr.n_cols;
+      scratch_bytes = std::max(scratch_bytes, eval_at_point_scratch_bytes(tr.n_cols, tr.coeff_log));
+    }
+  }
+  {
+    uint32_t* d_vals = nullptr;
+    void* scratch = nullptr;
+    GS_TRY(pv.A.alloc_n(4 * n_vals + 4, &d_vals));
+    GS_TRY(pv.A.alloc(scratch_bytes + 16, &scratch));
+    for (auto& r : reqs) {
+      Tree& tr = pv.trees[r.t];
+      GS_TRY(batch_eval_at_point(st, tr.coeff_tab, tr.n_cols, tr.coeff_log,
+                                 host::ptq_rep_double(r.p, lifting - tr.eval_log), d_vals + 4 * r.slot,
+                                 (uint32_t*)scratch));
+    }
+    std::vector<uint32_t> h(4 * n_vals);
+    if (n_vals) GS_CUDA_TRY(cudaMemcpyAsync(h.data(), d_vals, h.size() * 4, cudaMemcpyDeviceToHost, st));
+    GS_CUDA_TRY(cudaStreamSynchronize(st));
+    for (auto& r : reqs) {
+      Tree& tr = pv.trees[r.t];
       for (uint32_t c = 0; c < tr.n_cols; c++) {
-        samples[t][c].points.push_back(p);
-        samples[t][c].values.push_back(vals[c]);
+        const uint32_t* v = h.data() + 4 * (r.slot + c);
+        samples[r.t][c].points.push_back(r.p);
+        samples[r.t][c].values.push_back(qm_make(v[0], v[1], v[2], v[3]));
       }
     }
   }
@@ -58,6 +88,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   for (auto& tr : samples)
     for (auto& c : tr) flat.insert(flat.end(), c.values.begin(), c.values.end());
   pv.ch.mix_felts(flat);
+  pv.mark("oods_sample");
   // DEEP quotients: per (column size, point) batches of line-coefficient
   // terms, lifted per point, combined over the lifting domain.
   qm31 qrc = pv.ch.draw_felt();
@@ -161,15 +192,18 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     GS_TRY(pv.ctx.stage_bytes(qaccs.data(), qaccs.size() * sizeof(QuotAcc), &d));
     GS_TRY(compute_quotients_and_combine(st, d, (uint32_t)qaccs.size(), dt, Planes{{quot[0], quot[1], quot[2], quot[3]}}));
   }
+  pv.mark("quotients");
   // FRI commit, proof of work
   FriLayerDev first;
   std::vector<FriLayerDev> inner;
   std::vector<qm31> last;
   GS_TRY(fri_commit(pv, quot, lifting, first, inner, last));
+  pv.mark("fri_commit");
   auto pre = pv.ch.pow_prefixed(cfg.pow_bits);
   uint64_t nonce = 0;
   GS_TRY(grind_blake2s(st, pre.data(), cfg.pow_bits, (uint32_t*)pv.ctx.d_small, &nonce));
   pv.ch.mix_u64(nonce);
+  pv.mark("grind");
   // queries
   auto raw = host::draw_queries(pv.ch, lifting, cfg.n_queries);
   std::vector<size_t> queries(raw);
@@ -211,7 +245,9 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     for (uint32_t c = 0; c < tr.n_cols; c++) cols.push_back(tr.eval_col(c));
     tree_plans[t].plan(g, tr.layers, cols, pos);
   }
+  pv.mark("decommit_plan");
   GS_TRY(g.run(pv.ctx, pv.A));
+  pv.mark("decommit_gather");
   // assemble the proof
   host::Proof P;
   P.pow_bits = cfg.pow_bits;
@@ -258,6 +294,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   qm31 dinv = qm_inv(host::canonic_vanishing(max_ldb, oods));
   qm31 cons = eval_at_point(air, P.sampled_values, random_coeff, dinv);
   if (stats) stats->constraint_check = qm_eq(total, cons) ? 1.0 : 0.0;
+  pv.mark("sanity_check");
   *proof_bytes = host::serialize(P);
   if (!qm_eq(total, cons)) {
     set_error("constraints not satisfied: composition OODS value differs from the constraints at the mask");

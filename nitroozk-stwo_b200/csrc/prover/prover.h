@@ -109,16 +109,20 @@ struct MerkleDecommitPlan {
     value_base = g.words.size();
     for (size_t node : pos)
       for (auto* c : cols) g.add_word(c, node);
-    std::vector<size_t> prev = pos;
+    // positions are sorted and unique at every layer, so membership of a
+    // sibling is a linear merge against the previous layer's list
+    std::vector<size_t> prev = pos, merged;
     for (int L = (int)layers.size() - 2; L >= 0; L--) {
-      std::set<size_t> prev_set(prev.begin(), prev.end());
-      std::vector<size_t> merged;
+      merged.clear();
       for (size_t q : prev)
         if (merged.empty() || merged.back() != q / 2) merged.push_back(q / 2);
+      size_t ip = 0;
       for (size_t node : merged)
-        for (size_t ch = 2 * node; ch <= 2 * node + 1; ch++)
-          if (!prev_set.count(ch)) hash_slots.push_back(g.add_hash(layers[L + 1], ch));
-      prev = merged;
+        for (size_t ch = 2 * node; ch <= 2 * node + 1; ch++) {
+          while (ip < prev.size() && prev[ip] < ch) ip++;
+          if (ip == prev.size() || prev[ip] != ch) hash_slots.push_back(g.add_hash(layers[L + 1], ch));
+        }
+      prev.swap(merged);
     }
   }
   void assemble(const GatherPlan& g, std::vector<uint32_t>& queried, host::Decommitment& d) const {

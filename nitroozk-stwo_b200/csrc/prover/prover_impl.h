@@ -4,18 +4,79 @@
 #include "prover.h"
 #include "host_air.h"
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 
 namespace gs {
 int fold_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itw,
                     uint32_t tw_log, uint32_t* leaf_out);
 int fold_circle_into_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst,
                                 const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out);
+int fold_line_dev_alpha(cudaStream_t st, CPlanes src, uint32_t log_n, const uint32_t* d_alpha, Planes dst,
+                        const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out);
+int fold_circle_into_line_dev_alpha(cudaStream_t st, CPlanes src, uint32_t log_n, const uint32_t* d_alpha, Planes dst,
+                                    const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out);
+int channel_mix_root_draw(cudaStream_t st, uint32_t* d_state, const uint32_t* d_root, uint32_t* d_root_copy,
+                          uint32_t* d_felt);
 int interpolate_columns_to(cudaStream_t st, const uint32_t* const* d_src, uint32_t* const* d_dst, uint32_t n_cols,
                            uint32_t log_n, const uint32_t* d_itwiddles, uint32_t tw_log);
 
 namespace prover {
 
 using host::Hash;
+
+// Phase timeline of one proof, enabled by the environment variable
+// GS_PHASE_LOG=1: at each mark, a CUDA event on the prover's stream and the
+// host clock. At the end one JSON line goes to stderr with, per phase, the
+// device time between events and the host time spent enqueuing it; a phase
+// whose host time exceeds its device time leaves the GPU idle.
+struct PhaseLog {
+  bool on = false;
+  cudaStream_t st = nullptr;
+  std::vector<const char*> names;
+  std::vector<cudaEvent_t> ev;
+  std::vector<std::chrono::steady_clock::time_point> host;
+  void init(cudaStream_t s) {
+    const char* e = getenv("GS_PHASE_LOG");
+    on = e && e[0] == '1';
+    st = s;
+  }
+  void mark(const char* name) {
+    if (!on) return;
+    cudaEvent_t x;
+    cudaEventCreate(&x);
+    cudaEventRecord(x, st);
+    names.push_back(name);
+    ev.push_back(x);
+    host.push_back(std::chrono::steady_clock::now());
+  }
+  void report() {
+    if (!on || ev.size() < 2) return;
+    cudaEventSynchronize(ev.back());
+    std::string js = "{\"phases\": [";
+    for (size_t i = 1; i < ev.size(); i++) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[i - 1], ev[i]);
+      double hms = std::chrono::duration<double, std::milli>(host[i] - host[i - 1]).count();
+      char buf[160];
+      snprintf(buf, sizeof buf, "%s[\"%s\", %.3f, %.3f]", i > 1 ? ", " : "", names[i], ms, hms);
+      js += buf;
+    }
+    float tot = 0;
+    cudaEventElapsedTime(&tot, ev.front(), ev.back());
+    double htot = std::chrono::duration<double, std::milli>(host.back() - host.front()).count();
+    char buf[96];
+    snprintf(buf, sizeof buf, "], \"device_ms\": %.3f, \"host_ms\": %.3f}\n", tot, htot);
+    js += buf;
+    fputs(js.c_str(), stderr);
+    for (auto x : ev) cudaEventDestroy(x);
+    ev.clear();
+  }
+  ~PhaseLog() {
+    for (auto x : ev) cudaEventDestroy(x);
+  }
+};
 
 struct Prover {
   Context& ctx;
@@ -27,8 +88,13 @@ struct Prover {
   const uint32_t* tw = nullptr;
   const uint32_t* itw = nullptr;
   uint32_t tw_log = 0;
+  PhaseLog phases;
 
-  Prover(Context& c, const PcsConfig& p) : ctx(c), st(c.stream), cfg(p) { A.st = st; }
+  Prover(Context& c, const PcsConfig& p) : ctx(c), st(c.stream), cfg(p) {
+    A.st = st;
+    phases.init(st);
+  }
+  void mark(const char* name) { phases.mark(name); }
 
   int twiddles_for(uint32_t root_log) {
     GS_TRY(ctx.twiddles(root_log, &tw, &itw));

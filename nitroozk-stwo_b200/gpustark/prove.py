@@ -36,7 +36,7 @@ def _run(fn, args, ctx, capacity):
     if st == GS_ERR_PROOF:
         raise ConstraintsNotSatisfied(L.lib().gs_last_error().decode())
     L.check(st, fn.__name__)
-    return bytes(buf[: n.value])
+    return C.string_at(buf, n.value)
 
 
 def _inputs(host_inputs):
@@ -47,7 +47,7 @@ def _inputs(host_inputs):
 
 
 def prove_wide_fibonacci(log_n_rows, n_columns=100, seed=0, input_mode=INPUT_REFERENCE, host_inputs=None,
-                         config=None, ctx=None, capacity=1 << 24):
+                         config=None, ctx=None, capacity=1 << 21):
     """host_inputs (INPUT_HOST): array (2, 2^log_n_rows) of columns 0 and 1."""
     ctx = ctx or default_context()
     keep, ptr = _inputs(host_inputs)
@@ -57,7 +57,7 @@ def prove_wide_fibonacci(log_n_rows, n_columns=100, seed=0, input_mode=INPUT_REF
 
 
 def prove_poseidon(log_n_instances, seed=0, input_mode=INPUT_REFERENCE, host_inputs=None, composition_log_split=2,
-                   config=None, ctx=None, capacity=1 << 24):
+                   config=None, ctx=None, capacity=1 << 21):
     """host_inputs (INPUT_HOST): array (16, 2^log_n_instances) of initial states."""
     ctx = ctx or default_context()
     keep, ptr = _inputs(host_inputs)

@@ -29,7 +29,7 @@ class ProofServer:
                                          C.byref(cfg), C.byref(jid)), "gs_server_submit")
         return jid.value
 
-    def wait(self, job_id, capacity=1 << 24):
+    def wait(self, job_id, capacity=1 << 20):
         """Blocks until the job is done; returns (proof bytes, submit-to-done latency in ms)."""
         n = C.c_size_t()
         lat = C.c_double()
@@ -42,7 +42,7 @@ class ProofServer:
         if st == GS_ERR_PROOF:
             raise ConstraintsNotSatisfied(L.lib().gs_last_error().decode())
         L.check(st, "gs_server_wait")
-        return bytes(buf[: n.value]), lat.value
+        return C.string_at(buf, n.value), lat.value
 
     def close(self):
         if self.handle:
