@@ -218,6 +218,10 @@ __device__ __forceinline__ uint32_t prev_row(uint32_t i, uint32_t trace_log, uin
   return __brev(idx) >> (32 - eval_log);
 }
 
+// Lazy accumulation: products are below 2^62 and a folded accumulator below
+// 2^34, so three terms fit in 64 bits between folds; a fold follows every
+// third term of a round and the round's last term. The round loops stay
+// rolled: unrolled, the kernel outgrows the instruction cache.
 __global__ void __launch_bounds__(128) poseidon_constraints_kernel(const uint32_t* __restrict__ trace,
                                                                    const uint32_t* __restrict__ inter, uint32_t eval_log,
                                                                    uint32_t trace_log, ConstraintParams prm,
@@ -226,42 +230,54 @@ __global__ void __launch_bounds__(128) poseidon_constraints_kernel(const uint32_
   for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
     uint64_t acc[4] = {0, 0, 0, 0};
     uint32_t k = 0;  // constraint index
-    auto add_cons = [&](uint32_t c) {
+    // term i of the current round; folds after every third term and the last
+    auto add_cons = [&](uint32_t c, int i, int last) {
       const uint32_t* p = prm.powers + 4 * k;
 #pragma unroll
-      for (int q = 0; q < 4; q++) acc[q] = fold64a(acc[q] + (uint64_t)p[q] * c);
+      for (int q = 0; q < 4; q++) acc[q] += (uint64_t)p[q] * c;
+      if (i % 3 == 2 || i == last) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[q] = fold64a(acc[q]);
+      }
       k++;
     };
+    const uint32_t* col = trace + r;
     uint32_t s[16];
-    uint32_t col = 0;
 #pragma unroll
-    for (int i = 0; i < 16; i++) s[i] = __ldg(trace + (size_t)(col++) * n + r);
+    for (int i = 0; i < 16; i++) s[i] = __ldg(col + (size_t)i * n);
+    col += 16 * n;
+#pragma unroll 1
     for (int round = 0; round < 4; round++) {
 #pragma unroll
       for (int i = 0; i < 16; i++) s[i] = add(s[i], PN_RC);
       p2_external(s);
 #pragma unroll
       for (int i = 0; i < 16; i++) {
-        uint32_t m = __ldg(trace + (size_t)(col++) * n + r);
-        add_cons(sub(pow5(s[i]), m));
+        uint32_t m = __ldg(col);
+        col += n;
+        add_cons(sub(pow5(s[i]), m), i, 15);
         s[i] = m;
       }
     }
+#pragma unroll 1
     for (int round = 0; round < 14; round++) {
       s[0] = add(s[0], PN_RC);
       p2_internal(s);
-      uint32_t m = __ldg(trace + (size_t)(col++) * n + r);
-      add_cons(sub(pow5(s[0]), m));
+      uint32_t m = __ldg(col);
+      col += n;
+      add_cons(sub(pow5(s[0]), m), 0, 0);
       s[0] = m;
     }
+#pragma unroll 1
     for (int round = 0; round < 4; round++) {
 #pragma unroll
       for (int i = 0; i < 16; i++) s[i] = add(s[i], PN_RC);
       p2_external(s);
 #pragma unroll
       for (int i = 0; i < 16; i++) {
-        uint32_t m = __ldg(trace + (size_t)(col++) * n + r);
-        add_cons(sub(pow5(s[i]), m));
+        uint32_t m = __ldg(col);
+        col += n;
+        add_cons(sub(pow5(s[i]), m), i, 15);
         s[i] = m;
       }
     }

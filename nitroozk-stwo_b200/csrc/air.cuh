@@ -39,5 +39,18 @@ struct GatherItem {
 };
 int gather_words(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out);
 int gather_hashes(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out);
+// Values of n_cols columns at a list of positions, written position-major
+// (for each position, every column): columns given explicitly (n_cols <= 4)
+// or as base + c * stride.
+struct ColGather {
+  const uint32_t* cols[4];
+  const uint32_t* base;
+  uint64_t stride;
+  uint32_t n_cols, n_pos;
+  uint64_t pos_off;  // first position in the shared position list
+  uint64_t out_off;  // first output word
+};
+int gather_cols(cudaStream_t st, const ColGather* d_blocks, uint32_t n_blocks, uint32_t max_items,
+                const uint32_t* d_positions, uint32_t* d_out);
 
 }  // namespace gs

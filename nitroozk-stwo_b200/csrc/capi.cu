@@ -339,7 +339,8 @@ static int run_prove(gs_ctx* ctx, prover::ProveRequest& req, const gs_pcs_config
   GS_REQUIRE(req.input_mode <= 2, "unknown input mode");
   GS_REQUIRE(req.input_mode != 2 || req.host_inputs != nullptr, "host inputs required");
   GS_REQUIRE(req.cfg.pow_bits <= 32 && req.cfg.n_queries >= 1 && req.cfg.log_last_layer <= 10, "bad PCS config");
-  std::string bytes;
+  // reused per thread: the proof's pages are touched once, not per proof
+  static thread_local std::string bytes;
   int st = prover::prove_component(ctx->c, req, &bytes, nullptr);
   *proof_len = bytes.size();
   if (st != OK) {

@@ -10,55 +10,14 @@
 //
 // The host replays the same steps on the roots read back at the end of the
 // phase and checks every challenge against the device's.
-#include "runtime.cuh"
-#include "blake2s.cuh"
+#include "channel.cuh"
 
 namespace gs {
 
-// state: 8 digest words, n_draws, status (nonzero: no felt within the bound).
 __global__ void channel_mix_root_draw_kernel(uint32_t* state, const uint32_t* root, uint32_t* root_copy,
                                              uint32_t* felt_out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  uint32_t m[16], d[8];
-#pragma unroll
-  for (int j = 0; j < 8; j++) {
-    m[j] = state[j];
-    m[8 + j] = root[j];
-  }
-  blake2s_init(d);
-  blake2s_compress(d, m, 64, true);
-  if (root_copy)
-    for (int j = 0; j < 8; j++) root_copy[j] = root[j];
-  uint32_t n_draws = 0;
-  // A draw is rejected with probability < 2^-27; 64 rejections in a row do
-  // not happen for a hash, and running out is reported, never looped on.
-  for (int attempt = 0; attempt < 64; attempt++) {
-    uint32_t h[8];
-#pragma unroll
-    for (int j = 0; j < 8; j++) m[j] = d[j];
-    m[8] = n_draws;
-#pragma unroll
-    for (int j = 9; j < 16; j++) m[j] = 0;
-    blake2s_init(h);
-    blake2s_compress(h, m, 37, true);
-    n_draws++;
-    bool ok = true;
-#pragma unroll
-    for (int j = 0; j < 8; j++) ok = ok && h[j] < 2u * P;
-    if (ok) {
-      qm31 a = qm_make(h[0] >= P ? h[0] - P : h[0], h[1] >= P ? h[1] - P : h[1], h[2] >= P ? h[2] - P : h[2],
-                       h[3] >= P ? h[3] - P : h[3]);
-      qm31 a2 = qm_mul(a, a);
-      felt_out[0] = a.x.a; felt_out[1] = a.x.b; felt_out[2] = a.y.a; felt_out[3] = a.y.b;
-      felt_out[4] = a2.x.a; felt_out[5] = a2.x.b; felt_out[6] = a2.y.a; felt_out[7] = a2.y.b;
-      for (int j = 0; j < 8; j++) state[j] = d[j];
-      state[8] = n_draws;
-      return;
-    }
-  }
-  for (int j = 0; j < 8; j++) state[j] = d[j];
-  state[8] = n_draws;
-  state[9] = 1;
+  channel_mix_root_draw_dev(state, root, root_copy, felt_out);
 }
 
 int channel_mix_root_draw(cudaStream_t st, uint32_t* d_state, const uint32_t* d_root, uint32_t* d_root_copy,

@@ -204,6 +204,152 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const uint32_t* const* __
   }
 }
 
+// ---------------------------------------------------------------------------
+// Geometry-specialised pass: the same index mapping as fft_pass_kernel with
+// L (layers) and C (contiguous low bits) fixed at compile time, so every
+// stage's window, shift and shared-memory offset is a constant:
+//  * shared memory is padded (word e at e + e/32) instead of XOR-swizzled;
+//    for disjoint bit fields the padding is additive, so the offset of
+//    element q folds into the load/store's immediate and each access costs
+//    no address arithmetic — and every access pattern of the pass stays
+//    bank-conflict free (bank = lane);
+//  * the first add of every field add/sub is an IMAD with a runtime 1 / -1
+//    (the integer ALU pipe is the bottleneck of the butterfly; IMAD runs on
+//    the FMA pipe), leaving one add-then-min (VIADDMNMX) per add/sub on the
+//    ALU pipe.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t imad_u32(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+  return r;
+}
+// a + b (one = 1 at run time)
+__device__ __forceinline__ uint32_t add_f(uint32_t a, uint32_t b, uint32_t one) {
+  uint32_t s = imad_u32(a, one, b);
+  return __viaddmin_u32(s, 0u - P, s);
+}
+// a - b (neg1 = 2^32 - 1 at run time)
+__device__ __forceinline__ uint32_t sub_f(uint32_t a, uint32_t b, uint32_t neg1) {
+  uint32_t d = imad_u32(b, neg1, a);
+  return __viaddmin_u32(d, P, d);
+}
+template <bool INV>
+__device__ __forceinline__ void bfly_f(uint32_t& a, uint32_t& b, uint32_t w, uint32_t one, uint32_t neg1) {
+  if (INV) {
+    uint32_t t0 = a;
+    a = add_f(t0, b, one);
+    b = mul(sub_f(t0, b, neg1), w);
+  } else {
+    uint32_t t0 = mul(b, w);
+    b = sub_f(a, t0, neg1);
+    a = add_f(a, t0, one);
+  }
+}
+__host__ __device__ constexpr uint32_t padw(uint32_t e) { return e + (e >> 5); }
+
+template <bool INV, int L, int C>
+__global__ void __launch_bounds__(256) fft_tile_kernel(const uint32_t* const* __restrict__ src_tab,
+                                                       uint32_t* const* __restrict__ dst_tab,
+                                                       const uint32_t* __restrict__ tw, FftPass a, uint32_t one,
+                                                       uint32_t neg1) {
+  extern __shared__ uint32_t sm[];
+  constexpr int R = 5, NQ = 32;
+  constexpr int T = L + C;
+  constexpr int K = (L + R - 1) / R;
+  constexpr int TPT_LOG = T - R;
+  constexpr uint32_t CMASK = (1u << C) - 1u;
+  const uint32_t col = blockIdx.y;
+  const uint32_t* __restrict__ src = src_tab[col];
+  uint32_t* __restrict__ dst = dst_tab[col];
+  const uint32_t ltid = threadIdx.x & ((1u << TPT_LOG) - 1u);
+  const uint32_t sub_tile = threadIdx.x >> TPT_LOG;
+  const uint32_t tile = (blockIdx.x << a.tile_shift) | sub_tile;
+  const uint32_t ml = a.lo - C;
+  const uint32_t midlow = tile & ((1u << ml) - 1u);
+  const uint32_t hi = tile >> ml;
+  const uint32_t basev = (hi << (a.lo + L)) | (midlow << C);
+  const uint32_t tile_pad = padw(sub_tile << T);
+  uint32_t x[NQ];
+
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const int s0 = INV ? ((k + 1 < K) ? C + k * R : T - R) : ((k + 1 < K) ? T - (k + 1) * R : C);
+    const int ja = INV ? ((k + 1 < K) ? 0 : C + k * R - s0) : 0;
+    const int jb = INV ? R : ((k + 1 < K) ? R : T - k * R - C);
+    const uint32_t ebase = ((ltid >> s0) << (s0 + R)) | (ltid & ((1u << s0) - 1u));
+    const uint32_t pbase = tile_pad + padw(ebase);
+    // global offset of element q relative to q = 0 (bits of q << s0 above C
+    // move up to the pass's layer bits)
+    const uint32_t gbase = basev | ((ebase >> C) << a.lo) | (ebase & CMASK);
+    if (k == 0) {
+      if (C == 0 && s0 == 0 && a.vec_ok && a.src_mask == 0xffffffffu) {
+        const uint4* p = reinterpret_cast<const uint4*>(src + gbase);
+#pragma unroll
+        for (int g = 0; g < NQ / 4; g++) {
+          uint4 v = __ldg(p + g);
+          x[4 * g] = v.x; x[4 * g + 1] = v.y; x[4 * g + 2] = v.z; x[4 * g + 3] = v.w;
+        }
+      } else {
+        // s0 >= C in every stage, so element q sits at gbase + q * 2^(s0-C+lo);
+        // with the LDE mask, (gbase | off) & mask = (gbase & mask) + (off & mask)
+        const uint32_t* p0 = src + (gbase & a.src_mask);
+        const uint32_t stride = 1u << (s0 - C + a.lo);
+        if (a.src_mask == 0xffffffffu) {
+#pragma unroll
+          for (int q = 0; q < NQ; q++) x[q] = __ldg(p0 + (size_t)((uint32_t)q * stride));
+        } else {
+#pragma unroll
+          for (int q = 0; q < NQ; q++) x[q] = __ldg(p0 + (((uint32_t)q * stride) & a.src_mask));
+        }
+      }
+    } else {
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < NQ; q++) x[q] = sm[pbase + padw((uint32_t)q << s0)];
+      __syncthreads();
+    }
+#pragma unroll
+    for (int jj = 0; jj < R; jj++) {
+      const int j = INV ? jj : (R - 1 - jj);
+      if (j < ja || j >= jb) continue;
+      const uint32_t i = a.lo + (uint32_t)(s0 + j - C);
+      const uint32_t hth = gbase >> (i + 1);
+      uint32_t w[NQ / 2];
+      switch (R - 1 - j) {
+        case 0: load_twiddles<1>(w, tw, a.tw_len, a.n, i, hth); break;
+        case 1: load_twiddles<2>(w, tw, a.tw_len, a.n, i, hth); break;
+        case 2: load_twiddles<4>(w, tw, a.tw_len, a.n, i, hth); break;
+        case 3: load_twiddles<8>(w, tw, a.tw_len, a.n, i, hth); break;
+        default: load_twiddles<16>(w, tw, a.tw_len, a.n, i, hth); break;
+      }
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        if (q & (1 << j)) continue;
+        bfly_f<INV>(x[q], x[q | (1 << j)], w[q >> (j + 1)], one, neg1);
+      }
+    }
+    if (k + 1 < K) {
+#pragma unroll
+      for (int q = 0; q < NQ; q++) sm[pbase + padw((uint32_t)q << s0)] = x[q];
+    } else {
+      if (a.has_scale) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) x[q] = mul(x[q], a.scale);
+      }
+      if (C == 0 && s0 == 0 && a.vec_ok) {
+        uint4* p = reinterpret_cast<uint4*>(dst + gbase);
+#pragma unroll
+        for (int g = 0; g < NQ / 4; g++) p[g] = make_uint4(x[4 * g], x[4 * g + 1], x[4 * g + 2], x[4 * g + 3]);
+      } else {
+        uint32_t* p0 = dst + gbase;
+        const uint32_t stride = 1u << (s0 - C + a.lo);
+#pragma unroll
+        for (int q = 0; q < NQ; q++) p0[(size_t)((uint32_t)q * stride)] = x[q];
+      }
+    }
+  }
+}
+
 // Domains of log size 1 and 2: closed forms of cpu/circle.rs:37-60 and
 // :193-208, with constants precomputed on the host.
 struct SmallFft {
@@ -325,6 +471,40 @@ static void launch_pass(cudaStream_t st, dim3 grid, uint32_t threads, size_t sme
   note_launch();
 }
 
+template <bool INV, int L, int C>
+static void launch_tile(cudaStream_t st, dim3 grid, uint32_t threads, const uint32_t* const* s, uint32_t* const* d,
+                        const uint32_t* tw, const FftPass& a) {
+  const uint32_t words = 1u << (a.t + a.tile_shift);
+  const size_t smem = (size_t)4 * (words + (words >> 5));
+  fft_tile_kernel<INV, L, C><<<grid, threads, smem, st>>>(s, d, tw, a, 1u, 0xffffffffu);
+  note_launch();
+}
+
+// The specialised kernel covers the partitions of the default tuning
+// (first pass C = 0 with 5..13 layers, later passes C = 4 with 5..9 layers);
+// anything else runs the generic pass. GS_FFT_GENERIC=1 forces the generic
+// pass (for comparisons).
+template <bool INV>
+static bool launch_tile_any(cudaStream_t st, dim3 grid, uint32_t threads, const uint32_t* const* s,
+                            uint32_t* const* d, const uint32_t* tw, const FftPass& a) {
+  static const bool generic = [] {
+    const char* e = getenv("GS_FFT_GENERIC");
+    return e && e[0] == '1';
+  }();
+  if (generic) return false;
+#define GS_TILE(LL, CC) \
+  case LL: launch_tile<INV, LL, CC>(st, grid, threads, s, d, tw, a); return true;
+  if (a.c == 0) {
+    switch (a.L) { GS_TILE(5, 0) GS_TILE(6, 0) GS_TILE(7, 0) GS_TILE(8, 0) GS_TILE(9, 0) GS_TILE(10, 0)
+                   GS_TILE(11, 0) GS_TILE(12, 0) GS_TILE(13, 0) default: return false; }
+  }
+  if (a.c == 4) {
+    switch (a.L) { GS_TILE(5, 4) GS_TILE(6, 4) GS_TILE(7, 4) GS_TILE(8, 4) GS_TILE(9, 4) default: return false; }
+  }
+#undef GS_TILE
+  return false;
+}
+
 // Column pointers of the current call are 16-byte aligned (checked by the
 // callers that know them on the host; the device tables are opaque here).
 static thread_local bool g_cols_aligned = true;
@@ -359,6 +539,10 @@ static int run_passes(cudaStream_t st, const uint32_t* const* src, uint32_t* con
     const size_t smem = (size_t)4 << (a.t + tile_shift);
     dim3 grid(1u << (tiles_log - tile_shift), n_cols);
     const uint32_t* const* s = (p == 0) ? src : (const uint32_t* const*)dst;
+    if (R == 5 && launch_tile_any<INV>(st, grid, threads, s, dst, tw, a)) {
+      GS_CUDA_TRY(cudaGetLastError());
+      continue;
+    }
     switch (R) {
       case 1: launch_pass<INV, 1>(st, grid, threads, smem, s, dst, tw, a); break;
       case 2: launch_pass<INV, 2>(st, grid, threads, smem, s, dst, tw, a); break;

@@ -16,6 +16,7 @@
 // its leaf hashes.
 #include "runtime.cuh"
 #include "blake2s.cuh"
+#include "channel.cuh"
 
 namespace gs {
 
@@ -27,6 +28,12 @@ __device__ __forceinline__ void leaf_hash4(uint32_t* leaf_out, size_t i, qm31 v)
   for (int j = 4; j < 16; j++) m[j] = 0;
   blake2s_compress(h, m, 16, true);
   uint4* o = reinterpret_cast<uint4*>(leaf_out + 8 * i);
+  o[0] = make_uint4(h[0], h[1], h[2], h[3]);
+  o[1] = make_uint4(h[4], h[5], h[6], h[7]);
+}
+
+__device__ __forceinline__ void store_hash8(uint32_t* out, size_t i, const uint32_t h[8]) {
+  uint4* o = reinterpret_cast<uint4*>(out + 8 * i);
   o[0] = make_uint4(h[0], h[1], h[2], h[3]);
   o[1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
@@ -154,6 +161,67 @@ int fold_circle_into_line_fused(cudaStream_t st, CPlanes src, uint32_t log_n, qm
 int fold_circle_into_line_dev_alpha(cudaStream_t st, CPlanes src, uint32_t log_n, const uint32_t* d_alpha, Planes dst,
                                     const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out) {
   return fold_circle_launch(st, src, log_n, qm_zero(), dst, d_itw, tw_log, leaf_out, d_alpha);
+}
+
+// Fused tail of the FRI commit phase: every layer of log size <= 11 in one
+// block of 1024 threads. For layer k (log size log0 - k, leaves already
+// hashed): its Merkle node layers, the channel step on its root (thread 0),
+// then fold_line into layer k + 1 with that layer's leaf hashes — the same
+// three steps the per-layer kernels run, with block barriers in place of
+// kernel boundaries. Data written inside the kernel is read with plain loads.
+__global__ void __launch_bounds__(1024) fri_tail_kernel(FriTail a, uint32_t* state, const uint32_t* __restrict__ itw,
+                                                        uint32_t tw_len) {
+  const uint32_t tid = threadIdx.x, bs = blockDim.x;
+  for (uint32_t k = 0; k < a.n; k++) {
+    const uint32_t log = a.log0 - k;
+    for (int L = (int)log - 1; L >= 0; L--) {
+      const uint32_t* prev = a.tree[k][L + 1];
+      uint32_t* out = a.tree[k][L];
+      for (uint32_t i = tid; i < (1u << L); i += bs) {
+        uint32_t h[8], m[16];
+        blake2s_init(h);
+        const uint4* pp = reinterpret_cast<const uint4*>(prev + 16 * i);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          uint4 v = pp[q];
+          m[4 * q] = v.x; m[4 * q + 1] = v.y; m[4 * q + 2] = v.z; m[4 * q + 3] = v.w;
+        }
+        blake2s_compress(h, m, 64, true);
+        store_hash8(out, i, h);
+      }
+      __syncthreads();
+    }
+    if (tid == 0) channel_mix_root_draw_dev(state, a.tree[k][0], a.roots + 8 * k, a.felts + 8 * k);
+    __syncthreads();
+    const uint32_t* f = a.felts + 8 * k;
+    const qm31 alpha = qm_make(f[0], f[1], f[2], f[3]);
+    const size_t half = (size_t)1 << (log - 1);
+    const uint32_t* lvl = itw + (tw_len - (1u << log));
+    uint32_t* const* sp = a.planes[k];
+    uint32_t* const* dp = a.planes[k + 1];
+    uint32_t* leaves = (k + 1 < a.n) ? a.tree[k + 1][log - 1] : nullptr;
+    for (uint32_t i = tid; i < half; i += bs) {
+      qm31 fx = qm_make(sp[0][2 * i], sp[1][2 * i], sp[2][2 * i], sp[3][2 * i]);
+      qm31 fnx = qm_make(sp[0][2 * i + 1], sp[1][2 * i + 1], sp[2][2 * i + 1], sp[3][2 * i + 1]);
+      uint32_t xinv = __ldg(lvl + i);
+      qm31 f0 = qm_add(fx, fnx);
+      qm31 f1 = qm_mul_m31(qm_sub(fx, fnx), xinv);
+      qm31 r = qm_add(f0, qm_mul(alpha, f1));
+      dp[0][i] = r.x.a; dp[1][i] = r.x.b; dp[2][i] = r.y.a; dp[3][i] = r.y.b;
+      if (leaves) leaf_hash4(leaves, i, r);
+    }
+    __syncthreads();
+  }
+}
+
+int fri_tail(cudaStream_t st, const FriTail& a, uint32_t* d_state, const uint32_t* d_itw, uint32_t tw_log) {
+  GS_REQUIRE(a.n >= 1 && a.n <= FRI_TAIL_MAX && a.log0 <= FRI_TAIL_MAX - 1 && a.log0 >= a.n,
+             "FRI tail: layer sizes out of range");
+  GS_REQUIRE(a.log0 <= tw_log, "FRI tail: line domain must fit the twiddle tree");
+  fri_tail_kernel<<<1, 1024, 0, st>>>(a, d_state, d_itw, 1u << tw_log);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
 }
 
 int fold_line(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itwiddles,

@@ -23,6 +23,29 @@ __global__ void gather_hashes_kernel(const GatherItem* __restrict__ items, size_
   }
 }
 
+// grid.y = descriptor, grid.x covers its n_pos * n_cols outputs.
+__global__ void gather_cols_kernel(const ColGather* __restrict__ blocks, const uint32_t* __restrict__ positions,
+                                   uint32_t* __restrict__ out) {
+  const ColGather b = blocks[blockIdx.y];
+  const uint32_t n = b.n_pos * b.n_cols;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const uint32_t p = t / b.n_cols, c = t - p * b.n_cols;
+    const uint32_t* src = b.n_cols <= 4 ? b.cols[c] : b.base + c * b.stride;
+    out[b.out_off + t] = __ldg(src + positions[b.pos_off + p]);
+  }
+}
+
+int gather_cols(cudaStream_t st, const ColGather* d_blocks, uint32_t n_blocks, uint32_t max_items,
+                const uint32_t* d_positions, uint32_t* d_out) {
+  if (n_blocks == 0 || max_items == 0) return OK;
+  GS_REQUIRE(n_blocks <= 65535, "too many gather descriptors");
+  dim3 grid((max_items + 255) / 256 < 64 ? (max_items + 255) / 256 : 64, n_blocks);
+  gather_cols_kernel<<<grid, 256, 0, st>>>(d_blocks, d_positions, d_out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
 int gather_words(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out) {
   if (n == 0) return OK;
   unsigned blocks = (unsigned)((n + 255) / 256);

@@ -12,6 +12,7 @@
 // read as 4 x 16-byte vector loads. No byte-wise buffering.
 #include "runtime.cuh"
 #include "blake2s.cuh"
+#include <cstdlib>
 
 namespace gs {
 
@@ -21,9 +22,11 @@ __device__ __forceinline__ void store_hash(uint32_t* out, size_t i, const uint32
   o[1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
 
+// FMA: adds of the compression on the FMA pipe (blake2s_compress_f).
+template <bool FMA>
 __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, const uint32_t* __restrict__ prev,
                                                            const uint32_t* const* __restrict__ cols, uint32_t n_cols,
-                                                           uint32_t* __restrict__ out) {
+                                                           uint32_t* __restrict__ out, uint32_t one) {
   const size_t n = (size_t)1 << log_size;
   const uint32_t prev_words = prev ? 16u : 0u;
   const uint32_t total_words = prev_words + n_cols;
@@ -44,7 +47,8 @@ __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, co
       m[12] = d.x; m[13] = d.y; m[14] = d.z; m[15] = d.w;
       blk = 1;
       uint32_t t = total_bytes < 64u ? total_bytes : 64u;
-      blake2s_compress(h, m, t, n_blocks == 1);
+      if (FMA) blake2s_compress_f(h, m, t, n_blocks == 1, one);
+      else blake2s_compress(h, m, t, n_blocks == 1);
     }
     for (; blk < n_blocks; blk++) {
 #pragma unroll
@@ -55,7 +59,8 @@ __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, co
       col += 16;
       uint32_t t = 64u * (blk + 1);
       if (t > total_bytes) t = total_bytes;
-      blake2s_compress(h, m, t, blk + 1 == n_blocks);
+      if (FMA) blake2s_compress_f(h, m, t, blk + 1 == n_blocks, one);
+      else blake2s_compress(h, m, t, blk + 1 == n_blocks);
     }
     store_hash(out, i, h);
   }
@@ -72,14 +77,21 @@ int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, 
   size_t blocks = (n + threads - 1) / threads;
   size_t cap = (size_t)num_sms() * 8;
   if (blocks > cap) blocks = cap;
-  merkle_layer_kernel<<<(unsigned)blocks, threads, 0, st>>>(log_size, d_prev, d_cols, n_cols, d_out);
+  static const bool alu_only = [] {
+    const char* e = getenv("GS_BLAKE_ALU");
+    return e && e[0] == '1';
+  }();
+  if (alu_only)
+    merkle_layer_kernel<false><<<(unsigned)blocks, threads, 0, st>>>(log_size, d_prev, d_cols, n_cols, d_out, 1u);
+  else
+    merkle_layer_kernel<true><<<(unsigned)blocks, threads, 0, st>>>(log_size, d_prev, d_cols, n_cols, d_out, 1u);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;
 }
 
 // Node-only layers of a small subtree in one block: starting from the layer
-// of log size `top_log` (<= 11, already in memory), computes every layer
+// of log size `top_log` (<= MERKLE_TAIL_LOG, already in memory), computes every layer
 // down to the root, each node = Blake2s(left || right) (no columns injected
 // at these layers). Layer L is written to layers.p[L]; one launch replaces
 // top_log launches of the per-layer kernel.
@@ -107,9 +119,15 @@ __global__ void __launch_bounds__(1024) merkle_tail_kernel(uint32_t top_log, Lay
 
 int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers) {
   GS_REQUIRE(top_log <= 30, "layer log size out of range");
-  // per-layer kernel down to 2^11 nodes, then one block for the rest
-  int L = (int)top_log - 1;
-  for (; L >= 11; L--) GS_TRY(commit_on_layer(st, (uint32_t)L, layers[L + 1], nullptr, 0, layers[L]));
+  // Layers of 2^8 nodes and more: one full-GPU launch each. A single block
+  // computes the rest: below 2^8 nodes a level is latency-bound, above it
+  // one SM's throughput would be the limit.
+  uint32_t top = top_log;
+  while (top > MERKLE_TAIL_LOG) {
+    GS_TRY(commit_on_layer(st, top - 1, layers[top], nullptr, 0, layers[top - 1]));
+    top--;
+  }
+  int L = (int)top - 1;
   uint32_t tail_top = (uint32_t)(L + 1);
   if (tail_top == 0) return OK;
   LayerPtrs lp{};

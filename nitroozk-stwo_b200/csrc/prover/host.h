@@ -227,18 +227,28 @@ struct Proof {
 // Option as a 1-byte tag, hash = 32 raw bytes, QM31 = 4 x u32; field order of
 // CommitmentSchemeProof (config, commitments, sampled_values, decommitments,
 // queried_values, proof_of_work, fri_proof).
+static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "proof serialization assumes a little-endian host");
+// Two passes over the proof: the first only counts bytes, the second writes
+// them into an output string sized once (callers that reuse the string keep
+// its pages from proof to proof).
 struct Writer {
-  std::string b;
-  void u8(uint8_t v) { b.push_back((char)v); }
-  void u32(uint32_t v) { for (int i = 0; i < 4; i++) b.push_back((char)(v >> (8 * i))); }
-  void u64(uint64_t v) { for (int i = 0; i < 8; i++) b.push_back((char)(v >> (8 * i))); }
-  void hash(const Hash& h) { b.append((const char*)h.data(), 32); }
+  char* out = nullptr;  // null: counting pass
+  size_t len = 0;
+  void put(const void* p, size_t n) {
+    if (out) memcpy(out + len, p, n);
+    len += n;
+  }
+  void u8(uint8_t v) { put(&v, 1); }
+  void u32(uint32_t v) { put(&v, 4); }
+  void u64(uint64_t v) { put(&v, 8); }
+  void hash(const Hash& h) { put(h.data(), 32); }
   void qm(const qm31& q) { u32(q.x.a); u32(q.x.b); u32(q.y.a); u32(q.y.b); }
   void dec(const Decommitment& d) {
     u64(d.hash_witness.size());
-    for (auto& h : d.hash_witness) hash(h);
+    static_assert(sizeof(Hash) == 32, "Hash is 32 contiguous bytes");
+    if (!d.hash_witness.empty()) put(d.hash_witness.data(), 32 * d.hash_witness.size());
     u64(d.column_witness.size());
-    for (auto v : d.column_witness) u32(v);
+    if (!d.column_witness.empty()) put(d.column_witness.data(), 4 * d.column_witness.size());
   }
   void layer(const FriLayerProof& l) {
     u64(l.fri_witness.size());
@@ -248,8 +258,7 @@ struct Writer {
   }
 };
 
-inline std::string serialize(const Proof& p) {
-  Writer w;
+inline void write_proof(Writer& w, const Proof& p) {
   w.u32(p.pow_bits);
   w.u32(p.log_blowup);
   w.u32(p.log_last_layer);
@@ -271,7 +280,7 @@ inline std::string serialize(const Proof& p) {
   w.u64(p.queried_values.size());
   for (auto& t : p.queried_values) {
     w.u64(t.size());
-    for (auto v : t) w.u32(v);
+    if (!t.empty()) w.put(t.data(), 4 * t.size());
   }
   w.u64(p.proof_of_work);
   w.layer(p.fri_first);
@@ -280,7 +289,21 @@ inline std::string serialize(const Proof& p) {
   w.u64(p.last_layer.size());
   for (auto& q : p.last_layer) w.qm(q);
   w.u32(p.last_layer_log);
-  return w.b;
+}
+
+inline void serialize_into(const Proof& p, std::string& out) {
+  Writer count;
+  write_proof(count, p);
+  out.resize(count.len);
+  Writer w;
+  w.out = count.len ? &out[0] : nullptr;
+  write_proof(w, p);
+}
+
+inline std::string serialize(const Proof& p) {
+  std::string s;
+  serialize_into(p, s);
+  return s;
 }
 
 }  // namespace host

@@ -82,6 +82,27 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
                                          pv.itw, pv.tw_log, cur.log > last_log ? cur.layers[cur.log] : nullptr));
   uint32_t k = 1;
   while (cur.log > last_log) {
+    if (cur.log <= FRI_TAIL_LOG) {
+      // every remaining layer in one fused launch
+      FriTail ft;
+      ft.log0 = cur.log;
+      ft.n = cur.log - last_log;
+      ft.roots = d_roots + 8 * k;
+      ft.felts = d_felts + 8 * k;
+      std::vector<FriLayerDev> rest(ft.n + 1);
+      rest[0] = std::move(cur);
+      for (uint32_t j = 1; j <= ft.n; j++) take_layer(rest[j], rest[0].log - j);
+      for (uint32_t j = 0; j <= ft.n; j++) {
+        for (int c = 0; c < 4; c++) ft.planes[j][c] = rest[j].planes[c];
+        if (j < ft.n)
+          for (uint32_t L = 0; L <= rest[j].log; L++) ft.tree[j][L] = rest[j].layers[L];
+      }
+      GS_TRY(fri_tail(st, ft, ctl, pv.itw, pv.tw_log));
+      for (uint32_t j = 0; j < ft.n; j++) inner.push_back(std::move(rest[j]));
+      cur = std::move(rest[ft.n]);
+      k += ft.n;
+      break;
+    }
     GS_TRY(commit_node_layers(st, cur.log, cur.layers.data()));
     GS_TRY(channel_mix_root_draw(st, ctl, cur.layers[0], d_roots + 8 * k, d_felts + 8 * k));
     FriLayerDev next;

@@ -3,6 +3,7 @@
 // check (crates/stwo/src/prover/mod.rs:50-150, prover/pcs/mod.rs:151-357).
 #include "prover_impl.h"
 #include "prove_api.h"
+#include <future>
 
 namespace gs {
 namespace prover {
@@ -89,6 +90,27 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     for (auto& c : tr) flat.insert(flat.end(), c.values.begin(), c.values.end());
   pv.ch.mix_felts(flat);
   pv.mark("oods_sample");
+  // Sanity check (composition at the OODS point vs the constraints evaluated
+  // from the mask values) on a host thread, overlapping the device work of
+  // the quotients, FRI and the proof of work.
+  std::vector<std::vector<std::vector<qm31>>> sv(n_trees);
+  for (size_t t = 0; t < n_trees; t++)
+    for (auto& cs : samples[t]) sv[t].push_back(cs.values);
+  std::future<bool> sanity = std::async(std::launch::async, [&air, sv = std::move(sv), split, oods, E, max_ldb,
+                                                            random_coeff]() {
+    auto& cv = sv.back();
+    qm31 total = qm_zero();
+    for (uint32_t t = 0; t < (1u << split); t++) {
+      qm31 e4[4] = {cv[4 * t][0], cv[4 * t + 1][0], cv[4 * t + 2][0], cv[4 * t + 3][0]};
+      qm31 v = from_partial_evals(e4);
+      for (uint32_t b = 0; b < split; b++)
+        if ((t >> b) & 1) v = qm_mul(v, host::ptq_rep_double(oods, E - split + b - 1).x);
+      total = qm_add(total, v);
+    }
+    qm31 dinv = qm_inv(host::canonic_vanishing(max_ldb, oods));
+    qm31 cons = eval_at_point(air, sv, random_coeff, dinv);
+    return qm_eq(total, cons);
+  });
   // DEEP quotients: per (column size, point) batches of line-coefficient
   // terms, lifted per point, combined over the lifting domain.
   qm31 qrc = pv.ch.draw_felt();
@@ -217,16 +239,14 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     size_t val_base = 0;
     MerkleDecommitPlan merkle;
   };
-  auto plan_fri = [&](FriLayerDev& L, const std::vector<size_t>& q, FriPlan& fp) {
+  auto plan_fri = [&](FriLayerDev& L, const std::vector<size_t>& q, FriPlan& fp) -> int {
     fri_positions(q, fp.pos, fp.wit);
-    fp.val_base = g.words.size();
-    for (size_t p : fp.pos)
-      for (int c = 0; c < 4; c++) g.add_word(L.planes[c], p);
     std::vector<const uint32_t*> cols = {L.planes[0], L.planes[1], L.planes[2], L.planes[3]};
-    fp.merkle.plan(g, L.layers, cols, fp.pos);
+    GS_TRY(g.add_cols(cols, fp.pos, &fp.val_base));
+    return fp.merkle.plan(g, L.layers, cols, fp.pos, false);
   };
   FriPlan first_plan;
-  plan_fri(first, queries, first_plan);
+  GS_TRY(plan_fri(first, queries, first_plan));
   std::vector<FriPlan> inner_plans(inner.size());
   std::vector<size_t> lq = queries;
   for (size_t i = 0; i < inner.size(); i++) {
@@ -234,7 +254,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     for (size_t q : lq)
       if (f.empty() || f.back() != (q >> 1)) f.push_back(q >> 1);
     lq = f;
-    plan_fri(inner[i], lq, inner_plans[i]);
+    GS_TRY(plan_fri(inner[i], lq, inner_plans[i]));
   }
   std::vector<MerkleDecommitPlan> tree_plans(n_trees);
   for (size_t t = 0; t < n_trees; t++) {
@@ -243,7 +263,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     std::vector<size_t> pos = prepare_positions(queries, lifting, tr.max_log());
     std::vector<const uint32_t*> cols;
     for (uint32_t c = 0; c < tr.n_cols; c++) cols.push_back(tr.eval_col(c));
-    tree_plans[t].plan(g, tr.layers, cols, pos);
+    GS_TRY(tree_plans[t].plan(g, tr.layers, cols, pos));
   }
   pv.mark("decommit_plan");
   GS_TRY(g.run(pv.ctx, pv.A));
@@ -281,22 +301,12 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     for (auto& cs : samples[t]) P.sampled_values[t].push_back(cs.values);
     if (tr.n_cols) tree_plans[t].assemble(g, P.queried_values[t], P.decommitments[t]);
   }
-  // sanity check: composition at the OODS point vs constraints from the mask
-  auto& cv = P.sampled_values.back();
-  qm31 total = qm_zero();
-  for (uint32_t t = 0; t < (1u << split); t++) {
-    qm31 e4[4] = {cv[4 * t][0], cv[4 * t + 1][0], cv[4 * t + 2][0], cv[4 * t + 3][0]};
-    qm31 v = from_partial_evals(e4);
-    for (uint32_t b = 0; b < split; b++)
-      if ((t >> b) & 1) v = qm_mul(v, host::ptq_rep_double(oods, E - split + b - 1).x);
-    total = qm_add(total, v);
-  }
-  qm31 dinv = qm_inv(host::canonic_vanishing(max_ldb, oods));
-  qm31 cons = eval_at_point(air, P.sampled_values, random_coeff, dinv);
-  if (stats) stats->constraint_check = qm_eq(total, cons) ? 1.0 : 0.0;
+  const bool sane = sanity.get();
+  if (stats) stats->constraint_check = sane ? 1.0 : 0.0;
   pv.mark("sanity_check");
-  *proof_bytes = host::serialize(P);
-  if (!qm_eq(total, cons)) {
+  host::serialize_into(P, *proof_bytes);
+  pv.mark("serialize");
+  if (!sane) {
     set_error("constraints not satisfied: composition OODS value differs from the constraints at the mask");
     return ERR_PROOF;
   }

@@ -60,34 +60,80 @@ struct Tree {
   const uint32_t* eval_col(uint32_t c) const { return evals + ((size_t)c << eval_log); }
 };
 
-// Batched device gathers for decommitments: items are queued on the host,
-// fetched with one launch per kind and read back with one copy.
+// Batched device gathers for decommitments: column values are described per
+// (column set, sorted positions) block and expanded on the device; hash
+// witnesses are (layer, index) items. One launch per kind, one read-back.
 struct GatherPlan {
-  std::vector<GatherItem> words, hashes;
+  std::vector<ColGather> blocks;
+  std::vector<uint32_t> positions;
+  std::vector<GatherItem> hashes;
+  size_t n_words = 0;
+  uint32_t max_items = 0;
   std::vector<uint32_t> word_out, hash_out;
-  size_t add_word(const uint32_t* src, size_t idx) { words.push_back({src, idx}); return words.size() - 1; }
+  // Values of `cols` at `pos`, position-major; returns the first output word.
+  // More than 4 columns must be equally spaced (one tree's columns are).
+  int add_cols(const std::vector<const uint32_t*>& cols, const std::vector<size_t>& pos, size_t* first) {
+    ColGather b{};
+    b.n_cols = (uint32_t)cols.size();
+    b.n_pos = (uint32_t)pos.size();
+    b.pos_off = positions.size();
+    b.out_off = n_words;
+    if (b.n_cols <= 4) {
+      for (uint32_t c = 0; c < b.n_cols; c++) b.cols[c] = cols[c];
+    } else {
+      b.base = cols[0];
+      b.stride = (uint64_t)(cols[1] - cols[0]);
+      for (uint32_t c = 2; c < b.n_cols; c++)
+        GS_REQUIRE((uint64_t)(cols[c] - cols[0]) == c * b.stride, "decommitted columns are not equally spaced");
+    }
+    for (size_t p : pos) positions.push_back((uint32_t)p);
+    *first = n_words;
+    n_words += (size_t)b.n_cols * b.n_pos;
+    max_items = std::max<uint32_t>(max_items, b.n_cols * b.n_pos);
+    if (b.n_cols && b.n_pos) blocks.push_back(b);
+    return OK;
+  }
   size_t add_hash(const uint32_t* src, size_t idx) { hashes.push_back({src, idx}); return hashes.size() - 1; }
+  template <class T>
+  static int upload(Context& ctx, T* dst, const std::vector<T>& v) {
+    const size_t bytes = v.size() * sizeof(T);
+    if (!bytes) return OK;
+    if (bytes <= ctx.ring_cap / 2) {  // through the pinned staging ring
+      const void* d = nullptr;
+      GS_TRY(ctx.stage_bytes(v.data(), bytes, &d));
+      GS_CUDA_TRY(cudaMemcpyAsync(dst, d, bytes, cudaMemcpyDeviceToDevice, ctx.stream));
+    } else {
+      GS_CUDA_TRY(cudaMemcpyAsync(dst, v.data(), bytes, cudaMemcpyHostToDevice, ctx.stream));
+    }
+    return OK;
+  }
   int run(Context& ctx, Arena& A) {
     cudaStream_t st = ctx.stream;
-    size_t nw = words.size(), nh = hashes.size();
-    GatherItem *d_items = nullptr;
+    const size_t nh = hashes.size();
+    ColGather* d_blocks = nullptr;
+    uint32_t* d_pos = nullptr;
+    GatherItem* d_items = nullptr;
     uint32_t* d_out = nullptr;
     // hashes are written as 16-byte vectors: their region starts at a
     // multiple of 4 words
-    const size_t hbase = (nw + 3) & ~(size_t)3;
-    GS_TRY(A.alloc_n(nw + nh + 1, &d_items));
+    const size_t hbase = (n_words + 3) & ~(size_t)3;
+    GS_TRY(A.alloc_n(blocks.size() + 1, &d_blocks));
+    GS_TRY(A.alloc_n(positions.size() + 1, &d_pos));
+    GS_TRY(A.alloc_n(nh + 1, &d_items));
     GS_TRY(A.alloc_n(hbase + 8 * nh + 4, &d_out));
-    std::vector<GatherItem> all(words);
-    all.insert(all.end(), hashes.begin(), hashes.end());
-    if (!all.empty())
-      GS_CUDA_TRY(cudaMemcpyAsync(d_items, all.data(), all.size() * sizeof(GatherItem), cudaMemcpyHostToDevice, st));
-    GS_TRY(gather_words(st, d_items, nw, d_out));
-    GS_TRY(gather_hashes(st, d_items + nw, nh, d_out + hbase));
-    std::vector<uint32_t> out(hbase + 8 * nh);
-    if (!out.empty()) GS_CUDA_TRY(cudaMemcpyAsync(out.data(), d_out, out.size() * 4, cudaMemcpyDeviceToHost, st));
+    GS_TRY(upload(ctx, d_blocks, blocks));
+    GS_TRY(upload(ctx, d_pos, positions));
+    GS_TRY(upload(ctx, d_items, hashes));
+    GS_TRY(gather_cols(st, d_blocks, (uint32_t)blocks.size(), max_items, d_pos, d_out));
+    GS_TRY(gather_hashes(st, d_items, nh, d_out + hbase));
+    const size_t out_words = hbase + 8 * nh;
+    void* hr = nullptr;
+    GS_TRY(ctx.read_buffer(out_words * 4, &hr));
+    if (out_words) GS_CUDA_TRY(cudaMemcpyAsync(hr, d_out, out_words * 4, cudaMemcpyDeviceToHost, st));
     GS_CUDA_TRY(cudaStreamSynchronize(st));
-    word_out.assign(out.begin(), out.begin() + nw);
-    hash_out.assign(out.begin() + hbase, out.end());
+    const uint32_t* o = (const uint32_t*)hr;
+    word_out.assign(o, o + n_words);
+    hash_out.assign(o + hbase, o + out_words);
     return OK;
   }
   host::Hash hash(size_t slot) const { return host::hash_from_words(hash_out.data() + 8 * slot); }
@@ -102,13 +148,12 @@ struct MerkleDecommitPlan {
   std::vector<size_t> positions;
   size_t value_base = 0, n_cols = 0;
   std::vector<size_t> hash_slots;
-  void plan(GatherPlan& g, const std::vector<uint32_t*>& layers, const std::vector<const uint32_t*>& cols,
-            const std::vector<size_t>& pos) {
+  // with_values = false: the caller gathers the queried values itself.
+  int plan(GatherPlan& g, const std::vector<uint32_t*>& layers, const std::vector<const uint32_t*>& cols,
+           const std::vector<size_t>& pos, bool with_values = true) {
     positions = pos;
-    n_cols = cols.size();
-    value_base = g.words.size();
-    for (size_t node : pos)
-      for (auto* c : cols) g.add_word(c, node);
+    n_cols = with_values ? cols.size() : 0;
+    if (with_values) GS_TRY(g.add_cols(cols, pos, &value_base));
     // positions are sorted and unique at every layer, so membership of a
     // sibling is a linear merge against the previous layer's list
     std::vector<size_t> prev = pos, merged;
@@ -124,10 +169,15 @@ struct MerkleDecommitPlan {
         }
       prev.swap(merged);
     }
+    return OK;
   }
   void assemble(const GatherPlan& g, std::vector<uint32_t>& queried, host::Decommitment& d) const {
     queried.assign(g.word_out.begin() + value_base, g.word_out.begin() + value_base + positions.size() * n_cols);
-    for (size_t s : hash_slots) d.hash_witness.push_back(g.hash(s));
+    d.hash_witness.reserve(d.hash_witness.size() + hash_slots.size());
+    for (size_t s : hash_slots) {
+      d.hash_witness.emplace_back();
+      memcpy(d.hash_witness.back().data(), g.hash_out.data() + 8 * s, 32);
+    }
   }
 };
 

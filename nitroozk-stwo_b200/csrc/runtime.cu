@@ -66,6 +66,9 @@ void Context::destroy() {
   if (d_ring) cudaFree(d_ring);
   if (d_small) cudaFree(d_small);
   if (h_small) cudaFreeHost(h_small);
+  if (h_read) cudaFreeHost(h_read);
+  h_read = nullptr;
+  read_cap = 0;
   if (own_stream && stream) cudaStreamDestroy(stream);
   h_ring = d_ring = d_small = h_small = nullptr;
   stream = nullptr;
@@ -91,6 +94,22 @@ int Context::stage_ptrs(const void* const* host_ptrs, size_t n, const void* cons
   const void* d = nullptr;
   GS_TRY(stage_bytes(host_ptrs, n * sizeof(void*), &d));
   *out = (const void* const*)d;
+  return OK;
+}
+
+int Context::read_buffer(size_t bytes, void** out) {
+  if (bytes > read_cap) {
+    if (h_read) {
+      GS_CUDA_TRY(cudaStreamSynchronize(stream));
+      cudaFreeHost(h_read);
+    }
+    h_read = nullptr;
+    read_cap = 0;
+    size_t cap = bytes < (1u << 20) ? (1u << 20) : bytes + bytes / 2;
+    GS_CUDA_TRY(cudaMallocHost((void**)&h_read, cap));
+    read_cap = cap;
+  }
+  *out = h_read;
   return OK;
 }
 

@@ -80,6 +80,10 @@ struct Context {
   uint8_t* h_small = nullptr;  // pinned mirror
   size_t small_cap = 0;
 
+  // growable pinned host buffer for read-backs (decommitment values)
+  uint8_t* h_read = nullptr;
+  size_t read_cap = 0;
+  int read_buffer(size_t bytes, void** out);
   // growable device scratch (stream ordered)
   void* scratch = nullptr;
   size_t scratch_cap = 0;
@@ -122,6 +126,23 @@ int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, 
                     uint32_t n_cols, uint32_t* d_out);
 // All node-only layers below `top_log` (layers[L] has 2^L hashes, layers[top_log] given).
 int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers);
+
+// FRI layers of log size <= 11 in one launch (fri.cu): layer k has log size
+// log0 - k; layers 0..n-1 are committed (tree[k][L] = their Merkle layers,
+// leaves of layer 0 already hashed), layer n is the last layer.
+constexpr uint32_t FRI_TAIL_MAX = 12;
+// Largest layer (log size) handled by the single-block tails: Merkle node
+// layers below it, and the fused FRI tail from it down.
+constexpr uint32_t MERKLE_TAIL_LOG = 8;
+constexpr uint32_t FRI_TAIL_LOG = 8;
+struct FriTail {
+  uint32_t n = 0, log0 = 0;
+  uint32_t* planes[FRI_TAIL_MAX + 1][4] = {};
+  uint32_t* tree[FRI_TAIL_MAX][FRI_TAIL_MAX] = {};
+  uint32_t* roots = nullptr;  // 8 words per committed layer
+  uint32_t* felts = nullptr;  // 8 words per committed layer (challenge, square)
+};
+int fri_tail(cudaStream_t st, const FriTail& a, uint32_t* d_state, const uint32_t* d_itw, uint32_t tw_log);
 
 // fri.cu
 int fold_line(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alpha, Planes dst, const uint32_t* d_itwiddles,

@@ -7,6 +7,7 @@ Mirrors the reference's example drivers cuda_prove_wide_fibonacci
 the generic prove(); the result is the serialised StarkProof.
 """
 import ctypes as C
+import threading
 
 import numpy as np
 
@@ -26,13 +27,27 @@ def pcs_config(pow_bits=10, log_blowup=1, log_last_layer=0, n_queries=70, line_f
     return L.PcsConfig(pow_bits, log_blowup, log_last_layer, n_queries, line_fold_step)
 
 
+_tls = threading.local()
+
+
+def _buffer(capacity):
+    """Per-thread output buffer, reused across proofs (a fresh multi-MB buffer
+    per call would cost its page faults every time)."""
+    buf = getattr(_tls, "buf", None)
+    if buf is None or len(buf) < capacity:
+        buf = (C.c_uint8 * capacity)()
+        _tls.buf = buf
+    return buf
+
+
 def _run(fn, args, ctx, capacity):
     n = C.c_size_t()
-    buf = (C.c_uint8 * capacity)()
+    buf = _buffer(capacity)
+    capacity = len(buf)
     st = fn(*args, C.cast(buf, C.c_void_p), capacity, C.byref(n))
     if st == 1 and n.value > capacity:  # retry with the exact size
-        buf = (C.c_uint8 * n.value)()
-        st = fn(*args, C.cast(buf, C.c_void_p), n.value, C.byref(n))
+        buf = _buffer(n.value)
+        st = fn(*args, C.cast(buf, C.c_void_p), len(buf), C.byref(n))
     if st == GS_ERR_PROOF:
         raise ConstraintsNotSatisfied(L.lib().gs_last_error().decode())
     L.check(st, fn.__name__)
