@@ -558,7 +558,7 @@ def proof_roofline(args, log_n, wl, ctx):
             traffic = json.load(open(tpath)).get("lde_%s_%d" % (wl, log_n))
         except Exception:
             traffic = None
-    return {"kernel": "fft_pass_kernel (LDE %d cols 2^%d -> 2^%d)" % (cols, log_n, target), "bound": "hbm",
+    return {"kernel": "fft_tile_kernel (LDE %d cols 2^%d -> 2^%d, 2 launches)" % (cols, log_n, target), "bound": "hbm",
             "achieved": round(achieved, 1), "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
             "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "algorithmic_bytes": alg,
             "avg_ms": round(ms, 4)}
@@ -705,8 +705,8 @@ def run_reference(args, world, rank):
 
 
 def run_case(args):
-    """One op on a small case, for ncu captures: `--case fft:26`, `--case lde:18:162` (blowup-2
-    extension of 162 columns), `--case merkle:20:64`, `--case fold:22`."""
+    """One op on a small case, for ncu captures: `--case fft:26`, `--case lde:18:162:2` (extension
+    of 162 columns from 2^18 to 2^20), `--case merkle:20:64`, `--case fold:22`."""
     import torch
     from gpustark.backend import GpuBackend as B, to_device, Context
     kind, *params = args.case.split(":")
@@ -720,10 +720,13 @@ def run_case(args):
         work = lambda: (B.evaluate_polynomials([x], n, tw, out=[y], ctx=ctx), B.interpolate_columns([y], n, tw, ctx=ctx))
     elif kind == "lde":
         n, k = int(params[0]), int(params[1])
-        tw = B.precompute_twiddles(n + 1, ctx=ctx)
-        cs = [to_device(rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32)) for _ in range(k)]
-        ev = [torch.empty(1 << (n + 1), dtype=torch.int32, device="cuda") for _ in range(k)]
-        work = lambda: B.evaluate_polynomials(cs, n + 1, tw, out=ev, ctx=ctx)
+        b = int(params[2]) if len(params) > 2 else 1
+        tw = B.precompute_twiddles(n + b - 1, ctx=ctx)
+        src = torch.from_numpy(rng.integers(0, P, (k, 1 << n), dtype=np.int64).astype(np.int32)).cuda()
+        dst = torch.empty((k, 1 << (n + b)), dtype=torch.int32, device="cuda")
+        cs = [src[i] for i in range(k)]
+        ev = [dst[i] for i in range(k)]
+        work = lambda: B.evaluate_polynomials(cs, n + b, tw, out=ev, ctx=ctx)
     elif kind == "merkle":
         n, k = int(params[0]), int(params[1])
         cols = [to_device(rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32)) for _ in range(k)]
@@ -755,7 +758,7 @@ def main():
     ap.add_argument("--log-n", type=int, default=0, help="override the proof size (log instances / rows)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", default=None,
-                    help="profiling case: fft:<log>, lde:<log>:<cols>, merkle:<log>:<cols>, fold:<log> (one op, no JSON contract)")
+                    help="profiling case: fft:<log>, lde:<log>:<cols>[:<ext>], merkle:<log>:<cols>, fold:<log> (one op, no JSON contract)")
     args = ap.parse_args()
     if args.case:
         run_case(args)
