@@ -593,8 +593,9 @@ def run_serving(args, world, rank, local):
             return G.prove_wide_fibonacci(n, c, seed=sd, input_mode=G.INPUT_SEEDED, ctx=ctx)
         return G.prove_poseidon(n, seed=sd, input_mode=G.INPUT_SEEDED, ctx=ctx)
 
-    for j in jobs[:4]:
-        single(*j)
+    # warm-up: every distinct shape once (pool growth, twiddle trees, pinned buffers)
+    for shape in sorted({(a, n, c) for a, n, c, _ in jobs}):
+        single(*shape, 0)
     torch.cuda.synchronize()
     # sequential: one proof at a time on one stream
     barrier(world)
@@ -609,8 +610,12 @@ def run_serving(args, world, rank, local):
     workers = args.workers
     arrivals = None
     with S.ProofServer(workers, 96 << 30) as sv:
-        for j in jobs[:workers]:          # warm the workers' contexts
-            sv.wait(sv.submit(j[0], j[1], j[2] or 100, j[3]))
+        # warm every worker's context on every shape (twiddle trees, domain
+        # tables and pool growth happen once per context): `workers` copies
+        # of each shape in flight at once
+        for a, n, c in sorted({(a, n, c) for a, n, c, _ in jobs}):
+            for i in [sv.submit(a, n, c or 100, 0) for _ in range(workers)]:
+                sv.wait(i)
         barrier(world)
         t0 = time.perf_counter()
         if args.workload == "batched":
@@ -753,7 +758,7 @@ def main():
     ap.add_argument("--impl", default="gpustark", choices=["gpustark", "reference"])
     ap.add_argument("--workload", default="poseidon",
                     choices=["poseidon", "wide_fibonacci", "kernels", "batched", "served"])
-    ap.add_argument("--workers", type=int, default=8, help="server workers (batched / served)")
+    ap.add_argument("--workers", type=int, default=16, help="server workers (batched / served)")
     ap.add_argument("--load", type=float, default=2.0, help="served: arrival rate / sequential proof rate")
     ap.add_argument("--log-n", type=int, default=0, help="override the proof size (log instances / rows)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -341,7 +341,7 @@ size_t logup_scratch_bytes(uint32_t log_n) {
 // Interaction column: writes the 4 coordinate columns (out, 4 x 2^log_n) and
 // the claimed sum (host). scratch: logup_scratch_bytes(log_n).
 int poseidon_interaction(cudaStream_t st, const uint32_t* trace, uint32_t log_n, const LookupParams& lp,
-                         uint32_t* out, void* scratch, qm31* claimed_sum) {
+                         uint32_t* out, void* scratch, qm31* claimed_sum, void* h_pinned) {
   size_t n = (size_t)1 << log_n;
   uint4* vals = (uint4*)scratch;
   uint4* scan = vals + n;
@@ -353,9 +353,11 @@ int poseidon_interaction(cudaStream_t st, const uint32_t* trace, uint32_t log_n,
   GS_CUDA_TRY(cudaGetLastError());
   GS_CUDA_TRY(cub::DeviceScan::InclusiveScan(temp, temp_bytes, (const uint4*)vals, scan, AddQM(), (int)n, st));
   note_launch();
-  uint4 total;
-  GS_CUDA_TRY(cudaMemcpyAsync(&total, scan + (n - 1), sizeof(uint4), cudaMemcpyDeviceToHost, st));
-  GS_CUDA_TRY(cudaStreamSynchronize(st));
+  uint4 local;
+  uint4* ht = h_pinned ? (uint4*)h_pinned : &local;  // pinned when the caller has a mailbox
+  GS_CUDA_TRY(cudaMemcpyAsync(ht, scan + (n - 1), sizeof(uint4), cudaMemcpyDeviceToHost, st));
+  GS_TRY(stream_sync(st));
+  uint4 total = *ht;
   qm31 cs = qm_make(total.x, total.y, total.z, total.w);
   *claimed_sum = cs;
   qm31 shift = qm_mul_m31(cs, inv((uint32_t)(n % P)));

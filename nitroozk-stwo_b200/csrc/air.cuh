@@ -27,7 +27,7 @@ int wf_constraints(cudaStream_t st, const uint32_t* cols, uint32_t n_cols, uint3
 int poseidon_trace(cudaStream_t st, uint32_t* cols, uint32_t log_n, uint64_t seed, uint32_t mode);
 size_t logup_scratch_bytes(uint32_t log_n);
 int poseidon_interaction(cudaStream_t st, const uint32_t* trace, uint32_t log_n, const LookupParams& lp,
-                         uint32_t* out, void* scratch, qm31* claimed_sum);
+                         uint32_t* out, void* scratch, qm31* claimed_sum, void* h_pinned = nullptr);
 int poseidon_constraints(cudaStream_t st, const uint32_t* trace, const uint32_t* inter, uint32_t eval_log,
                          uint32_t trace_log, const ConstraintParams& prm, const LookupParams& lp, qm31 cumsum_shift,
                          Planes out);

@@ -322,7 +322,8 @@ int gs_batch_eval_at_point(gs_ctx* ctx, const uint32_t* const* polys, uint32_t n
 int gs_grind_blake2s(gs_ctx* ctx, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint64_t* nonce) {
   CTX_REQUIRED(ctx);
   GS_REQUIRE(prefixed_digest != nullptr, "null digest");
-  return grind_blake2s(ctx->c.stream, prefixed_digest, pow_bits, (uint32_t*)ctx->c.d_small, nonce);
+  return grind_blake2s(ctx->c.stream, prefixed_digest, pow_bits, (uint32_t*)ctx->c.d_small, nonce,
+                       (uint32_t*)ctx->c.h_small);
 }
 
 static int run_prove(gs_ctx* ctx, prover::ProveRequest& req, const gs_pcs_config* config, uint8_t* proof,

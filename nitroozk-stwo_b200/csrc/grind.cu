@@ -33,8 +33,9 @@ __global__ void grind_kernel(Digest8 d, uint32_t hi, uint32_t pow_bits, uint32_t
   if (tz >= pow_bits) atomicMin(result, low);
 }
 
+// h_word (optional): a pinned host word for the per-chunk read-back.
 int grind_blake2s(cudaStream_t st, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint32_t* d_scratch,
-                  uint64_t* nonce_out) {
+                  uint64_t* nonce_out, uint32_t* h_word) {
   GS_REQUIRE(pow_bits <= 32, "pow_bits > 32 is not supported");
   GS_REQUIRE(d_scratch != nullptr && nonce_out != nullptr, "null scratch/result");
   Digest8 d;
@@ -42,14 +43,15 @@ int grind_blake2s(cudaStream_t st, const uint32_t prefixed_digest[8], uint32_t p
   // Bounded search: 2^12 chunks of 2^20 nonces covers pow_bits far beyond 32
   // with overwhelming probability; running out is reported, never looped on.
   for (uint32_t hi = 0; hi < (1u << 12); hi++) {
-    uint32_t none = 0xffffffffu;
-    GS_CUDA_TRY(cudaMemcpyAsync(d_scratch, &none, 4, cudaMemcpyHostToDevice, st));
+    GS_CUDA_TRY(cudaMemsetAsync(d_scratch, 0xff, 4, st));
     grind_kernel<<<(1u << 20) / 256, 256, 0, st>>>(d, hi, pow_bits, d_scratch);
     note_launch();
     GS_CUDA_TRY(cudaGetLastError());
-    uint32_t found = 0;
-    GS_CUDA_TRY(cudaMemcpyAsync(&found, d_scratch, 4, cudaMemcpyDeviceToHost, st));
-    GS_CUDA_TRY(cudaStreamSynchronize(st));
+    uint32_t local = 0;
+    uint32_t* hw = h_word ? h_word : &local;
+    GS_CUDA_TRY(cudaMemcpyAsync(hw, d_scratch, 4, cudaMemcpyDeviceToHost, st));
+    GS_TRY(stream_sync(st));
+    uint32_t found = *hw;
     if (found != 0xffffffffu) {
       *nonce_out = ((uint64_t)hi << 32) | found;
       return OK;

@@ -26,7 +26,9 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
     for (uint32_t k = 0; k <= log; k++) w += up((size_t)8 << k);
     return w;
   };
-  const size_t ctl_words = up(16 + 16 * (size_t)n_roots);
+  // channel state, roots, challenges, then a copy of the last layer
+  const size_t ctl_used = 16 + 16 * (size_t)n_roots + 4 * ((size_t)1 << last_log);
+  const size_t ctl_words = up(ctl_used);
   size_t words = ctl_words + tree_words(lifting);
   for (uint32_t lg = lifting - 1;; lg--) {
     words += 4 * up((size_t)1 << lg);
@@ -114,14 +116,15 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
     cur = std::move(next);
     k++;
   }
-  // one read-back: channel state, roots, challenges, then the last layer
-  std::vector<uint32_t> hc(16 + 16 * (size_t)n_roots);
-  GS_CUDA_TRY(cudaMemcpyAsync(hc.data(), ctl, hc.size() * 4, cudaMemcpyDeviceToHost, st));
+  // one read-back through pinned memory: channel state, roots, challenges
+  // and the last layer (copied next to them on the device)
   size_t n = (size_t)1 << cur.log;
-  std::vector<uint32_t> h(4 * n);
+  uint32_t* d_last = ctl + 16 + 16 * (size_t)n_roots;
   for (int c = 0; c < 4; c++)
-    GS_CUDA_TRY(cudaMemcpyAsync(h.data() + c * n, cur.planes[c], 4 * n, cudaMemcpyDeviceToHost, st));
-  GS_CUDA_TRY(cudaStreamSynchronize(st));
+    GS_CUDA_TRY(cudaMemcpyAsync(d_last + c * n, cur.planes[c], 4 * n, cudaMemcpyDeviceToDevice, st));
+  std::vector<uint32_t> hc(ctl_used);
+  GS_TRY(pv.ctx.read_back(ctl, hc.size() * 4, hc.data()));
+  std::vector<uint32_t> h(hc.begin() + 16 + 16 * (size_t)n_roots, hc.end());
   GS_REQUIRE(hc[9] == 0, "device channel: no challenge within the draw bound");
   for (uint32_t r = 0; r < n_roots; r++) {
     host::Hash root = host::hash_from_words(hc.data() + 16 + 8 * r);
@@ -232,7 +235,7 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
     GS_TRY(pv.A.alloc(logup_scratch_bytes(T), &scratch));
     uint32_t* inter = nullptr;
     GS_TRY(pv.A.alloc_n((size_t)4 << T, &inter));
-    GS_TRY(poseidon_interaction(st, trace, T, air.lookup, inter, scratch, &air.claimed_sum));
+    GS_TRY(poseidon_interaction(st, trace, T, air.lookup, inter, scratch, &air.claimed_sum, pv.ctx.h_small));
     pv.mark("interaction");
     GS_TRY(pv.commit_evals(inter, 4, T));
     pv.mark("interaction_commit");

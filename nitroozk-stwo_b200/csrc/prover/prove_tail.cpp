@@ -74,8 +74,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
                                  (uint32_t*)scratch));
     }
     std::vector<uint32_t> h(4 * n_vals);
-    if (n_vals) GS_CUDA_TRY(cudaMemcpyAsync(h.data(), d_vals, h.size() * 4, cudaMemcpyDeviceToHost, st));
-    GS_CUDA_TRY(cudaStreamSynchronize(st));
+    GS_TRY(pv.ctx.read_back(d_vals, h.size() * 4, h.data()));
     for (auto& r : reqs) {
       Tree& tr = pv.trees[r.t];
       for (uint32_t c = 0; c < tr.n_cols; c++) {
@@ -223,7 +222,8 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   pv.mark("fri_commit");
   auto pre = pv.ch.pow_prefixed(cfg.pow_bits);
   uint64_t nonce = 0;
-  GS_TRY(grind_blake2s(st, pre.data(), cfg.pow_bits, (uint32_t*)pv.ctx.d_small, &nonce));
+  GS_TRY(grind_blake2s(st, pre.data(), cfg.pow_bits, (uint32_t*)pv.ctx.d_small, &nonce,
+                       (uint32_t*)pv.ctx.h_small));
   pv.ch.mix_u64(nonce);
   pv.mark("grind");
   // queries

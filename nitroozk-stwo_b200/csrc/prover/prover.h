@@ -25,10 +25,12 @@ struct PcsConfig {
 // Stream-ordered device allocations released together.
 struct Arena {
   cudaStream_t st = nullptr;
+  cudaMemPool_t pool = nullptr;  // the context's pool (default pool if null)
   std::vector<void*> ptrs;
   int alloc(size_t bytes, void** out) {
     void* p = nullptr;
-    cudaError_t e = cudaMallocAsync(&p, bytes ? bytes : 16, st);
+    cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, pool, st)
+                         : cudaMallocAsync(&p, bytes ? bytes : 16, st);
     if (e != cudaSuccess) {
       cudaGetLastError();
       set_error(std::string("device allocation failed: ") + cudaGetErrorString(e));
@@ -130,7 +132,7 @@ struct GatherPlan {
     void* hr = nullptr;
     GS_TRY(ctx.read_buffer(out_words * 4, &hr));
     if (out_words) GS_CUDA_TRY(cudaMemcpyAsync(hr, d_out, out_words * 4, cudaMemcpyDeviceToHost, st));
-    GS_CUDA_TRY(cudaStreamSynchronize(st));
+    GS_TRY(stream_sync(st));
     const uint32_t* o = (const uint32_t*)hr;
     word_out.assign(o, o + n_words);
     hash_out.assign(o + hbase, o + out_words);

@@ -92,6 +92,7 @@ struct Prover {
 
   Prover(Context& c, const PcsConfig& p) : ctx(c), st(c.stream), cfg(p) {
     A.st = st;
+    A.pool = c.pool;
     phases.init(st);
   }
   void mark(const char* name) { phases.mark(name); }
@@ -119,8 +120,7 @@ struct Prover {
     GS_TRY(commit_on_layer(st, t.eval_log, nullptr, tab, t.n_cols, t.layers[t.eval_log]));
     GS_TRY(commit_node_layers(st, t.eval_log, t.layers.data()));
     uint32_t w[8];
-    GS_CUDA_TRY(cudaMemcpyAsync(w, t.layers[0], 32, cudaMemcpyDeviceToHost, st));
-    GS_CUDA_TRY(cudaStreamSynchronize(st));
+    GS_TRY(ctx.read_back(t.layers[0], 32, w));
     t.root = host::hash_from_words(w);
     return OK;
   }
@@ -222,22 +222,6 @@ struct Prover {
     const uint32_t* const* ctab = nullptr;
     GS_TRY(table(cp, &ctab));
     GS_TRY(interpolate_columns(st, (uint32_t* const*)ctab, 4, E, itw, tw_log));
-    return OK;
-  }
-
-  // Values of every column of tree t at `pt` (already doubled for the tree).
-  int sample_tree(const Tree& t, const ptq& pt, std::vector<qm31>& out) {
-    out.resize(t.n_cols);
-    if (t.n_cols == 0) return OK;
-    size_t need = eval_at_point_scratch_bytes(t.n_cols, t.coeff_log) + 16 * (size_t)t.n_cols;
-    void* scratch = nullptr;
-    GS_TRY(A.alloc(need, &scratch));
-    uint32_t* d_out = (uint32_t*)((uint8_t*)scratch + eval_at_point_scratch_bytes(t.n_cols, t.coeff_log));
-    GS_TRY(batch_eval_at_point(st, t.coeff_tab, t.n_cols, t.coeff_log, pt, d_out, (uint32_t*)scratch));
-    std::vector<uint32_t> h(4 * (size_t)t.n_cols);
-    GS_CUDA_TRY(cudaMemcpyAsync(h.data(), d_out, h.size() * 4, cudaMemcpyDeviceToHost, st));
-    GS_CUDA_TRY(cudaStreamSynchronize(st));
-    for (uint32_t c = 0; c < t.n_cols; c++) out[c] = qm_make(h[4 * c], h[4 * c + 1], h[4 * c + 2], h[4 * c + 3]);
     return OK;
   }
 };

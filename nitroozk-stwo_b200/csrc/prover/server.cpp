@@ -63,6 +63,9 @@ struct Server {
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     Context ctx;
     int init = ctx.init(st);
+    cudaEvent_t wait_ev = nullptr;
+    if (cudaEventCreateWithFlags(&wait_ev, cudaEventBlockingSync | cudaEventDisableTiming) == cudaSuccess)
+      set_thread_wait_event(wait_ev);
     for (;;) {
       Job job;
       {
@@ -83,7 +86,7 @@ struct Server {
       } else {
         d.status = prove_component(ctx, job.req, &d.proof, nullptr);
         if (d.status != OK) d.error = last_error();
-        cudaStreamSynchronize(st);
+        stream_sync(st);
       }
       auto t1 = std::chrono::steady_clock::now();
       d.service_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
@@ -96,7 +99,9 @@ struct Server {
       cv_done.notify_all();
       cv_jobs.notify_all();
     }
+    set_thread_wait_event(nullptr);
     ctx.destroy();
+    if (wait_ev) cudaEventDestroy(wait_ev);
     cudaStreamDestroy(st);
   }
 };

@@ -14,6 +14,18 @@ static std::atomic<unsigned long long> g_launches{0};
 void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
+static thread_local cudaEvent_t g_wait_ev = nullptr;
+void set_thread_wait_event(cudaEvent_t ev) { g_wait_ev = ev; }
+int stream_sync(cudaStream_t st) {
+  if (g_wait_ev) {
+    GS_CUDA_TRY(cudaEventRecord(g_wait_ev, st));
+    GS_CUDA_TRY(cudaEventSynchronize(g_wait_ev));
+  } else {
+    GS_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  return OK;
+}
+
 int num_sms() {
   static int cached[64] = {0};
   int dev = 0;
@@ -34,12 +46,14 @@ int Context::init(void* user_stream) {
   stream = (cudaStream_t)user_stream;
   own_stream = false;
   {
-    // Stream-ordered allocations stay in the device pool between proofs.
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-      uint64_t threshold = UINT64_MAX;
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
-    }
+    // A pool of this context's own; freed memory stays in it between proofs.
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    GS_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
+    uint64_t threshold = UINT64_MAX;
+    GS_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
   }
   ring_cap = 4 << 20;
   ring_off = 0;
@@ -53,7 +67,10 @@ int Context::init(void* user_stream) {
 
 void Context::destroy() {
   if (stream) cudaStreamSynchronize(stream);
-  if (scratch) cudaFree(scratch);
+  if (scratch) {
+    cudaFreeAsync(scratch, stream);
+    cudaStreamSynchronize(stream);
+  }
   scratch = nullptr;
   for (int i = 0; i < 31; i++) {
     if (dom_buf[i]) cudaFree(dom_buf[i]);
@@ -69,6 +86,8 @@ void Context::destroy() {
   if (h_read) cudaFreeHost(h_read);
   h_read = nullptr;
   read_cap = 0;
+  if (pool) cudaMemPoolDestroy(pool);  // released once its last allocation is freed
+  pool = nullptr;
   if (own_stream && stream) cudaStreamDestroy(stream);
   h_ring = d_ring = d_small = h_small = nullptr;
   stream = nullptr;
@@ -97,6 +116,31 @@ int Context::stage_ptrs(const void* const* host_ptrs, size_t n, const void* cons
   return OK;
 }
 
+int Context::alloc_async(size_t bytes, void** out) {
+  cudaError_t e = pool ? cudaMallocFromPoolAsync(out, bytes ? bytes : 16, pool, stream)
+                       : cudaMallocAsync(out, bytes ? bytes : 16, stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(std::string("device allocation failed: ") + cudaGetErrorString(e));
+    return ERR_OOM;
+  }
+  return OK;
+}
+
+int Context::read_back(const void* d_src, size_t bytes, void* host_dst) {
+  if (bytes == 0) return OK;
+  void* h = nullptr;
+  if (bytes <= small_cap) {
+    h = h_small;
+  } else {
+    GS_TRY(read_buffer(bytes, &h));
+  }
+  GS_CUDA_TRY(cudaMemcpyAsync(h, d_src, bytes, cudaMemcpyDeviceToHost, stream));
+  GS_TRY(stream_sync(stream));
+  memcpy(host_dst, h, bytes);
+  return OK;
+}
+
 int Context::read_buffer(size_t bytes, void** out) {
   if (bytes > read_cap) {
     if (h_read) {
@@ -118,9 +162,7 @@ int Context::get_scratch(size_t bytes, void** out) {
     if (scratch) GS_CUDA_TRY(cudaFreeAsync(scratch, stream));
     scratch = nullptr;
     size_t cap = bytes < (1u << 20) ? (1u << 20) : bytes;
-    cudaError_t e = cudaMallocAsync(&scratch, cap, stream);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
+    if (alloc_async(cap, &scratch) != OK) {
       scratch_cap = 0;
       set_error("scratch allocation failed");
       return ERR_OOM;
@@ -158,7 +200,7 @@ int Context::twiddles(uint32_t root_log, const uint32_t** tw, const uint32_t** i
 }
 
 int Context::sync() {
-  GS_CUDA_TRY(cudaStreamSynchronize(stream));
+  GS_TRY(stream_sync(stream));
   return OK;
 }
 

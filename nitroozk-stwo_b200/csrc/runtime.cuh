@@ -62,6 +62,12 @@ struct DomainTables {
   uint32_t lift;
 };
 
+// Waits for `st`. By default a spin-wait (the lowest latency for one proof at
+// a time); a thread that installs a blocking-sync event (the proof server's
+// workers) sleeps instead, leaving the host cores to the other workers.
+int stream_sync(cudaStream_t st);
+void set_thread_wait_event(cudaEvent_t ev);
+
 // Number of SMs of the current device (cached).
 int num_sms();
 
@@ -80,6 +86,13 @@ struct Context {
   uint8_t* h_small = nullptr;  // pinned mirror
   size_t small_cap = 0;
 
+  // Stream-ordered memory pool owned by this context. Contexts that run
+  // concurrently (the proof server's workers) do not share a pool, so
+  // reusing freed memory never inserts a dependency on another stream.
+  cudaMemPool_t pool = nullptr;
+  int alloc_async(size_t bytes, void** out);
+  // Small device-to-host read through the pinned mailbox, then synchronise.
+  int read_back(const void* d_src, size_t bytes, void* host_dst);
   // growable pinned host buffer for read-backs (decommitment values)
   uint8_t* h_read = nullptr;
   size_t read_cap = 0;
@@ -177,6 +190,6 @@ int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_
 
 // grind.cu
 int grind_blake2s(cudaStream_t st, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint32_t* d_scratch,
-                  uint64_t* nonce_out);
+                  uint64_t* nonce_out, uint32_t* h_word = nullptr);
 
 }  // namespace gs
