@@ -13,6 +13,7 @@ Sources (paths inside the reference checkout):
   crates/stwo/src/core/fields/m31.rs           doc-tests of partial_reduce / reduce
   crates/stwo/src/core/circle.rs               M31_CIRCLE_GEN, SECURE_FIELD_CIRCLE_GEN,
                                                test_secure_field_circle_gen prime factors
+  crates/stwo/src/prover/backend/cuda/poly.rs  test_interpolate_from_fib (twiddle tree literals)
 """
 import json
 import os
@@ -65,6 +66,23 @@ def main(root):
     out["secure_circle_gen"] = [[int(v) for v in sg.group(1).split(",")], [int(v) for v in sg.group(2).split(",")]]
     pf = re.search(r"let prime_factors = \[(.*?)\];", circ, re.S).group(1)
     out["secure_circle_order_factors"] = [[int(a), int(b)] for a, b in re.findall(r"\((\d+),\s*(\d+)\)", pf)]
+
+    # Twiddle tree literals of the CUDA backend's interpolation test
+    # (cuda/poly.rs, test_interpolate_from_fib): twiddles and itwiddles of
+    # the root coset, which pin the twiddle-tree layout.
+    poly = _read(root, "crates/stwo/src/prover/backend/cuda/poly.rs")
+    body = poly[poly.index("fn test_interpolate_from_fib"):]
+    def vec_of(name):
+        block = re.search(r"let %s = vec!\[(.*?)\];" % name, body, re.S).group(1)
+        return [int(v) for v in re.findall(r"BaseField::from\((\d+)\)", block)]
+    rc = body[body.index("let root_coset"):]
+    out["cuda_interpolate_twiddle_tree"] = {
+        "root_initial_index": int(re.search(r"initial_index: CirclePointIndex\((\d+)\)", rc).group(1)),
+        "root_step_index": int(re.search(r"step_size: CirclePointIndex\((\d+)\)", rc).group(1)),
+        "root_log_size": int(re.search(r"log_size: (\d+)", rc).group(1)),
+        "twiddles": vec_of("twiddles"),
+        "itwiddles": vec_of("itwiddles"),
+    }
 
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_vectors.json")
     with open(dst, "w") as f:

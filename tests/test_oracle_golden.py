@@ -176,3 +176,15 @@ def test_fold_line_formula():
         L.oracle_qm31_mul(O.u32(alpha)[1], O.u32(np.array(f1, np.uint32))[1], r.ctypes.data_as(O.U32P))
         expect = [(a + int(b)) % P for a, b in zip(f0, r)]
         assert _qm(out[i]) == expect
+
+
+def test_twiddle_tree_matches_reference_literals():
+    """Twiddles and itwiddles of Coset::half_odds(6), as written out in the
+    reference CUDA backend's interpolation test: pins the twiddle-tree layout
+    (per-level x coordinates, bit-reversed, padded) and its inverses."""
+    g = GOLDEN["cuda_interpolate_twiddle_tree"]
+    log = g["root_log_size"]
+    assert g["root_initial_index"] == 1 << (31 - log - 2) and g["root_step_index"] == 1 << (31 - log)
+    tw, itw = O.twiddles_half_odds(log)
+    assert [int(v) for v in tw] == g["twiddles"]
+    assert [int(v) for v in itw] == g["itwiddles"]
