@@ -35,6 +35,17 @@ def rand_m31(rng, *shape):
     return rng.integers(0, P, shape, dtype=np.int64).astype(np.uint32)
 
 
+def test_twiddles_match_reference_literals(B):
+    """The device twiddle tree of half_odds(6) against the literal values in
+    the reference CUDA backend's interpolation test."""
+    import json, os
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_vectors.json")))
+    g = g["cuda_interpolate_twiddle_tree"]
+    t = B.precompute_twiddles(g["root_log_size"])
+    assert [int(v) for v in host(t.twiddles)] == g["twiddles"]
+    assert [int(v) for v in host(t.itwiddles)] == g["itwiddles"]
+
+
 @pytest.mark.parametrize("root_log", [1, 2, 3, 5, 8, 13, 17])
 def test_twiddles(B, root_log):
     t = B.precompute_twiddles(root_log)
