@@ -678,7 +678,59 @@ def run_serving(args, world, rank, local):
     }
     if arrivals is not None:
         out["arrival_rate_per_s"] = round(args.load * len(jobs) / seq_s, 2)
+    if args.workload == "batched":
+        out["commit"] = run_batched_commit(ctx, 1 + rank)
     return out
+
+
+def run_batched_commit(ctx, seed, n_cols=256, lo=12, hi=24, blowup=1, reps=5):
+    """configs[3], commitment part: 256 columns with log sizes uniform in
+    12..24, extended by 2^blowup and committed in one Merkle tree. Times the
+    batched plan eagerly and replayed from a CUDA graph (same inputs, same
+    root), and the FFT part issued one column per launch for comparison."""
+    import torch
+    from gpustark.backend import CommitPlan, GpuBackend as B
+    rng = np.random.default_rng(seed)
+    logs = [int(v) for v in rng.integers(lo, hi + 1, n_cols)]
+    cols = [torch.randint(0, P, (1 << lg,), dtype=torch.int32, device="cuda") for lg in logs]
+    st = torch.cuda.current_stream()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            r = fn()
+            b.record(st)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts), r
+
+    eager = CommitPlan(logs, blowup, use_graph=False, ctx=ctx)
+    graph = CommitPlan(logs, blowup, use_graph=True, ctx=ctx)
+    e_ms, e_root = timed(lambda: eager.run(cols))
+    g_ms, g_root = timed(lambda: graph.run(cols))
+    eager.close()
+    graph.close()
+    # FFT part, one column per launch (interpolate in place on a copy, extend)
+    tw = B.precompute_twiddles(hi + blowup - 1, ctx=ctx)
+    work = [c.clone() for c in cols]
+    outs = [torch.empty(1 << (lg + blowup), dtype=torch.int32, device="cuda") for lg in logs]
+
+    def per_column():
+        for c, o, lg in zip(work, outs, logs):
+            B.interpolate_columns([c], lg, tw, ctx=ctx)
+            B.evaluate_polynomials([c], lg + blowup, tw, out=[o], ctx=ctx)
+    pc_ms, _ = timed(per_column)
+    alg = sum(4 * ((1 << lg) + (1 << (lg + blowup))) for lg in logs)  # read evals, write extension
+    alg += sum(4 * (1 << (lg + blowup)) for lg in logs) + 32 * (1 << (hi + blowup + 1))  # leaves + hashes
+    return {"columns": n_cols, "log_sizes": "uniform %d..%d (seed %d)" % (lo, hi, seed), "log_blowup": blowup,
+            "eager_ms": round(e_ms, 3), "graph_ms": round(g_ms, 3), "graph_root_equals_eager": e_root == g_root,
+            "fft_one_column_per_launch_ms": round(pc_ms, 3),
+            "algorithmic_gbs_graph": round(alg / (g_ms / 1e3) / 1e9, 1)}
 
 
 def run_reference(args, world, rank):

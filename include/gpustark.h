@@ -231,6 +231,28 @@ int gs_server_wait(gs_server* server, uint64_t job_id, uint8_t* proof, size_t ca
                    double* latency_ms);
 int gs_server_destroy(gs_server* server);
 
+/* ------------------------------------------------ batched commitment plans */
+/* TreeBuilder::extend_evals + commit (prover/pcs/mod.rs:388-430) followed by
+ * MerkleProver::commit (prover/vcs/prover.rs:39-62) for columns of mixed
+ * sizes, batched: a plan fixes the shape (log sizes, blowup) and owns every
+ * buffer. gs_commit_plan_run interpolates each size group (one launch per FFT
+ * pass per group), evaluates it on CanonicCoset(log + log_blowup), and commits
+ * all columns in one Merkle tree (columns sorted by size, stable; each size
+ * injected at its layer), then writes the 8-word root to host memory.
+ * Inputs: device pointers to bit-reversed evaluations on CanonicCoset(log).
+ * use_graph != 0: the first run captures the work into a CUDA graph on the
+ * plan's own stream and later runs replay it (the input pointers may change
+ * between runs; a change of their 16-byte alignment runs the work eagerly).
+ * The extended columns and every Merkle layer stay readable until the next
+ * run (gs_commit_plan_extended, gs_commit_plan_layer). Synchronises. */
+typedef struct gs_commit_plan gs_commit_plan;
+int gs_commit_plan_create(gs_ctx* ctx, const uint32_t* log_sizes, uint32_t n_columns, uint32_t log_blowup,
+                          uint32_t use_graph, gs_commit_plan** out);
+int gs_commit_plan_run(gs_commit_plan* plan, const uint32_t* const* columns, uint32_t root[8]);
+int gs_commit_plan_extended(gs_commit_plan* plan, uint32_t column, const uint32_t** evals);
+int gs_commit_plan_layer(gs_commit_plan* plan, uint32_t log_size, const uint32_t** layer);
+int gs_commit_plan_destroy(gs_commit_plan* plan);
+
 #ifdef __cplusplus
 }
 #endif

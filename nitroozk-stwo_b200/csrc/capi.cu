@@ -384,4 +384,42 @@ int gs_prove_poseidon(gs_ctx* ctx, uint32_t log_n_instances, uint64_t seed, uint
   return run_prove(ctx, req, config, proof, capacity, proof_len);
 }
 
+// ------------------------------------------------------------ commit plans
+struct gs_commit_plan {
+  prover::CommitPlan* p;
+  gs_ctx* ctx;
+};
+
+int gs_commit_plan_create(gs_ctx* ctx, const uint32_t* log_sizes, uint32_t n_columns, uint32_t log_blowup,
+                          uint32_t use_graph, gs_commit_plan** out) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(log_sizes && out, "null argument");
+  prover::CommitPlan* p = nullptr;
+  GS_TRY(prover::plan_create(ctx->c, log_sizes, n_columns, log_blowup, use_graph != 0, &p));
+  *out = new gs_commit_plan{p, ctx};
+  return OK;
+}
+
+int gs_commit_plan_run(gs_commit_plan* plan, const uint32_t* const* columns, uint32_t root[8]) {
+  GS_REQUIRE(plan && columns && root, "null argument");
+  return prover::plan_run(plan->p, columns, root);
+}
+
+int gs_commit_plan_extended(gs_commit_plan* plan, uint32_t column, const uint32_t** evals) {
+  GS_REQUIRE(plan && evals, "null argument");
+  return prover::plan_extended(plan->p, column, evals);
+}
+
+int gs_commit_plan_layer(gs_commit_plan* plan, uint32_t log_size, const uint32_t** layer) {
+  GS_REQUIRE(plan && layer, "null argument");
+  return prover::plan_layer(plan->p, log_size, layer);
+}
+
+int gs_commit_plan_destroy(gs_commit_plan* plan) {
+  if (!plan) return OK;
+  prover::plan_destroy(plan->p);
+  delete plan;
+  return OK;
+}
+
 }  // extern "C"

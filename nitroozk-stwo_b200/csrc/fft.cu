@@ -364,7 +364,10 @@ __global__ void fft_small_kernel(const uint32_t* const* src_tab, uint32_t* const
   const uint32_t* s = src_tab[col];
   uint32_t* d = dst_tab[col];
   if (a.n == 1) {
-    uint32_t v0 = s[0], v1 = s[1 & a.src_mask];
+    // coefficients beyond 2^coeff_log are zero: these closed forms run every
+    // butterfly, so the padding is explicit (the pass kernels skip the copy
+    // layers and replicate instead)
+    uint32_t v0 = s[0], v1 = 1 <= a.src_mask ? s[1] : 0u;
     if (a.inverse) {  // k = {y_inv, n_inv}
       uint32_t r0 = add(v0, v1), r1 = mul(sub(v0, v1), a.k[0]);
       d[0] = mul(r0, a.k[1]);
@@ -375,7 +378,8 @@ __global__ void fft_small_kernel(const uint32_t* const* src_tab, uint32_t* const
       d[1] = sub(v0, tmp);
     }
   } else {
-    uint32_t v0 = s[0], v1 = s[1 & a.src_mask], v2 = s[2 & a.src_mask], v3 = s[3 & a.src_mask];
+    uint32_t v0 = s[0], v1 = 1 <= a.src_mask ? s[1] : 0u, v2 = 2 <= a.src_mask ? s[2] : 0u,
+             v3 = 3 <= a.src_mask ? s[3] : 0u;
     if (a.inverse) {  // k = {x_inv, y_inv, n_inv}
       auto ib = [](uint32_t& p, uint32_t& q, uint32_t w) { uint32_t t0 = p; p = add(t0, q); q = mul(sub(t0, q), w); };
       ib(v0, v1, a.k[1]);

@@ -26,5 +26,14 @@ struct AirHost;
 int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_bytes, ProveStats* stats);
 int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_bytes, ProveStats* stats);
 
+// Batched commitment of columns of mixed sizes (commit.cpp).
+struct CommitPlan;
+int plan_create(Context& ctx, const uint32_t* log_sizes, uint32_t n, uint32_t blowup, bool use_graph,
+                CommitPlan** out);
+int plan_run(CommitPlan* p, const uint32_t* const* inputs, uint32_t root[8]);
+int plan_extended(CommitPlan* p, uint32_t column, const uint32_t** out);
+int plan_layer(CommitPlan* p, uint32_t log_size, const uint32_t** out);
+void plan_destroy(CommitPlan* p);
+
 }  // namespace prover
 }  // namespace gs

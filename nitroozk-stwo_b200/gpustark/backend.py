@@ -264,3 +264,54 @@ class GpuBackend:
         nonce = C.c_uint64()
         L.check(L.lib().gs_grind_blake2s(ctx.handle, words, pow_bits, C.byref(nonce)), "grind")
         return nonce.value
+
+
+class CommitPlan:
+    """Batched TreeBuilder::extend_evals + commit for columns of mixed sizes
+    (gs_commit_plan_*): interpolation and extension batched per size group,
+    one Merkle tree over all columns; optionally replayed from a CUDA graph."""
+
+    def __init__(self, log_sizes, log_blowup=1, use_graph=True, ctx=None):
+        self.ctx = ctx or default_context()
+        self.log_sizes = [int(v) for v in log_sizes]
+        self.log_blowup = log_blowup
+        logs = (C.c_uint32 * len(self.log_sizes))(*self.log_sizes)
+        h = C.c_void_p()
+        L.check(L.lib().gs_commit_plan_create(self.ctx.handle, logs, len(self.log_sizes), log_blowup,
+                                              1 if use_graph else 0, C.byref(h)), "gs_commit_plan_create")
+        self.handle = h
+
+    def run(self, columns):
+        """columns: device tensors (bit-reversed evaluations); returns the 32-byte root."""
+        pp, keep = L.ptr_array([c.data_ptr() for c in columns])
+        root = (C.c_uint32 * 8)()
+        L.check(L.lib().gs_commit_plan_run(self.handle, pp, root), "gs_commit_plan_run")
+        return struct.pack("<8I", *root)
+
+    def _read(self, ptr, words):
+        out = np.zeros(words, np.uint32)
+        L.check(L.lib().gs_memcpy_d2h(self.ctx.handle, out.ctypes.data_as(C.c_void_p), ptr, 4 * words), "d2h")
+        return out
+
+    def extended(self, i):
+        """Host copy of column i on CanonicCoset(log + log_blowup)."""
+        p = C.c_void_p()
+        L.check(L.lib().gs_commit_plan_extended(self.handle, i, C.byref(p)), "gs_commit_plan_extended")
+        return self._read(p, 1 << (self.log_sizes[i] + self.log_blowup))
+
+    def layer(self, log_size):
+        """Host copy of Merkle layer log_size as (2^log_size, 32) bytes."""
+        p = C.c_void_p()
+        L.check(L.lib().gs_commit_plan_layer(self.handle, log_size, C.byref(p)), "gs_commit_plan_layer")
+        return self._read(p, 8 << log_size).view(np.uint8).reshape(-1, 32)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.lib().gs_commit_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -68,7 +68,7 @@ def test_interpolate_matches_oracle(B, log_n):
         assert np.array_equal(host(g), e)
 
 
-@pytest.mark.parametrize("coeff_log,log_n", [(1, 1), (2, 2), (1, 3), (3, 3), (4, 5), (8, 9), (10, 12), (12, 12),
+@pytest.mark.parametrize("coeff_log,log_n", [(1, 1), (1, 2), (2, 2), (1, 3), (3, 3), (4, 5), (8, 9), (10, 12), (12, 12),
                                               (13, 14), (15, 16), (16, 17), (18, 19), (19, 20), (5, 18), (20, 22), (22, 22),
                                               (23, 24)])
 def test_evaluate_matches_oracle(B, coeff_log, log_n):
