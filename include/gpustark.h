@@ -104,6 +104,17 @@ int gs_commit_on_layer(gs_ctx* ctx, uint32_t log_size, const uint32_t* prev_laye
  * layers[top_log] is the input, all smaller layers are written. */
 int gs_commit_node_layers(gs_ctx* ctx, uint32_t top_log, uint32_t* const* layers);
 
+/* MerkleOpsLifted::build_leaves (prover/vcs_lifted/ops.rs:8-18; CPU
+ * prover/backend/cpu/merkle_lifted.rs:12-77; reference CUDA blake2s.cu:
+ * 210-452): the leaves of a lifted Merkle commitment. Columns (any order;
+ * sorted here by increasing size, stably) are bit-reversed evaluations of
+ * log size in [1, lifting_log_size]; leaf i hashes each column's value at
+ * ((i >> (lifting_log_size - log + 1)) << 1) + (i & 1). out: 2^lifting_log_size
+ * hashes, or one hash (of nothing) when n_cols == 0. build_next_layer is
+ * gs_commit_node_layers. */
+int gs_lifted_build_leaves(gs_ctx* ctx, const uint32_t* const* cols, const uint32_t* log_sizes, uint32_t n_cols,
+                           uint32_t lifting_log_size, uint32_t* out);
+
 /* ---------------------------------------------------------------- FriOps */
 /* fold_line (bindings.rs:196-203); FriOps::fold_line (prover/fri.rs:39-44),
  * fold_step 1: line evaluation on half_odds(log_size) -> 2^(log_size-1).

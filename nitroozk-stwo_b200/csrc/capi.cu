@@ -3,6 +3,8 @@
 #include "runtime.cuh"
 #include "prover/prove_api.h"
 #include <cstring>
+#include <algorithm>
+#include <vector>
 
 struct gs_ctx {
   gs::Context c;
@@ -382,6 +384,41 @@ int gs_prove_poseidon(gs_ctx* ctx, uint32_t log_n_instances, uint64_t seed, uint
   req.host_inputs = host_inputs;
   req.split_log = composition_log_split;
   return run_prove(ctx, req, config, proof, capacity, proof_len);
+}
+
+// ------------------------------------------------------------ lifted Merkle
+int gs_lifted_build_leaves(gs_ctx* ctx, const uint32_t* const* cols, const uint32_t* log_sizes, uint32_t n_cols,
+                           uint32_t lifting_log_size, uint32_t* out) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(out != nullptr && ((uintptr_t)out & 15) == 0, "output must be a 16-byte aligned device buffer");
+  GS_REQUIRE(lifting_log_size <= 30, "lifting log size out of range");
+  if (n_cols == 0) {  // the hash of nothing
+    host::Hash h = host::hash_bytes(nullptr, 0);
+    const void* d = nullptr;
+    GS_TRY(ctx->c.stage_bytes(h.data(), 32, &d));
+    GS_CUDA_TRY(cudaMemcpyAsync(out, d, 32, cudaMemcpyDeviceToDevice, ctx->c.stream));
+    return OK;
+  }
+  GS_REQUIRE(cols && log_sizes, "null argument");
+  std::vector<uint32_t> order(n_cols);
+  for (uint32_t i = 0; i < n_cols; i++) {
+    GS_REQUIRE(cols[i] != nullptr, "null column");
+    GS_REQUIRE(log_sizes[i] >= 1 && log_sizes[i] <= lifting_log_size, "column log size must be in [1, lifting]");
+    order[i] = i;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return log_sizes[a] < log_sizes[b]; });
+  std::vector<const void*> ptrs(n_cols);
+  std::vector<uint8_t> shifts(n_cols);
+  for (uint32_t k = 0; k < n_cols; k++) {
+    ptrs[k] = cols[order[k]];
+    shifts[k] = (uint8_t)(lifting_log_size - log_sizes[order[k]]);
+  }
+  const void* const* d_cols = nullptr;
+  const void* d_shifts = nullptr;
+  GS_TRY(ctx->c.stage_ptrs(ptrs.data(), n_cols, &d_cols));
+  GS_TRY(ctx->c.stage_bytes(shifts.data(), n_cols, &d_shifts));
+  return lifted_leaves(ctx->c.stream, lifting_log_size, (const uint32_t* const*)d_cols, (const uint8_t*)d_shifts,
+                       n_cols, out);
 }
 
 // ------------------------------------------------------------ commit plans

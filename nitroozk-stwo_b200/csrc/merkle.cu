@@ -66,6 +66,56 @@ __global__ void __launch_bounds__(256) merkle_layer_kernel(uint32_t log_size, co
   }
 }
 
+// Lifted Merkle leaves (MerkleOpsLifted::build_leaves, crates/stwo/src/
+// prover/backend/cpu/merkle_lifted.rs:12-77): leaf i of 2^lift hashes every
+// column's value at its lifted index ((i >> (lift - log + 1)) << 1) + (i & 1),
+// columns in increasing size order (the caller sorts, stably). One leaf per
+// thread; message blocks are filled straight from the column loads.
+__global__ void __launch_bounds__(256) merkle_lifted_leaves_kernel(uint32_t lift, const uint32_t* const* __restrict__ cols,
+                                                                   const uint8_t* __restrict__ shifts, uint32_t n_cols,
+                                                                   uint32_t* __restrict__ out, uint32_t one) {
+  const size_t n = (size_t)1 << lift;
+  const uint32_t total_bytes = 4u * n_cols;
+  const uint32_t n_blocks = (n_cols + 15u) / 16u;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t h[8], m[16];
+    blake2s_init(h);
+    uint32_t col = 0;
+    for (uint32_t blk = 0; blk < n_blocks; blk++) {
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        uint32_t c = col + j;
+        uint32_t v = 0;
+        if (c < n_cols) {
+          const uint32_t s = shifts[c];  // lift - log
+          const size_t idx = ((i >> (s + 1)) << 1) + (i & 1);
+          v = __ldg(cols[c] + idx);
+        }
+        m[j] = v;
+      }
+      col += 16;
+      uint32_t t = 64u * (blk + 1);
+      if (t > total_bytes) t = total_bytes;
+      blake2s_compress_f(h, m, t, blk + 1 == n_blocks, one);
+    }
+    store_hash(out, i, h);
+  }
+}
+
+int lifted_leaves(cudaStream_t st, uint32_t lift, const uint32_t* const* d_cols, const uint8_t* d_shifts,
+                  uint32_t n_cols, uint32_t* d_out) {
+  GS_REQUIRE(lift <= 30 && n_cols >= 1, "bad lifted leaf layer");
+  GS_REQUIRE(((uintptr_t)d_out & 15) == 0, "hash buffers must be 16-byte aligned");
+  size_t n = (size_t)1 << lift;
+  size_t blocks = (n + 255) / 256;
+  size_t cap = (size_t)num_sms() * 8;
+  if (blocks > cap) blocks = cap;
+  merkle_lifted_leaves_kernel<<<(unsigned)blocks, 256, 0, st>>>(lift, d_cols, d_shifts, n_cols, d_out, 1u);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
 int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, const uint32_t* const* d_cols,
                     uint32_t n_cols, uint32_t* d_out) {
   GS_REQUIRE(log_size <= 30, "layer log size out of range");

@@ -139,6 +139,10 @@ int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, 
                     uint32_t n_cols, uint32_t* d_out);
 // All node-only layers below `top_log` (layers[L] has 2^L hashes, layers[top_log] given).
 int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers);
+// Lifted Merkle leaves; d_shifts[c] = lift - log size of column c (columns in
+// increasing size order).
+int lifted_leaves(cudaStream_t st, uint32_t lift, const uint32_t* const* d_cols, const uint8_t* d_shifts,
+                  uint32_t n_cols, uint32_t* d_out);
 
 // FRI layers of log size <= 11 in one launch (fri.cu): layer k has log size
 // log0 - k; layers 0..n-1 are committed (tree[k][L] = their Merkle layers,

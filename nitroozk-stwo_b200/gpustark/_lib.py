@@ -75,6 +75,7 @@ _PROTOS = {
     "gs_server_wait": [C.c_void_p, C.c_uint64, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t),
                        C.POINTER(C.c_double)],
     "gs_server_destroy": [C.c_void_p],
+    "gs_lifted_build_leaves": [C.c_void_p, VPP, U32P, C.c_uint32, C.c_uint32, C.c_void_p],
     "gs_commit_plan_create": [C.c_void_p, U32P, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)],
     "gs_commit_plan_run": [C.c_void_p, VPP, U32P],
     "gs_commit_plan_extended": [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)],

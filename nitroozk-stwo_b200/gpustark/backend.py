@@ -146,6 +146,20 @@ class GpuBackend:
         return out
 
     @staticmethod
+    def build_leaves_lifted(columns, lifting_log_size, ctx=None, out=None):
+        """MerkleOpsLifted::build_leaves (prover/vcs_lifted/ops.rs:8-18): leaf hashes of a lifted
+        commitment, 8 words per leaf (one leaf, the hash of nothing, for no columns)."""
+        ctx = ctx or default_context()
+        n = (1 << lifting_log_size) if columns else 1
+        if out is None:
+            out = torch.empty(n * 8, dtype=torch.int32, device="cuda")
+        logs = (C.c_uint32 * max(len(columns), 1))(*[c.numel().bit_length() - 1 for c in columns])
+        pp, keep = L.ptr_array([c.data_ptr() for c in columns])
+        L.check(L.lib().gs_lifted_build_leaves(ctx.handle, pp, logs, len(columns), lifting_log_size, _p(out)),
+                "build_leaves_lifted")
+        return out
+
+    @staticmethod
     def commit_node_layers(layers, ctx=None):
         """Fills layers[L] (2^L hashes) for L < len(layers)-1 from the top layer (node-only layers)."""
         ctx = ctx or default_context()

@@ -115,6 +115,16 @@ void oracle_commit_on_layer(uint32_t log_size, const uint8_t* prev, uint32_t n_c
   memcpy(out, r.data(), 32 * n);
 }
 
+// Lifted Merkle leaves (2^lift hashes, or 1 for no columns).
+void oracle_lifted_leaves(uint32_t n_cols, const uint32_t* const* cols, const uint32_t* log_sizes, uint32_t lift,
+                          uint8_t* out) {
+  std::vector<std::vector<M31>> cv(n_cols);
+  std::vector<const std::vector<M31>*> cp;
+  for (uint32_t c = 0; c < n_cols; c++) { cv[c] = col_in(cols[c], (size_t)1 << log_sizes[c]); cp.push_back(&cv[c]); }
+  auto r = lifted_leaves(cp, lift);
+  memcpy(out, r.data(), 32 * r.size());
+}
+
 // Full Merkle commit of columns with the given log sizes; writes the root.
 void oracle_merkle_root(uint32_t n_cols, const uint32_t* const* cols, const uint32_t* log_sizes, uint8_t* root) {
   std::vector<std::vector<M31>> cv(n_cols);

@@ -6,10 +6,12 @@
 //   crates/stwo/src/prover/vcs/prover.rs:22-48            (commit: sort by length desc, stable)
 //   crates/stwo/src/prover/vcs/prover.rs:50-210           (decommit: witness order)
 //   crates/stwo/src/prover/backend/mod.rs:70-86           (batch_at_multi row-major order)
+//   crates/stwo/src/prover/backend/cpu/merkle_lifted.rs:12-88 (lifted leaves, next layer)
 #pragma once
 #include "blake2s.h"
 #include "fields.h"
 #include "circle.h"
+#include <algorithm>
 #include <map>
 #include <set>
 
@@ -33,6 +35,39 @@ inline std::vector<Hash32> commit_on_layer(uint32_t log_size, const std::vector<
     for (size_t c = 0; c < cols.size(); c++) vals[c] = (*cols[c])[i];
     if (prev) out[i] = hash_node(&(*prev)[2 * i], &(*prev)[2 * i + 1], vals.data(), vals.size());
     else out[i] = hash_node(nullptr, nullptr, vals.data(), vals.size());
+  }
+  return out;
+}
+
+// Lifted Merkle leaves (MerkleOpsLifted::build_leaves, crates/stwo/src/
+// prover/backend/cpu/merkle_lifted.rs:12-77): columns sorted by increasing
+// length (stable); leaf i of 2^lift hashes, in that order, every column's
+// value at the lifted index ((i >> (lift - log + 1)) << 1) + (i & 1). The
+// reference shares hasher prefixes between sizes; the byte stream hashed per
+// leaf is the same. No columns: the single leaf is the hash of nothing.
+inline std::vector<Hash32> lifted_leaves(const std::vector<const std::vector<M31>*>& columns_in, uint32_t lift) {
+  if (columns_in.empty()) {
+    Blake2s s;
+    return {s.finalize()};
+  }
+  std::vector<size_t> order(columns_in.size());
+  for (size_t i = 0; i < order.size(); i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](size_t a, size_t b) { return columns_in[a]->size() < columns_in[b]->size(); });
+  size_t n = (size_t)1 << lift;
+  std::vector<Hash32> out(n);
+#pragma omp parallel for schedule(static)
+  for (long long ii = 0; ii < (long long)n; ii++) {
+    size_t i = (size_t)ii;
+    Blake2s s;
+    for (size_t k : order) {
+      const auto& c = *columns_in[k];
+      uint32_t lg = 0;
+      while (((size_t)1 << lg) < c.size()) lg++;
+      size_t idx = ((i >> (lift - lg + 1)) << 1) + (i & 1);
+      s.update_u32(c[idx].v);
+    }
+    out[i] = s.finalize();
   }
   return out;
 }

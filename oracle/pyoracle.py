@@ -61,6 +61,7 @@ def _declare(L):
     f("oracle_bit_reverse", None, U32P, C.c_uint32)
     f("oracle_commit_on_layer", None, C.c_uint32, U8P, C.c_uint32, PP, U8P)
     f("oracle_merkle_root", None, C.c_uint32, PP, U32P, U8P)
+    f("oracle_lifted_leaves", None, C.c_uint32, PP, U32P, C.c_uint32, U8P)
     f("oracle_channel_mix_u32s", None, U32P, C.c_size_t, U8P)
     f("oracle_channel_mix_u64", None, C.c_uint64, U8P)
     f("oracle_channel_draw_secure_felts", C.c_uint32, U8P, C.c_size_t, U32P)
@@ -175,6 +176,17 @@ def merkle_root(cols):
     out = (C.c_uint8 * 32)()
     lib().oracle_merkle_root(len(cols), pp, logs.ctypes.data_as(U32P), out)
     return bytes(out)
+
+
+def lifted_leaves(cols, lift):
+    """MerkleOpsLifted::build_leaves: (2^lift, 32) leaf hashes ((1, 32) for no columns)."""
+    cols = [np.ascontiguousarray(c, dtype=np.uint32) for c in cols]
+    logs = np.array([int(len(c)).bit_length() - 1 for c in cols] or [0], np.uint32)
+    pp, keep = ptr_array(cols) if cols else (C.cast(None, PP), None)
+    n = (1 << lift) if cols else 1
+    out = np.zeros(n * 32, np.uint8)
+    lib().oracle_lifted_leaves(len(cols), pp, logs.ctypes.data_as(U32P), lift, out.ctypes.data_as(U8P))
+    return out.reshape(-1, 32)
 
 
 def channel_mix_u32s(words):

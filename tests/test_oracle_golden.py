@@ -188,3 +188,31 @@ def test_twiddle_tree_matches_reference_literals():
     tw, itw = O.twiddles_half_odds(log)
     assert [int(v) for v in tw] == g["twiddles"]
     assert [int(v) for v in itw] == g["itwiddles"]
+
+
+def test_lifted_leaves_follow_the_reference_lifting_table():
+    """The lifting example of the reference's lifted build_leaves doc comment
+    (cpu/merkle_lifted.rs): a size-8 column in bit-reversed order
+    a e c g b f d h, lifted to 16 leaves, reads a e a e c g c g b f b f d h d h."""
+    col = np.arange(10, 18, dtype=np.uint32)  # a..h = 10..17 in natural order
+    a, b, c, d, e, f, g, h = [int(v) for v in col]
+    bitrev = [a, e, c, g, b, f, d, h]
+    lifted = [a, e, a, e, c, g, c, g, b, f, b, f, d, h, d, h]
+    leaves = O.lifted_leaves([np.array(bitrev, np.uint32)], 4)
+    for i, v in enumerate(lifted):
+        assert bytes(leaves[i]) == hashlib.blake2s(int(v).to_bytes(4, "little")).digest()
+
+
+def test_lifted_leaves_order_and_empty():
+    """Columns are hashed in increasing size order (stable); no columns give one
+    leaf, the hash of nothing."""
+    rng = np.random.default_rng(5)
+    c3 = rng.integers(0, P, 8, dtype=np.int64).astype(np.uint32)
+    c1 = rng.integers(0, P, 2, dtype=np.int64).astype(np.uint32)
+    c3b = rng.integers(0, P, 8, dtype=np.int64).astype(np.uint32)
+    leaves = O.lifted_leaves([c3, c1, c3b], 3)
+    for i in range(8):
+        j1 = ((i >> 3) << 1) + (i & 1)
+        msg = b"".join(int(v).to_bytes(4, "little") for v in (c1[j1], c3[i], c3b[i]))
+        assert bytes(leaves[i]) == hashlib.blake2s(msg).digest()
+    assert bytes(O.lifted_leaves([], 5)[0]) == hashlib.blake2s(b"").digest()
