@@ -17,6 +17,7 @@
 #include "runtime.cuh"
 #include "blake2s.cuh"
 #include "channel.cuh"
+#include "merkle_tail.cuh"
 
 namespace gs {
 
@@ -164,45 +165,38 @@ int fold_circle_into_line_dev_alpha(cudaStream_t st, CPlanes src, uint32_t log_n
 }
 
 // Fused tail of the FRI commit phase: every layer of log size <= 11 in one
-// block of 1024 threads. For layer k (log size log0 - k, leaves already
-// hashed): its Merkle node layers, the channel step on its root (thread 0),
-// then fold_line into layer k + 1 with that layer's leaf hashes — the same
-// three steps the per-layer kernels run, with block barriers in place of
-// kernel boundaries. Data written inside the kernel is read with plain loads.
-__global__ void __launch_bounds__(1024) fri_tail_kernel(FriTail a, uint32_t* state, const uint32_t* __restrict__ itw,
-                                                        uint32_t tw_len) {
-  const uint32_t tid = threadIdx.x, bs = blockDim.x;
+// launch of one 8-CTA thread-block cluster. For layer k (log size log0 - k,
+// leaves already hashed): its Merkle node layers (each CTA its eighth of the
+// tree, then CTA 0 the last three levels), the channel step on its root (one
+// thread), then fold_line into layer k + 1 with that layer's leaf hashes,
+// split over the cluster — the same steps the per-layer kernels run, with
+// cluster barriers in place of kernel boundaries. Data written inside the
+// kernel by another CTA is read at L2 (__ldcg) after a cluster barrier.
+__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(1024) fri_tail_kernel(FriTail a, uint32_t* state,
+                                                                                  const uint32_t* __restrict__ itw,
+                                                                                  uint32_t tw_len) {
+  __shared__ uint4 buf[2][256];
+  cg::cluster_group cluster = cg::this_cluster();
+  const uint32_t gtid = cluster.block_rank() * blockDim.x + threadIdx.x;
+  const uint32_t gthreads = 8 * blockDim.x;
   for (uint32_t k = 0; k < a.n; k++) {
     const uint32_t log = a.log0 - k;
-    for (int L = (int)log - 1; L >= 0; L--) {
-      const uint32_t* prev = a.tree[k][L + 1];
-      uint32_t* out = a.tree[k][L];
-      for (uint32_t i = tid; i < (1u << L); i += bs) {
-        uint32_t h[8], m[16];
-        blake2s_init(h);
-        const uint4* pp = reinterpret_cast<const uint4*>(prev + 16 * i);
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          uint4 v = pp[q];
-          m[4 * q] = v.x; m[4 * q + 1] = v.y; m[4 * q + 2] = v.z; m[4 * q + 3] = v.w;
-        }
-        blake2s_compress(h, m, 64, true);
-        store_hash8(out, i, h);
-      }
-      __syncthreads();
-    }
-    if (tid == 0) channel_mix_root_draw_dev(state, a.tree[k][0], a.roots + 8 * k, a.felts + 8 * k);
-    __syncthreads();
+    cluster_tree_levels(log, a.tree[k], k > 0, buf, cluster);
+    if (cluster.block_rank() == 0 && threadIdx.x == 0)
+      channel_mix_root_draw_dev(state, a.tree[k][0], a.roots + 8 * k, a.felts + 8 * k);
+    cluster.sync();
     const uint32_t* f = a.felts + 8 * k;
-    const qm31 alpha = qm_make(f[0], f[1], f[2], f[3]);
-    const size_t half = (size_t)1 << (log - 1);
+    const qm31 alpha = qm_make(__ldcg(f), __ldcg(f + 1), __ldcg(f + 2), __ldcg(f + 3));
+    const uint32_t half = 1u << (log - 1);
     const uint32_t* lvl = itw + (tw_len - (1u << log));
     uint32_t* const* sp = a.planes[k];
     uint32_t* const* dp = a.planes[k + 1];
     uint32_t* leaves = (k + 1 < a.n) ? a.tree[k + 1][log - 1] : nullptr;
-    for (uint32_t i = tid; i < half; i += bs) {
-      qm31 fx = qm_make(sp[0][2 * i], sp[1][2 * i], sp[2][2 * i], sp[3][2 * i]);
-      qm31 fnx = qm_make(sp[0][2 * i + 1], sp[1][2 * i + 1], sp[2][2 * i + 1], sp[3][2 * i + 1]);
+    for (uint32_t i = gtid; i < half; i += gthreads) {
+      // layer 0's planes come from the previous kernel; later ones from this one
+      qm31 fx = qm_make(__ldcg(sp[0] + 2 * i), __ldcg(sp[1] + 2 * i), __ldcg(sp[2] + 2 * i), __ldcg(sp[3] + 2 * i));
+      qm31 fnx = qm_make(__ldcg(sp[0] + 2 * i + 1), __ldcg(sp[1] + 2 * i + 1), __ldcg(sp[2] + 2 * i + 1),
+                         __ldcg(sp[3] + 2 * i + 1));
       uint32_t xinv = __ldg(lvl + i);
       qm31 f0 = qm_add(fx, fnx);
       qm31 f1 = qm_mul_m31(qm_sub(fx, fnx), xinv);
@@ -210,7 +204,7 @@ __global__ void __launch_bounds__(1024) fri_tail_kernel(FriTail a, uint32_t* sta
       dp[0][i] = r.x.a; dp[1][i] = r.x.b; dp[2][i] = r.y.a; dp[3][i] = r.y.b;
       if (leaves) leaf_hash4(leaves, i, r);
     }
-    __syncthreads();
+    cluster.sync();
   }
 }
 
@@ -218,7 +212,7 @@ int fri_tail(cudaStream_t st, const FriTail& a, uint32_t* d_state, const uint32_
   GS_REQUIRE(a.n >= 1 && a.n <= FRI_TAIL_MAX && a.log0 <= FRI_TAIL_MAX - 1 && a.log0 >= a.n,
              "FRI tail: layer sizes out of range");
   GS_REQUIRE(a.log0 <= tw_log, "FRI tail: line domain must fit the twiddle tree");
-  fri_tail_kernel<<<1, 1024, 0, st>>>(a, d_state, d_itw, 1u << tw_log);
+  fri_tail_kernel<<<8, 1024, 0, st>>>(a, d_state, d_itw, 1u << tw_log);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;

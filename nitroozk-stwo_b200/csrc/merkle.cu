@@ -12,6 +12,8 @@
 // read as 4 x 16-byte vector loads. No byte-wise buffering.
 #include "runtime.cuh"
 #include "blake2s.cuh"
+#include "merkle_tail.cuh"
+#include "channel.cuh"
 #include <cstdlib>
 
 namespace gs {
@@ -140,38 +142,40 @@ int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, 
   return OK;
 }
 
-// Node-only layers of a small subtree in one block: starting from the layer
-// of log size `top_log` (<= MERKLE_TAIL_LOG, already in memory), computes every layer
-// down to the root, each node = Blake2s(left || right) (no columns injected
-// at these layers). Layer L is written to layers.p[L]; one launch replaces
-// top_log launches of the per-layer kernel.
+// Node-only layers of a small tree in one launch of one 8-CTA thread-block
+// cluster: starting from the layer of log size `top` (<= MERKLE_TAIL_LOG,
+// already in memory), every layer down to the root, node = Blake2s(left ||
+// right). Each CTA first computes its own eighth of the tree (layers top-1
+// down to 3) with block barriers only, passing each level to the next through
+// shared memory (and writing it to its global layer); after one cluster
+// barrier, CTA 0 computes the last 3 layers from the 8 subtree roots. Below
+// 2^11 nodes a per-layer launch is latency-bound; 8 SMs give the first levels
+// enough throughput.
 struct LayerPtrs { uint32_t* p[12]; };
 
-__global__ void __launch_bounds__(1024) merkle_tail_kernel(uint32_t top_log, LayerPtrs layers) {
-  for (int L = (int)top_log - 1; L >= 0; L--) {
-    const uint32_t* prev = layers.p[L + 1];
-    uint32_t* out = layers.p[L];
-    for (uint32_t i = threadIdx.x; i < (1u << L); i += blockDim.x) {
-      uint32_t h[8], m[16];
-      blake2s_init(h);
-      const uint4* pp = reinterpret_cast<const uint4*>(prev + 16 * i);
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        uint4 v = pp[q];  // written by this block in the previous iteration: plain loads
-        m[4 * q] = v.x; m[4 * q + 1] = v.y; m[4 * q + 2] = v.z; m[4 * q + 3] = v.w;
-      }
-      blake2s_compress(h, m, 64, true);
-      store_hash(out, i, h);
-    }
-    __syncthreads();
-  }
+// With `state`, the channel step (mix_root + draw_secure_felt) on the new
+// root follows in the same launch (FRI layers).
+__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(1024) merkle_tail_kernel(uint32_t top, LayerPtrs layers,
+                                                                                    uint32_t* state, uint32_t* root_copy,
+                                                                                    uint32_t* felt) {
+  __shared__ uint4 buf[2][256];
+  cg::cluster_group cluster = cg::this_cluster();
+  cluster_tree_levels(top, layers.p, false, buf, cluster);
+  if (state && cluster.block_rank() == 0 && threadIdx.x == 0)
+    channel_mix_root_draw_dev(state, layers.p[0], root_copy, felt);
 }
 
+int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_state,
+                          uint32_t* d_root_copy, uint32_t* d_felt);
 int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers) {
+  return commit_node_layers_ch(st, top_log, layers, nullptr, nullptr, nullptr);
+}
+
+int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_state,
+                          uint32_t* d_root_copy, uint32_t* d_felt) {
   GS_REQUIRE(top_log <= 30, "layer log size out of range");
-  // Layers of 2^8 nodes and more: one full-GPU launch each. A single block
-  // computes the rest: below 2^8 nodes a level is latency-bound, above it
-  // one SM's throughput would be the limit.
+  // Layers of 2^11 nodes and more: one full-GPU launch each; the rest in
+  // one cluster launch.
   uint32_t top = top_log;
   while (top > MERKLE_TAIL_LOG) {
     GS_TRY(commit_on_layer(st, top - 1, layers[top], nullptr, 0, layers[top - 1]));
@@ -179,13 +183,16 @@ int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layer
   }
   int L = (int)top - 1;
   uint32_t tail_top = (uint32_t)(L + 1);
-  if (tail_top == 0) return OK;
+  if (tail_top == 0) {  // a single node: it is the root already
+    GS_REQUIRE(d_state == nullptr, "channel step needs a tree of at least two leaves");
+    return OK;
+  }
   LayerPtrs lp{};
   for (uint32_t k = 0; k <= tail_top && k < 12; k++) {
     GS_REQUIRE(((uintptr_t)layers[k] & 15) == 0, "hash buffers must be 16-byte aligned");
     lp.p[k] = layers[k];
   }
-  merkle_tail_kernel<<<1, 1024, 0, st>>>(tail_top, lp);
+  merkle_tail_kernel<<<8, 1024, 0, st>>>(tail_top, lp, d_state, d_root_copy, d_felt);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;

@@ -73,8 +73,7 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
     GS_TRY(pv.table(cols, &tab));
     GS_TRY(commit_on_layer(st, lifting, nullptr, tab, 4, first.layers[lifting]));
   }
-  GS_TRY(commit_node_layers(st, first.log, first.layers.data()));
-  GS_TRY(channel_mix_root_draw(st, ctl, first.layers[0], d_roots, d_felts));
+  GS_TRY(commit_node_layers_ch(st, first.log, first.layers.data(), ctl, d_roots, d_felts));
   // fold the circle evaluation into the first line layer (zero-initialised)
   FriLayerDev cur;
   take_layer(cur, lifting - 1);
@@ -105,8 +104,7 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
       k += ft.n;
       break;
     }
-    GS_TRY(commit_node_layers(st, cur.log, cur.layers.data()));
-    GS_TRY(channel_mix_root_draw(st, ctl, cur.layers[0], d_roots + 8 * k, d_felts + 8 * k));
+    GS_TRY(commit_node_layers_ch(st, cur.log, cur.layers.data(), ctl, d_roots + 8 * k, d_felts + 8 * k));
     FriLayerDev next;
     take_layer(next, cur.log - 1);
     GS_TRY(fold_line_dev_alpha(st, CPlanes{{cur.planes[0], cur.planes[1], cur.planes[2], cur.planes[3]}}, cur.log,

@@ -139,6 +139,10 @@ int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, 
                     uint32_t n_cols, uint32_t* d_out);
 // All node-only layers below `top_log` (layers[L] has 2^L hashes, layers[top_log] given).
 int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers);
+// The same, followed by the Fiat-Shamir channel step on the root in the last
+// launch (the FRI commit phase).
+int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_state,
+                          uint32_t* d_root_copy, uint32_t* d_felt);
 // Lifted Merkle leaves; d_shifts[c] = lift - log size of column c (columns in
 // increasing size order).
 int lifted_leaves(cudaStream_t st, uint32_t lift, const uint32_t* const* d_cols, const uint8_t* d_shifts,
@@ -148,10 +152,10 @@ int lifted_leaves(cudaStream_t st, uint32_t lift, const uint32_t* const* d_cols,
 // log0 - k; layers 0..n-1 are committed (tree[k][L] = their Merkle layers,
 // leaves of layer 0 already hashed), layer n is the last layer.
 constexpr uint32_t FRI_TAIL_MAX = 12;
-// Largest layer (log size) handled by the single-block tails: Merkle node
-// layers below it, and the fused FRI tail from it down.
-constexpr uint32_t MERKLE_TAIL_LOG = 8;
-constexpr uint32_t FRI_TAIL_LOG = 8;
+// Largest layer (log size) handled by the cluster tails: Merkle node layers
+// below it, and the fused FRI tail from it down.
+constexpr uint32_t MERKLE_TAIL_LOG = 11;
+constexpr uint32_t FRI_TAIL_LOG = 11;
 struct FriTail {
   uint32_t n = 0, log0 = 0;
   uint32_t* planes[FRI_TAIL_MAX + 1][4] = {};
