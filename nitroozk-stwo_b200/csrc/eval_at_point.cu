@@ -14,7 +14,7 @@
 
 namespace gs {
 
-constexpr uint32_t EAP_S = 10;                 // low bits per chunk: 1024 coefficients
+constexpr uint32_t EAP_S = 12;                 // default low bits per chunk: 4096 coefficients
 
 struct Factors { qm31 f[31]; };
 
@@ -30,13 +30,16 @@ __global__ void eap_weights_kernel(Factors fs, uint32_t s, uint32_t* w /* [j][4]
 
 __device__ __forceinline__ uint64_t fold64e(uint64_t x) { return (x & P) + (x >> 31); }
 
-// grid: (chunks per poly, n_polys). Each block handles one chunk of one poly.
+// grid: (chunks per poly, n_polys). Each block handles one chunk of 2^s
+// coefficients of one poly, 2^(s-8) per thread: products of M31 by the QM31
+// weights accumulate in 64 bits, folded every third term (a folded value is
+// below 2^34, a product below 2^62).
 __global__ void __launch_bounds__(256) eap_chunk_kernel(const uint32_t* const* __restrict__ polys, uint32_t log_n,
-                                                        const uint32_t* __restrict__ w, Factors fs, uint32_t* partials) {
+                                                        uint32_t s, const uint32_t* __restrict__ w, Factors fs,
+                                                        uint32_t* partials) {
   __shared__ uint32_t red[4][256 / 32];
   const uint32_t poly = blockIdx.y;
   const uint32_t chunk = blockIdx.x;
-  const uint32_t s = log_n < EAP_S ? log_n : EAP_S;
   const uint32_t clen = 1u << s;
   const uint32_t* c = polys[poly] + ((size_t)chunk << s);
   uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
@@ -45,7 +48,7 @@ __global__ void __launch_bounds__(256) eap_chunk_kernel(const uint32_t* const* _
     uint32_t v = __ldg(c + j);
     uint4 wj = __ldg(reinterpret_cast<const uint4*>(w) + j);
     a0 += (uint64_t)wj.x * v; a1 += (uint64_t)wj.y * v; a2 += (uint64_t)wj.z * v; a3 += (uint64_t)wj.w * v;
-    if (++cnt == 2) { a0 = fold64e(a0); a1 = fold64e(a1); a2 = fold64e(a2); a3 = fold64e(a3); cnt = 0; }
+    if (++cnt == 3) { a0 = fold64e(a0); a1 = fold64e(a1); a2 = fold64e(a2); a3 = fold64e(a3); cnt = 0; }
   }
   uint32_t r0 = reduce64(a0), r1 = reduce64(a1), r2 = reduce64(a2), r3 = reduce64(a3);
   // warp reduction (field adds)
@@ -115,19 +118,21 @@ static Factors eap_factors(const ptq& p, uint32_t log_n) {
   return fs;
 }
 
-size_t eval_at_point_scratch_bytes(uint32_t n_polys, uint32_t log_n) {
-  uint32_t s = log_n < EAP_S ? log_n : EAP_S;
+size_t eval_at_point_scratch_bytes(uint32_t n_polys, uint32_t log_n, uint32_t chunk_log) {
+  uint32_t s = log_n < chunk_log ? log_n : chunk_log;
   size_t chunks = (size_t)1 << (log_n - s);
   return 16 * ((size_t)1 << s) + 16 * chunks * n_polys;
 }
 
-// out: 4 words per polynomial (device). scratch: eval_at_point_scratch_bytes().
+// out: 4 words per polynomial (device). scratch: eval_at_point_scratch_bytes()
+// for the same chunk_log (coefficients per block, log 2).
 int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_t n_polys, uint32_t log_n, ptq point,
-                        uint32_t* d_out, uint32_t* d_scratch) {
+                        uint32_t* d_out, uint32_t* d_scratch, uint32_t chunk_log) {
   GS_REQUIRE(log_n <= 30, "log size out of range");
+  GS_REQUIRE(chunk_log >= 8 && chunk_log <= 14, "chunk log size out of range");
   if (n_polys == 0) return OK;
   Factors fs = eap_factors(point, log_n);
-  uint32_t s = log_n < EAP_S ? log_n : EAP_S;
+  uint32_t s = log_n < chunk_log ? log_n : chunk_log;
   uint32_t chunks = 1u << (log_n - s);
   GS_REQUIRE(chunks <= 65535 * 32768u, "too many chunks");
   uint32_t* w = d_scratch;
@@ -136,7 +141,7 @@ int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   dim3 grid(chunks, n_polys);
-  eap_chunk_kernel<<<grid, 256, 0, st>>>(d_polys, log_n, w, fs, partials);
+  eap_chunk_kernel<<<grid, 256, 0, st>>>(d_polys, log_n, s, w, fs, partials);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   eap_finalize_kernel<<<n_polys, 128, 0, st>>>(partials, chunks, n_polys, d_out);

@@ -24,6 +24,7 @@
 namespace gs {
 
 constexpr uint32_t EAPS_MAX_POLYS = 256;
+constexpr uint32_t EAPS_CHUNK_LOG = 10;                                 // 2^10 coefficients per chunk
 constexpr size_t EAPS_TABLE_BYTES = EAPS_MAX_POLYS * sizeof(void*);    // 2 KiB
 constexpr size_t EAPS_OUT_BYTES = 16 * (size_t)EAPS_MAX_POLYS;         // 4 KiB
 constexpr size_t EAPS_WORK_BYTES = (16u << 10) + (4u << 20);           // 2^10 weights + 2^18 partials
@@ -60,7 +61,7 @@ extern "C" int gs_batch_eval_at_point_noalloc(void* stream, const uint32_t* cons
   GS_REQUIRE(polys && out, "null argument");
   GS_REQUIRE(n_polys <= EAPS_MAX_POLYS, "more than 256 polynomials");
   GS_REQUIRE(log_size <= 30, "log size out of range");
-  GS_REQUIRE(eval_at_point_scratch_bytes(n_polys, log_size) <= EAPS_WORK_BYTES,
+  GS_REQUIRE(eval_at_point_scratch_bytes(n_polys, log_size, EAPS_CHUNK_LOG) <= EAPS_WORK_BYTES,
              "n_polys * 2^(log_size - 10) exceeds 2^18 chunks");
   PolyTable t;
   for (uint32_t i = 0; i < n_polys; i++) {
@@ -77,7 +78,8 @@ extern "C" int gs_batch_eval_at_point_noalloc(void* stream, const uint32_t* cons
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   ptq p = {qm_make(point.x.a, point.x.b, point.x.c, point.x.d), qm_make(point.y.a, point.y.b, point.y.c, point.y.d)};
-  GS_TRY(batch_eval_at_point(st, (const uint32_t* const*)d_table, n_polys, log_size, p, d_out, d_work));
+  GS_TRY(batch_eval_at_point(st, (const uint32_t* const*)d_table, n_polys, log_size, p, d_out, d_work,
+                             EAPS_CHUNK_LOG));
   GS_CUDA_TRY(cudaMemcpyAsync(out, d_out, 16 * (size_t)n_polys, cudaMemcpyDeviceToHost, st));
   GS_CUDA_TRY(cudaStreamSynchronize(st));
   return OK;

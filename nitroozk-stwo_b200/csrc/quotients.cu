@@ -38,33 +38,57 @@ __device__ __forceinline__ pt31 domain_point_bitrev(const DomainTables& t, uint3
 // ------------------------------------------------------------ numerators
 __device__ __forceinline__ uint64_t fold64(uint64_t x) { return (x & P) + (x >> 31); }
 
-__global__ void accumulate_numerators_kernel(const NumEntry* __restrict__ entries, uint32_t n_entries, qm31 b_sum,
-                                             uint32_t log_size, Planes out) {
+// Row per thread. The batch's entries are staged in shared memory once per
+// block; each step issues the column loads of 6 entries before using them
+// (enough loads in flight to cover DRAM latency), and the 64-bit
+// accumulators are folded after every third product (a folded value is below
+// 2^34, a product below 2^62).
+constexpr uint32_t ACC_MAX_SMEM_ENTRIES = 512;
+
+__device__ __forceinline__ void acc_term(uint64_t acc[4], const NumEntry& e, uint32_t v) {
+  acc[0] += (uint64_t)e.c[0] * v;
+  acc[1] += (uint64_t)e.c[1] * v;
+  acc[2] += (uint64_t)e.c[2] * v;
+  acc[3] += (uint64_t)e.c[3] * v;
+}
+
+__global__ void __launch_bounds__(256) accumulate_numerators_kernel(const NumEntry* __restrict__ entries,
+                                                                    uint32_t n_entries, qm31 b_sum, uint32_t log_size,
+                                                                    Planes out) {
+  __shared__ NumEntry se[ACC_MAX_SMEM_ENTRIES];
+  const bool staged = n_entries <= ACC_MAX_SMEM_ENTRIES;
+  if (staged)
+    for (uint32_t k = threadIdx.x; k < n_entries; k += blockDim.x) se[k] = entries[k];
+  __syncthreads();
+  const NumEntry* E = staged ? se : entries;
   const size_t n = (size_t)1 << log_size;
   for (size_t row = blockIdx.x * (size_t)blockDim.x + threadIdx.x; row < n; row += (size_t)gridDim.x * blockDim.x) {
-    uint64_t acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
+    uint64_t acc[4] = {0, 0, 0, 0};
     uint32_t k = 0;
-    for (; k + 1 < n_entries; k += 2) {
-      const NumEntry e0 = entries[k], e1 = entries[k + 1];
-      uint32_t v0 = __ldg(e0.col + row), v1 = __ldg(e1.col + row);
-      acc0 += (uint64_t)e0.c[0] * v0 + (uint64_t)e1.c[0] * v1;
-      acc1 += (uint64_t)e0.c[1] * v0 + (uint64_t)e1.c[1] * v1;
-      acc2 += (uint64_t)e0.c[2] * v0 + (uint64_t)e1.c[2] * v1;
-      acc3 += (uint64_t)e0.c[3] * v0 + (uint64_t)e1.c[3] * v1;
-      acc0 = fold64(acc0); acc1 = fold64(acc1); acc2 = fold64(acc2); acc3 = fold64(acc3);
+    for (; k + 6 <= n_entries; k += 6) {
+      uint32_t v[6];
+#pragma unroll
+      for (int j = 0; j < 6; j++) v[j] = __ldg(E[k + j].col + row);
+#pragma unroll
+      for (int j = 0; j < 6; j++) {
+        acc_term(acc, E[k + j], v[j]);
+        if (j == 2 || j == 5)
+#pragma unroll
+          for (int q = 0; q < 4; q++) acc[q] = fold64(acc[q]);
+      }
     }
-    if (k < n_entries) {
-      const NumEntry e0 = entries[k];
-      uint32_t v0 = __ldg(e0.col + row);
-      acc0 += (uint64_t)e0.c[0] * v0;
-      acc1 += (uint64_t)e0.c[1] * v0;
-      acc2 += (uint64_t)e0.c[2] * v0;
-      acc3 += (uint64_t)e0.c[3] * v0;
+    for (int cnt = 0; k < n_entries; k++) {
+      acc_term(acc, E[k], __ldg(E[k].col + row));
+      if (++cnt == 3) {
+        cnt = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[q] = fold64(acc[q]);
+      }
     }
-    out.p[0][row] = sub(reduce64(acc0), b_sum.x.a);
-    out.p[1][row] = sub(reduce64(acc1), b_sum.x.b);
-    out.p[2][row] = sub(reduce64(acc2), b_sum.y.a);
-    out.p[3][row] = sub(reduce64(acc3), b_sum.y.b);
+    out.p[0][row] = sub(reduce64(acc[0]), b_sum.x.a);
+    out.p[1][row] = sub(reduce64(acc[1]), b_sum.x.b);
+    out.p[2][row] = sub(reduce64(acc[2]), b_sum.y.a);
+    out.p[3][row] = sub(reduce64(acc[3]), b_sum.y.b);
   }
 }
 

@@ -192,9 +192,9 @@ struct QuotAcc {
 struct LiftCol { const uint32_t* p[4]; uint32_t log_size; uint32_t pad; };
 
 // eval_at_point.cu
-size_t eval_at_point_scratch_bytes(uint32_t n_polys, uint32_t log_n);
+size_t eval_at_point_scratch_bytes(uint32_t n_polys, uint32_t log_n, uint32_t chunk_log = 12);
 int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_t n_polys, uint32_t log_n, ptq point,
-                        uint32_t* d_out, uint32_t* d_scratch);
+                        uint32_t* d_out, uint32_t* d_scratch, uint32_t chunk_log = 12);
 
 // grind.cu
 int grind_blake2s(cudaStream_t st, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint32_t* d_scratch,
