@@ -232,9 +232,12 @@ int gs_accumulate_numerators(gs_ctx* ctx, uint32_t log_size, const uint32_t* con
     entries[k].c[2] = line_coeffs_c[k].c; entries[k].c[3] = line_coeffs_c[k].d;
     bsum = qm_add(bsum, to_qm(line_coeffs_b[k]));
   }
+  bool vec = true;
+  for (auto& e : entries) vec = vec && ((uintptr_t)e.col & 15) == 0;
+  for (int i = 0; i < 4; i++) vec = vec && ((uintptr_t)o.p[i] & 15) == 0;
   const void* d = nullptr;
   if (n_coeffs) GS_TRY(ctx->c.stage_bytes(entries.data(), entries.size() * sizeof(NumEntry), &d));
-  return accumulate_numerators(ctx->c.stream, d, n_coeffs, bsum, log_size, o);
+  return accumulate_numerators(ctx->c.stream, d, n_coeffs, bsum, log_size, o, vec);
 }
 
 int gs_compute_quotients_and_combine(gs_ctx* ctx, const gs_quotient_acc* accs, uint32_t n_accs,
@@ -315,7 +318,10 @@ int gs_batch_eval_at_point(gs_ctx* ctx, const uint32_t* const* polys, uint32_t n
   GS_TRY(ctx->c.stage_ptrs((const void* const*)polys, n_polys, &d));
   uint32_t* d_out = (uint32_t*)((uint8_t*)scratch + eval_at_point_scratch_bytes(n_polys, log_size));
   ptq p = {to_qm(point.x), to_qm(point.y)};
-  GS_TRY(batch_eval_at_point(ctx->c.stream, (const uint32_t* const*)d, n_polys, log_size, p, d_out, (uint32_t*)scratch));
+  bool vec = true;
+  for (uint32_t i = 0; i < n_polys; i++) vec = vec && ((uintptr_t)polys[i] & 15) == 0;
+  GS_TRY(batch_eval_at_point(ctx->c.stream, (const uint32_t* const*)d, n_polys, log_size, p, d_out, (uint32_t*)scratch,
+                             12, vec));
   GS_CUDA_TRY(cudaMemcpyAsync(out, d_out, 16 * (size_t)n_polys, cudaMemcpyDeviceToHost, ctx->c.stream));
   GS_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
   return OK;

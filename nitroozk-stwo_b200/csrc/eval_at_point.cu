@@ -36,7 +36,7 @@ __device__ __forceinline__ uint64_t fold64e(uint64_t x) { return (x & P) + (x >>
 // below 2^34, a product below 2^62).
 __global__ void __launch_bounds__(256) eap_chunk_kernel(const uint32_t* const* __restrict__ polys, uint32_t log_n,
                                                         uint32_t s, const uint32_t* __restrict__ w, Factors fs,
-                                                        uint32_t* partials) {
+                                                        uint32_t* partials, bool vec) {
   __shared__ uint32_t red[4][256 / 32];
   const uint32_t poly = blockIdx.y;
   const uint32_t chunk = blockIdx.x;
@@ -44,11 +44,34 @@ __global__ void __launch_bounds__(256) eap_chunk_kernel(const uint32_t* const* _
   const uint32_t* c = polys[poly] + ((size_t)chunk << s);
   uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
   int cnt = 0;
-  for (uint32_t j = threadIdx.x; j < clen; j += blockDim.x) {
-    uint32_t v = __ldg(c + j);
-    uint4 wj = __ldg(reinterpret_cast<const uint4*>(w) + j);
-    a0 += (uint64_t)wj.x * v; a1 += (uint64_t)wj.y * v; a2 += (uint64_t)wj.z * v; a3 += (uint64_t)wj.w * v;
-    if (++cnt == 3) { a0 = fold64e(a0); a1 = fold64e(a1); a2 = fold64e(a2); a3 = fold64e(a3); cnt = 0; }
+  if (vec && clen >= 4 * blockDim.x) {
+    // four consecutive coefficients per 16-byte load, two loads in flight
+    for (uint32_t j0 = 4 * threadIdx.x; j0 < clen; j0 += 8 * blockDim.x) {
+      uint4 v4[2];
+      v4[0] = __ldg(reinterpret_cast<const uint4*>(c + j0));
+      const bool two = j0 + 4 * blockDim.x < clen;
+      if (two) v4[1] = __ldg(reinterpret_cast<const uint4*>(c + j0 + 4 * blockDim.x));
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        if (h == 1 && !two) break;
+        const uint32_t jb = j0 + h * 4 * blockDim.x;
+        const uint32_t vv[4] = {v4[h].x, v4[h].y, v4[h].z, v4[h].w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          uint4 wj = __ldg(reinterpret_cast<const uint4*>(w) + jb + e);
+          const uint32_t v = vv[e];
+          a0 += (uint64_t)wj.x * v; a1 += (uint64_t)wj.y * v; a2 += (uint64_t)wj.z * v; a3 += (uint64_t)wj.w * v;
+          if (++cnt == 3) { a0 = fold64e(a0); a1 = fold64e(a1); a2 = fold64e(a2); a3 = fold64e(a3); cnt = 0; }
+        }
+      }
+    }
+  } else {
+    for (uint32_t j = threadIdx.x; j < clen; j += blockDim.x) {
+      uint32_t v = __ldg(c + j);
+      uint4 wj = __ldg(reinterpret_cast<const uint4*>(w) + j);
+      a0 += (uint64_t)wj.x * v; a1 += (uint64_t)wj.y * v; a2 += (uint64_t)wj.z * v; a3 += (uint64_t)wj.w * v;
+      if (++cnt == 3) { a0 = fold64e(a0); a1 = fold64e(a1); a2 = fold64e(a2); a3 = fold64e(a3); cnt = 0; }
+    }
   }
   uint32_t r0 = reduce64(a0), r1 = reduce64(a1), r2 = reduce64(a2), r3 = reduce64(a3);
   // warp reduction (field adds)
@@ -127,7 +150,7 @@ size_t eval_at_point_scratch_bytes(uint32_t n_polys, uint32_t log_n, uint32_t ch
 // out: 4 words per polynomial (device). scratch: eval_at_point_scratch_bytes()
 // for the same chunk_log (coefficients per block, log 2).
 int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_t n_polys, uint32_t log_n, ptq point,
-                        uint32_t* d_out, uint32_t* d_scratch, uint32_t chunk_log) {
+                        uint32_t* d_out, uint32_t* d_scratch, uint32_t chunk_log, bool vec) {
   GS_REQUIRE(log_n <= 30, "log size out of range");
   GS_REQUIRE(chunk_log >= 8 && chunk_log <= 14, "chunk log size out of range");
   if (n_polys == 0) return OK;
@@ -141,7 +164,7 @@ int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   dim3 grid(chunks, n_polys);
-  eap_chunk_kernel<<<grid, 256, 0, st>>>(d_polys, log_n, s, w, fs, partials);
+  eap_chunk_kernel<<<grid, 256, 0, st>>>(d_polys, log_n, s, w, fs, partials, vec);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   eap_finalize_kernel<<<n_polys, 128, 0, st>>>(partials, chunks, n_polys, d_out);

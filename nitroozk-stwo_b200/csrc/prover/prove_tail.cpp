@@ -69,9 +69,11 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     GS_TRY(pv.A.alloc(scratch_bytes + 16, &scratch));
     for (auto& r : reqs) {
       Tree& tr = pv.trees[r.t];
+      bool vec = true;
+      for (auto* c : tr.coeff_ptrs) vec = vec && ((uintptr_t)c & 15) == 0;
       GS_TRY(batch_eval_at_point(st, tr.coeff_tab, tr.n_cols, tr.coeff_log,
                                  host::ptq_rep_double(r.p, lifting - tr.eval_log), d_vals + 4 * r.slot,
-                                 (uint32_t*)scratch));
+                                 (uint32_t*)scratch, 12, vec));
     }
     std::vector<uint32_t> h(4 * n_vals);
     GS_TRY(pv.ctx.read_back(d_vals, h.size() * 4, h.data()));
@@ -166,8 +168,10 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     const void* d_entries = nullptr;
     GS_TRY(pv.ctx.stage_bytes(bt.entries.data(), bt.entries.size() * sizeof(NumEntry), &d_entries));
     size_t nn = (size_t)1 << bt.log;
+    bool vec = bt.log >= 2;  // tree columns and these planes sit at multiples of 2^log words
+    for (auto& e : bt.entries) vec = vec && ((uintptr_t)e.col & 15) == 0;
     GS_TRY(accumulate_numerators(st, d_entries, (uint32_t)bt.entries.size(), bt.b_sum, bt.log,
-                                 Planes{{planes, planes + nn, planes + 2 * nn, planes + 3 * nn}}));
+                                 Planes{{planes, planes + nn, planes + 2 * nn, planes + 3 * nn}}, vec));
     PointAcc2* pa = nullptr;
     for (auto& x : per_point)
       if (pt_eq(x.point, bt.point)) pa = &x;

@@ -38,11 +38,13 @@ __device__ __forceinline__ pt31 domain_point_bitrev(const DomainTables& t, uint3
 // ------------------------------------------------------------ numerators
 __device__ __forceinline__ uint64_t fold64(uint64_t x) { return (x & P) + (x >> 31); }
 
-// Row per thread. The batch's entries are staged in shared memory once per
-// block; each step issues the column loads of 6 entries before using them
-// (enough loads in flight to cover DRAM latency), and the 64-bit
-// accumulators are folded after every third product (a folded value is below
-// 2^34, a product below 2^62).
+// The batch's entries are staged in shared memory once per block. VEC: four
+// consecutive rows per thread, each column read as one 16-byte load (all
+// column pointers 16-byte aligned); otherwise one row per thread. Each step
+// issues the column loads of 6 entries before using them (enough bytes in
+// flight to cover DRAM latency), and the 64-bit accumulators are folded
+// after every third product (a folded value is below 2^34, a product below
+// 2^62).
 constexpr uint32_t ACC_MAX_SMEM_ENTRIES = 512;
 
 __device__ __forceinline__ void acc_term(uint64_t acc[4], const NumEntry& e, uint32_t v) {
@@ -52,6 +54,17 @@ __device__ __forceinline__ void acc_term(uint64_t acc[4], const NumEntry& e, uin
   acc[3] += (uint64_t)e.c[3] * v;
 }
 
+template <int R>
+__device__ __forceinline__ void load_rows(const uint32_t* col, size_t row0, uint32_t v[R]) {
+  if (R == 4) {
+    uint4 q = __ldg(reinterpret_cast<const uint4*>(col + row0));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+  } else {
+    v[0] = __ldg(col + row0);
+  }
+}
+
+template <int R>
 __global__ void __launch_bounds__(256) accumulate_numerators_kernel(const NumEntry* __restrict__ entries,
                                                                     uint32_t n_entries, qm31 b_sum, uint32_t log_size,
                                                                     Planes out) {
@@ -62,46 +75,144 @@ __global__ void __launch_bounds__(256) accumulate_numerators_kernel(const NumEnt
   __syncthreads();
   const NumEntry* E = staged ? se : entries;
   const size_t n = (size_t)1 << log_size;
-  for (size_t row = blockIdx.x * (size_t)blockDim.x + threadIdx.x; row < n; row += (size_t)gridDim.x * blockDim.x) {
-    uint64_t acc[4] = {0, 0, 0, 0};
+  for (size_t row0 = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) * R; row0 < n;
+       row0 += (size_t)gridDim.x * blockDim.x * R) {
+    uint64_t acc[R][4] = {};
     uint32_t k = 0;
     for (; k + 6 <= n_entries; k += 6) {
-      uint32_t v[6];
+      uint32_t v[6][R];
 #pragma unroll
-      for (int j = 0; j < 6; j++) v[j] = __ldg(E[k + j].col + row);
+      for (int j = 0; j < 6; j++) load_rows<R>(E[k + j].col, row0, v[j]);
 #pragma unroll
       for (int j = 0; j < 6; j++) {
-        acc_term(acc, E[k + j], v[j]);
-        if (j == 2 || j == 5)
 #pragma unroll
-          for (int q = 0; q < 4; q++) acc[q] = fold64(acc[q]);
+        for (int r = 0; r < R; r++) {
+          acc_term(acc[r], E[k + j], v[j][r]);
+          if (j == 2 || j == 5)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[r][q] = fold64(acc[r][q]);
+        }
       }
     }
     for (int cnt = 0; k < n_entries; k++) {
-      acc_term(acc, E[k], __ldg(E[k].col + row));
+      uint32_t v[R];
+      load_rows<R>(E[k].col, row0, v);
+#pragma unroll
+      for (int r = 0; r < R; r++) acc_term(acc[r], E[k], v[r]);
       if (++cnt == 3) {
         cnt = 0;
 #pragma unroll
-        for (int q = 0; q < 4; q++) acc[q] = fold64(acc[q]);
+        for (int r = 0; r < R; r++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) acc[r][q] = fold64(acc[r][q]);
       }
     }
-    out.p[0][row] = sub(reduce64(acc[0]), b_sum.x.a);
-    out.p[1][row] = sub(reduce64(acc[1]), b_sum.x.b);
-    out.p[2][row] = sub(reduce64(acc[2]), b_sum.y.a);
-    out.p[3][row] = sub(reduce64(acc[3]), b_sum.y.b);
+    uint32_t o[4][R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      o[0][r] = sub(reduce64(acc[r][0]), b_sum.x.a);
+      o[1][r] = sub(reduce64(acc[r][1]), b_sum.x.b);
+      o[2][r] = sub(reduce64(acc[r][2]), b_sum.y.a);
+      o[3][r] = sub(reduce64(acc[r][3]), b_sum.y.b);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      if (R == 4)
+        *reinterpret_cast<uint4*>(out.p[q] + row0) = make_uint4(o[q][0], o[q][1], o[q][2], o[q][3]);
+      else
+        out.p[q][row0] = o[q][0];
+    }
+  }
+}
+
+// Vector path with the entries split over the block's 8 warps: a block owns
+// 128 rows (lane l: rows 4l..4l+3, one 16-byte load per column), warp w
+// accumulates entries w, w + 8, ..., and the 8 partial sums meet in shared
+// memory. A thread's chain of dependent loads is n_entries / 48 steps long
+// instead of n_entries / 6.
+__global__ void __launch_bounds__(256) accumulate_numerators_split_kernel(const NumEntry* __restrict__ entries,
+                                                                          uint32_t n_entries, qm31 b_sum,
+                                                                          uint32_t log_size, Planes out) {
+  __shared__ NumEntry se[ACC_MAX_SMEM_ENTRIES];
+  __shared__ uint32_t part[8][4][128];  // [warp][coordinate][row in tile]
+  const bool staged = n_entries <= ACC_MAX_SMEM_ENTRIES;
+  if (staged)
+    for (uint32_t k = threadIdx.x; k < n_entries; k += blockDim.x) se[k] = entries[k];
+  __syncthreads();
+  const NumEntry* E = staged ? se : entries;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t n = (size_t)1 << log_size;
+  for (size_t tile = blockIdx.x; tile * 128 < n; tile += gridDim.x) {
+    const size_t row0 = tile * 128 + 4 * lane;
+    uint64_t acc[4][4] = {};
+    uint32_t k = warp;
+    for (; k + 40 < n_entries; k += 48) {  // entries k, k+8, ..., k+40
+      uint32_t v[6][4];
+#pragma unroll
+      for (int j = 0; j < 6; j++) load_rows<4>(E[k + 8 * j].col, row0, v[j]);
+#pragma unroll
+      for (int j = 0; j < 6; j++) {
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          acc_term(acc[r], E[k + 8 * j], v[j][r]);
+          if (j == 2 || j == 5)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[r][q] = fold64(acc[r][q]);
+        }
+      }
+    }
+    for (int cnt = 0; k < n_entries; k += 8) {
+      uint32_t v[4];
+      load_rows<4>(E[k].col, row0, v);
+#pragma unroll
+      for (int r = 0; r < 4; r++) acc_term(acc[r], E[k], v[r]);
+      if (++cnt == 3) {
+        cnt = 0;
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) acc[r][q] = fold64(acc[r][q]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) part[warp][q][4 * lane + r] = reduce64(acc[r][q]);
+    __syncthreads();
+    const uint32_t bs[4] = {b_sum.x.a, b_sum.x.b, b_sum.y.a, b_sum.y.b};
+    for (uint32_t idx = threadIdx.x; idx < 512; idx += blockDim.x) {
+      const uint32_t q = idx >> 7, rr = idx & 127;
+      uint32_t t = part[0][q][rr];
+#pragma unroll
+      for (int w = 1; w < 8; w++) t = add(t, part[w][q][rr]);
+      if (tile * 128 + rr < n) out.p[q][tile * 128 + rr] = sub(t, bs[q]);
+    }
+    __syncthreads();
   }
 }
 
 int accumulate_numerators(cudaStream_t st, const void* d_entries, uint32_t n_entries, qm31 b_sum, uint32_t log_size,
-                          Planes out) {
+                          Planes out, bool vec) {
   GS_REQUIRE(log_size <= 30, "log size out of range");
   size_t n = (size_t)1 << log_size;
   int threads = 256;
-  size_t blocks = (n + threads - 1) / threads;
+  const uint32_t R = (vec && log_size >= 2) ? 4 : 1;
+  if (R == 4)
+    for (int q = 0; q < 4; q++) GS_REQUIRE(((uintptr_t)out.p[q] & 15) == 0, "vector path needs aligned planes");
+  size_t blocks = (n / R + threads - 1) / threads;
   size_t cap = (size_t)num_sms() * 16;
   if (blocks > cap) blocks = cap;
-  accumulate_numerators_kernel<<<(unsigned)blocks, threads, 0, st>>>((const NumEntry*)d_entries, n_entries, b_sum,
-                                                                      log_size, out);
+  if (R == 4 && log_size >= 7) {
+    size_t tiles = n / 128;
+    size_t cap2 = (size_t)num_sms() * 8;
+    accumulate_numerators_split_kernel<<<(unsigned)(tiles < cap2 ? tiles : cap2), 256, 0, st>>>(
+        (const NumEntry*)d_entries, n_entries, b_sum, log_size, out);
+  } else if (R == 4)
+    accumulate_numerators_kernel<4><<<(unsigned)blocks, threads, 0, st>>>((const NumEntry*)d_entries, n_entries,
+                                                                         b_sum, log_size, out);
+  else
+    accumulate_numerators_kernel<1><<<(unsigned)blocks, threads, 0, st>>>((const NumEntry*)d_entries, n_entries,
+                                                                         b_sum, log_size, out);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;

@@ -172,8 +172,10 @@ int fold_circle_into_line(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alp
                           const uint32_t* d_itwiddles, uint32_t tw_log);
 
 // quotients.cu
+// vec: every column pointer and output plane is 16-byte aligned (4 rows per
+// thread with vector loads).
 int accumulate_numerators(cudaStream_t st, const void* d_entries, uint32_t n_entries, qm31 b_sum, uint32_t log_size,
-                          Planes out);
+                          Planes out, bool vec = false);
 int compute_quotients_and_combine(cudaStream_t st, const void* d_accs, uint32_t n_accs, const DomainTables& dt,
                                   Planes out);
 int lift_and_accumulate(cudaStream_t st, const void* d_cols, uint32_t n_cols, uint32_t log_size, Planes out);
@@ -194,7 +196,7 @@ struct LiftCol { const uint32_t* p[4]; uint32_t log_size; uint32_t pad; };
 // eval_at_point.cu
 size_t eval_at_point_scratch_bytes(uint32_t n_polys, uint32_t log_n, uint32_t chunk_log = 12);
 int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_t n_polys, uint32_t log_n, ptq point,
-                        uint32_t* d_out, uint32_t* d_scratch, uint32_t chunk_log = 12);
+                        uint32_t* d_out, uint32_t* d_scratch, uint32_t chunk_log = 12, bool vec = false);
 
 // grind.cu
 int grind_blake2s(cudaStream_t st, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint32_t* d_scratch,
