@@ -1,0 +1,128 @@
+"""The library's kernels against the reference's own CUDA kernels, built for
+sm_100a from the reference sources by oracle/Makefile.refcuda into
+oracle/_ref/libstwo_cuda_ref.so (skipped when that library is absent): the
+circle FFT (ntt_n2b_columns / ntt_b2n_column) and the Blake2s leaf layer
+(commit_on_first_layer) must give identical outputs on the same inputs.
+With -s, the timing test prints both implementations' device times."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as O
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+P = O.P
+REF_LIB = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                       "libstwo_cuda_ref.so")
+
+
+@pytest.fixture(scope="module")
+def ref():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    if not os.path.exists(REF_LIB):
+        pytest.skip("reference CUDA library not built (oracle/Makefile.refcuda)")
+    lib = C.CDLL(REF_LIB)
+    VP = C.c_void_p
+    # bindings.rs:503-519, 262-275
+    lib.ntt_n2b_columns.argtypes = [C.POINTER(VP), C.c_uint, C.c_uint, VP, C.c_uint, C.c_uint]
+    lib.ntt_b2n_column.argtypes = [C.POINTER(VP), C.c_uint32, C.c_uint32, VP, C.c_uint32, C.c_uint32]
+    lib.commit_on_first_layer.argtypes = [C.c_uint32, C.c_uint32, VP, VP]
+    for f in (lib.ntt_n2b_columns, lib.ntt_b2n_column, lib.commit_on_first_layer):
+        f.restype = None
+    return lib
+
+
+@pytest.fixture(scope="module")
+def B():
+    from gpustark.backend import GpuBackend
+    return GpuBackend
+
+
+def ptrs(tensors):
+    return (C.c_void_p * len(tensors))(*[t.data_ptr() for t in tensors])
+
+
+def ref_evaluate(ref, cols, log, tw):
+    arr = ptrs(cols)
+    ref.ntt_n2b_columns(arr, log, len(cols), tw.twiddles.data_ptr(), 1 << (log - 1), 1 << (log - 1))
+
+
+def ref_interpolate(ref, cols, log, tw):
+    arr = ptrs(cols)
+    ref.ntt_b2n_column(arr, log, len(cols), tw.itwiddles.data_ptr(), 1 << (log - 1), 1 << (log - 1))
+
+
+@pytest.mark.parametrize("log,n_cols", [(13, 3), (16, 2), (19, 1), (20, 4), (24, 1)])
+def test_fft_matches_reference_cuda(ref, B, log, n_cols):
+    from gpustark.backend import to_device
+    rng = np.random.default_rng(log)
+    tw = B.precompute_twiddles(log - 1)
+    coeffs = [to_device(rng.integers(0, P, 1 << log, dtype=np.int64).astype(np.uint32)) for _ in range(n_cols)]
+    ours = B.evaluate_polynomials(coeffs, log, tw)
+    theirs = [c.clone() for c in coeffs]
+    ref_evaluate(ref, theirs, log, tw)
+    torch.cuda.synchronize()
+    for a, b in zip(ours, theirs):
+        assert torch.equal(a, b)
+    back = [t.clone() for t in theirs]
+    ref_interpolate(ref, back, log, tw)
+    B.interpolate_columns(theirs, log, tw)
+    torch.cuda.synchronize()
+    for a, b, c in zip(back, theirs, coeffs):
+        assert torch.equal(a, b) and torch.equal(b, c)
+
+
+@pytest.mark.parametrize("log,n_cols", [(10, 1), (14, 7), (16, 64)])
+def test_merkle_leaves_match_reference_cuda(ref, B, log, n_cols):
+    from gpustark.backend import to_device
+    rng = np.random.default_rng(100 + n_cols)
+    cols = [to_device(rng.integers(0, P, 1 << log, dtype=np.int64).astype(np.uint32)) for _ in range(n_cols)]
+    ours = B.commit_on_layer(log, None, cols)
+    table = torch.tensor([c.data_ptr() for c in cols], dtype=torch.int64, device="cuda")
+    theirs = torch.empty_like(ours)
+    ref.commit_on_first_layer(1 << log, n_cols, table.data_ptr(), theirs.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(ours, theirs)
+
+
+def _time(fn, reps=5):
+    fn()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    b.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def test_timing_against_reference_cuda(ref, B):
+    """Device time of the same work through both libraries (printed with -s);
+    asserts only that both ran."""
+    from gpustark.backend import to_device
+    rng = np.random.default_rng(1)
+    rows = []
+    for log in (20, 24, 26):
+        tw = B.precompute_twiddles(log - 1)
+        x = to_device(rng.integers(0, P, 1 << log, dtype=np.int64).astype(np.uint32))
+        y = torch.empty_like(x)
+        ours = _time(lambda: (B.evaluate_polynomials([x], log, tw, out=[y]), B.interpolate_columns([y], log, tw)))
+        z = x.clone()
+        theirs = _time(lambda: (ref_evaluate(ref, [z], log, tw), ref_interpolate(ref, [z], log, tw)))
+        rows.append(("fft%d eval+interp" % log, ours, theirs))
+    cols = [to_device(rng.integers(0, P, 1 << 20, dtype=np.int64).astype(np.uint32)) for _ in range(64)]
+    out = torch.empty((1 << 20) * 8, dtype=torch.int32, device="cuda")
+    table = torch.tensor([c.data_ptr() for c in cols], dtype=torch.int64, device="cuda")
+    ours = _time(lambda: B.commit_on_layer(20, None, cols, out=out))
+    theirs = _time(lambda: ref.commit_on_first_layer(1 << 20, 64, table.data_ptr(), out.data_ptr()))
+    rows.append(("merkle leaves 64x2^20", ours, theirs))
+    print()
+    for name, o, t in rows:
+        print("%-24s gpustark %8.3f ms   reference CUDA %8.3f ms   %5.1fx" % (name, o, t, t / o))
+    assert all(o > 0 and t > 0 for _, o, t in rows)
