@@ -1,8 +1,9 @@
 """The library's kernels against the reference's own CUDA kernels, built for
 sm_100a from the reference sources by oracle/Makefile.refcuda into
 oracle/_ref/libstwo_cuda_ref.so (skipped when that library is absent): the
-circle FFT (ntt_n2b_columns / ntt_b2n_column) and the Blake2s leaf layer
-(commit_on_first_layer) must give identical outputs on the same inputs.
+circle FFT (ntt_n2b_columns / ntt_b2n_column), the Blake2s leaf layer
+(commit_on_first_layer) and the FRI line fold (fold_line) must give
+identical outputs on the same inputs.
 With -s, the timing test prints both implementations' device times."""
 import ctypes as C
 import os
@@ -19,6 +20,11 @@ REF_LIB = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
                        "libstwo_cuda_ref.so")
 
 
+class QM31(C.Structure):
+    """CudaSecureField (bindings.rs:9-15), passed by value."""
+    _fields_ = [("a", C.c_uint32), ("b", C.c_uint32), ("c", C.c_uint32), ("d", C.c_uint32)]
+
+
 @pytest.fixture(scope="module")
 def ref():
     if not torch.cuda.is_available():
@@ -31,7 +37,9 @@ def ref():
     lib.ntt_n2b_columns.argtypes = [C.POINTER(VP), C.c_uint, C.c_uint, VP, C.c_uint, C.c_uint]
     lib.ntt_b2n_column.argtypes = [C.POINTER(VP), C.c_uint32, C.c_uint32, VP, C.c_uint32, C.c_uint32]
     lib.commit_on_first_layer.argtypes = [C.c_uint32, C.c_uint32, VP, VP]
-    for f in (lib.ntt_n2b_columns, lib.ntt_b2n_column, lib.commit_on_first_layer):
+    # fold_line.cu: void fold_line(m31*, uint32_t offset, uint32_t n, m31** eval, qm31 alpha, m31** folded)
+    lib.fold_line.argtypes = [VP, C.c_uint32, C.c_uint32, C.POINTER(VP), QM31, C.POINTER(VP)]
+    for f in (lib.ntt_n2b_columns, lib.ntt_b2n_column, lib.commit_on_first_layer, lib.fold_line):
         f.restype = None
     return lib
 
@@ -40,6 +48,11 @@ def ref():
 def B():
     from gpustark.backend import GpuBackend
     return GpuBackend
+
+
+def ref_fold_line(ref, planes, log, alpha, tw, out):
+    tw_len = 1 << tw.root_log
+    ref.fold_line(tw.itwiddles.data_ptr(), tw_len - (1 << log), 1 << log, ptrs(planes), QM31(*alpha), ptrs(out))
 
 
 def ptrs(tensors):
@@ -89,6 +102,21 @@ def test_merkle_leaves_match_reference_cuda(ref, B, log, n_cols):
     assert torch.equal(ours, theirs)
 
 
+@pytest.mark.parametrize("log", [3, 12, 22])
+def test_fold_line_matches_reference_cuda(ref, B, log):
+    from gpustark.backend import to_device
+    rng = np.random.default_rng(200 + log)
+    tw = B.precompute_twiddles(log + 1)
+    planes = [to_device(rng.integers(0, P, 1 << log, dtype=np.int64).astype(np.uint32)) for _ in range(4)]
+    alpha = [int(v) for v in rng.integers(0, P, 4)]
+    ours = B.fold_line(planes, log, alpha, tw)
+    theirs = [torch.empty_like(o) for o in ours]
+    ref_fold_line(ref, planes, log, alpha, tw, theirs)
+    torch.cuda.synchronize()
+    for a, b in zip(ours, theirs):
+        assert torch.equal(a, b)
+
+
 def _time(fn, reps=5):
     fn()
     torch.cuda.synchronize()
@@ -122,6 +150,12 @@ def test_timing_against_reference_cuda(ref, B):
     ours = _time(lambda: B.commit_on_layer(20, None, cols, out=out))
     theirs = _time(lambda: ref.commit_on_first_layer(1 << 20, 64, table.data_ptr(), out.data_ptr()))
     rows.append(("merkle leaves 64x2^20", ours, theirs))
+    tw = B.precompute_twiddles(23)
+    planes = [to_device(rng.integers(0, P, 1 << 22, dtype=np.int64).astype(np.uint32)) for _ in range(4)]
+    folded = [torch.empty(1 << 21, dtype=torch.int32, device="cuda") for _ in range(4)]
+    ours = _time(lambda: B.fold_line(planes, 22, [1, 2, 3, 4], tw))
+    theirs = _time(lambda: ref_fold_line(ref, planes, 22, [1, 2, 3, 4], tw, folded))
+    rows.append(("fold_line 2^22", ours, theirs))
     print()
     for name, o, t in rows:
         print("%-24s gpustark %8.3f ms   reference CUDA %8.3f ms   %5.1fx" % (name, o, t, t / o))
