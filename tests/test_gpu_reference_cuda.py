@@ -2,8 +2,9 @@
 sm_100a from the reference sources by oracle/Makefile.refcuda into
 oracle/_ref/libstwo_cuda_ref.so (skipped when that library is absent): the
 circle FFT (ntt_n2b_columns / ntt_b2n_column), the Blake2s leaf layer
-(commit_on_first_layer) and the FRI line fold (fold_line) must give
-identical outputs on the same inputs.
+(commit_on_first_layer), the FRI folds (fold_line, fold_circle_into_line),
+the OODS evaluation (batch_eval_at_points) and the proof of work
+(grind_blake2s) must give identical outputs on the same inputs.
 With -s, the timing test prints both implementations' device times."""
 import ctypes as C
 import os
@@ -39,7 +40,12 @@ def ref():
     lib.commit_on_first_layer.argtypes = [C.c_uint32, C.c_uint32, VP, VP]
     # fold_line.cu: void fold_line(m31*, uint32_t offset, uint32_t n, m31** eval, qm31 alpha, m31** folded)
     lib.fold_line.argtypes = [VP, C.c_uint32, C.c_uint32, C.POINTER(VP), QM31, C.POINTER(VP)]
-    for f in (lib.ntt_n2b_columns, lib.ntt_b2n_column, lib.commit_on_first_layer, lib.fold_line):
+    lib.fold_circle_into_line.argtypes = [VP, C.c_uint32, C.c_uint32, C.POINTER(VP), QM31, C.POINTER(VP)]
+    lib.batch_eval_at_points.argtypes = [VP, C.c_int, C.c_int, QM31, QM31, C.POINTER(QM31)]
+    lib.grind_blake2s.argtypes = [C.POINTER(C.c_uint32), C.c_uint32]
+    lib.grind_blake2s.restype = C.c_uint64
+    for f in (lib.ntt_n2b_columns, lib.ntt_b2n_column, lib.commit_on_first_layer, lib.fold_line,
+              lib.fold_circle_into_line, lib.batch_eval_at_points):
         f.restype = None
     return lib
 
@@ -115,6 +121,51 @@ def test_fold_line_matches_reference_cuda(ref, B, log):
     torch.cuda.synchronize()
     for a, b in zip(ours, theirs):
         assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("log", [4, 13, 21])
+def test_fold_circle_into_line_matches_reference_cuda(ref, B, log):
+    from gpustark.backend import to_device
+    rng = np.random.default_rng(300 + log)
+    tw = B.precompute_twiddles(log - 1)
+    src = [to_device(rng.integers(0, P, 1 << log, dtype=np.int64).astype(np.uint32)) for _ in range(4)]
+    dst0 = [rng.integers(0, P, 1 << (log - 1), dtype=np.int64).astype(np.uint32) for _ in range(4)]
+    alpha = [int(v) for v in rng.integers(0, P, 4)]
+    ours = [to_device(d) for d in dst0]
+    B.fold_circle_into_line(ours, src, log, alpha, tw)
+    theirs = [to_device(d) for d in dst0]
+    ref.fold_circle_into_line(tw.itwiddles.data_ptr(), (1 << tw.root_log) - (1 << (log - 1)), 1 << log, ptrs(src),
+                              QM31(*alpha), ptrs(theirs))
+    torch.cuda.synchronize()
+    for a, b in zip(ours, theirs):
+        assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("log,n_polys", [(8, 3), (16, 20), (18, 5)])
+def test_batch_eval_at_point_matches_reference_cuda(ref, B, log, n_polys):
+    from gpustark.backend import to_device
+    rng = np.random.default_rng(400 + log)
+    polys = [to_device(rng.integers(0, P, 1 << log, dtype=np.int64).astype(np.uint32)) for _ in range(n_polys)]
+    point = [int(v) for v in rng.integers(0, P, 8)]
+    ours = B.batch_eval_at_point(polys, point)
+    table = torch.tensor([p.data_ptr() for p in polys], dtype=torch.int64, device="cuda")
+    res = (QM31 * n_polys)()
+    ref.batch_eval_at_points(table.data_ptr(), 1 << log, n_polys, QM31(*point[:4]), QM31(*point[4:]), res)
+    assert [[r.a, r.b, r.c, r.d] for r in res] == [[int(v) for v in o] for o in ours]
+
+
+@pytest.mark.parametrize("pow_bits", [1, 10, 18])
+def test_grind_matches_reference_cuda(ref, B, pow_bits):
+    import hashlib
+    import struct
+    from gpustark import _lib as L
+    from gpustark.backend import default_context
+    digest = hashlib.blake2s(b"grind %d" % pow_bits).digest()
+    pre = hashlib.blake2s(struct.pack("<I", 0x12345678) + bytes(12) + digest + struct.pack("<I", pow_bits)).digest()
+    words = (C.c_uint32 * 8)(*struct.unpack("<8I", pre))
+    nonce = C.c_uint64()
+    L.check(L.lib().gs_grind_blake2s(default_context().handle, words, pow_bits, C.byref(nonce)), "grind")
+    assert ref.grind_blake2s(words, pow_bits) == nonce.value
 
 
 def _time(fn, reps=5):
