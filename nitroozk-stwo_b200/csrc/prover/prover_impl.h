@@ -17,8 +17,6 @@ int fold_line_dev_alpha(cudaStream_t st, CPlanes src, uint32_t log_n, const uint
                         const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out);
 int fold_circle_into_line_dev_alpha(cudaStream_t st, CPlanes src, uint32_t log_n, const uint32_t* d_alpha, Planes dst,
                                     const uint32_t* d_itw, uint32_t tw_log, uint32_t* leaf_out);
-int channel_mix_root_draw(cudaStream_t st, uint32_t* d_state, const uint32_t* d_root, uint32_t* d_root_copy,
-                          uint32_t* d_felt);
 int interpolate_columns_to(cudaStream_t st, const uint32_t* const* d_src, uint32_t* const* d_dst, uint32_t n_cols,
                            uint32_t log_n, const uint32_t* d_itwiddles, uint32_t tw_log);
 
