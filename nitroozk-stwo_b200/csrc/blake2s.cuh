@@ -25,14 +25,30 @@ GS_HD uint32_t rotr32(uint32_t x, int n) {
 #endif
 }
 
+// Rotations by 16 and 8 are byte permutes (PRMT) on the device.
+GS_HD uint32_t rotr16(uint32_t x) {
+#ifdef __CUDA_ARCH__
+  return __byte_perm(x, 0, 0x1032);
+#else
+  return rotr32(x, 16);
+#endif
+}
+GS_HD uint32_t rotr8(uint32_t x) {
+#ifdef __CUDA_ARCH__
+  return __byte_perm(x, 0, 0x0321);
+#else
+  return rotr32(x, 8);
+#endif
+}
+
 #define GS_G(a, b, c, d, x, y)         \
   do {                                 \
     v[a] = v[a] + v[b] + (x);          \
-    v[d] = rotr32(v[d] ^ v[a], 16);    \
+    v[d] = rotr16(v[d] ^ v[a]);        \
     v[c] = v[c] + v[d];                \
     v[b] = rotr32(v[b] ^ v[c], 12);    \
     v[a] = v[a] + v[b] + (y);          \
-    v[d] = rotr32(v[d] ^ v[a], 8);     \
+    v[d] = rotr8(v[d] ^ v[a]);         \
     v[c] = v[c] + v[d];                \
     v[b] = rotr32(v[b] ^ v[c], 7);     \
   } while (0)
@@ -82,11 +98,11 @@ __device__ __forceinline__ uint32_t b2_imad(uint32_t a, uint32_t b, uint32_t c) 
 #define GS_GF(a, b, c, d, x, y)                                    \
   do {                                                             \
     v[a] = b2_imad(b2_imad(v[a], one, v[b]), one, (x));            \
-    v[d] = rotr32(v[d] ^ v[a], 16);                                \
+    v[d] = rotr16(v[d] ^ v[a]);                                  \
     v[c] = b2_imad(v[c], one, v[d]);                               \
     v[b] = rotr32(v[b] ^ v[c], 12);                                \
     v[a] = b2_imad(b2_imad(v[a], one, v[b]), one, (y));            \
-    v[d] = rotr32(v[d] ^ v[a], 8);                                 \
+    v[d] = rotr8(v[d] ^ v[a]);                                   \
     v[c] = b2_imad(v[c], one, v[d]);                               \
     v[b] = rotr32(v[b] ^ v[c], 7);                                 \
   } while (0)
