@@ -290,10 +290,22 @@ def cpu_sweep_sample(threads):
     return total / dt / 1e9, dt, "oracle: FFT 2^20 eval+interp, Merkle 64x2^16, fold_line 2^20; %d reps" % reps
 
 
+def fft_autotune(args, hi):
+    """Installs the FFT pass splits the library's autotuner picks for log
+    sizes 8..hi (set-up, outside every timed region); returns the picks that
+    differ from the default 13/4 as {log: "tile_log/coalesce_bits"}."""
+    if args.fft_autotune == "off":
+        return "off"
+    from gpustark.backend import GpuBackend
+    picks = GpuBackend.fft_autotune(8, min(hi, 27))
+    return {str(k): "%d/%d" % v for k, v in picks.items() if v != (13, 4)}
+
+
 def run_kernels(args, world, rank, local):
     import torch
     from gpustark import lib as gslib
     torch.cuda.set_device(local)
+    tuning = fft_autotune(args, max(FFT_LOGS))
     hbm_peak, peak_kind = load_peaks()
     sw = KernelSweep(seed=1234 + rank)
     fft_b, leaf_b, node_b, fold_b = sweep_bytes()
@@ -376,10 +388,10 @@ def run_kernels(args, world, rank, local):
         "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic: seeded uniform M31",
-        "config": {"workload": "kernel sweep (configs[1]): circle-FFT evaluate+interpolate log 16..26, "
+        "config": {"workload": "kernel sweep: circle-FFT evaluate+interpolate log 16..26, "
                                "Blake2s Merkle commit 64 cols x 2^20, QM31 fold_line 2^22",
                    "l2": "flushed between timed steps (write of 2x L2)",
-                   "parallelism": "replicas x%d" % world},
+                   "parallelism": "replicas x%d" % world, "fft_tuning": tuning},
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
                      "traffic": traffic, "algorithmic_bytes": alg[dom], "avg_ms": round(avg[dom], 4)},
@@ -456,6 +468,7 @@ def run_proof(args, world, rank, local):
     log_n = args.log_n or PROOF_SIZES[wl]
     ctx = Context(torch.cuda.current_stream())
     stream = torch.cuda.current_stream()
+    tuning = fft_autotune(args, 22)
 
     def one(mode=G.INPUT_SEEDED, host=None):
         if wl == "poseidon":
@@ -519,7 +532,7 @@ def run_proof(args, world, rank, local):
         "value": round(value, 3), "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_per_step, 3), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 (M31/QM31 integer arithmetic)", "data": "synthetic: seeded uniform M31",
-        "config": dict(proof_config(wl, log_n), parallelism="independent proofs x%d" % world),
+        "config": dict(proof_config(wl, log_n), parallelism="independent proofs x%d" % world, fft_tuning=tuning),
         "proofs_per_s": round(1e3 / value, 2), "proof_bytes": len(proof),
         "latency_ms": {"p50": round(statistics.median(lat), 3), "max": round(max(lat), 3)},
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(host.nbytes),
@@ -607,6 +620,7 @@ def run_serving(args, world, rank, local):
     from gpustark.backend import Context
     torch.cuda.set_device(local)
     ctx = Context(torch.cuda.current_stream())
+    tuning = fft_autotune(args, 23)
     jobs = job_mix(args.workload, 1 + rank)
 
     def single(a, n, c, sd):
@@ -668,7 +682,7 @@ def run_serving(args, world, rank, local):
         "dtype": "u32 (M31/QM31 integer arithmetic)", "data": "synthetic: seeded uniform M31",
         "config": {"workload": "%s: %d jobs, %d workers (one CUDA stream each), admission by HBM footprint"
                                % (args.workload, len(jobs), workers),
-                   "parallelism": "replicas x%d" % world},
+                   "parallelism": "replicas x%d" % world, "fft_tuning": tuning},
         "sequential_proofs_per_s": round(seq_pps, 2), "speedup_vs_sequential": round(pps / seq_pps, 2),
         "latency_ms": {"p50": round(q(lat, 50), 2), "p99": round(q(lat, 99), 2)},
         "sequential_latency_ms": {"p50": round(q(seq_lat, 50), 2), "p99": round(q(seq_lat, 99), 2)},
@@ -684,7 +698,7 @@ def run_serving(args, world, rank, local):
 
 
 def run_batched_commit(ctx, seed, n_cols=256, lo=12, hi=24, blowup=1, reps=5):
-    """configs[3], commitment part: 256 columns with log sizes uniform in
+    """Mixed-size commitment: 256 columns with log sizes uniform in
     12..24, extended by 2^blowup and committed in one Merkle tree. Times the
     batched plan eagerly and replayed from a CUDA graph (same inputs, same
     root), and the FFT part issued one column per launch for comparison."""
@@ -756,7 +770,7 @@ def run_reference(args, world, rank):
             "value": round(v, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * t_all / max(args.steps, 1), 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic: seeded uniform M31",
-            "config": {"workload": "kernel sweep (configs[1]), bounded CPU sample", "parallelism": "cpu threads"},
+            "config": {"workload": "kernel sweep, bounded CPU sample", "parallelism": "cpu threads"},
             "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc},
             "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
@@ -847,6 +861,8 @@ def main():
     ap.add_argument("--load", type=float, default=2.0, help="served: arrival rate / sequential proof rate")
     ap.add_argument("--log-n", type=int, default=0, help="override the proof size (log instances / rows)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fft-autotune", default="on", choices=["on", "off"],
+                    help="time the FFT pass splits per log size before warm-up and install the fastest")
     ap.add_argument("--case", default=None,
                     help="profiling case: fft:<log>, lde:<log>:<cols>[:<ext>], merkle:<log>:<cols>, fold:<log> (one op, no JSON contract)")
     args = ap.parse_args()

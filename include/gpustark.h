@@ -91,6 +91,22 @@ int gs_interpolate_columns(gs_ctx* ctx, uint32_t* const* cols, uint32_t n_cols, 
 int gs_evaluate_columns(gs_ctx* ctx, const uint32_t* const* coeffs, uint32_t coeffs_log_size, uint32_t* const* evals,
                         uint32_t n_cols, uint32_t log_size, const uint32_t* twiddles, uint32_t twiddles_log_size);
 
+/* FFT pass-split tuning. No counterpart in the reference, whose CUDA FFT
+ * (ntt.cu) has one fixed geometry. An FFT computing n layers runs in passes
+ * over shared-memory tiles of 2^tile_log words, 2^coalesce_bits of them
+ * contiguous in memory; the split changes speed only, never the values.
+ * gs_fft_autotune times the round trip evaluate + interpolate of every split
+ * candidate for each n in [min_log, max_log] (3 <= min_log <= max_log <= 27)
+ * on scratch columns (2^max(24, max_log) words) and installs the fastest for
+ * all contexts of the process; tile_logs / coalesce_bits (max_log - min_log
+ * + 1 entries each) receive the choices when non-NULL. Both set-up calls:
+ * no other FFT may be in flight. gs_fft_set_tuning installs one split
+ * (log_size 0: every size; tile_log in [6, 13], coalesce_bits <= min(5,
+ * tile_log - 5)); gs_fft_get_tuning reads it. Default: 13 / 4. */
+int gs_fft_autotune(gs_ctx* ctx, uint32_t min_log, uint32_t max_log, uint32_t* tile_logs, uint32_t* coalesce_bits);
+int gs_fft_set_tuning(uint32_t log_size, uint32_t tile_log, uint32_t coalesce_bits);
+int gs_fft_get_tuning(uint32_t log_size, uint32_t* tile_log, uint32_t* coalesce_bits);
+
 /* -------------------------------------------------------------- MerkleOps */
 /* commit_on_first_layer / commit_on_layer_with_previous (bindings.rs:262-275);
  * MerkleOps<Blake2sMerkleHasher>::commit_on_layer (prover/vcs/ops.rs:24-28).

@@ -28,6 +28,7 @@
 // are computed — no zero-extension pass.
 #include "runtime.cuh"
 #include <algorithm>
+#include <iterator>
 #include <cstdlib>
 
 namespace gs {
@@ -136,7 +137,8 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const uint32_t* const* __
     }
     const uint32_t ebase = ((ltid >> s0) << (s0 + R)) | (ltid & ((1u << s0) - 1u));
     if (k == 0) {
-      if (a.vec_ok && s0 == 0 && a.c == 0 && a.src_mask == 0xffffffffu && NQ >= 4) {
+      // the tile's elements are contiguous only when it starts at layer 0
+      if (a.vec_ok && s0 == 0 && a.c == 0 && a.lo == 0 && a.src_mask == 0xffffffffu && NQ >= 4) {
         const uint4* p = reinterpret_cast<const uint4*>(src + (basev | ebase));
 #pragma unroll
         for (int g = 0; g < NQ / 4; g++) {
@@ -188,7 +190,7 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const uint32_t* const* __
 #pragma unroll
         for (int q = 0; q < NQ; q++) x[q] = mul(x[q], a.scale);
       }
-      if (a.vec_ok && s0 == 0 && a.c == 0 && NQ >= 4) {
+      if (a.vec_ok && s0 == 0 && a.c == 0 && a.lo == 0 && NQ >= 4) {
         uint4* p = reinterpret_cast<uint4*>(dst + (basev | ebase));
 #pragma unroll
         for (int g = 0; g < NQ / 4; g++) p[g] = make_uint4(x[4 * g], x[4 * g + 1], x[4 * g + 2], x[4 * g + 3]);
@@ -282,7 +284,9 @@ __global__ void __launch_bounds__(256) fft_tile_kernel(const uint32_t* const* __
     // move up to the pass's layer bits)
     const uint32_t gbase = basev | ((ebase >> C) << a.lo) | (ebase & CMASK);
     if (k == 0) {
-      if (C == 0 && s0 == 0 && a.vec_ok && a.src_mask == 0xffffffffu) {
+      // contiguous only when the tile starts at layer 0 (C == 0 with lo > 0
+      // spaces the elements 2^lo apart)
+      if (C == 0 && s0 == 0 && a.lo == 0 && a.vec_ok && a.src_mask == 0xffffffffu) {
         const uint4* p = reinterpret_cast<const uint4*>(src + gbase);
 #pragma unroll
         for (int g = 0; g < NQ / 4; g++) {
@@ -336,7 +340,7 @@ __global__ void __launch_bounds__(256) fft_tile_kernel(const uint32_t* const* __
 #pragma unroll
         for (int q = 0; q < NQ; q++) x[q] = mul(x[q], a.scale);
       }
-      if (C == 0 && s0 == 0 && a.vec_ok) {
+      if (C == 0 && s0 == 0 && a.lo == 0 && a.vec_ok) {
         uint4* p = reinterpret_cast<uint4*>(dst + gbase);
 #pragma unroll
         for (int g = 0; g < NQ / 4; g++) p[g] = make_uint4(x[4 * g], x[4 * g + 1], x[4 * g + 2], x[4 * g + 3]);
@@ -447,12 +451,17 @@ struct FftTuning {
   uint32_t tile_log = 13;      // log2 of the shared-memory tile (elements), <= 13
   uint32_t coalesce_bits = 4;  // contiguous low bits per strided tile row
 };
-static FftTuning g_fft_tuning;
+// Per number of computed layers (an FFT of 2^n, or an LDE from 2^n
+// coefficients, computes n layers). Written at set-up (set_fft_tuning,
+// fft_autotune), read by every launch.
+static FftTuning g_fft_tuning[32];
+static FftTuning tuning_for(uint32_t layers) { return g_fft_tuning[layers < 32 ? layers : 31]; }
 
 // Splits layers [0, layers) into balanced passes (lo, L): the first pass has
 // the whole tile for layers, later ones reserve `coalesce_bits` of it.
 static void fft_partition(uint32_t layers, std::vector<std::pair<uint32_t, uint32_t>>& parts) {
-  const uint32_t T = g_fft_tuning.tile_log, C = g_fft_tuning.coalesce_bits;
+  const FftTuning tn = tuning_for(layers);
+  const uint32_t T = tn.tile_log, C = tn.coalesce_bits;
   if (layers <= T) {
     parts.push_back({0, layers});
     return;
@@ -525,7 +534,7 @@ static int run_passes(cudaStream_t st, const uint32_t* const* src, uint32_t* con
     a.n = n;
     a.lo = parts[p].first;
     a.L = parts[p].second;
-    a.c = std::min(g_fft_tuning.coalesce_bits, a.lo);
+    a.c = std::min(tuning_for(layers).coalesce_bits, a.lo);
     a.t = a.c + a.L;
     const uint32_t R = std::min<uint32_t>(5, a.L);
     a.K = (a.L + R - 1) / R;
@@ -593,9 +602,108 @@ int evaluate_columns(cudaStream_t st, const uint32_t* const* d_src, uint32_t coe
   return run_passes<false>(st, d_src, d_dst, n_cols, log_n, coeff_log, src_mask, d_twiddles, 1u << tw_log);
 }
 
-void set_fft_tuning(uint32_t tile_log, uint32_t coalesce_bits) {
-  if (tile_log >= 6 && tile_log <= 13) g_fft_tuning.tile_log = tile_log;
-  if (coalesce_bits <= 5 && coalesce_bits + 5 <= g_fft_tuning.tile_log) g_fft_tuning.coalesce_bits = coalesce_bits;
+// Installs the tuning for FFTs computing `layers` layers (0: every size).
+// A tile holds 2^tile_log words (at most 2^13, 32 KiB of shared memory), of
+// which 2^coalesce_bits are contiguous in memory; a pass needs room for 5
+// layers besides them.
+int set_fft_tuning(uint32_t layers, uint32_t tile_log, uint32_t coalesce_bits) {
+  GS_REQUIRE(layers < 32, "log size out of range");
+  GS_REQUIRE(tile_log >= 6 && tile_log <= 13, "tile log must be in [6, 13]");
+  GS_REQUIRE(coalesce_bits <= 5 && coalesce_bits + 5 <= tile_log, "coalesced bits must be <= min(5, tile_log - 5)");
+  for (uint32_t l = layers; l < (layers ? layers + 1 : 32u); l++) g_fft_tuning[l] = FftTuning{tile_log, coalesce_bits};
+  return OK;
+}
+
+// Picks, for every FFT log size n in [lo, hi], the tile size and coalesced
+// row width whose pass split gives the fastest evaluate + interpolate round
+// trip of scratch columns (2^24 words in all, or one column of 2^n), and
+// installs it for n computed layers. Each split is timed with CUDA events as
+// the best of 3 trials of 3 round trips; the installed split (first in the
+// list) is replaced only by one at least 2% faster, so timing noise does not
+// move it. Candidates that give the same pass split as an earlier one are not
+// timed again. Every candidate computes the same values; only the split, and
+// so the speed, differ. Not thread-safe against concurrent launches (a set-up
+// step).
+int fft_autotune(cudaStream_t st, uint32_t lo, uint32_t hi, const uint32_t* tw, const uint32_t* itw, uint32_t tw_log,
+                 uint32_t* out_tile, uint32_t* out_coalesce) {
+  GS_REQUIRE(lo >= 3 && hi <= 27 && lo <= hi && tw_log + 1 >= hi, "autotune range out of bounds");
+  static const FftTuning fixed[] = {{13, 4}, {12, 4}, {11, 4}, {10, 4}, {13, 3}, {12, 5}};
+  const size_t words = (size_t)1 << (hi > 24 ? hi : 24);
+  uint32_t* buf = nullptr;
+  uint32_t** tab = nullptr;
+  const uint32_t max_cols = 32768;
+  GS_CUDA_TRY(cudaMallocAsync((void**)&buf, 4 * words, st));
+  GS_CUDA_TRY(cudaMallocAsync((void**)&tab, sizeof(void*) * max_cols, st));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = OK;
+  if (cudaMemsetAsync(buf, 0, 4 * words, st) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+      cudaEventCreate(&e1) != cudaSuccess)
+    rc = ERR_CUDA;
+  const bool aligned = g_cols_aligned;
+  g_cols_aligned = true;
+  std::vector<uint32_t*> h;
+  for (uint32_t n = lo; n <= hi && rc == OK; n++) {
+    const uint32_t cols = (uint32_t)std::min<size_t>(words >> n, max_cols);
+    h.resize(cols);
+    for (uint32_t c = 0; c < cols; c++) h[c] = buf + ((size_t)c << n);
+    if (cudaMemcpyAsync(tab, h.data(), sizeof(void*) * cols, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      rc = ERR_CUDA;
+      break;
+    }
+    const FftTuning keep = g_fft_tuning[n];
+    float best = 1e30f, keep_ms = 1e30f;
+    FftTuning pick = keep;
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> seen;
+    std::vector<FftTuning> cand(1, keep);
+    cand.insert(cand.end(), std::begin(fixed), std::end(fixed));
+    for (const FftTuning& c : cand) {
+      g_fft_tuning[n] = c;
+      std::vector<std::pair<uint32_t, uint32_t>> parts;
+      fft_partition(n, parts);
+      for (auto& pr : parts) pr.first = std::min(c.coalesce_bits, pr.first) | (pr.first << 8);
+      if (std::find(seen.begin(), seen.end(), parts) != seen.end()) continue;
+      seen.push_back(parts);
+      float ms = 1e30f;
+      for (int trial = 0; trial < 4 && rc == OK; trial++) {  // trial 0 warms up
+        for (int rep = 0; rep < 3 && rc == OK; rep++) {
+          if (rep == 0 && cudaEventRecord(e0, st) != cudaSuccess) rc = ERR_CUDA;
+          if (rc == OK) rc = run_passes<false>(st, (const uint32_t* const*)tab, tab, cols, n, n, 0xffffffffu, tw,
+                                               1u << tw_log);
+          if (rc == OK) rc = run_passes<true>(st, (const uint32_t* const*)tab, tab, cols, n, n, 0xffffffffu, itw,
+                                              1u << tw_log);
+        }
+        float t = 0;
+        if (rc == OK && (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                         cudaEventElapsedTime(&t, e0, e1) != cudaSuccess))
+          rc = ERR_CUDA;
+        if (rc == OK && trial > 0) ms = std::min(ms, t);
+      }
+      if (rc != OK) break;
+      if (&c == &cand[0]) keep_ms = ms;
+      if (ms < best) {
+        best = ms;
+        pick = c;
+      }
+    }
+    if (best > 0.98f * keep_ms) pick = keep;
+    g_fft_tuning[n] = rc == OK ? pick : keep;
+    if (out_tile) out_tile[n - lo] = g_fft_tuning[n].tile_log;
+    if (out_coalesce) out_coalesce[n - lo] = g_fft_tuning[n].coalesce_bits;
+  }
+  g_cols_aligned = aligned;
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFreeAsync(tab, st);
+  cudaFreeAsync(buf, st);
+  if (rc == ERR_CUDA) set_error(std::string("fft autotune: ") + cudaGetErrorString(cudaGetLastError()));
+  return rc;
+}
+
+void get_fft_tuning(uint32_t layers, uint32_t* tile_log, uint32_t* coalesce_bits) {
+  const FftTuning t = tuning_for(layers);
+  *tile_log = t.tile_log;
+  *coalesce_bits = t.coalesce_bits;
 }
 
 // In-place bit reversal of one column (ColumnOps::bit_reverse_column).

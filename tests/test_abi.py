@@ -38,3 +38,23 @@ def test_python_binding_declares_only_exported_symbols():
     for n in gpustark.declared_symbols():
         assert hasattr(lib, n), n
     assert set(gpustark.declared_symbols()) <= set(declared())
+
+
+def test_fft_tuning_setter_validates_without_gpu():
+    """gs_fft_set_tuning / gs_fft_get_tuning are host-only: bad splits are
+    refused with ERR_INVALID, good ones read back, and the default 13 / 4 is
+    put back."""
+    lib = ctypes.CDLL(LIB)
+    t, c = ctypes.c_uint32(), ctypes.c_uint32()
+    assert lib.gs_fft_get_tuning(20, ctypes.byref(t), ctypes.byref(c)) == 0
+    assert (t.value, c.value) == (13, 4)
+    for bad in [(20, 14, 4), (20, 5, 0), (20, 13, 6), (20, 9, 5), (32, 13, 4)]:
+        assert lib.gs_fft_set_tuning(*bad) == 1, bad
+    try:
+        assert lib.gs_fft_set_tuning(20, 11, 3) == 0
+        assert lib.gs_fft_get_tuning(20, ctypes.byref(t), ctypes.byref(c)) == 0
+        assert (t.value, c.value) == (11, 3)
+        assert lib.gs_fft_get_tuning(21, ctypes.byref(t), ctypes.byref(c)) == 0
+        assert (t.value, c.value) == (13, 4)
+    finally:
+        assert lib.gs_fft_set_tuning(0, 13, 4) == 0
