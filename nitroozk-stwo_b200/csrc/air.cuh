@@ -32,13 +32,15 @@ int poseidon_constraints(cudaStream_t st, const uint32_t* trace, const uint32_t*
                          uint32_t trace_log, const ConstraintParams& prm, const LookupParams& lp, qm31 cumsum_shift,
                          Planes out);
 
-// gather.cu: out[k] = src_k[idx_k] (words) and 8-word hash gathers.
-struct GatherItem {
+// gather.cu: hash witnesses as runs read from one Merkle layer each; item i
+// (out hash i) is hash idx[i] of its run's layer, the items of a run
+// consecutive from `first`.
+struct HashRun {
   const uint32_t* src;
-  uint64_t idx;
+  uint32_t first, count;
 };
-int gather_words(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out);
-int gather_hashes(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out);
+int gather_hash_runs(cudaStream_t st, const HashRun* d_runs, uint32_t n_runs, const uint32_t* d_idx,
+                     uint32_t* d_out);
 // Values of n_cols columns at a list of positions, written position-major
 // (for each position, every column): columns given explicitly (n_cols <= 4)
 // or as base + c * stride.

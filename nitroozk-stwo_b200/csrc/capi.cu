@@ -198,7 +198,7 @@ int gs_commit_node_layers(gs_ctx* ctx, uint32_t top_log, uint32_t* const* layers
   CTX_REQUIRED(ctx);
   GS_REQUIRE(layers != nullptr, "null layer list");
   for (uint32_t k = 0; k <= top_log; k++) GS_REQUIRE(layers[k] != nullptr, "null layer buffer");
-  return commit_node_layers(ctx->c.stream, top_log, layers);
+  return commit_node_layers(ctx->c.stream, top_log, layers, ctx->c.tree_counters);
 }
 
 int gs_fold_line(gs_ctx* ctx, const uint32_t* const src[4], uint32_t log_size, gs_qm31 alpha, uint32_t* const dst[4],

@@ -6,17 +6,14 @@
 
 namespace gs {
 
-__global__ void gather_words_kernel(const GatherItem* __restrict__ items, size_t n, uint32_t* __restrict__ out) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    GatherItem it = items[i];
-    out[i] = __ldg(it.src + it.idx);
-  }
-}
-
-__global__ void gather_hashes_kernel(const GatherItem* __restrict__ items, size_t n, uint32_t* __restrict__ out) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    GatherItem it = items[i];
-    const uint4* s = reinterpret_cast<const uint4*>(it.src + 8 * it.idx);
+// One block per run: the run's witnesses are spread over its threads, each
+// copying one 32-byte hash as two 16-byte vectors.
+__global__ void gather_hash_runs_kernel(const HashRun* __restrict__ runs, const uint32_t* __restrict__ idx,
+                                        uint32_t* __restrict__ out) {
+  const HashRun r = runs[blockIdx.x];
+  for (uint32_t k = threadIdx.x; k < r.count; k += blockDim.x) {
+    const size_t i = (size_t)r.first + k;
+    const uint4* s = reinterpret_cast<const uint4*>(r.src + 8 * (size_t)__ldg(idx + i));
     uint4* o = reinterpret_cast<uint4*>(out + 8 * i);
     o[0] = __ldg(s);
     o[1] = __ldg(s + 1);
@@ -46,20 +43,11 @@ int gather_cols(cudaStream_t st, const ColGather* d_blocks, uint32_t n_blocks, u
   return OK;
 }
 
-int gather_words(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out) {
-  if (n == 0) return OK;
-  unsigned blocks = (unsigned)((n + 255) / 256);
-  gather_words_kernel<<<blocks, 256, 0, st>>>(d_items, n, d_out);
-  note_launch();
-  GS_CUDA_TRY(cudaGetLastError());
-  return OK;
-}
-
-int gather_hashes(cudaStream_t st, const GatherItem* d_items, size_t n, uint32_t* d_out) {
-  if (n == 0) return OK;
+int gather_hash_runs(cudaStream_t st, const HashRun* d_runs, uint32_t n_runs, const uint32_t* d_idx,
+                     uint32_t* d_out) {
+  if (n_runs == 0) return OK;
   GS_REQUIRE(((uintptr_t)d_out & 15) == 0, "hash gather output must be 16-byte aligned");
-  unsigned blocks = (unsigned)((n + 255) / 256);
-  gather_hashes_kernel<<<blocks, 256, 0, st>>>(d_items, n, d_out);
+  gather_hash_runs_kernel<<<n_runs, 128, 0, st>>>(d_runs, d_idx, d_out);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;

@@ -9,7 +9,12 @@
 // crates/stwo/src/prover/backend/simd/grind.rs) and CPU grind (cpu/grind.rs).
 //
 // One thread per candidate low word, one compression each; the smallest hit
-// of a chunk is kept with atomicMin in a caller-provided device word.
+// of a chunk is kept with atomicMin in a caller-provided device word. The
+// grid is persistent and walks the chunk in 256-nonce steps in increasing
+// order; a block stops as soon as the recorded minimum lies below its next
+// step (a plain read, nothing waits), so a search that hits early costs a
+// few thousand compressions instead of 2^20, and the answer is still the
+// smallest hit: steps are skipped only when a smaller hit exists.
 #include "runtime.cuh"
 #include "blake2s.cuh"
 
@@ -17,20 +22,26 @@ namespace gs {
 
 struct Digest8 { uint32_t w[8]; };
 
-__global__ void grind_kernel(Digest8 d, uint32_t hi, uint32_t pow_bits, uint32_t* result) {
-  uint32_t low = blockIdx.x * blockDim.x + threadIdx.x;
-  if (low >= (1u << 20)) return;
-  uint32_t h[8], m[16];
-  blake2s_init(h);
+constexpr uint32_t GRIND_LOW_LOG = 20, GRIND_STEP = 256;
+
+__global__ void __launch_bounds__(GRIND_STEP) grind_kernel(Digest8 d, uint32_t hi, uint32_t pow_bits,
+                                                           uint32_t* result) {
+  const volatile uint32_t* best = result;
+  for (uint32_t step = blockIdx.x; step < ((1u << GRIND_LOW_LOG) / GRIND_STEP); step += gridDim.x) {
+    if (*best < step * GRIND_STEP) return;  // a smaller nonce already passed
+    const uint32_t low = step * GRIND_STEP + threadIdx.x;
+    uint32_t h[8], m[16];
+    blake2s_init(h);
 #pragma unroll
-  for (int j = 0; j < 8; j++) m[j] = d.w[j];
-  m[8] = low;
-  m[9] = hi;
+    for (int j = 0; j < 8; j++) m[j] = d.w[j];
+    m[8] = low;
+    m[9] = hi;
 #pragma unroll
-  for (int j = 10; j < 16; j++) m[j] = 0;
-  blake2s_compress(h, m, 40, true);
-  uint32_t tz = h[0] == 0 ? 32u : (uint32_t)__ffs(h[0]) - 1u;
-  if (tz >= pow_bits) atomicMin(result, low);
+    for (int j = 10; j < 16; j++) m[j] = 0;
+    blake2s_compress(h, m, 40, true);
+    uint32_t tz = h[0] == 0 ? 32u : (uint32_t)__ffs(h[0]) - 1u;
+    if (tz >= pow_bits) atomicMin(result, low);
+  }
 }
 
 // h_word (optional): a pinned host word for the per-chunk read-back.
@@ -42,9 +53,14 @@ int grind_blake2s(cudaStream_t st, const uint32_t prefixed_digest[8], uint32_t p
   for (int j = 0; j < 8; j++) d.w[j] = prefixed_digest[j];
   // Bounded search: 2^12 chunks of 2^20 nonces covers pow_bits far beyond 32
   // with overwhelming probability; running out is reported, never looped on.
+  // Blocks: enough for about 16 expected hits in the first sweep of the grid
+  // (2^pow_bits tries per hit), at least one per SM, at most 8 per SM.
+  const uint64_t want = ((uint64_t)1 << (pow_bits < 24 ? pow_bits : 24)) * 16 / GRIND_STEP;
+  const uint64_t lo_b = (uint64_t)num_sms(), hi_b = 8 * (uint64_t)num_sms();
+  const unsigned blocks = (unsigned)(want < lo_b ? lo_b : want > hi_b ? hi_b : want);
   for (uint32_t hi = 0; hi < (1u << 12); hi++) {
     GS_CUDA_TRY(cudaMemsetAsync(d_scratch, 0xff, 4, st));
-    grind_kernel<<<(1u << 20) / 256, 256, 0, st>>>(d, hi, pow_bits, d_scratch);
+    grind_kernel<<<blocks, GRIND_STEP, 0, st>>>(d, hi, pow_bits, d_scratch);
     note_launch();
     GS_CUDA_TRY(cudaGetLastError());
     uint32_t local = 0;

@@ -165,15 +165,109 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(1024) merkle_tail_ke
     channel_mix_root_draw_dev(state, layers.p[0], root_copy, felt);
 }
 
-int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_state,
-                          uint32_t* d_root_copy, uint32_t* d_felt);
-int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers) {
-  return commit_node_layers_ch(st, top_log, layers, nullptr, nullptr, nullptr);
+// Every node layer of a tree in one launch. A unit is a 512-child subtree:
+// a block of 256 threads hashes its 256 parents, then each level above
+// through shared memory, down to the unit's root (9 levels), writing every
+// level to its global layer. Stage 1 has one block per unit of the input
+// layer. The block that finishes last among the units under one next-stage
+// unit goes on to hash that unit from the global layer; it learns that it is
+// last from a ticket (atomicInc after __threadfence, the counter wrapping
+// back to 0 for the next launch). No block waits for another, so there is no
+// spinning and nothing to bound. The block that writes the root runs the
+// optional channel step. Critical path: one compression per level, against
+// one launch per level before.
+struct TreePtrs { uint32_t* p[TREE_MAX_LOG + 1]; };
+
+__global__ void __launch_bounds__(256, 4) merkle_tree_kernel(uint32_t top, TreePtrs layers, uint32_t* counters,
+                                                             uint32_t* state, uint32_t* root_copy, uint32_t* felt) {
+  __shared__ uint4 buf[2][512];
+  __shared__ uint32_t last;
+  const uint32_t tid = threadIdx.x;
+  uint32_t in_log = top;
+  uint32_t u = blockIdx.x;
+  uint32_t cnt_off = 0;
+  for (;;) {
+    const uint32_t out_log = in_log > 9 ? in_log - 9 : 0;
+    int cur = 0;
+    for (int L = (int)in_log - 1; L >= (int)out_log; L--) {
+      const uint32_t n = 1u << (L - (int)out_log);  // this unit's nodes on level L (<= 256)
+      if (tid < n) {
+        const size_t node = ((size_t)u << (L - (int)out_log)) + tid;
+        uint4 c[4];
+        if (L == (int)in_log - 1) {
+          // written before the launch, or by other blocks of this launch:
+          // read at L2, not through the non-coherent path
+          const uint4* src = reinterpret_cast<const uint4*>(layers.p[L + 1]) + 4 * node;
+#pragma unroll
+          for (int q = 0; q < 4; q++) c[q] = __ldcg(src + q);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; q++) c[q] = buf[cur ^ 1][4 * tid + q];
+        }
+        uint32_t h[8];
+        hash_children16(c, h);
+        tail_store_hash(layers.p[L], node, h);
+        buf[cur][2 * tid] = make_uint4(h[0], h[1], h[2], h[3]);
+        buf[cur][2 * tid + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+      }
+      __syncthreads();
+      cur ^= 1;
+    }
+    if (out_log == 0) break;  // this block wrote the root
+    const uint32_t group_log = out_log > 9 ? 9u : out_log;
+    const uint32_t next_u = u >> group_log;
+    if (tid == 0) {
+      __threadfence();  // this unit's root (written by thread 0) before the ticket
+      const uint32_t ticket = atomicInc(counters + cnt_off + next_u, (1u << group_log) - 1u);
+      last = ticket == (1u << group_log) - 1u;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    cnt_off += 1u << (out_log - group_log);
+    u = next_u;
+    in_log = out_log;
+  }
+  if (state && tid == 0) channel_mix_root_draw_dev(state, layers.p[0], root_copy, felt);
 }
 
-int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_state,
-                          uint32_t* d_root_copy, uint32_t* d_felt) {
+int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters,
+                          uint32_t* d_state, uint32_t* d_root_copy, uint32_t* d_felt);
+int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters) {
+  return commit_node_layers_ch(st, top_log, layers, d_counters, nullptr, nullptr, nullptr);
+}
+
+// Stage-1 units of a tree of top_log <= TREE_MAX_LOG use at most 2^9 + 1
+// counters (TREE_COUNTERS).
+int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters,
+                          uint32_t* d_state, uint32_t* d_root_copy, uint32_t* d_felt) {
   GS_REQUIRE(top_log <= 30, "layer log size out of range");
+  static const bool legacy = [] {
+    const char* e = getenv("GS_MERKLE_LEGACY");
+    return e && e[0] == '1';
+  }();
+  if (!legacy) {
+    uint32_t top = top_log;
+    while (top > TREE_MAX_LOG) {  // layers above 2^27 nodes: one launch each
+      GS_TRY(commit_on_layer(st, top - 1, layers[top], nullptr, 0, layers[top - 1]));
+      top--;
+    }
+    if (top == 0) {
+      GS_REQUIRE(d_state == nullptr, "channel step needs a tree of at least two leaves");
+      return OK;
+    }
+    GS_REQUIRE(d_counters != nullptr, "tree kernel needs its counters");
+    TreePtrs tp{};
+    for (uint32_t k = 0; k <= top; k++) {
+      GS_REQUIRE(((uintptr_t)layers[k] & 15) == 0, "hash buffers must be 16-byte aligned");
+      tp.p[k] = layers[k];
+    }
+    const uint32_t blocks = top > 9 ? 1u << (top - 9) : 1u;
+    merkle_tree_kernel<<<blocks, 256, 0, st>>>(top, tp, d_counters, d_state, d_root_copy, d_felt);
+    note_launch();
+    GS_CUDA_TRY(cudaGetLastError());
+    return OK;
+  }
   // Layers of 2^11 nodes and more: one full-GPU launch each; the rest in
   // one cluster launch.
   uint32_t top = top_log;

@@ -43,6 +43,7 @@ struct CommitPlan {
   };
   std::vector<Group> groups;
   std::vector<uint32_t*> layers;        // layers[L]: 2^L hashes
+  uint32_t* counters = nullptr;         // Merkle tree kernel tickets (in `block`)
   void* block = nullptr;                // one device allocation for everything
   const void** d_src_table = nullptr;   // input pointers in group order (rewritten per run)
   const uint32_t* tw = nullptr;
@@ -85,7 +86,7 @@ int CommitPlan::enqueue(bool inputs_aligned) {
     // node-only layers down to the next injected size (or the root)
     uint32_t stop = gi < groups.size() ? groups[gi].log + blowup : 0;  // next injected layer
     if (stop == 0) {
-      GS_TRY(commit_node_layers(st, L + 1, layers.data()));
+      GS_TRY(commit_node_layers(st, L + 1, layers.data(), counters));
       break;
     }
     while (L > stop) {
@@ -185,6 +186,7 @@ int plan_create(Context& ctx, const uint32_t* log_sizes, uint32_t n, uint32_t bl
   size_t words = 3 * up64(2 * (size_t)n);  // src / coeff / eval tables (8 bytes per pointer)
   for (auto& g : p->groups) words += g.cols.size() * (g.stride_c + g.stride_e);
   for (uint32_t L = 0; L <= p->max_eval; L++) words += up64((size_t)8 << L);
+  words += up64(TREE_COUNTERS);  // the tree kernel's tickets, owned by the plan's stream
   GS_CUDA_TRY(cudaMalloc(&p->block, words * 4));
   uint32_t* carve = (uint32_t*)p->block;
   auto take = [&](size_t w) { uint32_t* q = carve; carve += up64(w); return q; };
@@ -208,12 +210,14 @@ int plan_create(Context& ctx, const uint32_t* log_sizes, uint32_t n, uint32_t bl
   }
   p->layers.resize(p->max_eval + 1);
   for (uint32_t L = 0; L <= p->max_eval; L++) p->layers[L] = take((size_t)8 << L);
+  p->counters = take(TREE_COUNTERS);
   GS_CUDA_TRY(cudaMemcpy(t_coef, h_coef.data(), h_coef.size() * sizeof(void*), cudaMemcpyHostToDevice));
   GS_CUDA_TRY(cudaMemcpy(t_eval, h_eval.data(), h_eval.size() * sizeof(void*), cudaMemcpyHostToDevice));
   p->tw_log = p->max_eval - 1;
   GS_TRY(ctx.twiddles(p->tw_log, &p->tw, &p->itw));
   GS_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
   GS_CUDA_TRY(cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking));
+  GS_CUDA_TRY(cudaMemsetAsync(p->counters, 0, 4 * TREE_COUNTERS, p->st));  // ordered before every run
   GS_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming));
   GS_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
   *out = p.release();

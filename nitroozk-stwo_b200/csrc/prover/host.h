@@ -203,6 +203,10 @@ inline size_t bitrev(size_t i, uint32_t log) {
 // ------------------------------------------------------------- proof
 struct Decommitment {
   std::vector<Hash> hash_witness;
+  // further witnesses held elsewhere (8 words each), serialised after
+  // hash_witness: the prover points into its gather read-back
+  const uint32_t* witness_words = nullptr;
+  size_t n_witness = 0;
   std::vector<uint32_t> column_witness;
 };
 struct FriLayerProof {
@@ -244,9 +248,10 @@ struct Writer {
   void hash(const Hash& h) { put(h.data(), 32); }
   void qm(const qm31& q) { u32(q.x.a); u32(q.x.b); u32(q.y.a); u32(q.y.b); }
   void dec(const Decommitment& d) {
-    u64(d.hash_witness.size());
+    u64(d.hash_witness.size() + d.n_witness);
     static_assert(sizeof(Hash) == 32, "Hash is 32 contiguous bytes");
     if (!d.hash_witness.empty()) put(d.hash_witness.data(), 32 * d.hash_witness.size());
+    if (d.n_witness) put(d.witness_words, 32 * d.n_witness);
     u64(d.column_witness.size());
     if (!d.column_witness.empty()) put(d.column_witness.data(), 4 * d.column_witness.size());
   }

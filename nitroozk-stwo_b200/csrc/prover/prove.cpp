@@ -1,5 +1,6 @@
 // prove() driver for the two benchmark components on the GPU prover.
 #include "prover_impl.h"
+#include <functional>
 #include "prove_api.h"
 
 namespace gs {
@@ -13,8 +14,11 @@ namespace prover {
 // challenge the next fold reads from device memory. Roots, challenges and the
 // last layer come back in one read at the end; the host replays the channel
 // on the roots and checks every challenge.
+// `while_busy` runs on the host after every FRI launch is enqueued and before
+// the one blocking read-back, overlapping host work with the device's.
 int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first,
-                      std::vector<FriLayerDev>& inner, std::vector<qm31>& last_coeffs) {
+                      std::vector<FriLayerDev>& inner, std::vector<qm31>& last_coeffs,
+                      const std::function<void()>& while_busy) {
   cudaStream_t st = pv.st;
   const uint32_t last_log = pv.cfg.log_last_layer + pv.cfg.log_blowup;
   GS_REQUIRE(lifting >= last_log + 1, "FRI: lifting domain below the last layer");
@@ -73,7 +77,7 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
     GS_TRY(pv.table(cols, &tab));
     GS_TRY(commit_on_layer(st, lifting, nullptr, tab, 4, first.layers[lifting]));
   }
-  GS_TRY(commit_node_layers_ch(st, first.log, first.layers.data(), ctl, d_roots, d_felts));
+  GS_TRY(commit_node_layers_ch(st, first.log, first.layers.data(), pv.ctx.tree_counters, ctl, d_roots, d_felts));
   // fold the circle evaluation into the first line layer (zero-initialised)
   FriLayerDev cur;
   take_layer(cur, lifting - 1);
@@ -104,7 +108,8 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
       k += ft.n;
       break;
     }
-    GS_TRY(commit_node_layers_ch(st, cur.log, cur.layers.data(), ctl, d_roots + 8 * k, d_felts + 8 * k));
+    GS_TRY(commit_node_layers_ch(st, cur.log, cur.layers.data(), pv.ctx.tree_counters, ctl, d_roots + 8 * k,
+                                 d_felts + 8 * k));
     FriLayerDev next;
     take_layer(next, cur.log - 1);
     GS_TRY(fold_line_dev_alpha(st, CPlanes{{cur.planes[0], cur.planes[1], cur.planes[2], cur.planes[3]}}, cur.log,
@@ -121,6 +126,7 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
   for (int c = 0; c < 4; c++)
     GS_CUDA_TRY(cudaMemcpyAsync(d_last + c * n, cur.planes[c], 4 * n, cudaMemcpyDeviceToDevice, st));
   std::vector<uint32_t> hc(ctl_used);
+  if (while_busy) while_busy();
   GS_TRY(pv.ctx.read_back(ctl, hc.size() * 4, hc.data()));
   std::vector<uint32_t> h(hc.begin() + 16 + 16 * (size_t)n_roots, hc.end());
   GS_REQUIRE(hc[9] == 0, "device channel: no challenge within the draw bound");

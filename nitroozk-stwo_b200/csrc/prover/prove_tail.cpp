@@ -3,13 +3,13 @@
 // check (crates/stwo/src/prover/mod.rs:50-150, prover/pcs/mod.rs:151-357).
 #include "prover_impl.h"
 #include "prove_api.h"
-#include <future>
+#include <functional>
 
 namespace gs {
 namespace prover {
 
 int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first, std::vector<FriLayerDev>& inner,
-               std::vector<qm31>& last_coeffs);
+               std::vector<qm31>& last_coeffs, const std::function<void()>& while_busy);
 void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::vector<bool>& is_witness);
 
 struct ColSamples {
@@ -90,15 +90,16 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   for (auto& tr : samples)
     for (auto& c : tr) flat.insert(flat.end(), c.values.begin(), c.values.end());
   pv.ch.mix_felts(flat);
+  pv.mark("oods_mix");
   pv.mark("oods_sample");
   // Sanity check (composition at the OODS point vs the constraints evaluated
-  // from the mask values) on a host thread, overlapping the device work of
-  // the quotients, FRI and the proof of work.
+  // from the mask values), run on this thread while the device works on the
+  // FRI layers (fri_commit calls it before its read-back).
   std::vector<std::vector<std::vector<qm31>>> sv(n_trees);
   for (size_t t = 0; t < n_trees; t++)
     for (auto& cs : samples[t]) sv[t].push_back(cs.values);
-  std::future<bool> sanity = std::async(std::launch::async, [&air, sv = std::move(sv), split, oods, E, max_ldb,
-                                                            random_coeff]() {
+  bool sane = false;
+  auto sanity = [&air, &sv, &sane, split, oods, E, max_ldb, random_coeff]() {
     auto& cv = sv.back();
     qm31 total = qm_zero();
     for (uint32_t t = 0; t < (1u << split); t++) {
@@ -110,8 +111,8 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     }
     qm31 dinv = qm_inv(host::canonic_vanishing(max_ldb, oods));
     qm31 cons = eval_at_point(air, sv, random_coeff, dinv);
-    return qm_eq(total, cons);
-  });
+    sane = qm_eq(total, cons);
+  };
   // DEEP quotients: per (column size, point) batches of line-coefficient
   // terms, lifted per point, combined over the lifting domain.
   qm31 qrc = pv.ch.draw_felt();
@@ -156,6 +157,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
       }
     }
   }
+  pv.mark("quot_plan");
   struct PointAcc2 {
     ptq point;
     std::vector<std::pair<uint32_t, uint32_t*>> parts;  // (log, planes base of 4 x 2^log)
@@ -222,7 +224,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   FriLayerDev first;
   std::vector<FriLayerDev> inner;
   std::vector<qm31> last;
-  GS_TRY(fri_commit(pv, quot, lifting, first, inner, last));
+  GS_TRY(fri_commit(pv, quot, lifting, first, inner, last, sanity));
   pv.mark("fri_commit");
   auto pre = pv.ch.pow_prefixed(cfg.pow_bits);
   uint64_t nonce = 0;
@@ -235,8 +237,10 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   std::vector<size_t> queries(raw);
   std::sort(queries.begin(), queries.end());
   queries.erase(std::unique(queries.begin(), queries.end()), queries.end());
+  pv.mark("queries");
   // plan all gathers of the decommitment
-  GatherPlan g;
+  static thread_local GatherPlan g;  // keeps its capacity across proofs
+  g.clear();
   struct FriPlan {
     std::vector<size_t> pos;
     std::vector<bool> wit;
@@ -260,6 +264,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     lq = f;
     GS_TRY(plan_fri(inner[i], lq, inner_plans[i]));
   }
+  pv.mark("fri_plans");
   std::vector<MerkleDecommitPlan> tree_plans(n_trees);
   for (size_t t = 0; t < n_trees; t++) {
     Tree& tr = pv.trees[t];
@@ -282,7 +287,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   auto fri_layer_proof = [&](const FriPlan& fp, const FriLayerDev& L, host::FriLayerProof& out) {
     for (size_t k = 0; k < fp.pos.size(); k++)
       if (fp.wit[k]) {
-        const uint32_t* w = g.word_out.data() + fp.val_base + 4 * k;
+        const uint32_t* w = g.word_out + fp.val_base + 4 * k;
         out.fri_witness.push_back(qm_make(w[0], w[1], w[2], w[3]));
       }
     std::vector<uint32_t> unused;
@@ -305,9 +310,8 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     for (auto& cs : samples[t]) P.sampled_values[t].push_back(cs.values);
     if (tr.n_cols) tree_plans[t].assemble(g, P.queried_values[t], P.decommitments[t]);
   }
-  const bool sane = sanity.get();
   if (stats) stats->constraint_check = sane ? 1.0 : 0.0;
-  pv.mark("sanity_check");
+  pv.mark("assemble");
   host::serialize_into(P, *proof_bytes);
   pv.mark("serialize");
   if (!sane) {

@@ -68,10 +68,26 @@ struct Tree {
 struct GatherPlan {
   std::vector<ColGather> blocks;
   std::vector<uint32_t> positions;
-  std::vector<GatherItem> hashes;
+  std::vector<HashRun> runs;
+  std::vector<uint32_t> hidx;    // hash index of every witness, in output order
+  std::vector<uint8_t> packed;   // the upload: blocks | positions | runs | hidx
   size_t n_words = 0;
   uint32_t max_items = 0;
-  std::vector<uint32_t> word_out, hash_out;
+  // results, in the context's pinned read-back buffer (valid until its next
+  // read-back): gathered words, then 8 words per hash
+  const uint32_t* word_out = nullptr;
+  const uint32_t* hash_out = nullptr;
+  // Empties the plan, keeping its capacity (one plan serves many proofs).
+  void clear() {
+    blocks.clear();
+    positions.clear();
+    runs.clear();
+    hidx.clear();
+    n_words = 0;
+    max_items = 0;
+    word_out = hash_out = nullptr;
+  }
+  size_t n_hashes() const { return hidx.size(); }
   // Values of `cols` at `pos`, position-major; returns the first output word.
   // More than 4 columns must be equally spaced (one tree's columns are).
   int add_cols(const std::vector<const uint32_t*>& cols, const std::vector<size_t>& pos, size_t* first) {
@@ -95,50 +111,55 @@ struct GatherPlan {
     if (b.n_cols && b.n_pos) blocks.push_back(b);
     return OK;
   }
-  size_t add_hash(const uint32_t* src, size_t idx) { hashes.push_back({src, idx}); return hashes.size() - 1; }
-  template <class T>
-  static int upload(Context& ctx, T* dst, const std::vector<T>& v) {
-    const size_t bytes = v.size() * sizeof(T);
-    if (!bytes) return OK;
-    if (bytes <= ctx.ring_cap / 2) {  // through the pinned staging ring
-      const void* d = nullptr;
-      GS_TRY(ctx.stage_bytes(v.data(), bytes, &d));
-      GS_CUDA_TRY(cudaMemcpyAsync(dst, d, bytes, cudaMemcpyDeviceToDevice, ctx.stream));
-    } else {
-      GS_CUDA_TRY(cudaMemcpyAsync(dst, v.data(), bytes, cudaMemcpyHostToDevice, ctx.stream));
-    }
-    return OK;
+  // Witnesses hidx[first, first + count) read from the layer at `src`.
+  void add_run(const uint32_t* src, size_t first, size_t count) {
+    runs.push_back(HashRun{src, (uint32_t)first, (uint32_t)count});
   }
   int run(Context& ctx, Arena& A) {
     cudaStream_t st = ctx.stream;
-    const size_t nh = hashes.size();
-    ColGather* d_blocks = nullptr;
-    uint32_t* d_pos = nullptr;
-    GatherItem* d_items = nullptr;
-    uint32_t* d_out = nullptr;
+    const size_t nh = hidx.size();
+    auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const size_t o_pos = al(blocks.size() * sizeof(ColGather));
+    const size_t o_runs = o_pos + al(positions.size() * 4);
+    const size_t o_idx = o_runs + al(runs.size() * sizeof(HashRun));
+    const size_t total = o_idx + al(nh * 4);
+    packed.resize(total);
+    if (!blocks.empty()) memcpy(packed.data(), blocks.data(), blocks.size() * sizeof(ColGather));
+    if (!positions.empty()) memcpy(packed.data() + o_pos, positions.data(), positions.size() * 4);
+    if (!runs.empty()) memcpy(packed.data() + o_runs, runs.data(), runs.size() * sizeof(HashRun));
+    if (nh) memcpy(packed.data() + o_idx, hidx.data(), nh * 4);
+    // kernels read the upload where it lands: the staging ring when it fits
+    const uint8_t* d_in = nullptr;
+    if (total == 0) {
+    } else if (total <= ctx.ring_cap / 2) {
+      const void* d = nullptr;
+      GS_TRY(ctx.stage_bytes(packed.data(), total, &d));
+      d_in = (const uint8_t*)d;
+    } else {
+      uint8_t* d = nullptr;
+      GS_TRY(A.alloc_n(total, &d));
+      GS_CUDA_TRY(cudaMemcpyAsync(d, packed.data(), total, cudaMemcpyHostToDevice, st));
+      d_in = d;
+    }
     // hashes are written as 16-byte vectors: their region starts at a
     // multiple of 4 words
     const size_t hbase = (n_words + 3) & ~(size_t)3;
-    GS_TRY(A.alloc_n(blocks.size() + 1, &d_blocks));
-    GS_TRY(A.alloc_n(positions.size() + 1, &d_pos));
-    GS_TRY(A.alloc_n(nh + 1, &d_items));
-    GS_TRY(A.alloc_n(hbase + 8 * nh + 4, &d_out));
-    GS_TRY(upload(ctx, d_blocks, blocks));
-    GS_TRY(upload(ctx, d_pos, positions));
-    GS_TRY(upload(ctx, d_items, hashes));
-    GS_TRY(gather_cols(st, d_blocks, (uint32_t)blocks.size(), max_items, d_pos, d_out));
-    GS_TRY(gather_hashes(st, d_items, nh, d_out + hbase));
     const size_t out_words = hbase + 8 * nh;
+    uint32_t* d_out = nullptr;
+    GS_TRY(A.alloc_n(out_words + 4, &d_out));
+    GS_TRY(gather_cols(st, (const ColGather*)d_in, (uint32_t)blocks.size(), max_items, (const uint32_t*)(d_in + o_pos),
+                       d_out));
+    GS_TRY(gather_hash_runs(st, (const HashRun*)(d_in + o_runs), (uint32_t)runs.size(),
+                            (const uint32_t*)(d_in + o_idx), d_out + hbase));
     void* hr = nullptr;
     GS_TRY(ctx.read_buffer(out_words * 4, &hr));
     if (out_words) GS_CUDA_TRY(cudaMemcpyAsync(hr, d_out, out_words * 4, cudaMemcpyDeviceToHost, st));
     GS_TRY(stream_sync(st));
-    const uint32_t* o = (const uint32_t*)hr;
-    word_out.assign(o, o + n_words);
-    hash_out.assign(o + hbase, o + out_words);
+    word_out = (const uint32_t*)hr;
+    hash_out = word_out + hbase;
     return OK;
   }
-  host::Hash hash(size_t slot) const { return host::hash_from_words(hash_out.data() + 8 * slot); }
+  host::Hash hash(size_t slot) const { return host::hash_from_words(hash_out + 8 * slot); }
 };
 
 // Merkle decommitment of a tree whose columns all sit at the leaf layer
@@ -147,39 +168,55 @@ struct GatherPlan {
 // lists, layer by layer from the leaves up, the children that the verifier
 // cannot recompute. Pass 1 queues the gathers, pass 2 assembles.
 struct MerkleDecommitPlan {
-  std::vector<size_t> positions;
+  size_t n_positions = 0;
   size_t value_base = 0, n_cols = 0;
-  std::vector<size_t> hash_slots;
+  size_t hash_begin = 0, n_hashes = 0;  // this plan's witnesses: consecutive gather slots
   // with_values = false: the caller gathers the queried values itself.
   int plan(GatherPlan& g, const std::vector<uint32_t*>& layers, const std::vector<const uint32_t*>& cols,
            const std::vector<size_t>& pos, bool with_values = true) {
-    positions = pos;
+    n_positions = pos.size();
     n_cols = with_values ? cols.size() : 0;
     if (with_values) GS_TRY(g.add_cols(cols, pos, &value_base));
-    // positions are sorted and unique at every layer, so membership of a
-    // sibling is a linear merge against the previous layer's list
-    std::vector<size_t> prev = pos, merged;
+    // Positions are sorted and unique on every layer, so a node's sibling is
+    // known exactly when it is the neighbour in the list; otherwise the
+    // sibling is a witness. Witnesses come out parent by parent, left child
+    // first, as the verifier consumes them.
+    // The loop body has no data-dependent branch: every position writes its
+    // sibling and its parent, and the counts advance only for a missing
+    // sibling and for a new parent.
+    hash_begin = g.n_hashes();
+    static thread_local std::vector<size_t> prev, next;
+    prev.assign(pos.begin(), pos.end());
     for (int L = (int)layers.size() - 2; L >= 0; L--) {
-      merged.clear();
-      for (size_t q : prev)
-        if (merged.empty() || merged.back() != q / 2) merged.push_back(q / 2);
-      size_t ip = 0;
-      for (size_t node : merged)
-        for (size_t ch = 2 * node; ch <= 2 * node + 1; ch++) {
-          while (ip < prev.size() && prev[ip] < ch) ip++;
-          if (ip == prev.size() || prev[ip] != ch) hash_slots.push_back(g.add_hash(layers[L + 1], ch));
-        }
-      prev.swap(merged);
+      const size_t n = prev.size();
+      const size_t base = g.hidx.size();
+      g.hidx.resize(base + n);  // at most one witness per position
+      uint32_t* w = g.hidx.data() + base;
+      next.resize(n);
+      size_t nw = 0, nn = 0, last_parent = ~(size_t)0;
+      for (size_t i = 0; i < n; i++) {
+        const size_t q = prev[i];
+        const bool sib = (q & 1) ? (i > 0 && prev[i - 1] == q - 1) : (i + 1 < n && prev[i + 1] == q + 1);
+        w[nw] = (uint32_t)(q ^ 1);
+        nw += sib ? 0 : 1;
+        const size_t par = q >> 1;
+        next[nn] = par;
+        nn += par != last_parent ? 1 : 0;
+        last_parent = par;
+      }
+      g.hidx.resize(base + nw);
+      if (nw) g.add_run(layers[L + 1], base, nw);
+      next.resize(nn);
+      prev.swap(next);
     }
+    n_hashes = g.n_hashes() - hash_begin;
     return OK;
   }
+  // The witnesses stay in the gather's read-back buffer; `d` refers to them.
   void assemble(const GatherPlan& g, std::vector<uint32_t>& queried, host::Decommitment& d) const {
-    queried.assign(g.word_out.begin() + value_base, g.word_out.begin() + value_base + positions.size() * n_cols);
-    d.hash_witness.reserve(d.hash_witness.size() + hash_slots.size());
-    for (size_t s : hash_slots) {
-      d.hash_witness.emplace_back();
-      memcpy(d.hash_witness.back().data(), g.hash_out.data() + 8 * s, 32);
-    }
+    queried.assign(g.word_out + value_base, g.word_out + value_base + n_positions * n_cols);
+    d.witness_words = g.hash_out + 8 * hash_begin;
+    d.n_witness = n_hashes;
   }
 };
 

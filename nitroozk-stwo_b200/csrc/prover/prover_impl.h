@@ -116,7 +116,7 @@ struct Prover {
     const uint32_t* const* tab = nullptr;
     GS_TRY(table(cols, &tab));
     GS_TRY(commit_on_layer(st, t.eval_log, nullptr, tab, t.n_cols, t.layers[t.eval_log]));
-    GS_TRY(commit_node_layers(st, t.eval_log, t.layers.data()));
+    GS_TRY(commit_node_layers(st, t.eval_log, t.layers.data(), ctx.tree_counters));
     uint32_t w[8];
     GS_TRY(ctx.read_back(t.layers[0], 32, w));
     t.root = host::hash_from_words(w);

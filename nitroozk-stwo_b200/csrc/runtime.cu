@@ -62,6 +62,8 @@ int Context::init(void* user_stream) {
   small_cap = 4096;
   GS_CUDA_TRY(cudaMalloc((void**)&d_small, small_cap));
   GS_CUDA_TRY(cudaMallocHost((void**)&h_small, small_cap));
+  GS_CUDA_TRY(cudaMalloc((void**)&tree_counters, 4 * TREE_COUNTERS));
+  GS_CUDA_TRY(cudaMemsetAsync(tree_counters, 0, 4 * TREE_COUNTERS, stream));
   return OK;
 }
 
@@ -82,6 +84,8 @@ void Context::destroy() {
   if (h_ring) cudaFreeHost(h_ring);
   if (d_ring) cudaFree(d_ring);
   if (d_small) cudaFree(d_small);
+  if (tree_counters) cudaFree(tree_counters);
+  tree_counters = nullptr;
   if (h_small) cudaFreeHost(h_small);
   if (h_read) cudaFreeHost(h_read);
   h_read = nullptr;

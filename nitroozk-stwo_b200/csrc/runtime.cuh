@@ -85,6 +85,8 @@ struct Context {
   uint8_t* d_small = nullptr;
   uint8_t* h_small = nullptr;  // pinned mirror
   size_t small_cap = 0;
+  // ticket counters of the one-launch Merkle tree kernel (TREE_COUNTERS words)
+  uint32_t* tree_counters = nullptr;
 
   // Stream-ordered memory pool owned by this context. Contexts that run
   // concurrently (the proof server's workers) do not share a pool, so
@@ -142,12 +144,17 @@ int fft_autotune(cudaStream_t st, uint32_t lo, uint32_t hi, const uint32_t* tw, 
 // merkle.cu
 int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, const uint32_t* const* d_cols,
                     uint32_t n_cols, uint32_t* d_out);
-// All node-only layers below `top_log` (layers[L] has 2^L hashes, layers[top_log] given).
-int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers);
-// The same, followed by the Fiat-Shamir channel step on the root in the last
+// All node-only layers below `top_log` (layers[L] has 2^L hashes, layers[top_log] given),
+// in one launch up to TREE_MAX_LOG. d_counters: TREE_COUNTERS zeroed words
+// owned by the calling stream (left zeroed); no two launches that share them
+// may run at the same time.
+constexpr uint32_t TREE_MAX_LOG = 27;
+constexpr uint32_t TREE_COUNTERS = 1024;
+int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters);
+// The same, followed by the Fiat-Shamir channel step on the root in the same
 // launch (the FRI commit phase).
-int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_state,
-                          uint32_t* d_root_copy, uint32_t* d_felt);
+int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters,
+                          uint32_t* d_state, uint32_t* d_root_copy, uint32_t* d_felt);
 // Lifted Merkle leaves; d_shifts[c] = lift - log size of column c (columns in
 // increasing size order).
 int lifted_leaves(cudaStream_t st, uint32_t lift, const uint32_t* const* d_cols, const uint8_t* d_shifts,

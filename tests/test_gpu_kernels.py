@@ -150,10 +150,22 @@ def test_fold_circle_into_line(B, log_n):
     assert np.array_equal(got, expect)
 
 
-@pytest.mark.parametrize("pow_bits", [0, 1, 10, 14])
-def test_grind(B, pow_bits):
-    digest = hashlib.blake2s(b"channel-%d" % pow_bits, digest_size=32).digest()
-    assert B.grind(digest, pow_bits) == O.grind(digest, pow_bits)
+@pytest.mark.parametrize("pow_bits,salt", [(0, 0), (1, 0), (5, 0), (10, 0), (10, 1), (10, 2), (10, 3), (14, 0),
+                                           (18, 0), (21, 0)])
+def test_grind(B, pow_bits, salt):
+    """The smallest passing nonce (the early-exit grid skips only steps above
+    a recorded hit). The device searches low words below 2^20 under high word
+    0, 1, ... (simd/grind.rs, the reference CUDA grind); the oracle searches
+    0, 1, 2, ... (cpu/grind.rs). They meet whenever a hit lies below 2^20;
+    otherwise the device's nonce has a higher word and passes the check."""
+    digest = hashlib.blake2s(b"channel-%d-%d" % (pow_bits, salt), digest_size=32).digest()
+    got = B.grind(digest, pow_bits)
+    want = O.grind(digest, pow_bits)
+    if want < (1 << 20):
+        assert got == want
+    else:
+        assert got >> 32 >= 1 and (got & 0xFFFFFFFF) < (1 << 20)
+        assert O.verify_pow(digest, pow_bits, got)
 
 
 # ---------------------------------------------------------------- full sizes
@@ -181,9 +193,11 @@ def test_merkle_64x2p20_root(B):
     assert host(prev).view(np.uint8).tobytes() == O.merkle_root(cols)
 
 
-@pytest.mark.parametrize("top", [1, 5, 11, 12, 15])
+@pytest.mark.parametrize("top", [1, 5, 9, 10, 11, 12, 15, 18, 19, 20])
 def test_commit_node_layers_fused(B, top):
-    """The fused node-only layers equal per-layer commit_on_layer calls."""
+    """The one-launch tree (512-child units, the last block of each group
+    going on to the next stage) equals per-layer oracle commit_on_layer
+    calls, across the unit boundaries (9/10 and 18/19/20 leaves-log)."""
     rng = np.random.default_rng(900 + top)
     leaves = rng.integers(0, 256, (1 << top) * 32, dtype=np.uint8)
     layers = [__import__("torch").empty((1 << L) * 8, dtype=__import__("torch").int32, device="cuda")
@@ -194,6 +208,22 @@ def test_commit_node_layers_fused(B, top):
     for L in range(top - 1, -1, -1):
         prev = O.commit_on_layer(L, prev.reshape(-1), [])
         assert np.array_equal(host(layers[L]).view(np.uint8).reshape(-1, 32), prev), L
+
+
+def test_commit_node_layers_repeated_launches(B):
+    """The ticket counters wrap back to zero: trees of different sizes
+    launched back to back on one context keep giving the oracle's roots."""
+    import torch
+    rng = np.random.default_rng(950)
+    for top in (19, 12, 20, 10, 19, 3, 19):
+        leaves = rng.integers(0, 256, (1 << top) * 32, dtype=np.uint8)
+        layers = [torch.empty((1 << L) * 8, dtype=torch.int32, device="cuda") for L in range(top + 1)]
+        layers[top].copy_(dev(leaves.view(np.uint32)))
+        B.commit_node_layers(layers)
+        prev = leaves
+        for L in range(top - 1, -1, -1):
+            prev = O.commit_on_layer(L, prev.reshape(-1), [])
+        assert np.array_equal(host(layers[0]).view(np.uint8).reshape(-1, 32), prev), top
 
 
 def test_fold_line_2p22(B):
