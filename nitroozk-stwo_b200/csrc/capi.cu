@@ -368,19 +368,22 @@ static int run_prove(gs_ctx* ctx, prover::ProveRequest& req, const gs_pcs_config
   GS_REQUIRE(req.input_mode <= 2, "unknown input mode");
   GS_REQUIRE(req.input_mode != 2 || req.host_inputs != nullptr, "host inputs required");
   GS_REQUIRE(req.cfg.pow_bits <= 32 && req.cfg.n_queries >= 1 && req.cfg.log_last_layer <= 10, "bad PCS config");
-  // reused per thread: the proof's pages are touched once, not per proof
+  // serialised straight into the caller's buffer when it fits; the string
+  // (reused per thread) only holds a proof that does not, for its length
   static thread_local std::string bytes;
-  int st = prover::prove_component(ctx->c, req, &bytes, nullptr);
-  *proof_len = bytes.size();
+  req.out_buf = proof;
+  req.out_cap = proof ? capacity : 0;
+  prover::ProveStats stats;
+  int st = prover::prove_component(ctx->c, req, &bytes, &stats);
+  *proof_len = stats.proof_len;
   if (st != OK) {
     cudaStreamSynchronize(ctx->c.stream);
     return st;
   }
-  if (bytes.size() > capacity || !proof) {
+  if (!stats.in_out_buf) {
     set_error("proof buffer too small");
     return ERR_INVALID;
   }
-  memcpy(proof, bytes.data(), bytes.size());
   return OK;
 }
 

@@ -493,9 +493,9 @@ static void launch_tile(cudaStream_t st, dim3 grid, uint32_t threads, const uint
   note_launch();
 }
 
-// The specialised kernel covers the partitions of the default tuning
-// (first pass C = 0 with 5..13 layers, later passes C = 4 with 5..9 layers);
-// anything else runs the generic pass. GS_FFT_GENERIC=1 forces the generic
+// The specialised kernel covers first passes (C = 0, 5..13 layers) and later
+// passes with 16 or 32 contiguous words per tile row (C = 4 with 5..9 layers,
+// C = 5 with 5..8); anything else runs the generic pass. GS_FFT_GENERIC=1 forces the generic
 // pass (for comparisons).
 template <bool INV>
 static bool launch_tile_any(cudaStream_t st, dim3 grid, uint32_t threads, const uint32_t* const* s,
@@ -513,6 +513,9 @@ static bool launch_tile_any(cudaStream_t st, dim3 grid, uint32_t threads, const 
   }
   if (a.c == 4) {
     switch (a.L) { GS_TILE(5, 4) GS_TILE(6, 4) GS_TILE(7, 4) GS_TILE(8, 4) GS_TILE(9, 4) default: return false; }
+  }
+  if (a.c == 5) {
+    switch (a.L) { GS_TILE(5, 5) GS_TILE(6, 5) GS_TILE(7, 5) GS_TILE(8, 5) default: return false; }
   }
 #undef GS_TILE
   return false;
@@ -627,7 +630,7 @@ int set_fft_tuning(uint32_t layers, uint32_t tile_log, uint32_t coalesce_bits) {
 int fft_autotune(cudaStream_t st, uint32_t lo, uint32_t hi, const uint32_t* tw, const uint32_t* itw, uint32_t tw_log,
                  uint32_t* out_tile, uint32_t* out_coalesce) {
   GS_REQUIRE(lo >= 3 && hi <= 27 && lo <= hi && tw_log + 1 >= hi, "autotune range out of bounds");
-  static const FftTuning fixed[] = {{13, 4}, {12, 4}, {11, 4}, {10, 4}, {13, 3}, {12, 5}};
+  static const FftTuning fixed[] = {{13, 4}, {12, 4}, {11, 4}, {10, 4}, {13, 5}, {12, 5}, {11, 5}, {13, 3}};
   const size_t words = (size_t)1 << (hi > 24 ? hi : 24);
   uint32_t* buf = nullptr;
   uint32_t** tab = nullptr;

@@ -305,6 +305,25 @@ inline void serialize_into(const Proof& p, std::string& out) {
   write_proof(w, p);
 }
 
+// Into `buf` when the proof fits its `cap` bytes (returns true), else into
+// `out`; *len receives the proof's length either way.
+inline bool serialize_to(const Proof& p, uint8_t* buf, size_t cap, std::string& out, size_t* len) {
+  Writer count;
+  write_proof(count, p);
+  *len = count.len;
+  if (buf && count.len <= cap) {
+    Writer w;
+    w.out = (char*)buf;
+    write_proof(w, p);
+    return true;
+  }
+  out.resize(count.len);
+  Writer w;
+  w.out = count.len ? &out[0] : nullptr;
+  write_proof(w, p);
+  return false;
+}
+
 inline std::string serialize(const Proof& p) {
   std::string s;
   serialize_into(p, s);

@@ -244,7 +244,7 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
     GS_TRY(pv.commit_evals(inter, 4, T));
     pv.mark("interaction_commit");
   }
-  int rc = prove_tail(pv, air, split, proof_bytes, stats);
+  int rc = prove_tail(pv, air, split, proof_bytes, stats, req.out_buf, req.out_cap);
   pv.mark("end");
   pv.phases.report();
   return rc;

@@ -15,16 +15,23 @@ struct ProveRequest {
   const uint32_t* host_inputs = nullptr;  // mode 2: WF a,b columns; Poseidon 16 state columns
   uint32_t split_log = 1;    // composition split
   PcsConfig cfg;
+  // Optional caller buffer: when the proof fits, it is serialised straight
+  // into it (ProveStats::in_out_buf) and the string stays untouched.
+  uint8_t* out_buf = nullptr;
+  size_t out_cap = 0;
 };
 
 struct ProveStats {
   double constraint_check = 0;  // 1 if the composition sanity check passed
+  size_t proof_len = 0;         // serialised proof bytes
+  bool in_out_buf = false;      // written to ProveRequest::out_buf
 };
 
 struct Prover;
 struct AirHost;
 int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_bytes, ProveStats* stats);
-int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_bytes, ProveStats* stats);
+int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_bytes, ProveStats* stats,
+               uint8_t* out_buf = nullptr, size_t out_cap = 0);
 
 // Batched commitment of columns of mixed sizes (commit.cpp).
 struct CommitPlan;

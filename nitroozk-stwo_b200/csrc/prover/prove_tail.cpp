@@ -17,7 +17,8 @@ struct ColSamples {
   std::vector<qm31> values;
 };
 
-int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_bytes, ProveStats* stats) {
+int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_bytes, ProveStats* stats,
+               uint8_t* out_buf, size_t out_cap) {
   cudaStream_t st = pv.st;
   const PcsConfig& cfg = pv.cfg;
   const uint32_t E = air.max_constraint_log();
@@ -312,7 +313,14 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   }
   if (stats) stats->constraint_check = sane ? 1.0 : 0.0;
   pv.mark("assemble");
-  host::serialize_into(P, *proof_bytes);
+  {
+    size_t len = 0;
+    const bool direct = host::serialize_to(P, out_buf, out_cap, *proof_bytes, &len);
+    if (stats) {
+      stats->proof_len = len;
+      stats->in_out_buf = direct;
+    }
+  }
   pv.mark("serialize");
   if (!sane) {
     set_error("constraints not satisfied: composition OODS value differs from the constraints at the mask");

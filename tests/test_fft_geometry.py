@@ -26,7 +26,7 @@ def partition(layers, T, C):
 
 
 def specialised(R, c, L):
-    return R == 5 and ((c == 0 and 5 <= L <= 13) or (c == 4 and 5 <= L <= 9))
+    return R == 5 and ((c == 0 and 5 <= L <= 13) or (c == 4 and 5 <= L <= 9) or (c == 5 and 5 <= L <= 8))
 
 
 def padw(e):
@@ -130,7 +130,7 @@ def check_split(n, layers, T, C, INV, src_mask, tw_len):
             ld = np.sort(np.concatenate(loads))
             assert (ld == np.arange(N)).all(), "loads not a permutation"
         if spec:
-            assert (c, L) in [(0, l) for l in range(5, 14)] + [(4, l) for l in range(5, 10)]
+            assert (c, L) in [(0, l) for l in range(5, 14)] + [(4, l) for l in range(5, 10)] + [(5, l) for l in range(5, 9)]
 
 
 SPLITS = [(T, C) for T in range(6, 14) for C in range(0, 6) if C + 5 <= T]

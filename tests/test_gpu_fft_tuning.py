@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 P = O.P
 
-SPLITS = [(13, 4), (12, 4), (11, 4), (10, 4), (13, 3), (12, 5), (8, 3), (6, 0), (13, 0)]
+SPLITS = [(13, 4), (12, 4), (11, 4), (10, 4), (13, 3), (13, 5), (12, 5), (11, 5), (10, 5), (8, 3), (6, 0), (13, 0)]
 
 
 @pytest.fixture(scope="module")
