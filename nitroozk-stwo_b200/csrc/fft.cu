@@ -220,21 +220,7 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const uint32_t* const* __
 //    the FMA pipe), leaving one add-then-min (VIADDMNMX) per add/sub on the
 //    ALU pipe.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t imad_u32(uint32_t a, uint32_t b, uint32_t c) {
-  uint32_t r;
-  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
-  return r;
-}
-// a + b (one = 1 at run time)
-__device__ __forceinline__ uint32_t add_f(uint32_t a, uint32_t b, uint32_t one) {
-  uint32_t s = imad_u32(a, one, b);
-  return __viaddmin_u32(s, 0u - P, s);
-}
-// a - b (neg1 = 2^32 - 1 at run time)
-__device__ __forceinline__ uint32_t sub_f(uint32_t a, uint32_t b, uint32_t neg1) {
-  uint32_t d = imad_u32(b, neg1, a);
-  return __viaddmin_u32(d, P, d);
-}
+// (imad_u32, add_f, sub_f: m31.cuh)
 template <bool INV>
 __device__ __forceinline__ void bfly_f(uint32_t& a, uint32_t& b, uint32_t w, uint32_t one, uint32_t neg1) {
   if (INV) {

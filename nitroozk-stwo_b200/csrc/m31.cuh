@@ -61,6 +61,29 @@ __device__ __forceinline__ uint32_t mul_b2(uint32_t a, uint32_t b2) {
   uint32_t r = (uint32_t)(p >> 32) + ((uint32_t)p >> 1);
   return __viaddmin_u32(r, 0u - P, r);
 }
+// FMA-pipe forms. The integer ALU pipe bounds the FFT, Blake2s and
+// constraint kernels while the FMA pipe idles; an add issued as an IMAD
+// against a runtime 1 (or -1), which the compiler cannot fold, runs there
+// instead, leaving one add-then-min per field add/sub on the ALU pipe.
+__device__ __forceinline__ uint32_t imad_u32(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+  return r;
+}
+// a + b (one = 1 at run time)
+__device__ __forceinline__ uint32_t add_f(uint32_t a, uint32_t b, uint32_t one) {
+  uint32_t s = imad_u32(a, one, b);
+  return __viaddmin_u32(s, 0u - P, s);
+}
+// a - b (neg1 = 2^32 - 1 at run time)
+__device__ __forceinline__ uint32_t sub_f(uint32_t a, uint32_t b, uint32_t neg1) {
+  uint32_t d = imad_u32(b, neg1, a);
+  return __viaddmin_u32(d, P, d);
+}
+// a * b with the doubling of b on the FMA pipe
+__device__ __forceinline__ uint32_t mul_f(uint32_t a, uint32_t b, uint32_t one) {
+  return mul_b2(a, imad_u32(b, one, b));
+}
 GS_HD uint32_t mul(uint32_t a, uint32_t b) {
 #ifdef __CUDA_ARCH__
   return mul_b2(a, b << 1);
