@@ -292,13 +292,14 @@ def cpu_sweep_sample(threads):
 
 def fft_autotune(args, hi):
     """Installs the FFT pass splits the library's autotuner picks for log
-    sizes 8..hi (set-up, outside every timed region); returns the picks that
-    differ from the default 13/4 as {log: "tile_log/coalesce_bits"}."""
+    sizes 8..hi and LDE extensions 0..2 (set-up, outside every timed region);
+    returns the picks that differ from the default 13/4 as
+    {"log+extension": "tile_log/coalesce_bits"}."""
     if args.fft_autotune == "off":
         return "off"
     from gpustark.backend import GpuBackend
-    picks = GpuBackend.fft_autotune(8, min(hi, 27))
-    return {str(k): "%d/%d" % v for k, v in picks.items() if v != (13, 4)}
+    picks = GpuBackend.fft_autotune(8, min(hi, 27), 2)
+    return {"%d+%d" % k: "%d/%d" % v for k, v in picks.items() if v != (13, 4)}
 
 
 def run_kernels(args, world, rank, local):

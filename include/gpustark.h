@@ -92,20 +92,25 @@ int gs_evaluate_columns(gs_ctx* ctx, const uint32_t* const* coeffs, uint32_t coe
                         uint32_t n_cols, uint32_t log_size, const uint32_t* twiddles, uint32_t twiddles_log_size);
 
 /* FFT pass-split tuning. No counterpart in the reference, whose CUDA FFT
- * (ntt.cu) has one fixed geometry. An FFT computing n layers runs in passes
- * over shared-memory tiles of 2^tile_log words, 2^coalesce_bits of them
- * contiguous in memory; the split changes speed only, never the values.
- * gs_fft_autotune times the round trip evaluate + interpolate of every split
- * candidate for each n in [min_log, max_log] (3 <= min_log <= max_log <= 27)
- * on scratch columns (2^max(24, max_log) words) and installs the fastest for
- * all contexts of the process; tile_logs / coalesce_bits (max_log - min_log
- * + 1 entries each) receive the choices when non-NULL. Both set-up calls:
- * no other FFT may be in flight. gs_fft_set_tuning installs one split
- * (log_size 0: every size; tile_log in [6, 13], coalesce_bits <= min(5,
- * tile_log - 5)); gs_fft_get_tuning reads it. Default: 13 / 4. */
-int gs_fft_autotune(gs_ctx* ctx, uint32_t min_log, uint32_t max_log, uint32_t* tile_logs, uint32_t* coalesce_bits);
-int gs_fft_set_tuning(uint32_t log_size, uint32_t tile_log, uint32_t coalesce_bits);
-int gs_fft_get_tuning(uint32_t log_size, uint32_t* tile_log, uint32_t* coalesce_bits);
+ * (ntt.cu) has one fixed geometry. An FFT that computes n layers runs in
+ * passes over shared-memory tiles of 2^tile_log words, 2^coalesce_bits of
+ * them contiguous in memory; the split changes speed only, never the values.
+ * A split is kept per (n, extension): extension 0 for an FFT of 2^n points, e
+ * for an LDE of 2^n coefficients onto 2^(n+e) points (e >= 3 share one).
+ * gs_fft_autotune times every split candidate for each n in [min_log,
+ * max_log] (3 <= min_log <= max_log <= 27) and extension in [0,
+ * max_extension] (<= 3) on scratch columns (2^max(24, max_log) output words;
+ * larger LDEs keep their split) and installs the fastest for all contexts of
+ * the process; tile_logs / coalesce_bits, when non-NULL, receive the choices,
+ * (max_log - min_log + 1) x (max_extension + 1) entries by log size. Both
+ * set-up calls: no other FFT may be in flight. gs_fft_set_tuning installs one
+ * split (log_size 0: every size; extension > 3: every extension; tile_log in
+ * [6, 13], coalesce_bits <= min(5, tile_log - 5)); gs_fft_get_tuning reads
+ * it. Default: 13 / 4. */
+int gs_fft_autotune(gs_ctx* ctx, uint32_t min_log, uint32_t max_log, uint32_t max_extension, uint32_t* tile_logs,
+                    uint32_t* coalesce_bits);
+int gs_fft_set_tuning(uint32_t log_size, uint32_t extension, uint32_t tile_log, uint32_t coalesce_bits);
+int gs_fft_get_tuning(uint32_t log_size, uint32_t extension, uint32_t* tile_log, uint32_t* coalesce_bits);
 
 /* -------------------------------------------------------------- MerkleOps */
 /* commit_on_first_layer / commit_on_layer_with_previous (bindings.rs:262-275);

@@ -162,23 +162,26 @@ int gs_evaluate_columns(gs_ctx* ctx, const uint32_t* const* coeffs, uint32_t coe
                           log_size, twiddles, twiddles_log_size);
 }
 
-int gs_fft_autotune(gs_ctx* ctx, uint32_t min_log, uint32_t max_log, uint32_t* tile_logs, uint32_t* coalesce_bits) {
+int gs_fft_autotune(gs_ctx* ctx, uint32_t min_log, uint32_t max_log, uint32_t max_extension, uint32_t* tile_logs,
+                    uint32_t* coalesce_bits) {
   CTX_REQUIRED(ctx);
   GS_REQUIRE(min_log >= 3 && min_log <= max_log && max_log <= 27, "autotune range must satisfy 3 <= min <= max <= 27");
+  GS_REQUIRE(max_extension <= 3, "extension must be at most 3");
+  const uint32_t root = std::min<uint32_t>(max_log + max_extension, 28) - 1;
   const uint32_t* tw = nullptr;
   const uint32_t* itw = nullptr;
-  GS_TRY(ctx->c.twiddles(max_log - 1, &tw, &itw));
-  GS_TRY(fft_autotune(ctx->c.stream, min_log, max_log, tw, itw, max_log - 1, tile_logs, coalesce_bits));
+  GS_TRY(ctx->c.twiddles(root, &tw, &itw));
+  GS_TRY(fft_autotune(ctx->c.stream, min_log, max_log, max_extension, tw, itw, root, tile_logs, coalesce_bits));
   return ctx->c.sync();
 }
 
-int gs_fft_set_tuning(uint32_t log_size, uint32_t tile_log, uint32_t coalesce_bits) {
-  return set_fft_tuning(log_size, tile_log, coalesce_bits);
+int gs_fft_set_tuning(uint32_t log_size, uint32_t extension, uint32_t tile_log, uint32_t coalesce_bits) {
+  return set_fft_tuning(log_size, extension, tile_log, coalesce_bits);
 }
 
-int gs_fft_get_tuning(uint32_t log_size, uint32_t* tile_log, uint32_t* coalesce_bits) {
+int gs_fft_get_tuning(uint32_t log_size, uint32_t extension, uint32_t* tile_log, uint32_t* coalesce_bits) {
   GS_REQUIRE(log_size < 32 && tile_log && coalesce_bits, "bad arguments");
-  get_fft_tuning(log_size, tile_log, coalesce_bits);
+  get_fft_tuning(log_size, extension, tile_log, coalesce_bits);
   return OK;
 }
 

@@ -438,15 +438,22 @@ struct FftTuning {
   uint32_t coalesce_bits = 4;  // contiguous low bits per strided tile row
 };
 // Per number of computed layers (an FFT of 2^n, or an LDE from 2^n
-// coefficients, computes n layers). Written at set-up (set_fft_tuning,
-// fft_autotune), read by every launch.
-static FftTuning g_fft_tuning[32];
-static FftTuning tuning_for(uint32_t layers) { return g_fft_tuning[layers < 32 ? layers : 31]; }
+// coefficients, computes n layers) and extension (domain log size minus
+// layers: 0 for an FFT, the blowup for an LDE; capped at FFT_MAX_EXT). Written
+// at set-up (set_fft_tuning, fft_autotune), read by every launch.
+constexpr uint32_t FFT_MAX_EXT = 3;
+static FftTuning g_fft_tuning[32][FFT_MAX_EXT + 1];
+static uint32_t ext_slot(uint32_t layers, uint32_t n) {
+  return n - layers < FFT_MAX_EXT ? n - layers : FFT_MAX_EXT;
+}
+static FftTuning tuning_for(uint32_t layers, uint32_t n) {
+  return g_fft_tuning[layers < 32 ? layers : 31][ext_slot(layers, n)];
+}
 
 // Splits layers [0, layers) into balanced passes (lo, L): the first pass has
 // the whole tile for layers, later ones reserve `coalesce_bits` of it.
-static void fft_partition(uint32_t layers, std::vector<std::pair<uint32_t, uint32_t>>& parts) {
-  const FftTuning tn = tuning_for(layers);
+static void fft_partition(uint32_t layers, uint32_t n, std::vector<std::pair<uint32_t, uint32_t>>& parts) {
+  const FftTuning tn = tuning_for(layers, n);
   const uint32_t T = tn.tile_log, C = tn.coalesce_bits;
   if (layers <= T) {
     parts.push_back({0, layers});
@@ -516,14 +523,14 @@ template <bool INV>
 static int run_passes(cudaStream_t st, const uint32_t* const* src, uint32_t* const* dst, uint32_t n_cols, uint32_t n,
                       uint32_t layers, uint32_t src_mask, const uint32_t* tw, uint32_t tw_len) {
   std::vector<std::pair<uint32_t, uint32_t>> parts;
-  fft_partition(layers, parts);
+  fft_partition(layers, n, parts);
   if (!INV) std::reverse(parts.begin(), parts.end());
   for (size_t p = 0; p < parts.size(); p++) {
     FftPass a{};
     a.n = n;
     a.lo = parts[p].first;
     a.L = parts[p].second;
-    a.c = std::min(tuning_for(layers).coalesce_bits, a.lo);
+    a.c = std::min(tuning_for(layers, n).coalesce_bits, a.lo);
     a.t = a.c + a.L;
     const uint32_t R = std::min<uint32_t>(5, a.L);
     a.K = (a.L + R - 1) / R;
@@ -591,106 +598,141 @@ int evaluate_columns(cudaStream_t st, const uint32_t* const* d_src, uint32_t coe
   return run_passes<false>(st, d_src, d_dst, n_cols, log_n, coeff_log, src_mask, d_twiddles, 1u << tw_log);
 }
 
-// Installs the tuning for FFTs computing `layers` layers (0: every size).
-// A tile holds 2^tile_log words (at most 2^13, 32 KiB of shared memory), of
+// Installs the tuning for FFTs computing `layers` layers (0: every size) on
+// a domain `ext` log sizes larger (ext > FFT_MAX_EXT: every extension). A
+// tile holds 2^tile_log words (at most 2^13, 32 KiB of shared memory), of
 // which 2^coalesce_bits are contiguous in memory; a pass needs room for 5
 // layers besides them.
-int set_fft_tuning(uint32_t layers, uint32_t tile_log, uint32_t coalesce_bits) {
+int set_fft_tuning(uint32_t layers, uint32_t ext, uint32_t tile_log, uint32_t coalesce_bits) {
   GS_REQUIRE(layers < 32, "log size out of range");
   GS_REQUIRE(tile_log >= 6 && tile_log <= 13, "tile log must be in [6, 13]");
   GS_REQUIRE(coalesce_bits <= 5 && coalesce_bits + 5 <= tile_log, "coalesced bits must be <= min(5, tile_log - 5)");
-  for (uint32_t l = layers; l < (layers ? layers + 1 : 32u); l++) g_fft_tuning[l] = FftTuning{tile_log, coalesce_bits};
+  for (uint32_t l = layers; l < (layers ? layers + 1 : 32u); l++)
+    for (uint32_t e = 0; e <= FFT_MAX_EXT; e++)
+      if (ext > FFT_MAX_EXT || e == ext) g_fft_tuning[l][e] = FftTuning{tile_log, coalesce_bits};
   return OK;
 }
 
-// Picks, for every FFT log size n in [lo, hi], the tile size and coalesced
-// row width whose pass split gives the fastest evaluate + interpolate round
-// trip of scratch columns (2^24 words in all, or one column of 2^n), and
-// installs it for n computed layers. Each split is timed with CUDA events as
-// the best of 3 trials of 3 round trips; the installed split (first in the
-// list) is replaced only by one at least 2% faster, so timing noise does not
-// move it. Candidates that give the same pass split as an earlier one are not
-// timed again. Every candidate computes the same values; only the split, and
-// so the speed, differ. Not thread-safe against concurrent launches (a set-up
-// step).
-int fft_autotune(cudaStream_t st, uint32_t lo, uint32_t hi, const uint32_t* tw, const uint32_t* itw, uint32_t tw_log,
-                 uint32_t* out_tile, uint32_t* out_coalesce) {
-  GS_REQUIRE(lo >= 3 && hi <= 27 && lo <= hi && tw_log + 1 >= hi, "autotune range out of bounds");
+// Picks, for every FFT log size n in [lo, hi] and extension e in [0,
+// max_ext], the tile size and coalesced row width whose pass split is
+// fastest, and installs it. e = 0 times an evaluate + interpolate round trip
+// of 2^n-word columns in place; e > 0 an LDE of 2^n coefficients onto 2^(n+e)
+// points, the shape of a commitment's or constraint domain's extension.
+// Scratch columns fill 2^24 output words (or one column when larger); sizes
+// whose output exceeds the scratch keep their tuning. Each split is timed with
+// CUDA events as the best of 3 trials of 3 runs; the installed split (first
+// in the list) is replaced only by one at least 2% faster, so timing noise
+// does not move it. Candidates that give the same pass split as an earlier
+// one are not timed again. Every candidate computes the same values; only the
+// split, and so the speed, differ. Not thread-safe against concurrent
+// launches (a set-up step). Outputs: (hi - lo + 1) x (max_ext + 1), by size.
+int fft_autotune(cudaStream_t st, uint32_t lo, uint32_t hi, uint32_t max_ext, const uint32_t* tw, const uint32_t* itw,
+                 uint32_t tw_log, uint32_t* out_tile, uint32_t* out_coalesce) {
+  GS_REQUIRE(lo >= 3 && hi <= 27 && lo <= hi && max_ext <= FFT_MAX_EXT && tw_log + 1 >= hi,
+             "autotune range out of bounds");
   static const FftTuning fixed[] = {{13, 4}, {12, 4}, {11, 4}, {10, 4}, {13, 5}, {12, 5}, {11, 5}, {13, 3}};
-  const size_t words = (size_t)1 << (hi > 24 ? hi : 24);
-  uint32_t* buf = nullptr;
+  const uint32_t w_log = hi > 24 ? hi : 24;
+  const size_t words = (size_t)1 << w_log;
+  uint32_t* buf = nullptr;  // outputs (and in-place round trips)
+  uint32_t* src = nullptr;  // LDE inputs
   uint32_t** tab = nullptr;
+  uint32_t** stab = nullptr;
   const uint32_t max_cols = 32768;
   GS_CUDA_TRY(cudaMallocAsync((void**)&buf, 4 * words, st));
+  GS_CUDA_TRY(cudaMallocAsync((void**)&src, 2 * words, st));
   GS_CUDA_TRY(cudaMallocAsync((void**)&tab, sizeof(void*) * max_cols, st));
+  GS_CUDA_TRY(cudaMallocAsync((void**)&stab, sizeof(void*) * max_cols, st));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int rc = OK;
-  if (cudaMemsetAsync(buf, 0, 4 * words, st) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
-      cudaEventCreate(&e1) != cudaSuccess)
+  if (cudaMemsetAsync(buf, 0, 4 * words, st) != cudaSuccess || cudaMemsetAsync(src, 0, 2 * words, st) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
     rc = ERR_CUDA;
   const bool aligned = g_cols_aligned;
   g_cols_aligned = true;
-  std::vector<uint32_t*> h;
+  std::vector<uint32_t*> h, hs;
   for (uint32_t n = lo; n <= hi && rc == OK; n++) {
-    const uint32_t cols = (uint32_t)std::min<size_t>(words >> n, max_cols);
-    h.resize(cols);
-    for (uint32_t c = 0; c < cols; c++) h[c] = buf + ((size_t)c << n);
-    if (cudaMemcpyAsync(tab, h.data(), sizeof(void*) * cols, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess) {
-      rc = ERR_CUDA;
-      break;
-    }
-    const FftTuning keep = g_fft_tuning[n];
-    float best = 1e30f, keep_ms = 1e30f;
-    FftTuning pick = keep;
-    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> seen;
-    std::vector<FftTuning> cand(1, keep);
-    cand.insert(cand.end(), std::begin(fixed), std::end(fixed));
-    for (const FftTuning& c : cand) {
-      g_fft_tuning[n] = c;
-      std::vector<std::pair<uint32_t, uint32_t>> parts;
-      fft_partition(n, parts);
-      for (auto& pr : parts) pr.first = std::min(c.coalesce_bits, pr.first) | (pr.first << 8);
-      if (std::find(seen.begin(), seen.end(), parts) != seen.end()) continue;
-      seen.push_back(parts);
-      float ms = 1e30f;
-      for (int trial = 0; trial < 4 && rc == OK; trial++) {  // trial 0 warms up
-        for (int rep = 0; rep < 3 && rc == OK; rep++) {
-          if (rep == 0 && cudaEventRecord(e0, st) != cudaSuccess) rc = ERR_CUDA;
-          if (rc == OK) rc = run_passes<false>(st, (const uint32_t* const*)tab, tab, cols, n, n, 0xffffffffu, tw,
-                                               1u << tw_log);
-          if (rc == OK) rc = run_passes<true>(st, (const uint32_t* const*)tab, tab, cols, n, n, 0xffffffffu, itw,
-                                              1u << tw_log);
+    for (uint32_t e = 0; e <= max_ext && rc == OK; e++) {
+      const uint32_t dn = n + e;  // domain log size
+      const size_t slot = (size_t)(n - lo) * (max_ext + 1) + e;
+      if (dn > w_log || tw_log + 1 < dn) {
+        if (out_tile) out_tile[slot] = g_fft_tuning[n][e].tile_log;
+        if (out_coalesce) out_coalesce[slot] = g_fft_tuning[n][e].coalesce_bits;
+        continue;
+      }
+      const uint32_t cols = (uint32_t)std::min<size_t>(words >> dn, max_cols);
+      h.resize(cols);
+      hs.resize(cols);
+      for (uint32_t c = 0; c < cols; c++) {
+        h[c] = buf + ((size_t)c << dn);
+        hs[c] = src + ((size_t)c << n);
+      }
+      if (cudaMemcpyAsync(tab, h.data(), sizeof(void*) * cols, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+          cudaMemcpyAsync(stab, hs.data(), sizeof(void*) * cols, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+          cudaStreamSynchronize(st) != cudaSuccess) {
+        rc = ERR_CUDA;
+        break;
+      }
+      const FftTuning keep = g_fft_tuning[n][e];
+      float best = 1e30f, keep_ms = 1e30f;
+      FftTuning pick = keep;
+      std::vector<std::vector<std::pair<uint32_t, uint32_t>>> seen;
+      std::vector<FftTuning> cand(1, keep);
+      cand.insert(cand.end(), std::begin(fixed), std::end(fixed));
+      for (size_t ci = 0; ci < cand.size() && rc == OK; ci++) {
+        const FftTuning c = cand[ci];
+        g_fft_tuning[n][e] = c;
+        std::vector<std::pair<uint32_t, uint32_t>> parts;
+        fft_partition(n, dn, parts);
+        for (auto& pr : parts) pr.first = std::min(c.coalesce_bits, pr.first) | (pr.first << 8);
+        if (std::find(seen.begin(), seen.end(), parts) != seen.end()) continue;
+        seen.push_back(parts);
+        float ms = 1e30f;
+        for (int trial = 0; trial < 4 && rc == OK; trial++) {  // trial 0 warms up
+          for (int rep = 0; rep < 3 && rc == OK; rep++) {
+            if (rep == 0 && cudaEventRecord(e0, st) != cudaSuccess) rc = ERR_CUDA;
+            if (rc != OK) break;
+            if (e == 0) {
+              rc = run_passes<false>(st, (const uint32_t* const*)tab, tab, cols, n, n, 0xffffffffu, tw, 1u << tw_log);
+              if (rc == OK)
+                rc = run_passes<true>(st, (const uint32_t* const*)tab, tab, cols, n, n, 0xffffffffu, itw,
+                                      1u << tw_log);
+            } else {
+              rc = run_passes<false>(st, (const uint32_t* const*)stab, tab, cols, dn, n, (1u << n) - 1u, tw,
+                                     1u << tw_log);
+            }
+          }
+          float t = 0;
+          if (rc == OK && (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                           cudaEventElapsedTime(&t, e0, e1) != cudaSuccess))
+            rc = ERR_CUDA;
+          if (rc == OK && trial > 0) ms = std::min(ms, t);
         }
-        float t = 0;
-        if (rc == OK && (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-                         cudaEventElapsedTime(&t, e0, e1) != cudaSuccess))
-          rc = ERR_CUDA;
-        if (rc == OK && trial > 0) ms = std::min(ms, t);
+        if (rc != OK) break;
+        if (ci == 0) keep_ms = ms;
+        if (ms < best) {
+          best = ms;
+          pick = c;
+        }
       }
-      if (rc != OK) break;
-      if (&c == &cand[0]) keep_ms = ms;
-      if (ms < best) {
-        best = ms;
-        pick = c;
-      }
+      if (best > 0.98f * keep_ms) pick = keep;
+      g_fft_tuning[n][e] = rc == OK ? pick : keep;
+      if (out_tile) out_tile[slot] = g_fft_tuning[n][e].tile_log;
+      if (out_coalesce) out_coalesce[slot] = g_fft_tuning[n][e].coalesce_bits;
     }
-    if (best > 0.98f * keep_ms) pick = keep;
-    g_fft_tuning[n] = rc == OK ? pick : keep;
-    if (out_tile) out_tile[n - lo] = g_fft_tuning[n].tile_log;
-    if (out_coalesce) out_coalesce[n - lo] = g_fft_tuning[n].coalesce_bits;
   }
   g_cols_aligned = aligned;
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
+  cudaFreeAsync(stab, st);
   cudaFreeAsync(tab, st);
+  cudaFreeAsync(src, st);
   cudaFreeAsync(buf, st);
   if (rc == ERR_CUDA) set_error(std::string("fft autotune: ") + cudaGetErrorString(cudaGetLastError()));
   return rc;
 }
 
-void get_fft_tuning(uint32_t layers, uint32_t* tile_log, uint32_t* coalesce_bits) {
-  const FftTuning t = tuning_for(layers);
+void get_fft_tuning(uint32_t layers, uint32_t ext, uint32_t* tile_log, uint32_t* coalesce_bits) {
+  const FftTuning t = g_fft_tuning[layers < 32 ? layers : 31][ext < FFT_MAX_EXT ? ext : FFT_MAX_EXT];
   *tile_log = t.tile_log;
   *coalesce_bits = t.coalesce_bits;
 }

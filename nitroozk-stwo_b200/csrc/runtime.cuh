@@ -135,11 +135,12 @@ int interpolate_columns(cudaStream_t st, uint32_t* const* d_cols, uint32_t n_col
 int evaluate_columns(cudaStream_t st, const uint32_t* const* d_src, uint32_t coeff_log, uint32_t* const* d_dst,
                      uint32_t n_cols, uint32_t log_n, const uint32_t* d_twiddles, uint32_t tw_log);
 int bit_reverse(cudaStream_t st, uint32_t* d, uint32_t log_n);
-// Pass-split tuning per number of computed layers (process-wide; set-up time).
-int set_fft_tuning(uint32_t layers, uint32_t tile_log, uint32_t coalesce_bits);
-void get_fft_tuning(uint32_t layers, uint32_t* tile_log, uint32_t* coalesce_bits);
-int fft_autotune(cudaStream_t st, uint32_t lo, uint32_t hi, const uint32_t* tw, const uint32_t* itw, uint32_t tw_log,
-                 uint32_t* out_tile, uint32_t* out_coalesce);
+// Pass-split tuning per number of computed layers and extension (domain log
+// size minus layers), process-wide, written at set-up time.
+int set_fft_tuning(uint32_t layers, uint32_t ext, uint32_t tile_log, uint32_t coalesce_bits);
+void get_fft_tuning(uint32_t layers, uint32_t ext, uint32_t* tile_log, uint32_t* coalesce_bits);
+int fft_autotune(cudaStream_t st, uint32_t lo, uint32_t hi, uint32_t max_ext, const uint32_t* tw, const uint32_t* itw,
+                 uint32_t tw_log, uint32_t* out_tile, uint32_t* out_coalesce);
 
 // merkle.cu
 int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, const uint32_t* const* d_cols,

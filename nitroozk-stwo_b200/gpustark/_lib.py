@@ -55,9 +55,9 @@ _PROTOS = {
     "gs_precompute_twiddles": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p],
     "gs_interpolate_columns": [C.c_void_p, VPP, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32],
     "gs_evaluate_columns": [C.c_void_p, VPP, C.c_uint32, VPP, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32],
-    "gs_fft_autotune": [C.c_void_p, C.c_uint32, C.c_uint32, U32P, U32P],
-    "gs_fft_set_tuning": [C.c_uint32, C.c_uint32, C.c_uint32],
-    "gs_fft_get_tuning": [C.c_uint32, U32P, U32P],
+    "gs_fft_autotune": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, U32P, U32P],
+    "gs_fft_set_tuning": [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32],
+    "gs_fft_get_tuning": [C.c_uint32, C.c_uint32, U32P, U32P],
     "gs_commit_on_layer": [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, VPP, C.c_void_p],
     "gs_commit_node_layers": [C.c_void_p, C.c_uint32, VPP],
     "gs_fold_line": [C.c_void_p, VPP, C.c_uint32, QM31, VPP, C.c_void_p, C.c_uint32, C.c_void_p],

@@ -133,26 +133,30 @@ class GpuBackend:
                                             _p(twiddles.twiddles), twiddles.root_log), "evaluate_polynomials")
         return out
 
+    ALL_EXTENSIONS = 0xFFFFFFFF
+
     @staticmethod
-    def fft_autotune(min_log, max_log, ctx=None):
+    def fft_autotune(min_log, max_log, max_extension=2, ctx=None):
         """Times the FFT pass splits for every log size in [min_log, max_log]
-        and installs the fastest (process-wide); returns {log: (tile_log,
+        and extension (LDE blowup log) in [0, max_extension] and installs the
+        fastest (process-wide); returns {(log, extension): (tile_log,
         coalesce_bits)}. The split changes speed, never the values."""
         ctx = ctx or default_context()
-        n = max_log - min_log + 1
+        n = (max_log - min_log + 1) * (max_extension + 1)
         tiles, coal = (C.c_uint32 * n)(), (C.c_uint32 * n)()
-        L.check(L.lib().gs_fft_autotune(ctx.handle, min_log, max_log, tiles, coal), "fft_autotune")
-        return {min_log + i: (tiles[i], coal[i]) for i in range(n)}
+        L.check(L.lib().gs_fft_autotune(ctx.handle, min_log, max_log, max_extension, tiles, coal), "fft_autotune")
+        return {(min_log + i // (max_extension + 1), i % (max_extension + 1)): (tiles[i], coal[i]) for i in range(n)}
 
     @staticmethod
-    def fft_set_tuning(log_size, tile_log, coalesce_bits):
-        """Installs one FFT pass split for log_size (0: every size)."""
-        L.check(L.lib().gs_fft_set_tuning(log_size, tile_log, coalesce_bits), "fft_set_tuning")
+    def fft_set_tuning(log_size, tile_log, coalesce_bits, extension=ALL_EXTENSIONS):
+        """Installs one FFT pass split for log_size (0: every size) and
+        extension (default: every extension)."""
+        L.check(L.lib().gs_fft_set_tuning(log_size, extension, tile_log, coalesce_bits), "fft_set_tuning")
 
     @staticmethod
-    def fft_get_tuning(log_size):
+    def fft_get_tuning(log_size, extension=0):
         t, c = C.c_uint32(), C.c_uint32()
-        L.check(L.lib().gs_fft_get_tuning(log_size, C.byref(t), C.byref(c)), "fft_get_tuning")
+        L.check(L.lib().gs_fft_get_tuning(log_size, extension, C.byref(t), C.byref(c)), "fft_get_tuning")
         return t.value, c.value
 
     # ------------------------------------------------------------ MerkleOps

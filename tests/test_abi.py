@@ -42,19 +42,24 @@ def test_python_binding_declares_only_exported_symbols():
 
 def test_fft_tuning_setter_validates_without_gpu():
     """gs_fft_set_tuning / gs_fft_get_tuning are host-only: bad splits are
-    refused with ERR_INVALID, good ones read back, and the default 13 / 4 is
-    put back."""
+    refused with ERR_INVALID, good ones read back per (log size, extension),
+    and the default 13 / 4 is put back."""
     lib = ctypes.CDLL(LIB)
+    ALL = 0xFFFFFFFF
     t, c = ctypes.c_uint32(), ctypes.c_uint32()
-    assert lib.gs_fft_get_tuning(20, ctypes.byref(t), ctypes.byref(c)) == 0
-    assert (t.value, c.value) == (13, 4)
-    for bad in [(20, 14, 4), (20, 5, 0), (20, 13, 6), (20, 9, 5), (32, 13, 4)]:
+
+    def get(log, ext):
+        assert lib.gs_fft_get_tuning(log, ext, ctypes.byref(t), ctypes.byref(c)) == 0
+        return t.value, c.value
+
+    assert get(20, 0) == (13, 4) and get(20, 2) == (13, 4)
+    for bad in [(20, ALL, 14, 4), (20, ALL, 5, 0), (20, 0, 13, 6), (20, 1, 9, 5), (32, ALL, 13, 4)]:
         assert lib.gs_fft_set_tuning(*bad) == 1, bad
     try:
-        assert lib.gs_fft_set_tuning(20, 11, 3) == 0
-        assert lib.gs_fft_get_tuning(20, ctypes.byref(t), ctypes.byref(c)) == 0
-        assert (t.value, c.value) == (11, 3)
-        assert lib.gs_fft_get_tuning(21, ctypes.byref(t), ctypes.byref(c)) == 0
-        assert (t.value, c.value) == (13, 4)
+        assert lib.gs_fft_set_tuning(20, ALL, 11, 3) == 0
+        assert get(20, 0) == (11, 3) and get(20, 3) == (11, 3) and get(20, 7) == (11, 3)
+        assert lib.gs_fft_set_tuning(20, 2, 12, 5) == 0
+        assert get(20, 2) == (12, 5) and get(20, 1) == (11, 3)
+        assert get(21, 0) == (13, 4)
     finally:
-        assert lib.gs_fft_set_tuning(0, 13, 4) == 0
+        assert lib.gs_fft_set_tuning(0, ALL, 13, 4) == 0

@@ -32,7 +32,7 @@ def _round_trip(B, coeffs, log, tw, blowup):
     return ev, back
 
 
-@pytest.mark.parametrize("log,n_cols,blowup", [(11, 3, 1), (14, 2, 0), (17, 2, 2), (21, 1, 1), (24, 1, 0)])
+@pytest.mark.parametrize("log,n_cols,blowup", [(11, 3, 1), (14, 2, 0), (17, 2, 2), (18, 3, 2), (21, 1, 1), (24, 1, 0)])
 def test_every_split_gives_the_same_values(B, log, n_cols, blowup):
     from gpustark.backend import to_device
     rng = np.random.default_rng(log * 7 + blowup)
@@ -58,11 +58,11 @@ def test_every_split_gives_the_same_values(B, log, n_cols, blowup):
 
 def test_autotune_installs_valid_splits(B):
     from gpustark.backend import to_device
-    picks = B.fft_autotune(8, 22)
-    assert sorted(picks) == list(range(8, 23))
-    for log, (tile, coal) in picks.items():
+    picks = B.fft_autotune(8, 22, 2)
+    assert sorted(picks) == [(n, e) for n in range(8, 23) for e in range(3)]
+    for (log, ext), (tile, coal) in picks.items():
         assert 6 <= tile <= 13 and coal <= 5 and coal + 5 <= tile
-        assert B.fft_get_tuning(log) == (tile, coal)
+        assert B.fft_get_tuning(log, ext) == (tile, coal)
     rng = np.random.default_rng(5)
     tw = B.precompute_twiddles(21)
     coeffs = [to_device(rng.integers(0, P, 1 << 21, dtype=np.int64).astype(np.uint32))]
