@@ -63,6 +63,7 @@ struct Server {
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     Context ctx;
     int init = ctx.init(st);
+    // waits of this worker: poll briefly, then sleep
     cudaEvent_t wait_ev = nullptr;
     if (cudaEventCreateWithFlags(&wait_ev, cudaEventBlockingSync | cudaEventDisableTiming) == cudaSuccess)
       set_thread_wait_event(wait_ev);

@@ -1,5 +1,7 @@
 // gpustark runtime: context, error state, pointer-table staging.
 #include "runtime.cuh"
+#include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <atomic>
@@ -16,9 +18,24 @@ unsigned long long launch_count() { return g_launches.load(std::memory_order_rel
 
 static thread_local cudaEvent_t g_wait_ev = nullptr;
 void set_thread_wait_event(cudaEvent_t ev) { g_wait_ev = ev; }
+static double wait_spin_us() {
+  static const double us = [] {
+    const char* e = getenv("GS_WAIT_SPIN_US");
+    return e ? atof(e) : 50.0;
+  }();
+  return us;
+}
 int stream_sync(cudaStream_t st) {
   if (g_wait_ev) {
     GS_CUDA_TRY(cudaEventRecord(g_wait_ev, st));
+    const double limit = wait_spin_us();
+    const auto t0 = std::chrono::steady_clock::now();
+    while (limit > 0) {
+      const cudaError_t q = cudaEventQuery(g_wait_ev);
+      if (q == cudaSuccess) return OK;
+      if (q != cudaErrorNotReady) GS_CUDA_TRY(q);
+      if (std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count() > limit) break;
+    }
     GS_CUDA_TRY(cudaEventSynchronize(g_wait_ev));
   } else {
     GS_CUDA_TRY(cudaStreamSynchronize(st));

@@ -62,9 +62,12 @@ struct DomainTables {
   uint32_t lift;
 };
 
-// Waits for `st`. By default a spin-wait (the lowest latency for one proof at
-// a time); a thread that installs a blocking-sync event (the proof server's
-// workers) sleeps instead, leaving the host cores to the other workers.
+// Waits for `st`. By default CUDA's own stream synchronisation (the lowest
+// latency for one proof at a time). A thread that installs a blocking-sync
+// event (the proof server's workers, many threads sharing one device and the
+// host cores) records it, polls it for a short window (GS_WAIT_SPIN_US,
+// default 50 µs: most waits are short read-backs, which a sleep and wake-up
+// would lengthen), then sleeps on it.
 int stream_sync(cudaStream_t st);
 void set_thread_wait_event(cudaEvent_t ev);
 
