@@ -14,6 +14,8 @@ Sources (paths inside the reference checkout):
   crates/stwo/src/core/circle.rs               M31_CIRCLE_GEN, SECURE_FIELD_CIRCLE_GEN,
                                                test_secure_field_circle_gen prime factors
   crates/stwo/src/prover/backend/cuda/poly.rs  test_interpolate_from_fib (twiddle tree literals)
+  crates/stwo/src/core/vcs/poseidon252_merkle.rs  test_vector (Poseidon252 hash_node)
+  crates/stwo/src/core/channel/poseidon252.rs     test_mix_u64, test_mix_u32s (Poseidon252 channel)
 """
 import json
 import os
@@ -82,6 +84,30 @@ def main(root):
         "root_log_size": int(re.search(r"log_size: (\d+)", rc).group(1)),
         "twiddles": vec_of("twiddles"),
         "itwiddles": vec_of("itwiddles"),
+    }
+
+    # Poseidon252 Merkle hasher: hash_node(None, [0, 1]) and
+    # hash_node(Some((1, 2)), [3]) as decimal felt252 strings
+    pm = _read(root, "crates/stwo/src/core/vcs/poseidon252_merkle.rs")
+    tv = pm[pm.index("fn test_vector"):]
+    decs = re.findall(r'from_dec_str\(\s*"(\d+)"', tv)[:2]
+    m1 = re.search(r"hash_node\(None, &\[m31!\((\d+)\), m31!\((\d+)\)\]\)", tv)
+    m2 = re.search(r"FieldElement252::from\((\d+)u32\), FieldElement252::from\((\d+)u32\)\)\),\s*&\[m31!\((\d+)\)\]", tv)
+    out["poseidon252_hash_node"] = [
+        {"children": None, "columns": [int(m1.group(1)), int(m1.group(2))], "hash": decs[0]},
+        {"children": [int(m2.group(1)), int(m2.group(2))], "columns": [int(m2.group(3))], "hash": decs[1]},
+    ]
+    # Poseidon252 channel: digest after mix_u64 / mix_u32s from the default channel
+    pc = _read(root, "crates/stwo/src/core/channel/poseidon252.rs")
+    t64 = pc[pc.index("fn test_mix_u64"):]
+    t32 = pc[pc.index("fn test_mix_u32s"):]
+    out["poseidon252_channel_mix_u64"] = {
+        "value": int(re.search(r"mix_u64\((0x[0-9a-fA-F]+)\)", t64).group(1), 16),
+        "digest": re.search(r'from_hex_be\(\s*"(0x[0-9a-fA-F]+)"', t64).group(1),
+    }
+    out["poseidon252_channel_mix_u32s"] = {
+        "words": [int(x) for x in re.search(r"mix_u32s\(&\[([0-9,\s]+)\]\)", t32).group(1).split(",") if x.strip()],
+        "digest": re.search(r'from_hex_be\(\s*"(0x[0-9a-fA-F]+)"', t32).group(1),
     }
 
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_vectors.json")

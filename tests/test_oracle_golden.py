@@ -216,3 +216,45 @@ def test_lifted_leaves_order_and_empty():
         msg = b"".join(int(v).to_bytes(4, "little") for v in (c1[j1], c3[i], c3b[i]))
         assert bytes(leaves[i]) == hashlib.blake2s(msg).digest()
     assert bytes(O.lifted_leaves([], 5)[0]) == hashlib.blake2s(b"").digest()
+
+
+# ------------------------------------------------------------ Poseidon252
+def test_poseidon252_hash_node_known_answers():
+    """The Poseidon252 restatement (starknet-crypto 0.6.2's Starknet Poseidon)
+    reproduces the reference's hash_node vectors."""
+    import poseidon252 as PS
+    for case in GOLDEN["poseidon252_hash_node"]:
+        ch = tuple(case["children"]) if case["children"] is not None else None
+        assert PS.hash_node(ch, case["columns"]) == int(case["hash"])
+
+
+def test_poseidon252_channel_known_answers():
+    import poseidon252 as PS
+    c = PS.Channel()
+    c.mix_u64(GOLDEN["poseidon252_channel_mix_u64"]["value"])
+    assert c.digest == int(GOLDEN["poseidon252_channel_mix_u64"]["digest"], 16)
+    c = PS.Channel()
+    c.mix_u32s(GOLDEN["poseidon252_channel_mix_u32s"]["words"])
+    assert c.digest == int(GOLDEN["poseidon252_channel_mix_u32s"]["digest"], 16)
+
+
+def test_poseidon252_channel_draw_counts_and_ranges():
+    """The draw bookkeeping of the reference's test_channel_draws, and the
+    ranges of drawn values."""
+    import poseidon252 as PS
+    c = PS.Channel()
+    w = c.draw_u32s()
+    assert c.n_draws == 1 and len(w) == 7 and all(0 <= x < 2 ** 32 for x in w)
+    f = c.draw_secure_felts(9)
+    assert c.n_draws == 6 and len(f) == 9 and len(set(f)) == 9
+    assert all(0 <= v < PS.M31 for q in f for v in q)
+    c.mix_felts(f[:3])
+    assert c.n_draws == 0
+
+
+def test_poseidon252_permutation_is_a_bijection_sample():
+    """Distinct inputs give distinct outputs and the state stays in the field."""
+    import poseidon252 as PS
+    outs = {tuple(PS.permute([i, 2 * i + 1, 3])) for i in range(32)}
+    assert len(outs) == 32
+    assert all(0 <= v < PS.P for o in outs for v in o)
