@@ -119,6 +119,21 @@ int gs_fft_get_tuning(uint32_t log_size, uint32_t extension, uint32_t* tile_log,
 int gs_commit_on_layer(gs_ctx* ctx, uint32_t log_size, const uint32_t* prev_layer, uint32_t n_cols,
                        const uint32_t* const* cols, uint32_t* out);
 
+/* poseidon252_commit_on_first_layer / poseidon252_commit_on_layer_with_previous
+ * (bindings.rs:592-612); MerkleOps<Poseidon252MerkleHasher>::commit_on_layer
+ * (prover/backend/cuda/poseidon252.rs:21-42; hash_node at core/vcs/
+ * poseidon252_merkle.rs:18-72). Hashes are felt252 values in the reference's
+ * device layout, 32 bytes big-endian each (stwo_cuda/poseidon252.rs);
+ * prev_layer: 2^(log_size+1) hashes or NULL; out: 2^log_size hashes; both
+ * 16-byte aligned. The hash is Starknet's Poseidon (starknet-crypto 0.6.2). */
+int gs_poseidon252_commit_on_layer(gs_ctx* ctx, uint32_t log_size, const uint8_t* prev_layer, uint32_t n_cols,
+                                   const uint32_t* const* cols, uint8_t* out);
+/* poseidon_permute_comp (starknet-crypto 0.6.2, called by core/channel/
+ * poseidon252.rs:37-45) on n states of 3 felt252 values, 96 bytes each in
+ * the same big-endian layout; in and out may not overlap. No counterpart in
+ * the reference's C ABI (it exposes no raw permutation). */
+int gs_poseidon252_permute(gs_ctx* ctx, const uint8_t* states, uint32_t n, uint8_t* out);
+
 /* The node-only part of MerkleProver::commit's layer loop (prover/vcs/
  * prover.rs:39-48) when no columns are injected below top_log: layers is a
  * host array of top_log + 1 device buffers, layers[L] holding 2^L hashes;

@@ -204,6 +204,24 @@ int gs_commit_node_layers(gs_ctx* ctx, uint32_t top_log, uint32_t* const* layers
   return commit_node_layers(ctx->c.stream, top_log, layers, ctx->c.tree_counters);
 }
 
+int gs_poseidon252_commit_on_layer(gs_ctx* ctx, uint32_t log_size, const uint8_t* prev_layer, uint32_t n_cols,
+                                   const uint32_t* const* cols, uint8_t* out) {
+  CTX_REQUIRED(ctx);
+  const void* const* d = nullptr;
+  if (n_cols) {
+    GS_REQUIRE(cols != nullptr, "null column list");
+    for (uint32_t i = 0; i < n_cols; i++) GS_REQUIRE(cols[i] != nullptr, "null column");
+    GS_TRY(ctx->c.stage_ptrs((const void* const*)cols, n_cols, &d));
+  }
+  return poseidon252_commit_on_layer(ctx->c.stream, log_size, prev_layer, (const uint32_t* const*)d, n_cols, out);
+}
+
+int gs_poseidon252_permute(gs_ctx* ctx, const uint8_t* states, uint32_t n, uint8_t* out) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(n == 0 || (states && out), "null state buffer");
+  return poseidon252_permute(ctx->c.stream, states, n, out);
+}
+
 int gs_fold_line(gs_ctx* ctx, const uint32_t* const src[4], uint32_t log_size, gs_qm31 alpha, uint32_t* const dst[4],
                  const uint32_t* itwiddles, uint32_t twiddles_log_size, uint32_t* leaf_hashes) {
   CTX_REQUIRED(ctx);

@@ -1,0 +1,300 @@
+// Poseidon252 Merkle hashing on the device: MerkleOps<Poseidon252MerkleHasher>
+// ::commit_on_layer (crates/stwo/src/core/vcs/poseidon252_merkle.rs:18-72;
+// reference CUDA poseidon252_commit_on_first_layer / _with_previous,
+// stwo_cuda/bindings.rs:592-612).
+//
+// The hash is Starknet's Poseidon (the Hades permutation of the crate
+// starknet-crypto 0.6.2 that the reference calls): field p = 2^251 +
+// 17·2^192 + 1, state of 3 elements, x^3 S-box, 4 full + 83 partial + 4 full
+// rounds, MDS [[3, 1, 1], [1, -1, 1], [1, 1, -2]], round constants from
+// poseidon252_constants.py.
+//
+//   hash_node(children, values): poseidon_hash(l, r) when there are children
+//   and no values; otherwise poseidon_hash_many([l, r,] felts of the values,
+//   8 M31 values per felt shifted in 31 bits at a time, a shorter last word
+//   carrying its length at bit 248).
+//
+// Field elements live in registers as 8 little-endian 32-bit limbs in
+// Montgomery form (R = 2^256). The modulus is sparse, limbs [1, 0, 0, 0, 0, 0,
+// 17, 2^27], and p = 1 mod 2^32, so the Montgomery quotient digit of each
+// reduction step is -t0 and adding m·p touches three limbs. Hashes in memory
+// are the reference's device layout: 32 bytes, big-endian.
+#include "runtime.cuh"
+
+namespace gs {
+
+struct Felt {
+  uint32_t v[8];
+};
+
+#include "poseidon252_constants.inc"
+
+constexpr uint32_t P252_L6 = 17u, P252_L7 = 0x08000000u;  // limbs 6 and 7 of p (limb 0 is 1, 1..5 are 0)
+
+// r = a - p when a >= p, else a
+__device__ __forceinline__ void reduce_once(uint32_t t[8]) {
+  uint32_t s[8];
+  int64_t x = (int64_t)t[0] - 1;
+  s[0] = (uint32_t)x;
+  int64_t br = x < 0;
+#pragma unroll
+  for (int j = 1; j < 6; j++) {
+    x = (int64_t)t[j] - br;
+    s[j] = (uint32_t)x;
+    br = x < 0;
+  }
+  x = (int64_t)t[6] - P252_L6 - br;
+  s[6] = (uint32_t)x;
+  br = x < 0;
+  x = (int64_t)t[7] - P252_L7 - br;
+  s[7] = (uint32_t)x;
+  br = x < 0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) t[j] = br ? t[j] : s[j];
+}
+
+// Montgomery product a·b·R^-1 mod p (CIOS), for a, b < p.
+__device__ __forceinline__ Felt fmul(const Felt& a, const Felt& b) {
+  uint32_t t[10];
+#pragma unroll
+  for (int j = 0; j < 10; j++) t[j] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    uint64_t c = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      c += (uint64_t)a.v[j] * b.v[i] + t[j];
+      t[j] = (uint32_t)c;
+      c >>= 32;
+    }
+    c += t[8];
+    t[8] = (uint32_t)c;
+    t[9] = (uint32_t)(c >> 32);
+    // t += m·p with m = -t0 (so the low limb becomes 0), then shift one limb
+    const uint32_t m = 0u - t[0];
+    uint64_t d = ((uint64_t)t[0] + m) >> 32;
+#pragma unroll
+    for (int j = 1; j < 6; j++) {
+      d += t[j];
+      t[j - 1] = (uint32_t)d;
+      d >>= 32;
+    }
+    d += (uint64_t)t[6] + (uint64_t)m * P252_L6;
+    t[5] = (uint32_t)d;
+    d >>= 32;
+    d += (uint64_t)t[7] + ((uint64_t)m << 27);
+    t[6] = (uint32_t)d;
+    d >>= 32;
+    d += t[8];
+    t[7] = (uint32_t)d;
+    d >>= 32;
+    t[8] = t[9] + (uint32_t)d;
+  }
+  reduce_once(t);  // t < 2p
+  Felt r;
+#pragma unroll
+  for (int j = 0; j < 8; j++) r.v[j] = t[j];
+  return r;
+}
+
+__device__ __forceinline__ Felt fadd(const Felt& a, const Felt& b) {
+  uint32_t t[8];
+  uint64_t c = 0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    c += (uint64_t)a.v[j] + b.v[j];
+    t[j] = (uint32_t)c;
+    c >>= 32;
+  }
+  reduce_once(t);  // a + b < 2p < 2^253: no carry out of limb 7
+  Felt r;
+#pragma unroll
+  for (int j = 0; j < 8; j++) r.v[j] = t[j];
+  return r;
+}
+
+__device__ __forceinline__ Felt fsub(const Felt& a, const Felt& b) {
+  uint32_t t[8];
+  int64_t br = 0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    int64_t x = (int64_t)a.v[j] - b.v[j] - br;
+    t[j] = (uint32_t)x;
+    br = x < 0;
+  }
+  // borrow: add p back
+  const uint32_t k = br ? 0xffffffffu : 0u;
+  uint64_t c = (uint64_t)t[0] + (1u & k);
+  t[0] = (uint32_t)c;
+  c >>= 32;
+#pragma unroll
+  for (int j = 1; j < 6; j++) {
+    c += t[j];
+    t[j] = (uint32_t)c;
+    c >>= 32;
+  }
+  c += (uint64_t)t[6] + (P252_L6 & k);
+  t[6] = (uint32_t)c;
+  c >>= 32;
+  t[7] = t[7] + (P252_L7 & k) + (uint32_t)c;
+  Felt r;
+#pragma unroll
+  for (int j = 0; j < 8; j++) r.v[j] = t[j];
+  return r;
+}
+
+__device__ __forceinline__ Felt fcube(const Felt& x) { return fmul(fmul(x, x), x); }
+
+// MDS [[3, 1, 1], [1, -1, 1], [1, 1, -2]] as t = s0 + s1 + s2 and
+// (t + 2 s0, t - 2 s1, t - 3 s2)
+__device__ __forceinline__ void mds(Felt s[3]) {
+  const Felt t = fadd(fadd(s[0], s[1]), s[2]);
+  const Felt s1x2 = fadd(s[1], s[1]);
+  const Felt s2x3 = fadd(fadd(s[2], s[2]), s[2]);
+  s[0] = fadd(t, fadd(s[0], s[0]));
+  s[1] = fsub(t, s1x2);
+  s[2] = fsub(t, s2x3);
+}
+
+__device__ __forceinline__ void hades(Felt s[3]) {
+  int r = 0;
+#pragma unroll 1
+  for (int k = 0; k < 4; k++, r++) {
+#pragma unroll
+    for (int j = 0; j < 3; j++) s[j] = fcube(fadd(s[j], P252_RC[3 * r + j]));
+    mds(s);
+  }
+#pragma unroll 1
+  for (int k = 0; k < 83; k++, r++) {
+    s[0] = fadd(s[0], P252_RC[3 * r]);
+    s[1] = fadd(s[1], P252_RC[3 * r + 1]);
+    s[2] = fcube(fadd(s[2], P252_RC[3 * r + 2]));
+    mds(s);
+  }
+#pragma unroll 1
+  for (int k = 0; k < 4; k++, r++) {
+#pragma unroll
+    for (int j = 0; j < 3; j++) s[j] = fcube(fadd(s[j], P252_RC[3 * r + j]));
+    mds(s);
+  }
+}
+
+// 32 big-endian bytes (as 8 little-endian-stored words) <-> canonical limbs
+__device__ __forceinline__ Felt from_be_words(const uint32_t w[8]) {
+  Felt x;
+#pragma unroll
+  for (int k = 0; k < 8; k++) x.v[7 - k] = __byte_perm(w[k], 0, 0x0123);
+  return x;
+}
+__device__ __forceinline__ void to_be_words(const Felt& x, uint32_t w[8]) {
+#pragma unroll
+  for (int k = 0; k < 8; k++) w[k] = __byte_perm(x.v[7 - k], 0, 0x0123);
+}
+__device__ __forceinline__ Felt to_mont(const Felt& x) { return fmul(x, P252_R2); }
+__device__ __forceinline__ Felt from_mont(const Felt& x) {
+  Felt one{};
+  one.v[0] = 1;
+  return fmul(x, one);
+}
+
+__device__ __forceinline__ Felt load_hash(const uint8_t* base, size_t i) {
+  const uint4* p = reinterpret_cast<const uint4*>(base + 32 * i);
+  const uint4 a = __ldg(p), b = __ldg(p + 1);
+  const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  return to_mont(from_be_words(w));
+}
+__device__ __forceinline__ void store_hash(uint8_t* base, size_t i, const Felt& m) {
+  uint32_t w[8];
+  to_be_words(from_mont(m), w);
+  uint4* p = reinterpret_cast<uint4*>(base + 32 * i);
+  p[0] = make_uint4(w[0], w[1], w[2], w[3]);
+  p[1] = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+// Value k of a node's input sequence: the children (when there is a previous
+// layer), then the column words of 8 values each.
+__device__ __forceinline__ Felt node_value(uint32_t k, size_t i, const uint8_t* prev,
+                                           const uint32_t* const* cols, uint32_t n_cols) {
+  if (prev) {
+    if (k < 2) return load_hash(prev, 2 * i + k);
+    k -= 2;
+  }
+  const uint32_t c0 = 8 * k;
+  const uint32_t len = n_cols - c0 < 8 ? n_cols - c0 : 8;
+  Felt f{};
+  for (uint32_t q = 0; q < len; q++) {
+    const uint32_t v = __ldg(cols[c0 + q] + i);
+    // f = f << 31 | v
+#pragma unroll
+    for (int j = 7; j >= 1; j--) f.v[j] = (f.v[j] << 31) | (f.v[j - 1] >> 1);
+    f.v[0] = (f.v[0] << 31) | v;
+  }
+  if (len < 8) f.v[7] += len << 24;  // length at bit 248
+  return to_mont(f);
+}
+
+// One node per thread: children from `prev` (or none) and columns [0, n_cols).
+// poseidon_hash_many of m values absorbs blocks of two from the sequence
+// values, 1, 0: m / 2 + 1 permutations; poseidon_hash(l, r) (children and no
+// columns) is one permutation of (l, r, 2). Either way one call site of the
+// permutation, inlined with the state in registers.
+__global__ void __launch_bounds__(128) poseidon252_layer_kernel(uint32_t log_size, const uint8_t* __restrict__ prev,
+                                                                const uint32_t* const* __restrict__ cols,
+                                                                uint32_t n_cols, uint8_t* __restrict__ out) {
+  const size_t n = (size_t)1 << log_size;
+  const bool node_only = prev && n_cols == 0;
+  const uint32_t m = (prev ? 2u : 0u) + (n_cols + 7) / 8;  // values
+  const uint32_t n_blocks = node_only ? 1u : m / 2 + 1;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    Felt s[3] = {};
+    if (node_only) s[2] = P252_TWO;
+    for (uint32_t b = 0; b < n_blocks; b++) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const uint32_t k = 2 * b + h;
+        if (k < m) s[h] = fadd(s[h], node_value(k, i, prev, cols, n_cols));
+        else if (k == m && !node_only) s[h] = fadd(s[h], P252_ONE);
+      }
+      hades(s);
+    }
+    store_hash(out, i, s[0]);
+  }
+}
+
+// A batch of permutations: states of 3 big-endian hashes each (tests).
+__global__ void poseidon252_permute_kernel(const uint8_t* __restrict__ in, uint32_t n, uint8_t* __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    Felt s[3] = {load_hash(in, 3 * (size_t)i), load_hash(in, 3 * (size_t)i + 1), load_hash(in, 3 * (size_t)i + 2)};
+    hades(s);
+#pragma unroll
+    for (int j = 0; j < 3; j++) store_hash(out, 3 * (size_t)i + j, s[j]);
+  }
+}
+
+int poseidon252_commit_on_layer(cudaStream_t st, uint32_t log_size, const uint8_t* d_prev,
+                                const uint32_t* const* d_cols, uint32_t n_cols, uint8_t* d_out) {
+  GS_REQUIRE(log_size <= 30, "layer log size out of range");
+  GS_REQUIRE(d_out != nullptr, "null output");
+  GS_REQUIRE(n_cols == 0 || d_cols != nullptr, "null column table");
+  GS_REQUIRE(((uintptr_t)d_out & 15) == 0 && ((uintptr_t)d_prev & 15) == 0, "hash buffers must be 16-byte aligned");
+  const size_t n = (size_t)1 << log_size;
+  size_t blocks = (n + 127) / 128;
+  const size_t cap = (size_t)num_sms() * 16;
+  if (blocks > cap) blocks = cap;
+  poseidon252_layer_kernel<<<(unsigned)blocks, 128, 0, st>>>(log_size, d_prev, d_cols, n_cols, d_out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+int poseidon252_permute(cudaStream_t st, const uint8_t* d_in, uint32_t n, uint8_t* d_out) {
+  if (n == 0) return OK;
+  GS_REQUIRE(((uintptr_t)d_in & 15) == 0 && ((uintptr_t)d_out & 15) == 0, "state buffers must be 16-byte aligned");
+  const uint32_t blocks = (n + 127) / 128;
+  poseidon252_permute_kernel<<<blocks, 128, 0, st>>>(d_in, n, d_out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+}  // namespace gs

@@ -164,6 +164,12 @@ int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* la
 int lifted_leaves(cudaStream_t st, uint32_t lift, const uint32_t* const* d_cols, const uint8_t* d_shifts,
                   uint32_t n_cols, uint32_t* d_out);
 
+// poseidon252.cu: Poseidon252 Merkle layers and permutations; hashes are
+// felt252 values as 32 big-endian bytes.
+int poseidon252_commit_on_layer(cudaStream_t st, uint32_t log_size, const uint8_t* d_prev,
+                                const uint32_t* const* d_cols, uint32_t n_cols, uint8_t* d_out);
+int poseidon252_permute(cudaStream_t st, const uint8_t* d_in, uint32_t n, uint8_t* d_out);
+
 // FRI layers of log size <= 11 in one launch (fri.cu): layer k has log size
 // log0 - k; layers 0..n-1 are committed (tree[k][L] = their Merkle layers,
 // leaves of layer 0 already hashed), layer n is the last layer.

@@ -193,6 +193,28 @@ class GpuBackend:
         L.check(L.lib().gs_commit_node_layers(ctx.handle, len(layers) - 1, pp), "commit_node_layers")
         return layers
 
+    @staticmethod
+    def poseidon252_commit_on_layer(log_size, prev_layer, columns, ctx=None, out=None):
+        """MerkleOps<Poseidon252MerkleHasher>::commit_on_layer (prover/backend/
+        cuda/poseidon252.rs:21-42): 2^log_size felt252 hashes as a uint8 tensor
+        of 32 big-endian bytes each."""
+        ctx = ctx or default_context()
+        if out is None:
+            out = torch.empty((1 << log_size) * 32, dtype=torch.uint8, device="cuda")
+        pp, keep = L.ptr_array([c.data_ptr() for c in columns]) if columns else (None, None)
+        L.check(L.lib().gs_poseidon252_commit_on_layer(ctx.handle, log_size, _p(prev_layer), len(columns), pp,
+                                                      _p(out)), "poseidon252_commit_on_layer")
+        return out
+
+    @staticmethod
+    def poseidon252_permute(states, ctx=None):
+        """Hades permutations of n states (uint8 tensor of n x 96 big-endian bytes)."""
+        ctx = ctx or default_context()
+        n = states.numel() // 96
+        out = torch.empty_like(states)
+        L.check(L.lib().gs_poseidon252_permute(ctx.handle, _p(states), n, _p(out)), "poseidon252_permute")
+        return out
+
     # --------------------------------------------------------------- FriOps
     @staticmethod
     def fold_line(eval_planes, log_size, alpha, twiddles: TwiddleTree, ctx=None, leaf_hashes=None):
