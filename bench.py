@@ -811,7 +811,8 @@ def run_reference(args, world, rank):
 
 def run_case(args):
     """One op on a small case, for ncu captures: `--case fft:26`, `--case lde:18:162:2` (extension
-    of 162 columns from 2^18 to 2^20), `--case merkle:20:64`, `--case fold:22`."""
+    of 162 columns from 2^18 to 2^20), `--case merkle:20:64`, `--case fold:22`, `--case p252:18:8`
+    (Poseidon252 Merkle leaves of 8 columns x 2^18 rows, then the node layer above them)."""
     import torch
     from gpustark.backend import GpuBackend as B, to_device, Context
     kind, *params = args.case.split(":")
@@ -837,6 +838,13 @@ def run_case(args):
         cols = [to_device(rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32)) for _ in range(k)]
         out = torch.empty((1 << n) * 8, dtype=torch.int32, device="cuda")
         work = lambda: B.commit_on_layer(n, None, cols, ctx=ctx, out=out)
+    elif kind == "p252":
+        n, k = int(params[0]), int(params[1])
+        cols = [to_device(rng.integers(0, P, 1 << n, dtype=np.int64).astype(np.uint32)) for _ in range(k)]
+        leaves = torch.empty((1 << n) * 32, dtype=torch.uint8, device="cuda")
+        nodes = torch.empty((1 << (n - 1)) * 32, dtype=torch.uint8, device="cuda")
+        work = lambda: (B.poseidon252_commit_on_layer(n, None, cols, ctx=ctx, out=leaves),
+                        B.poseidon252_commit_on_layer(n - 1, leaves, [], ctx=ctx, out=nodes))
     elif kind == "fold":
         n = int(params[0])
         tw = B.precompute_twiddles(n + 1, ctx=ctx)

@@ -17,8 +17,8 @@
 // Field elements live in registers as 8 little-endian 32-bit limbs in
 // Montgomery form (R = 2^256). The modulus is sparse, limbs [1, 0, 0, 0, 0, 0,
 // 17, 2^27], and p = 1 mod 2^32, so the Montgomery quotient digit of each
-// reduction step is -t0 and adding m·p touches three limbs. Hashes in memory
-// are the reference's device layout: 32 bytes, big-endian.
+// reduction step is -t0 and adding m·p touches limbs 0, 6, 7 and 8. Hashes in
+// memory are the reference's device layout: 32 bytes, big-endian.
 #include "runtime.cuh"
 
 namespace gs {
@@ -29,68 +29,87 @@ struct Felt {
 
 #include "poseidon252_constants.inc"
 
-constexpr uint32_t P252_L6 = 17u, P252_L7 = 0x08000000u;  // limbs 6 and 7 of p (limb 0 is 1, 1..5 are 0)
+// Carry chains in PTX (add.cc / addc, mad.lo.cc / madc.hi.cc): one
+// instruction per limb, the carry in the flag.
 
-// r = a - p when a >= p, else a
+// t -> t - p when t >= p (t < 2p); branch-free select
 __device__ __forceinline__ void reduce_once(uint32_t t[8]) {
-  uint32_t s[8];
-  int64_t x = (int64_t)t[0] - 1;
-  s[0] = (uint32_t)x;
-  int64_t br = x < 0;
+  uint32_t d[8], bw;
+  asm("sub.cc.u32 %0, %9, 1;\n\t"
+      "subc.cc.u32 %1, %10, 0;\n\t"
+      "subc.cc.u32 %2, %11, 0;\n\t"
+      "subc.cc.u32 %3, %12, 0;\n\t"
+      "subc.cc.u32 %4, %13, 0;\n\t"
+      "subc.cc.u32 %5, %14, 0;\n\t"
+      "subc.cc.u32 %6, %15, 17;\n\t"
+      "subc.cc.u32 %7, %16, 0x08000000;\n\t"
+      "subc.u32 %8, 0, 0;"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]), "=r"(bw)
+      : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]));
 #pragma unroll
-  for (int j = 1; j < 6; j++) {
-    x = (int64_t)t[j] - br;
-    s[j] = (uint32_t)x;
-    br = x < 0;
-  }
-  x = (int64_t)t[6] - P252_L6 - br;
-  s[6] = (uint32_t)x;
-  br = x < 0;
-  x = (int64_t)t[7] - P252_L7 - br;
-  s[7] = (uint32_t)x;
-  br = x < 0;
-#pragma unroll
-  for (int j = 0; j < 8; j++) t[j] = br ? t[j] : s[j];
+  for (int j = 0; j < 8; j++) t[j] = (t[j] & bw) | (d[j] & ~bw);  // borrow: t < p, keep it
 }
 
-// Montgomery product a·b·R^-1 mod p (CIOS), for a, b < p.
+// Montgomery product a·b·R^-1 mod p (CIOS), for a, b < p. Per limb b_i:
+// t += a·b_i, then t += m·p with m = -t0 (p = 1 mod 2^32), which zeroes
+// t0 and touches limbs 6, 7, 8 (17·2^192 and 2^251), then a one-limb shift.
+// t0 + m is 0 with a carry exactly when t0 != 0; that carry is fed into
+// limb 1 directly, and m·17 is formed outside the carry chain, which holds
+// plain add-with-carry only (a chain that mixed multiply-add-with-carry
+// with an immediate operand into the reduction produced wrong carries on
+// sm_100a). After each shift t < 2p < 2^253, so limb 8 is 0 before the next
+// product.
 __device__ __forceinline__ Felt fmul(const Felt& a, const Felt& b) {
   uint32_t t[10];
 #pragma unroll
   for (int j = 0; j < 10; j++) t[j] = 0;
 #pragma unroll
   for (int i = 0; i < 8; i++) {
-    uint64_t c = 0;
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      c += (uint64_t)a.v[j] * b.v[i] + t[j];
-      t[j] = (uint32_t)c;
-      c >>= 32;
-    }
-    c += t[8];
-    t[8] = (uint32_t)c;
-    t[9] = (uint32_t)(c >> 32);
-    // t += m·p with m = -t0 (so the low limb becomes 0), then shift one limb
+    asm("mad.lo.cc.u32 %0, %10, %18, %0;\n\t"
+        "madc.lo.cc.u32 %1, %11, %18, %1;\n\t"
+        "madc.lo.cc.u32 %2, %12, %18, %2;\n\t"
+        "madc.lo.cc.u32 %3, %13, %18, %3;\n\t"
+        "madc.lo.cc.u32 %4, %14, %18, %4;\n\t"
+        "madc.lo.cc.u32 %5, %15, %18, %5;\n\t"
+        "madc.lo.cc.u32 %6, %16, %18, %6;\n\t"
+        "madc.lo.cc.u32 %7, %17, %18, %7;\n\t"
+        "addc.u32 %8, %8, 0;\n\t"
+        "mad.hi.cc.u32 %1, %10, %18, %1;\n\t"
+        "madc.hi.cc.u32 %2, %11, %18, %2;\n\t"
+        "madc.hi.cc.u32 %3, %12, %18, %3;\n\t"
+        "madc.hi.cc.u32 %4, %13, %18, %4;\n\t"
+        "madc.hi.cc.u32 %5, %14, %18, %5;\n\t"
+        "madc.hi.cc.u32 %6, %15, %18, %6;\n\t"
+        "madc.hi.cc.u32 %7, %16, %18, %7;\n\t"
+        "madc.hi.cc.u32 %8, %17, %18, %8;\n\t"
+        "addc.u32 %9, 0, 0;"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7]),
+          "+r"(t[8]), "=r"(t[9])
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]),
+          "r"(a.v[7]), "r"(b.v[i]));
+    // reduction with plain add-with-carry: t0 + m is 0 with a carry exactly
+    // when t0 != 0; m·17 at limb 6 (two words); m·2^251 at limbs 7 and 8
     const uint32_t m = 0u - t[0];
-    uint64_t d = ((uint64_t)t[0] + m) >> 32;
+    const uint64_t m17 = (uint64_t)m * 17u;
+    asm("add.cc.u32 %0, %0, %9;\n\t"
+        "addc.cc.u32 %1, %1, 0;\n\t"
+        "addc.cc.u32 %2, %2, 0;\n\t"
+        "addc.cc.u32 %3, %3, 0;\n\t"
+        "addc.cc.u32 %4, %4, 0;\n\t"
+        "addc.cc.u32 %5, %5, %10;\n\t"
+        "addc.cc.u32 %6, %6, %11;\n\t"
+        "addc.cc.u32 %7, %7, 0;\n\t"
+        "addc.u32 %8, %8, 0;\n\t"
+        "add.cc.u32 %6, %6, %12;\n\t"
+        "addc.cc.u32 %7, %7, %13;\n\t"
+        "addc.u32 %8, %8, 0;"
+        : "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7]), "+r"(t[8]),
+          "+r"(t[9])
+        : "r"(t[0] != 0u ? 1u : 0u), "r"((uint32_t)m17), "r"((uint32_t)(m17 >> 32)), "r"(m << 27), "r"(m >> 5));
 #pragma unroll
-    for (int j = 1; j < 6; j++) {
-      d += t[j];
-      t[j - 1] = (uint32_t)d;
-      d >>= 32;
-    }
-    d += (uint64_t)t[6] + (uint64_t)m * P252_L6;
-    t[5] = (uint32_t)d;
-    d >>= 32;
-    d += (uint64_t)t[7] + ((uint64_t)m << 27);
-    t[6] = (uint32_t)d;
-    d >>= 32;
-    d += t[8];
-    t[7] = (uint32_t)d;
-    d >>= 32;
-    t[8] = t[9] + (uint32_t)d;
+    for (int j = 0; j < 9; j++) t[j] = t[j + 1];
   }
-  reduce_once(t);  // t < 2p
+  reduce_once(t);
   Felt r;
 #pragma unroll
   for (int j = 0; j < 8; j++) r.v[j] = t[j];
@@ -99,14 +118,18 @@ __device__ __forceinline__ Felt fmul(const Felt& a, const Felt& b) {
 
 __device__ __forceinline__ Felt fadd(const Felt& a, const Felt& b) {
   uint32_t t[8];
-  uint64_t c = 0;
-#pragma unroll
-  for (int j = 0; j < 8; j++) {
-    c += (uint64_t)a.v[j] + b.v[j];
-    t[j] = (uint32_t)c;
-    c >>= 32;
-  }
-  reduce_once(t);  // a + b < 2p < 2^253: no carry out of limb 7
+  asm("add.cc.u32 %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, %17;\n\t"
+      "addc.cc.u32 %2, %10, %18;\n\t"
+      "addc.cc.u32 %3, %11, %19;\n\t"
+      "addc.cc.u32 %4, %12, %20;\n\t"
+      "addc.cc.u32 %5, %13, %21;\n\t"
+      "addc.cc.u32 %6, %14, %22;\n\t"
+      "addc.u32 %7, %15, %23;"
+      : "=r"(t[0]), "=r"(t[1]), "=r"(t[2]), "=r"(t[3]), "=r"(t[4]), "=r"(t[5]), "=r"(t[6]), "=r"(t[7])
+      : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+        "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+  reduce_once(t);  // a + b < 2p < 2^253
   Felt r;
 #pragma unroll
   for (int j = 0; j < 8; j++) r.v[j] = t[j];
@@ -114,29 +137,30 @@ __device__ __forceinline__ Felt fadd(const Felt& a, const Felt& b) {
 }
 
 __device__ __forceinline__ Felt fsub(const Felt& a, const Felt& b) {
-  uint32_t t[8];
-  int64_t br = 0;
-#pragma unroll
-  for (int j = 0; j < 8; j++) {
-    int64_t x = (int64_t)a.v[j] - b.v[j] - br;
-    t[j] = (uint32_t)x;
-    br = x < 0;
-  }
-  // borrow: add p back
-  const uint32_t k = br ? 0xffffffffu : 0u;
-  uint64_t c = (uint64_t)t[0] + (1u & k);
-  t[0] = (uint32_t)c;
-  c >>= 32;
-#pragma unroll
-  for (int j = 1; j < 6; j++) {
-    c += t[j];
-    t[j] = (uint32_t)c;
-    c >>= 32;
-  }
-  c += (uint64_t)t[6] + (P252_L6 & k);
-  t[6] = (uint32_t)c;
-  c >>= 32;
-  t[7] = t[7] + (P252_L7 & k) + (uint32_t)c;
+  uint32_t t[8], bw;
+  asm("sub.cc.u32 %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32 %8, 0, 0;"
+      : "=r"(t[0]), "=r"(t[1]), "=r"(t[2]), "=r"(t[3]), "=r"(t[4]), "=r"(t[5]), "=r"(t[6]), "=r"(t[7]), "=r"(bw)
+      : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+        "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+  // a borrow (a < b): add p back
+  asm("add.cc.u32 %0, %0, %8;\n\t"
+      "addc.cc.u32 %1, %1, 0;\n\t"
+      "addc.cc.u32 %2, %2, 0;\n\t"
+      "addc.cc.u32 %3, %3, 0;\n\t"
+      "addc.cc.u32 %4, %4, 0;\n\t"
+      "addc.cc.u32 %5, %5, 0;\n\t"
+      "addc.cc.u32 %6, %6, %9;\n\t"
+      "addc.u32 %7, %7, %10;"
+      : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7])
+      : "r"(bw & 1u), "r"(bw & 17u), "r"(bw & 0x08000000u));
   Felt r;
 #pragma unroll
   for (int j = 0; j < 8; j++) r.v[j] = t[j];
@@ -156,25 +180,26 @@ __device__ __forceinline__ void mds(Felt s[3]) {
   s[2] = fsub(t, s2x3);
 }
 
+// The permutation with compressed partial rounds (one constant each, added
+// to s2; the folded remainder sits in the first of the last 4 full rounds'
+// constants): the same permutation, two constant additions fewer per
+// partial round (poseidon252_constants.py derives and checks the form).
 __device__ __forceinline__ void hades(Felt s[3]) {
-  int r = 0;
 #pragma unroll 1
-  for (int k = 0; k < 4; k++, r++) {
+  for (int r = 0; r < 4; r++) {
 #pragma unroll
-    for (int j = 0; j < 3; j++) s[j] = fcube(fadd(s[j], P252_RC[3 * r + j]));
+    for (int j = 0; j < 3; j++) s[j] = fcube(fadd(s[j], P252_FULL_RC[3 * r + j]));
     mds(s);
   }
 #pragma unroll 1
-  for (int k = 0; k < 83; k++, r++) {
-    s[0] = fadd(s[0], P252_RC[3 * r]);
-    s[1] = fadd(s[1], P252_RC[3 * r + 1]);
-    s[2] = fcube(fadd(s[2], P252_RC[3 * r + 2]));
+  for (int k = 0; k < 83; k++) {
+    s[2] = fcube(fadd(s[2], P252_PARTIAL_RC[k]));
     mds(s);
   }
 #pragma unroll 1
-  for (int k = 0; k < 4; k++, r++) {
+  for (int r = 4; r < 8; r++) {
 #pragma unroll
-    for (int j = 0; j < 3; j++) s[j] = fcube(fadd(s[j], P252_RC[3 * r + j]));
+    for (int j = 0; j < 3; j++) s[j] = fcube(fadd(s[j], P252_FULL_RC[3 * r + j]));
     mds(s);
   }
 }

@@ -4,7 +4,8 @@ oracle/_ref/libstwo_cuda_ref.so (skipped when that library is absent): the
 circle FFT (ntt_n2b_columns / ntt_b2n_column), the Blake2s leaf layer
 (commit_on_first_layer), the FRI folds (fold_line, fold_circle_into_line),
 the OODS evaluation (batch_eval_at_points) and the proof of work
-(grind_blake2s) must give identical outputs on the same inputs.
+(grind_blake2s) and the Poseidon252 Merkle layers (poseidon252_commit_on_
+first_layer / _with_previous) must give identical outputs on the same inputs.
 With -s, the timing test prints both implementations' device times."""
 import ctypes as C
 import os
@@ -44,8 +45,11 @@ def ref():
     lib.batch_eval_at_points.argtypes = [VP, C.c_int, C.c_int, QM31, QM31, C.POINTER(QM31)]
     lib.grind_blake2s.argtypes = [C.POINTER(C.c_uint32), C.c_uint32]
     lib.grind_blake2s.restype = C.c_uint64
+    lib.poseidon252_commit_on_first_layer.argtypes = [C.c_size_t, C.c_size_t, VP, VP]
+    lib.poseidon252_commit_on_layer_with_previous.argtypes = [C.c_size_t, C.c_size_t, VP, VP, VP]
     for f in (lib.ntt_n2b_columns, lib.ntt_b2n_column, lib.commit_on_first_layer, lib.fold_line,
-              lib.fold_circle_into_line, lib.batch_eval_at_points):
+              lib.fold_circle_into_line, lib.batch_eval_at_points, lib.poseidon252_commit_on_first_layer,
+              lib.poseidon252_commit_on_layer_with_previous):
         f.restype = None
     return lib
 
@@ -168,6 +172,33 @@ def test_grind_matches_reference_cuda(ref, B, pow_bits):
     assert ref.grind_blake2s(words, pow_bits) == nonce.value
 
 
+def _ref_poseidon252(ref, log, cols, prev, out):
+    table = torch.tensor([c.data_ptr() for c in cols] or [0], dtype=torch.int64, device="cuda")
+    if prev is None:
+        ref.poseidon252_commit_on_first_layer(1 << log, len(cols), table.data_ptr(), out.data_ptr())
+    else:
+        ref.poseidon252_commit_on_layer_with_previous(1 << log, len(cols), table.data_ptr(), prev.data_ptr(),
+                                                      out.data_ptr())
+    return table
+
+
+@pytest.mark.parametrize("log,n_cols,with_prev", [(10, 1, False), (12, 8, False), (12, 9, True), (13, 0, True),
+                                                  (14, 20, False), (15, 3, True)])
+def test_poseidon252_layer_matches_reference_cuda(ref, B, log, n_cols, with_prev):
+    from gpustark.backend import to_device
+    rng = np.random.default_rng(500 + log + n_cols)
+    cols = [to_device(rng.integers(0, P, 1 << log, dtype=np.int64).astype(np.uint32)) for _ in range(n_cols)]
+    prev = None
+    if with_prev:  # a valid previous layer: hashes of random leaves
+        leaf_cols = [to_device(rng.integers(0, P, 1 << (log + 1), dtype=np.int64).astype(np.uint32)) for _ in range(2)]
+        prev = B.poseidon252_commit_on_layer(log + 1, None, leaf_cols)
+    ours = B.poseidon252_commit_on_layer(log, prev, cols)
+    theirs = torch.empty_like(ours)
+    _ref_poseidon252(ref, log, cols, prev, theirs)
+    torch.cuda.synchronize()
+    assert torch.equal(ours, theirs)
+
+
 def _time(fn, reps=5):
     fn()
     torch.cuda.synchronize()
@@ -207,6 +238,15 @@ def test_timing_against_reference_cuda(ref, B):
     ours = _time(lambda: B.fold_line(planes, 22, [1, 2, 3, 4], tw))
     theirs = _time(lambda: ref_fold_line(ref, planes, 22, [1, 2, 3, 4], tw, folded))
     rows.append(("fold_line 2^22", ours, theirs))
+    pcols = [to_device(rng.integers(0, P, 1 << 18, dtype=np.int64).astype(np.uint32)) for _ in range(8)]
+    pout = torch.empty((1 << 18) * 32, dtype=torch.uint8, device="cuda")
+    ours = _time(lambda: B.poseidon252_commit_on_layer(18, None, pcols, out=pout), reps=3)
+    theirs = _time(lambda: _ref_poseidon252(ref, 18, pcols, None, pout), reps=3)
+    rows.append(("poseidon252 leaves 8x2^18", ours, theirs))
+    pnode = torch.empty((1 << 17) * 32, dtype=torch.uint8, device="cuda")
+    ours = _time(lambda: B.poseidon252_commit_on_layer(17, pout, [], out=pnode), reps=3)
+    theirs = _time(lambda: _ref_poseidon252(ref, 17, [], pout, pnode), reps=3)
+    rows.append(("poseidon252 nodes 2^17", ours, theirs))
     print()
     for name, o, t in rows:
         print("%-24s gpustark %8.3f ms   reference CUDA %8.3f ms   %5.1fx" % (name, o, t, t / o))
