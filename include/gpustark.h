@@ -133,6 +133,14 @@ int gs_poseidon252_commit_on_layer(gs_ctx* ctx, uint32_t log_size, const uint8_t
  * the same big-endian layout; in and out may not overlap. No counterpart in
  * the reference's C ABI (it exposes no raw permutation). */
 int gs_poseidon252_permute(gs_ctx* ctx, const uint8_t* states, uint32_t n, uint8_t* out);
+/* GrindOps<Poseidon252Channel>::grind (prover/backend/simd/grind.rs:152-190;
+ * the reference's CUDA backend delegates it to that CPU code, prover/backend/
+ * cuda/backend.rs:52-56): the smallest nonce (hi << 32) | low, low < 2^14,
+ * hi = 0, 1, ..., such that poseidon_hash(poseidon_hash_many([0x12345678,
+ * digest, pow_bits]), nonce) has pow_bits trailing zero bits in its low 128
+ * bits. digest: the channel's felt252 digest, 32 bytes big-endian (host
+ * memory). Synchronises. */
+int gs_poseidon252_grind(gs_ctx* ctx, const uint8_t digest[32], uint32_t pow_bits, uint64_t* nonce);
 
 /* The node-only part of MerkleProver::commit's layer loop (prover/vcs/
  * prover.rs:39-48) when no columns are injected below top_log: layers is a

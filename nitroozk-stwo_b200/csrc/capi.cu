@@ -216,6 +216,15 @@ int gs_poseidon252_commit_on_layer(gs_ctx* ctx, uint32_t log_size, const uint8_t
   return poseidon252_commit_on_layer(ctx->c.stream, log_size, prev_layer, (const uint32_t* const*)d, n_cols, out);
 }
 
+int gs_poseidon252_grind(gs_ctx* ctx, const uint8_t digest[32], uint32_t pow_bits, uint64_t* nonce) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(digest != nullptr && nonce != nullptr, "null digest/nonce");
+  const void* d_digest = nullptr;
+  GS_TRY(ctx->c.stage_bytes(digest, 32, &d_digest));
+  return poseidon252_grind(ctx->c.stream, (const uint8_t*)d_digest, pow_bits, ctx->c.d_small,
+                           (uint32_t*)ctx->c.h_small, nonce);
+}
+
 int gs_poseidon252_permute(gs_ctx* ctx, const uint8_t* states, uint32_t n, uint8_t* out) {
   CTX_REQUIRED(ctx);
   GS_REQUIRE(n == 0 || (states && out), "null state buffer");

@@ -20,6 +20,7 @@
 // reduction step is -t0 and adding m·p touches limbs 0, 6, 7 and 8. Hashes in
 // memory are the reference's device layout: 32 bytes, big-endian.
 #include "runtime.cuh"
+#include <cstring>
 
 namespace gs {
 
@@ -320,6 +321,109 @@ int poseidon252_permute(cudaStream_t st, const uint8_t* d_in, uint32_t n, uint8_
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;
+}
+
+}  // namespace gs
+
+namespace gs {
+
+// ------------------------------------------------ proof of work, Poseidon252
+// GrindOps<Poseidon252Channel>::grind (prover/backend/simd/grind.rs:152-190;
+// the reference's CUDA backend hands it to that CPU code, cuda/backend.rs:
+// 52-56): prefixed = poseidon_hash_many([POW_PREFIX, digest, pow_bits]); the
+// answer is the smallest nonce (hi << 32) | low, low < 2^14, hi = 0, 1, ...,
+// whose poseidon_hash(prefixed, nonce) has at least pow_bits trailing zero
+// bits in its low 128 bits.
+constexpr uint32_t P252_POW_PREFIX = 0x12345678u;
+constexpr uint32_t P252_GRIND_LOW_LOG = 14, P252_GRIND_STEP = 128;
+
+__device__ __forceinline__ Felt small_felt(uint32_t lo, uint32_t hi) {
+  Felt x{};
+  x.v[0] = lo;
+  x.v[1] = hi;
+  return to_mont(x);
+}
+
+// One thread: poseidon_hash_many of three values (two permutations).
+__global__ void poseidon252_pow_prefix_kernel(const uint8_t* __restrict__ digest, uint32_t pow_bits,
+                                              uint8_t* __restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Felt s[3] = {};
+  for (int b = 0; b < 2; b++) {
+    if (b == 0) {
+      s[0] = fadd(s[0], small_felt(P252_POW_PREFIX, 0));
+      s[1] = fadd(s[1], load_hash(digest, 0));
+    } else {
+      s[0] = fadd(s[0], small_felt(pow_bits, 0));
+      s[1] = fadd(s[1], P252_ONE);
+    }
+    hades(s);
+  }
+  store_hash(out, 0, s[0]);
+}
+
+// Persistent grid over 128-nonce steps of high words [hi0, hi0 + n_hi), in
+// increasing nonce order; a block stops at the first step above the recorded
+// minimum (a plain read, nothing waits), so the answer is still the smallest
+// passing nonce (atomicMin over the 64-bit nonce).
+__global__ void __launch_bounds__(P252_GRIND_STEP) poseidon252_grind_kernel(const uint8_t* __restrict__ prefixed,
+                                                                           uint32_t hi0, uint32_t n_hi,
+                                                                           uint32_t pow_bits,
+                                                                           unsigned long long* result) {
+  const volatile unsigned long long* best = result;
+  const Felt pre = load_hash(prefixed, 0);
+  constexpr uint32_t STEPS_PER_HI = (1u << P252_GRIND_LOW_LOG) / P252_GRIND_STEP;
+  for (uint32_t step = blockIdx.x; step < n_hi * STEPS_PER_HI; step += gridDim.x) {
+    const uint32_t hi = hi0 + step / STEPS_PER_HI;
+    const uint32_t low0 = (step % STEPS_PER_HI) * P252_GRIND_STEP;
+    if (*best < (((unsigned long long)hi << 32) | low0)) return;
+    const uint32_t low = low0 + threadIdx.x;
+    Felt s[3] = {pre, small_felt(low, hi), P252_TWO};
+    hades(s);
+    const Felt h = from_mont(s[0]);
+    // trailing zeros of the low 128 bits (limbs 0..3)
+    uint32_t tz = 128;
+#pragma unroll
+    for (int j = 3; j >= 0; j--)
+      if (h.v[j]) tz = 32u * j + (uint32_t)(__ffs(h.v[j]) - 1);
+    if (tz >= pow_bits) atomicMin(result, ((unsigned long long)hi << 32) | low);
+  }
+}
+
+int poseidon252_grind(cudaStream_t st, const uint8_t* d_digest, uint32_t pow_bits, uint8_t* d_scratch,
+                      uint32_t* h_word, uint64_t* nonce_out) {
+  GS_REQUIRE(pow_bits <= 128, "pow_bits > 128 is not supported");
+  GS_REQUIRE(((uintptr_t)d_digest & 15) == 0 && ((uintptr_t)d_scratch & 15) == 0, "buffers must be 16-byte aligned");
+  uint8_t* d_pre = d_scratch;                                                          // 32 bytes
+  unsigned long long* d_res = reinterpret_cast<unsigned long long*>(d_scratch + 32);  // 8 bytes
+  poseidon252_pow_prefix_kernel<<<1, 32, 0, st>>>(d_digest, pow_bits, d_pre);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  // high words per launch: about twice the expected number of chunks
+  // (2^(pow_bits - 14) each), 1 to 64
+  const uint32_t e = pow_bits > P252_GRIND_LOW_LOG ? pow_bits - P252_GRIND_LOW_LOG + 1 : 0;
+  const uint32_t n_hi = e >= 6 ? 64u : 1u << e;
+  const uint32_t steps = n_hi * ((1u << P252_GRIND_LOW_LOG) / P252_GRIND_STEP);
+  const uint32_t cap = 8u * (uint32_t)num_sms();
+  const unsigned blocks = steps < cap ? steps : cap;
+  // Bounded search: 2^20 high words cover pow_bits far beyond 40 with
+  // overwhelming probability; running out is reported, never looped on.
+  for (uint32_t hi = 0; hi < (1u << 20); hi += n_hi) {
+    GS_CUDA_TRY(cudaMemsetAsync(d_res, 0xff, 8, st));
+    poseidon252_grind_kernel<<<blocks, P252_GRIND_STEP, 0, st>>>(d_pre, hi, n_hi, pow_bits, d_res);
+    note_launch();
+    GS_CUDA_TRY(cudaGetLastError());
+    GS_CUDA_TRY(cudaMemcpyAsync(h_word, d_res, 8, cudaMemcpyDeviceToHost, st));
+    GS_TRY(stream_sync(st));
+    uint64_t found;
+    memcpy(&found, h_word, 8);
+    if (found != ~0ull) {
+      *nonce_out = found;
+      return OK;
+    }
+  }
+  set_error("poseidon252 grind: no nonce found within the search bound");
+  return ERR_TIMEOUT;
 }
 
 }  // namespace gs

@@ -62,6 +62,7 @@ _PROTOS = {
     "gs_commit_node_layers": [C.c_void_p, C.c_uint32, VPP],
     "gs_poseidon252_commit_on_layer": [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, VPP, C.c_void_p],
     "gs_poseidon252_permute": [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p],
+    "gs_poseidon252_grind": [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64)],
     "gs_fold_line": [C.c_void_p, VPP, C.c_uint32, QM31, VPP, C.c_void_p, C.c_uint32, C.c_void_p],
     "gs_fold_circle_into_line": [C.c_void_p, VPP, C.c_uint32, QM31, VPP, C.c_void_p, C.c_uint32, C.c_void_p],
     "gs_grind_blake2s": [C.c_void_p, U32P, C.c_uint32, C.POINTER(C.c_uint64)],

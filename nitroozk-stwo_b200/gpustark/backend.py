@@ -207,6 +207,18 @@ class GpuBackend:
         return out
 
     @staticmethod
+    def poseidon252_grind(digest, pow_bits, ctx=None):
+        """GrindOps<Poseidon252Channel>::grind; digest: int (felt252) or 32
+        big-endian bytes."""
+        ctx = ctx or default_context()
+        if isinstance(digest, int):
+            digest = digest.to_bytes(32, "big")
+        buf = (C.c_uint8 * 32).from_buffer_copy(digest)
+        nonce = C.c_uint64()
+        L.check(L.lib().gs_poseidon252_grind(ctx.handle, buf, pow_bits, C.byref(nonce)), "poseidon252_grind")
+        return nonce.value
+
+    @staticmethod
     def poseidon252_permute(states, ctx=None):
         """Hades permutations of n states (uint8 tensor of n x 96 big-endian bytes)."""
         ctx = ctx or default_context()

@@ -205,6 +205,22 @@ class Channel:
             out.append(r)
         return out
 
+    GRIND_LOW_BITS = 14  # prover/backend/simd/grind.rs:150
+
+    def grind(self, pow_bits):
+        """GrindOps<Poseidon252Channel>::grind (prover/backend/simd/grind.rs:
+        152-190): the smallest (hi << 32) | low, low < 2^14, hi = 0, 1, ..."""
+        pre = hash_many([self.POW_PREFIX, self.digest, pow_bits])
+        hi = 0
+        while True:
+            for low in range(1 << self.GRIND_LOW_BITS):
+                nonce = (hi << 32) | low
+                h = hash2(pre, nonce) & ((1 << 128) - 1)
+                tz = (h & -h).bit_length() - 1 if h else 128
+                if tz >= pow_bits:
+                    return nonce
+            hi += 1
+
     def verify_pow_nonce(self, n_bits, nonce):
         pre = hash_many([self.POW_PREFIX, self.digest, n_bits])
         h = hash2(pre, nonce)

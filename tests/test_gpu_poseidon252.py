@@ -85,3 +85,14 @@ def test_tree_root_matches_oracle(B):
         want = PS.commit_on_layer(L, want, [])
         assert dev_to_felts(layer) == want, L
     assert len(want) == 1
+
+
+@pytest.mark.parametrize("pow_bits,salt", [(0, 0), (1, 0), (6, 0), (10, 0), (10, 1), (12, 0)])
+def test_grind_matches_oracle(B, pow_bits, salt):
+    """GrindOps<Poseidon252Channel>: the same smallest nonce as the oracle's
+    sequential search, and the nonce passes the channel's check."""
+    ch = PS.Channel()
+    ch.mix_u64(0x1111222233334444 + 7 * salt + pow_bits)
+    got = B.poseidon252_grind(ch.digest, pow_bits)
+    assert got == ch.grind(pow_bits)
+    assert ch.verify_pow_nonce(pow_bits, got)
