@@ -60,7 +60,8 @@ __device__ __forceinline__ void reduce_once(uint32_t t[8]) {
 // with an immediate operand into the reduction produced wrong carries on
 // sm_100a). After each shift t < 2p < 2^253, so limb 8 is 0 before the next
 // product.
-__device__ __forceinline__ Felt fmul(const Felt& a, const Felt& b) {
+template <bool FULL>
+__device__ __forceinline__ Felt fmul_t(const Felt& a, const Felt& b) {
   uint32_t t[10];
 #pragma unroll
   for (int j = 0; j < 10; j++) t[j] = 0;
@@ -110,10 +111,72 @@ __device__ __forceinline__ Felt fmul(const Felt& a, const Felt& b) {
 #pragma unroll
     for (int j = 0; j < 9; j++) t[j] = t[j + 1];
   }
-  reduce_once(t);
+  if (FULL) reduce_once(t);
   Felt r;
 #pragma unroll
   for (int j = 0; j < 8; j++) r.v[j] = t[j];
+  return r;
+}
+
+// Fully reduced product (inputs below 2p): below p.
+__device__ __forceinline__ Felt fmul(const Felt& a, const Felt& b) { return fmul_t<true>(a, b); }
+// Lazy product: for inputs below 5.6p the result a·b/R + (< p) stays below
+// 2p; the permutation keeps every product input below 4.5p.
+__device__ __forceinline__ Felt fmul_l(const Felt& a, const Felt& b) { return fmul_t<false>(a, b); }
+
+// a + b without reduction (callers keep the sum below 2^256)
+__device__ __forceinline__ Felt ladd(const Felt& a, const Felt& b) {
+  Felt r;
+  asm("add.cc.u32 %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, %17;\n\t"
+      "addc.cc.u32 %2, %10, %18;\n\t"
+      "addc.cc.u32 %3, %11, %19;\n\t"
+      "addc.cc.u32 %4, %12, %20;\n\t"
+      "addc.cc.u32 %5, %13, %21;\n\t"
+      "addc.cc.u32 %6, %14, %22;\n\t"
+      "addc.u32 %7, %15, %23;"
+      : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
+        "=r"(r.v[7])
+      : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+        "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+  return r;
+}
+// a - b without reduction (callers guarantee a >= b)
+__device__ __forceinline__ Felt lsub(const Felt& a, const Felt& b) {
+  Felt r;
+  asm("sub.cc.u32 %0, %8, %16;\n\t"
+      "subc.cc.u32 %1, %9, %17;\n\t"
+      "subc.cc.u32 %2, %10, %18;\n\t"
+      "subc.cc.u32 %3, %11, %19;\n\t"
+      "subc.cc.u32 %4, %12, %20;\n\t"
+      "subc.cc.u32 %5, %13, %21;\n\t"
+      "subc.cc.u32 %6, %14, %22;\n\t"
+      "subc.u32 %7, %15, %23;"
+      : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
+        "=r"(r.v[7])
+      : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+        "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+  return r;
+}
+// x < 2^255 -> below 2p: with q = x >> 251, x - max(q - 1, 0)·p lies in
+// [p - q·(17·2^192 + 1), 2^251 + p) when q > 0 (and is x < 2^251 when q = 0):
+// no compare, no select.
+__device__ __forceinline__ Felt lreduce(const Felt& x) {
+  const uint32_t q = x.v[7] >> 27;
+  const uint32_t k = q > 0 ? q - 1 : 0;
+  Felt r;
+  asm("sub.cc.u32 %0, %8, %16;\n\t"
+      "subc.cc.u32 %1, %9, 0;\n\t"
+      "subc.cc.u32 %2, %10, 0;\n\t"
+      "subc.cc.u32 %3, %11, 0;\n\t"
+      "subc.cc.u32 %4, %12, 0;\n\t"
+      "subc.cc.u32 %5, %13, 0;\n\t"
+      "subc.cc.u32 %6, %14, %17;\n\t"
+      "subc.u32 %7, %15, %18;"
+      : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
+        "=r"(r.v[7])
+      : "r"(x.v[0]), "r"(x.v[1]), "r"(x.v[2]), "r"(x.v[3]), "r"(x.v[4]), "r"(x.v[5]), "r"(x.v[6]), "r"(x.v[7]),
+        "r"(k), "r"(k * 17u), "r"(k << 27));
   return r;
 }
 
@@ -168,39 +231,55 @@ __device__ __forceinline__ Felt fsub(const Felt& a, const Felt& b) {
   return r;
 }
 
-__device__ __forceinline__ Felt fcube(const Felt& x) { return fmul(fmul(x, x), x); }
+__device__ __forceinline__ Felt fcube(const Felt& x) { return fmul_l(fmul_l(x, x), x); }
 
-// MDS [[3, 1, 1], [1, -1, 1], [1, 1, -2]] as t = s0 + s1 + s2 and
-// (t + 2 s0, t - 2 s1, t - 3 s2)
+// 4p and 6p as plain integers (limbs 0, 6, 7 nonzero)
+__device__ __forceinline__ Felt p_times(uint32_t k) {
+  Felt r{};
+  r.v[0] = k;
+  r.v[6] = 17u * k;
+  r.v[7] = k << 27;
+  return r;
+}
+
+// MDS [[3, 1, 1], [1, -1, 1], [1, 1, -2]] on inputs below 2p:
+// t = s0 + s1 + s2 < 6p; (t + 2 s0, t + 4p - 2 s1, t + 6p - 3 s2), each
+// non-negative and below 12p, brought back below 2p.
 __device__ __forceinline__ void mds(Felt s[3]) {
-  const Felt t = fadd(fadd(s[0], s[1]), s[2]);
-  const Felt s1x2 = fadd(s[1], s[1]);
-  const Felt s2x3 = fadd(fadd(s[2], s[2]), s[2]);
-  s[0] = fadd(t, fadd(s[0], s[0]));
-  s[1] = fsub(t, s1x2);
-  s[2] = fsub(t, s2x3);
+  const Felt t = ladd(ladd(s[0], s[1]), s[2]);
+  const Felt s1x2 = ladd(s[1], s[1]);
+  const Felt s2x3 = ladd(ladd(s[2], s[2]), s[2]);
+  const Felt a0 = ladd(t, ladd(s[0], s[0]));
+  const Felt a1 = lsub(ladd(t, p_times(4)), s1x2);
+  const Felt a2 = lsub(ladd(t, p_times(6)), s2x3);
+  s[0] = lreduce(a0);
+  s[1] = lreduce(a1);
+  s[2] = lreduce(a2);
 }
 
 // The permutation with compressed partial rounds (one constant each, added
 // to s2; the folded remainder sits in the first of the last 4 full rounds'
 // constants): the same permutation, two constant additions fewer per
 // partial round (poseidon252_constants.py derives and checks the form).
+// Bounds: each round starts below 2p (below 3.5p right after absorbing a
+// block), adding a constant keeps every product input below 4.5p, products
+// return below 2p, and the MDS output is brought back below 2p.
 __device__ __forceinline__ void hades(Felt s[3]) {
 #pragma unroll 1
   for (int r = 0; r < 4; r++) {
 #pragma unroll
-    for (int j = 0; j < 3; j++) s[j] = fcube(fadd(s[j], P252_FULL_RC[3 * r + j]));
+    for (int j = 0; j < 3; j++) s[j] = fcube(ladd(s[j], P252_FULL_RC[3 * r + j]));
     mds(s);
   }
 #pragma unroll 1
   for (int k = 0; k < 83; k++) {
-    s[2] = fcube(fadd(s[2], P252_PARTIAL_RC[k]));
+    s[2] = fcube(ladd(s[2], P252_PARTIAL_RC[k]));
     mds(s);
   }
 #pragma unroll 1
   for (int r = 4; r < 8; r++) {
 #pragma unroll
-    for (int j = 0; j < 3; j++) s[j] = fcube(fadd(s[j], P252_FULL_RC[3 * r + j]));
+    for (int j = 0; j < 3; j++) s[j] = fcube(ladd(s[j], P252_FULL_RC[3 * r + j]));
     mds(s);
   }
 }
@@ -216,7 +295,7 @@ __device__ __forceinline__ void to_be_words(const Felt& x, uint32_t w[8]) {
 #pragma unroll
   for (int k = 0; k < 8; k++) w[k] = __byte_perm(x.v[7 - k], 0, 0x0123);
 }
-__device__ __forceinline__ Felt to_mont(const Felt& x) { return fmul(x, P252_R2); }
+__device__ __forceinline__ Felt to_mont(const Felt& x) { return fmul_l(x, P252_R2); }  // below 2p
 __device__ __forceinline__ Felt from_mont(const Felt& x) {
   Felt one{};
   one.v[0] = 1;
@@ -278,8 +357,8 @@ __global__ void __launch_bounds__(128) poseidon252_layer_kernel(uint32_t log_siz
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const uint32_t k = 2 * b + h;
-        if (k < m) s[h] = fadd(s[h], node_value(k, i, prev, cols, n_cols));
-        else if (k == m && !node_only) s[h] = fadd(s[h], P252_ONE);
+        if (k < m) s[h] = ladd(s[h], node_value(k, i, prev, cols, n_cols));
+        else if (k == m && !node_only) s[h] = ladd(s[h], P252_ONE);
       }
       hades(s);
     }
