@@ -18,6 +18,7 @@
 // collapses to res[i] = sum_c col_c[lift(i, L - L_c)] because lifted indices
 // compose; one pass reads each column once.
 #include "runtime.cuh"
+#include <cstdlib>
 
 namespace gs {
 
@@ -126,66 +127,115 @@ __global__ void __launch_bounds__(256) accumulate_numerators_kernel(const NumEnt
 }
 
 // Vector path with the entries split over the block's 8 warps: a block owns
-// 128 rows (lane l: rows 4l..4l+3, one 16-byte load per column), warp w
+// 128 rows (lane l: rows 4l..4l+3, one 16-byte word per column), warp w
 // accumulates entries w, w + 8, ..., and the 8 partial sums meet in shared
-// memory. A thread's chain of dependent loads is n_entries / 48 steps long
-// instead of n_entries / 6.
+// memory. Rounds of 6 entries stream through a per-warp double buffer with
+// cp.async: round r + 1 is in flight while round r computes. Each lane copies
+// exactly the 16 bytes it later reads, so its own cp.async.wait_group (a wait
+// on its own copies) is the only synchronisation inside the entry loop.
+constexpr int ACC_ROUND = 6;
+constexpr size_t ACC_DYN_SMEM = sizeof(uint4) * 8 * 2 * ACC_ROUND * 32;  // 48 KiB; the partial sums reuse it
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// EG entry groups x (8 / EG) row groups: warp w = (entry group w / RG, row
+// group w % RG); the block's tile is 128·RG rows, each warp 128 of them (lane
+// l: 4 rows, one 16-byte word per column), and the entry groups split the
+// entries (k = g, g + EG, ...). In a round the RG warps of an entry group
+// read 512·RG contiguous bytes of one column, which keeps HBM pages open.
+template <int EG>
 __global__ void __launch_bounds__(256) accumulate_numerators_split_kernel(const NumEntry* __restrict__ entries,
                                                                           uint32_t n_entries, qm31 b_sum,
                                                                           uint32_t log_size, Planes out) {
+  constexpr uint32_t RG = 8 / EG, TILE = 128 * RG, STRIDE = EG * ACC_ROUND;
   __shared__ NumEntry se[ACC_MAX_SMEM_ENTRIES];
-  __shared__ uint32_t part[8][4][128];  // [warp][coordinate][row in tile]
+  extern __shared__ uint4 dyn[];  // [warp][slot][entry][lane] in the loop; part[group][q][row] after it
+  uint32_t* part = reinterpret_cast<uint32_t*>(dyn);
   const bool staged = n_entries <= ACC_MAX_SMEM_ENTRIES;
   if (staged)
     for (uint32_t k = threadIdx.x; k < n_entries; k += blockDim.x) se[k] = entries[k];
   __syncthreads();
   const NumEntry* E = staged ? se : entries;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t eg = warp / RG, rg = warp % RG;
+  uint4* wbuf = dyn + (size_t)warp * 2 * ACC_ROUND * 32;
   const size_t n = (size_t)1 << log_size;
-  for (size_t tile = blockIdx.x; tile * 128 < n; tile += gridDim.x) {
-    const size_t row0 = tile * 128 + 4 * lane;
+  const uint32_t bs[4] = {b_sum.x.a, b_sum.x.b, b_sum.y.a, b_sum.y.b};
+  // full rounds of this entry group: entries eg + STRIDE r + EG j, j < 6
+  const uint32_t last = EG * (ACC_ROUND - 1);
+  const uint32_t rounds = eg + last < n_entries ? (n_entries - 1 - last - eg) / STRIDE + 1 : 0;
+  for (size_t tile = blockIdx.x; tile * TILE < n; tile += gridDim.x) {
+    const size_t row0 = tile * TILE + 128 * rg + 4 * lane;
+    auto issue = [&](uint32_t r) {
+      uint4* b = wbuf + (r & 1) * ACC_ROUND * 32;
+#pragma unroll
+      for (int j = 0; j < ACC_ROUND; j++) cp_async16(b + j * 32 + lane, E[eg + STRIDE * r + EG * j].col + row0);
+      cp_async_commit();
+    };
     uint64_t acc[4][4] = {};
-    uint32_t k = warp;
-    for (; k + 40 < n_entries; k += 48) {  // entries k, k+8, ..., k+40
-      uint32_t v[6][4];
+    if (rounds) issue(0);
+    for (uint32_t r = 0; r < rounds; r++) {
+      if (r + 1 < rounds) issue(r + 1);
+      else cp_async_commit();  // an empty group keeps the count uniform
+      cp_async_wait<1>();      // round r has landed (this lane's words)
+      const uint4* b = wbuf + (r & 1) * ACC_ROUND * 32;
+      const uint32_t k = eg + STRIDE * r;
 #pragma unroll
-      for (int j = 0; j < 6; j++) load_rows<4>(E[k + 8 * j].col, row0, v[j]);
+      for (int j = 0; j < ACC_ROUND; j++) {
+        const uint4 q4 = b[j * 32 + lane];
+        const uint32_t v[4] = {q4.x, q4.y, q4.z, q4.w};
 #pragma unroll
-      for (int j = 0; j < 6; j++) {
-#pragma unroll
-        for (int r = 0; r < 4; r++) {
-          acc_term(acc[r], E[k + 8 * j], v[j][r]);
+        for (int rr = 0; rr < 4; rr++) {
+          acc_term(acc[rr], E[k + EG * j], v[rr]);
           if (j == 2 || j == 5)
 #pragma unroll
-            for (int q = 0; q < 4; q++) acc[r][q] = fold64(acc[r][q]);
+            for (int q = 0; q < 4; q++) acc[rr][q] = fold64(acc[rr][q]);
         }
       }
     }
-    for (int cnt = 0; k < n_entries; k += 8) {
+    // the group's remaining entries (fewer than 6), loaded directly
+    for (uint32_t k = eg + STRIDE * rounds, cnt = 0; k < n_entries; k += EG) {
       uint32_t v[4];
       load_rows<4>(E[k].col, row0, v);
 #pragma unroll
-      for (int r = 0; r < 4; r++) acc_term(acc[r], E[k], v[r]);
+      for (int rr = 0; rr < 4; rr++) acc_term(acc[rr], E[k], v[rr]);
       if (++cnt == 3) {
         cnt = 0;
 #pragma unroll
-        for (int r = 0; r < 4; r++)
+        for (int rr = 0; rr < 4; rr++)
 #pragma unroll
-          for (int q = 0; q < 4; q++) acc[r][q] = fold64(acc[r][q]);
+          for (int q = 0; q < 4; q++) acc[rr][q] = fold64(acc[rr][q]);
       }
     }
+    if (EG == 1) {  // this warp holds its rows' whole sums
+      cp_async_wait<0>();
 #pragma unroll
-    for (int r = 0; r < 4; r++)
-#pragma unroll
-      for (int q = 0; q < 4; q++) part[warp][q][4 * lane + r] = reduce64(acc[r][q]);
+      for (int q = 0; q < 4; q++)
+        *reinterpret_cast<uint4*>(out.p[q] + row0) =
+            make_uint4(sub(reduce64(acc[0][q]), bs[q]), sub(reduce64(acc[1][q]), bs[q]),
+                       sub(reduce64(acc[2][q]), bs[q]), sub(reduce64(acc[3][q]), bs[q]));
+      continue;
+    }
+    // every copy of every warp has landed before the buffers turn into part
+    cp_async_wait<0>();
     __syncthreads();
-    const uint32_t bs[4] = {b_sum.x.a, b_sum.x.b, b_sum.y.a, b_sum.y.b};
-    for (uint32_t idx = threadIdx.x; idx < 512; idx += blockDim.x) {
-      const uint32_t q = idx >> 7, rr = idx & 127;
-      uint32_t t = part[0][q][rr];
 #pragma unroll
-      for (int w = 1; w < 8; w++) t = add(t, part[w][q][rr]);
-      if (tile * 128 + rr < n) out.p[q][tile * 128 + rr] = sub(t, bs[q]);
+    for (int rr = 0; rr < 4; rr++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) part[(eg * 4 + q) * TILE + 128 * rg + 4 * lane + rr] = reduce64(acc[rr][q]);
+    __syncthreads();
+    for (uint32_t idx = threadIdx.x; idx < 4 * TILE; idx += blockDim.x) {
+      const uint32_t q = idx / TILE, row = idx % TILE;
+      uint32_t t = part[q * TILE + row];
+#pragma unroll
+      for (int g = 1; g < EG; g++) t = add(t, part[(g * 4 + q) * TILE + row]);
+      if (tile * TILE + row < n) out.p[q][tile * TILE + row] = sub(t, bs[q]);
     }
     __syncthreads();
   }
@@ -202,11 +252,28 @@ int accumulate_numerators(cudaStream_t st, const void* d_entries, uint32_t n_ent
   size_t blocks = (n / R + threads - 1) / threads;
   size_t cap = (size_t)num_sms() * 16;
   if (blocks > cap) blocks = cap;
-  if (R == 4 && log_size >= 7) {
-    size_t tiles = n / 128;
+  static const int eg_env = [] {
+    const char* e = getenv("GS_ACC_EG");
+    return e ? atoi(e) : 1;
+  }();
+  if (R == 4 && log_size >= 10) {
+    const int eg = eg_env == 2 ? 2 : 1;
+    size_t tiles = n / (eg == 2 ? 512 : 1024);
     size_t cap2 = (size_t)num_sms() * 8;
-    accumulate_numerators_split_kernel<<<(unsigned)(tiles < cap2 ? tiles : cap2), 256, 0, st>>>(
-        (const NumEntry*)d_entries, n_entries, b_sum, log_size, out);
+    const unsigned grid = (unsigned)(tiles < cap2 ? tiles : cap2);
+    if (eg == 1) {
+      static const cudaError_t attr = cudaFuncSetAttribute(
+          accumulate_numerators_split_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ACC_DYN_SMEM);
+      GS_CUDA_TRY(attr);
+      accumulate_numerators_split_kernel<1><<<grid, 256, ACC_DYN_SMEM, st>>>((const NumEntry*)d_entries, n_entries,
+                                                                           b_sum, log_size, out);
+    } else {
+      static const cudaError_t attr = cudaFuncSetAttribute(
+          accumulate_numerators_split_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ACC_DYN_SMEM);
+      GS_CUDA_TRY(attr);
+      accumulate_numerators_split_kernel<2><<<grid, 256, ACC_DYN_SMEM, st>>>((const NumEntry*)d_entries, n_entries,
+                                                                           b_sum, log_size, out);
+    }
   } else if (R == 4)
     accumulate_numerators_kernel<4><<<(unsigned)blocks, threads, 0, st>>>((const NumEntry*)d_entries, n_entries,
                                                                          b_sum, log_size, out);
