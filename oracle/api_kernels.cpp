@@ -165,6 +165,68 @@ int oracle_verify_pow(const uint8_t* digest, uint32_t pow_bits, uint64_t nonce) 
   return ch.verify_pow_nonce(pow_bits, nonce) ? 1 : 0;
 }
 
+// ---- Poseidon252 (felt252 values as 32 big-endian bytes)
+// MerkleOps<Poseidon252MerkleHasher>::commit_on_layer; prev may be NULL.
+void oracle_p252_commit_on_layer(uint32_t log_size, const uint8_t* prev, uint32_t n_cols, const uint32_t* const* cols,
+                                 uint8_t* out) {
+  size_t n = (size_t)1 << log_size;
+  std::vector<std::vector<M31>> cv(n_cols);
+  std::vector<const std::vector<M31>*> cp;
+  for (uint32_t c = 0; c < n_cols; c++) { cv[c] = col_in(cols[c], n); cp.push_back(&cv[c]); }
+  std::vector<Hash32> pv;
+  if (prev) { pv.resize(2 * n); memcpy(pv.data(), prev, 64 * n); }
+  auto r = commit_on_layer(log_size, prev ? &pv : nullptr, cp, MerkleHash::Poseidon252);
+  memcpy(out, r.data(), 32 * n);
+}
+// The Hades permutation of n states (3 felts each, reduced mod p on input).
+void oracle_p252_permute(const uint8_t* in, size_t n, uint8_t* out) {
+  for (size_t k = 0; k < n; k++) {
+    std::array<p252::Fe, 3> s;
+    for (int j = 0; j < 3; j++) s[j] = p252::from_int(p252::reduce_be(in + 96 * k + 32 * j));
+    p252::permute(s);
+    for (int j = 0; j < 3; j++) memcpy(out + 96 * k + 32 * j, p252::to_hash(s[j]).data(), 32);
+  }
+}
+static p252::Channel p252_channel(const uint8_t* digest, uint32_t n_draws) {
+  p252::Channel ch;
+  ch.digest = p252::from_hash(digest);
+  ch.n_draws = n_draws;
+  return ch;
+}
+// One channel operation from the state (digest, n_draws); writes the new
+// digest and returns the new n_draws. op 0: mix_root(bytes), 1: mix_u64(v),
+// 2: mix_u32s(words, n), 3: mix_felts(n QM31 as 4n words), 4: draw n secure
+// felts into out (4n words), 5: draw_u32s n times into out (7n words).
+uint32_t oracle_p252_channel_op(const uint8_t* digest, uint32_t n_draws, uint32_t op, const uint8_t* bytes, uint64_t v,
+                                const uint32_t* words, size_t n, uint32_t* out, uint8_t* digest_out) {
+  p252::Channel ch = p252_channel(digest, n_draws);
+  if (op == 0) ch.mix_root(bytes);
+  else if (op == 1) ch.mix_u64(v);
+  else if (op == 2) ch.mix_u32s(std::vector<uint32_t>(words, words + n));
+  else if (op == 3) {
+    std::vector<std::array<uint32_t, 4>> f(n);
+    for (size_t i = 0; i < n; i++) for (int c = 0; c < 4; c++) f[i][c] = words[4 * i + c];
+    ch.mix_felts(f);
+  } else if (op == 4) {
+    Channel full(MerkleHash::Poseidon252);
+    full.pc = ch;
+    auto f = full.draw_secure_felts(n);
+    for (size_t i = 0; i < n; i++) q_out(f[i], out + 4 * i);
+    ch = full.pc;
+  } else if (op == 5) {
+    for (size_t i = 0; i < n; i++) {
+      auto w = ch.draw_u32s();
+      memcpy(out + 7 * i, w.data(), 28);
+    }
+  }
+  memcpy(digest_out, p252::to_hash(ch.digest).data(), 32);
+  return ch.n_draws;
+}
+uint64_t oracle_p252_grind(const uint8_t* digest, uint32_t pow_bits) { return p252_channel(digest, 0).grind(pow_bits); }
+int oracle_p252_verify_pow(const uint8_t* digest, uint32_t pow_bits, uint64_t nonce) {
+  return p252_channel(digest, 0).verify_pow_nonce(pow_bits, nonce) ? 1 : 0;
+}
+
 // fold_line on LineDomain(half_odds(log_n)); eval/out are QM31 planes.
 void oracle_fold_line(const uint32_t* const* eval, uint32_t log_n, const uint32_t* alpha, uint32_t* const* out) {
   auto v = planes_in(eval, (size_t)1 << log_n);

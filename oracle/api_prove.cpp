@@ -42,9 +42,11 @@ uint32_t oracle_seeded_m31(uint64_t seed, uint64_t col, uint64_t row) { return s
 // Returns 0 on success (proof bytes in out, length in *out_len), 1 if the
 // composition sanity check fails, 2 if the buffer is too small.
 // split_log: composition split (1 = the reference's fixed split).
+// merkle_channel: 0 = Blake2sMerkleChannel, 1 = Poseidon252MerkleChannel
+// (wide_fibonacci/mod.rs:335-379, poseidon/mod.rs:702-785).
 int oracle_prove(uint32_t air, uint32_t log_n, uint32_t n_cols, uint64_t seed, uint32_t input_mode, uint32_t pow_bits,
-                 uint32_t n_queries, uint32_t log_blowup, uint32_t log_last_layer, uint32_t split_log, void* out,
-                 size_t cap, size_t* out_len) {
+                 uint32_t n_queries, uint32_t log_blowup, uint32_t log_last_layer, uint32_t split_log,
+                 uint32_t merkle_channel, void* out, size_t cap, size_t* out_len) {
   PcsConfig cfg;
   cfg.log_last_layer = log_last_layer;
   cfg.pow_bits = pow_bits;
@@ -52,7 +54,7 @@ int oracle_prove(uint32_t air, uint32_t log_n, uint32_t n_cols, uint64_t seed, u
   cfg.log_blowup = log_blowup;
   CommitmentScheme cs;
   cs.config = cfg;
-  Channel ch;
+  Channel ch(merkle_channel ? MerkleHash::Poseidon252 : MerkleHash::Blake2s);
   cs.commit_evals({}, ch);  // empty preprocessed tree
   size_t n = (size_t)1 << log_n;
   AirSpec spec;

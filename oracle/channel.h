@@ -1,5 +1,7 @@
 // ORACLE — test infrastructure only (see fields.h).
-// Blake2s Fiat-Shamir channel, query drawing and proof-of-work.
+// Fiat-Shamir channel (Blake2s, or Poseidon252 when `kind` says so: the
+// MerkleChannel pairs each hasher with its channel), query drawing and
+// proof-of-work.
 // Follows:
 //   crates/stwo/src/core/channel/blake2s.rs:20-140   (digest, n_draws, mix/draw, verify_pow_nonce)
 //   crates/stwo/src/core/vcs/blake2_merkle.rs:53-58  (mix_root = H(digest || root))
@@ -7,43 +9,72 @@
 //   crates/stwo/src/prover/backend/cpu/grind.rs:5-16 (smallest nonce by linear search)
 #pragma once
 #include "blake2s.h"
+#include "felt252.h"
 #include "fields.h"
 
 namespace orc {
 
+// Blake2sMerkleChannel or Poseidon252MerkleChannel (the hasher of every
+// Merkle tree and the channel of the proof).
+enum class MerkleHash { Blake2s, Poseidon252 };
+
 struct Channel {
+  MerkleHash kind = MerkleHash::Blake2s;
   Hash32 digest{};
   uint32_t n_draws = 0;
+  p252::Channel pc;  // the Poseidon252 channel's state
   static constexpr uint32_t POW_PREFIX = 0x12345678u;
+
+  Channel() = default;
+  explicit Channel(MerkleHash k) : kind(k) {}
+  bool p252() const { return kind == MerkleHash::Poseidon252; }
 
   void update_digest(const Hash32& d) { digest = d; n_draws = 0; }
   void mix_root(const Hash32& root) {
+    if (p252()) return pc.mix_root(root.data());
     Blake2s s; s.update(digest.data(), 32); s.update(root.data(), 32);
     update_digest(s.finalize());
   }
   void mix_felts(const std::vector<QM31>& felts) {
+    if (p252()) {
+      std::vector<std::array<uint32_t, 4>> v;
+      for (auto& f : felts) v.push_back({f.coord(0), f.coord(1), f.coord(2), f.coord(3)});
+      return pc.mix_felts(v);
+    }
     Blake2s s; s.update(digest.data(), 32);
     for (auto& f : felts) for (int i = 0; i < 4; i++) s.update_u32(f.coord(i));
     update_digest(s.finalize());
   }
   void mix_u32s(const std::vector<uint32_t>& data) {
+    if (p252()) return pc.mix_u32s(data);
     Blake2s s; s.update(digest.data(), 32);
     for (uint32_t w : data) s.update_u32(w);
     update_digest(s.finalize());
   }
-  void mix_u64(uint64_t v) { mix_u32s({(uint32_t)v, (uint32_t)(v >> 32)}); }
-  std::array<uint32_t, 8> draw_u32s() {
+  void mix_u64(uint64_t v) {
+    if (p252()) return pc.mix_u64(v);
+    mix_u32s({(uint32_t)v, (uint32_t)(v >> 32)});
+  }
+  // 8 words (Blake2s) or 7 (Poseidon252)
+  std::vector<uint32_t> draw_u32s() {
+    if (p252()) return pc.draw_u32s();
     uint8_t in[37];
     memcpy(in, digest.data(), 32);
     for (int i = 0; i < 4; i++) in[32 + i] = (uint8_t)(n_draws >> (8 * i));
     in[36] = 0;
     n_draws++;
     Hash32 h = Blake2s::hash(in, 37);
-    std::array<uint32_t, 8> r;
+    std::vector<uint32_t> r(8);
     for (int i = 0; i < 8; i++) r[i] = hash_word(h, i);
     return r;
   }
   std::array<M31, 8> draw_base_felts() {
+    if (p252()) {
+      auto u = pc.draw_base_felts();
+      std::array<M31, 8> r;
+      for (int i = 0; i < 8; i++) r[i] = M31(u[i]);
+      return r;
+    }
     for (;;) {
       auto u = draw_u32s();
       bool ok = true;
@@ -94,8 +125,12 @@ struct Channel {
     }
     return tz >= n_bits;
   }
-  bool verify_pow_nonce(uint32_t n_bits, uint64_t nonce) const { return check_nonce(pow_prefixed_digest(n_bits), n_bits, nonce); }
+  bool verify_pow_nonce(uint32_t n_bits, uint64_t nonce) const {
+    if (p252()) return pc.verify_pow_nonce(n_bits, nonce);
+    return check_nonce(pow_prefixed_digest(n_bits), n_bits, nonce);
+  }
   uint64_t grind(uint32_t n_bits) const {
+    if (p252()) return pc.grind(n_bits);
     Hash32 pre = pow_prefixed_digest(n_bits);
     for (uint64_t nonce = 0;; nonce++) if (check_nonce(pre, n_bits, nonce)) return nonce;
   }

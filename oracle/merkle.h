@@ -1,14 +1,16 @@
 // ORACLE — test infrastructure only (see fields.h).
-// Blake2s Merkle tree: commit_on_layer, commit, decommit.
+// Merkle tree (Blake2s or Poseidon252 hashes): commit_on_layer, commit, decommit.
 // Follows:
 //   crates/stwo/src/core/vcs/blake2_merkle.rs:18-39       (hash_node)
 //   crates/stwo/src/prover/backend/cpu/blake2s.rs:13-26   (commit_on_layer)
+//   crates/stwo/src/prover/backend/cpu/poseidon252.rs:11-24 (the same with Poseidon252MerkleHasher)
 //   crates/stwo/src/prover/vcs/prover.rs:22-48            (commit: sort by length desc, stable)
 //   crates/stwo/src/prover/vcs/prover.rs:50-210           (decommit: witness order)
 //   crates/stwo/src/prover/backend/mod.rs:70-86           (batch_at_multi row-major order)
 //   crates/stwo/src/prover/backend/cpu/merkle_lifted.rs:12-88 (lifted leaves, next layer)
 #pragma once
 #include "blake2s.h"
+#include "channel.h"
 #include "fields.h"
 #include "circle.h"
 #include <algorithm>
@@ -17,7 +19,10 @@
 
 namespace orc {
 
-inline Hash32 hash_node(const Hash32* left, const Hash32* right, const M31* vals, size_t n) {
+inline Hash32 hash_node(const Hash32* left, const Hash32* right, const M31* vals, size_t n,
+                        MerkleHash kind = MerkleHash::Blake2s) {
+  if (kind == MerkleHash::Poseidon252)
+    return p252::hash_node(left ? left->data() : nullptr, right ? right->data() : nullptr, vals, n);
   Blake2s s;
   if (left) { s.update(left->data(), 32); s.update(right->data(), 32); }
   for (size_t i = 0; i < n; i++) s.update_u32(vals[i].v);
@@ -25,7 +30,8 @@ inline Hash32 hash_node(const Hash32* left, const Hash32* right, const M31* vals
 }
 
 inline std::vector<Hash32> commit_on_layer(uint32_t log_size, const std::vector<Hash32>* prev,
-                                           const std::vector<const std::vector<M31>*>& cols) {
+                                           const std::vector<const std::vector<M31>*>& cols,
+                                           MerkleHash kind = MerkleHash::Blake2s) {
   size_t n = (size_t)1 << log_size;
   std::vector<Hash32> out(n);
 #pragma omp parallel for schedule(static)
@@ -33,8 +39,8 @@ inline std::vector<Hash32> commit_on_layer(uint32_t log_size, const std::vector<
     size_t i = (size_t)ii;
     std::vector<M31> vals(cols.size());
     for (size_t c = 0; c < cols.size(); c++) vals[c] = (*cols[c])[i];
-    if (prev) out[i] = hash_node(&(*prev)[2 * i], &(*prev)[2 * i + 1], vals.data(), vals.size());
-    else out[i] = hash_node(nullptr, nullptr, vals.data(), vals.size());
+    if (prev) out[i] = hash_node(&(*prev)[2 * i], &(*prev)[2 * i + 1], vals.data(), vals.size(), kind);
+    else out[i] = hash_node(nullptr, nullptr, vals.data(), vals.size(), kind);
   }
   return out;
 }
@@ -80,10 +86,11 @@ struct MerkleDecommitment {
 struct MerkleProver {
   std::vector<std::vector<Hash32>> layers;  // layers[i] has 2^i nodes; layers[0] = root
 
-  static MerkleProver commit(const std::vector<const std::vector<M31>*>& columns_in) {
+  static MerkleProver commit(const std::vector<const std::vector<M31>*>& columns_in,
+                             MerkleHash kind = MerkleHash::Blake2s) {
     MerkleProver mp;
     if (columns_in.empty()) {
-      mp.layers.push_back(commit_on_layer(0, nullptr, {}));
+      mp.layers.push_back(commit_on_layer(0, nullptr, {}, kind));
       return mp;
     }
     std::vector<const std::vector<M31>*> cols(columns_in);
@@ -94,7 +101,7 @@ struct MerkleProver {
     for (int ls = (int)max_log; ls >= 0; ls--) {
       std::vector<const std::vector<M31>*> lc;
       while (ci < cols.size() && ilog2(cols[ci]->size()) == (uint32_t)ls) lc.push_back(cols[ci++]);
-      rev.push_back(commit_on_layer((uint32_t)ls, rev.empty() ? nullptr : &rev.back(), lc));
+      rev.push_back(commit_on_layer((uint32_t)ls, rev.empty() ? nullptr : &rev.back(), lc, kind));
     }
     mp.layers.assign(rev.rbegin(), rev.rend());
     return mp;

@@ -80,7 +80,7 @@ struct CommitmentScheme {
     }
     std::vector<const std::vector<M31>*> cols;
     for (auto& p : t.polys) cols.push_back(&p.evals);
-    t.merkle = MerkleProver::commit(cols);
+    t.merkle = MerkleProver::commit(cols, ch.kind);
     ch.mix_root(t.merkle.root());
     trees.push_back(std::move(t));
   }
@@ -167,11 +167,11 @@ inline void split_coords(const std::vector<QM31>& v, std::vector<std::vector<M31
   for (size_t i = 0; i < v.size(); i++)
     for (int c = 0; c < 4; c++) coords[c][i] = M31(v[i].coord(c));
 }
-inline void commit_fri_layer(FriLayer& L) {
+inline void commit_fri_layer(FriLayer& L, MerkleHash kind) {
   split_coords(L.values, L.coords);
   std::vector<const std::vector<M31>*> cols;
   for (auto& c : L.coords) cols.push_back(&c);
-  L.merkle = MerkleProver::commit(cols);
+  L.merkle = MerkleProver::commit(cols, kind);
 }
 
 // compute_decommitment_positions_and_witness_evals (prover/fri.rs:301-330), fold step 1.
@@ -208,7 +208,7 @@ struct FriProverState {
 inline FriProverState fri_commit(Channel& ch, const PcsConfig& cfg, const std::vector<QM31>& column, uint32_t lifting) {
   FriProverState st;
   st.first.values = column;
-  commit_fri_layer(st.first);
+  commit_fri_layer(st.first, ch.kind);
   ch.mix_root(st.first.merkle.root());
   uint32_t log = lifting - 1;
   std::vector<QM31> layer(1u << log);
@@ -220,7 +220,7 @@ inline FriProverState fri_commit(Channel& ch, const PcsConfig& cfg, const std::v
     while (ilog2(layer.size()) > last_log + cfg.fold_step) {
       FriLayer L;
       L.values = layer;
-      commit_fri_layer(L);
+      commit_fri_layer(L, ch.kind);
       ch.mix_root(L.merkle.root());
       alpha = ch.draw_secure_felt();
       layer = fold_line(L.values, domain, alpha);
@@ -230,7 +230,7 @@ inline FriProverState fri_commit(Channel& ch, const PcsConfig& cfg, const std::v
     // last fold (step 1 in every configuration used here)
     FriLayer L;
     L.values = layer;
-    commit_fri_layer(L);
+    commit_fri_layer(L, ch.kind);
     ch.mix_root(L.merkle.root());
     alpha = ch.draw_secure_felt();
     layer = fold_line(L.values, domain, alpha);

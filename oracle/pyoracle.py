@@ -74,7 +74,13 @@ def _declare(L):
     f("oracle_lift_and_accumulate", None, C.c_uint32, PP, U32P, PP)
     f("oracle_eval_at_point", None, U32P, C.c_uint32, U32P, U32P)
     f("oracle_prove", C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32,
-      C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t))
+      C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t))
+    f("oracle_p252_commit_on_layer", None, C.c_uint32, U8P, C.c_uint32, PP, U8P)
+    f("oracle_p252_permute", None, U8P, C.c_size_t, U8P)
+    f("oracle_p252_channel_op", C.c_uint32, U8P, C.c_uint32, C.c_uint32, U8P, C.c_uint64, U32P, C.c_size_t, U32P,
+      U8P)
+    f("oracle_p252_grind", C.c_uint64, U8P, C.c_uint32)
+    f("oracle_p252_verify_pow", C.c_int, U8P, C.c_uint32, C.c_uint64)
     f("oracle_seeded_m31", C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64)
 
 
@@ -212,6 +218,55 @@ def verify_pow(digest: bytes, pow_bits, nonce):
     return bool(lib().oracle_verify_pow(d, pow_bits, nonce))
 
 
+# ---- Poseidon252 (felt252 values as 32 big-endian bytes)
+def p252_commit_on_layer(log_size, prev, cols):
+    """MerkleOps<Poseidon252MerkleHasher>::commit_on_layer: (2^log_size, 32) bytes."""
+    cols = [np.ascontiguousarray(c, dtype=np.uint32) for c in cols]
+    out = np.zeros((1 << log_size) * 32, np.uint8)
+    pp, keep = ptr_array(cols) if cols else (C.cast(None, PP), None)
+    prev_p = None
+    if prev is not None:
+        prev = np.ascontiguousarray(prev, dtype=np.uint8)
+        prev_p = prev.ctypes.data_as(U8P)
+    lib().oracle_p252_commit_on_layer(log_size, prev_p, len(cols), pp, out.ctypes.data_as(U8P))
+    return out.reshape(-1, 32)
+
+
+def p252_permute(states_bytes: bytes):
+    n = len(states_bytes) // 96
+    src = (C.c_uint8 * len(states_bytes)).from_buffer_copy(states_bytes)
+    out = (C.c_uint8 * (96 * n))()
+    lib().oracle_p252_permute(src, n, out)
+    return bytes(out)
+
+
+P252_OPS = {"mix_root": 0, "mix_u64": 1, "mix_u32s": 2, "mix_felts": 3, "draw_secure_felts": 4, "draw_u32s": 5}
+
+
+def p252_channel_op(digest: bytes, n_draws, op, data=b"", v=0, words=(), n=0):
+    """One Poseidon252Channel operation from (digest, n_draws): returns
+    (new digest bytes, new n_draws, output words)."""
+    d = (C.c_uint8 * 32).from_buffer_copy(digest)
+    b = (C.c_uint8 * 32).from_buffer_copy(data.ljust(32, b"\0")[:32])
+    w, wp = u32(list(words) or [0])
+    count = n if op in ("draw_secure_felts", "draw_u32s") else (len(words) // 4 if op == "mix_felts" else len(words))
+    out = np.zeros(max(1, 7 * n, 4 * n), np.uint32)
+    dout = (C.c_uint8 * 32)()
+    nd = lib().oracle_p252_channel_op(d, n_draws, P252_OPS[op], b, v, wp, count, out.ctypes.data_as(U32P), dout)
+    used = 4 * n if op == "draw_secure_felts" else (7 * n if op == "draw_u32s" else 0)
+    return bytes(dout), nd, [int(x) for x in out[:used]]
+
+
+def p252_grind(digest: bytes, pow_bits):
+    d = (C.c_uint8 * 32).from_buffer_copy(digest)
+    return lib().oracle_p252_grind(d, pow_bits)
+
+
+def p252_verify_pow(digest: bytes, pow_bits, nonce):
+    d = (C.c_uint8 * 32).from_buffer_copy(digest)
+    return bool(lib().oracle_p252_verify_pow(d, pow_bits, nonce))
+
+
 def fold_line(eval_q, log_n, alpha):
     ps = planes(eval_q)
     outs = [np.zeros(1 << (log_n - 1), np.uint32) for _ in range(4)]
@@ -294,8 +349,9 @@ def default_split(air):
 
 
 def prove(air, log_n, n_cols=100, seed=0, input_mode=0, pow_bits=10, n_queries=70, log_blowup=1, split_log=None,
-          log_last_layer=0):
-    """Full proof bytes from the CPU restatement; air: 'wide_fibonacci' | 'poseidon'."""
+          log_last_layer=0, merkle_channel="blake2s"):
+    """Full proof bytes from the CPU restatement; air: 'wide_fibonacci' | 'poseidon';
+    merkle_channel: 'blake2s' | 'poseidon252'."""
     if split_log is None:
         split_log = default_split(air)
     L = lib()
@@ -303,7 +359,8 @@ def prove(air, log_n, n_cols=100, seed=0, input_mode=0, pow_bits=10, n_queries=7
     buf = (C.c_uint8 * cap)()
     n = C.c_size_t()
     st = L.oracle_prove(0 if air == "wide_fibonacci" else 1, log_n, n_cols, seed, input_mode, pow_bits, n_queries,
-                        log_blowup, log_last_layer, split_log, C.cast(buf, C.c_void_p), cap, C.byref(n))
+                        log_blowup, log_last_layer, split_log, 1 if merkle_channel == "poseidon252" else 0,
+                        C.cast(buf, C.c_void_p), cap, C.byref(n))
     if st == 1:
         raise ConstraintsNotSatisfied("composition OODS value does not match the constraints")
     if st != 0:

@@ -258,3 +258,90 @@ def test_poseidon252_permutation_is_a_bijection_sample():
     outs = {tuple(PS.permute([i, 2 * i + 1, 3])) for i in range(32)}
     assert len(outs) == 32
     assert all(0 <= v < PS.P for o in outs for v in o)
+
+
+# ---------------------------------------- Poseidon252 in the C++ oracle prover
+def _felt_bytes(v):
+    return int(v).to_bytes(32, "big")
+
+
+def test_cpp_poseidon252_known_answers():
+    """The C++ restatement used by the oracle prover reproduces the
+    reference's hash_node and channel vectors."""
+    for case in GOLDEN["poseidon252_hash_node"]:
+        cols = [np.array([v], np.uint32) for v in case["columns"]]
+        prev = None
+        if case["children"] is not None:
+            prev = np.frombuffer(b"".join(_felt_bytes(c) for c in case["children"]), np.uint8)
+        got = O.p252_commit_on_layer(0, prev, cols)
+        assert int.from_bytes(bytes(got[0]), "big") == int(case["hash"])
+    zero = _felt_bytes(0)
+    d, nd, _ = O.p252_channel_op(zero, 0, "mix_u64", v=GOLDEN["poseidon252_channel_mix_u64"]["value"])
+    assert int.from_bytes(d, "big") == int(GOLDEN["poseidon252_channel_mix_u64"]["digest"], 16) and nd == 0
+    d, nd, _ = O.p252_channel_op(zero, 0, "mix_u32s", words=GOLDEN["poseidon252_channel_mix_u32s"]["words"])
+    assert int.from_bytes(d, "big") == int(GOLDEN["poseidon252_channel_mix_u32s"]["digest"], 16)
+
+
+def test_cpp_poseidon252_matches_python_restatement():
+    """Permutations, Merkle layers (0..17 columns, with and without children)
+    and a random script of channel operations agree with the pure-Python
+    restatement."""
+    import poseidon252 as PS
+    rng = np.random.default_rng(3)
+    states = [[0, 0, 0], [PS.P - 1] * 3] + [[int.from_bytes(rng.bytes(32), "big") % PS.P for _ in range(3)]
+                                            for _ in range(6)]
+    out = O.p252_permute(b"".join(_felt_bytes(v) for s in states for v in s))
+    assert [int.from_bytes(out[32 * i:32 * i + 32], "big") for i in range(3 * len(states))] == \
+        [v for s in states for v in PS.permute(s)]
+    for n_cols in [0, 1, 7, 8, 9, 17]:
+        for with_prev in [False, True]:
+            n = 8
+            cols = [rng.integers(0, PS.M31, n, dtype=np.int64).astype(np.uint32) for _ in range(n_cols)]
+            prev = [int.from_bytes(rng.bytes(32), "big") % PS.P for _ in range(2 * n)] if with_prev else None
+            pb = np.frombuffer(b"".join(_felt_bytes(v) for v in prev), np.uint8) if prev else None
+            if n_cols == 0 and not with_prev:
+                got = O.p252_commit_on_layer(0, None, [])
+                assert int.from_bytes(bytes(got[0]), "big") == PS.hash_node(None, [])
+                continue
+            got = O.p252_commit_on_layer(3, pb, cols)
+            assert [int.from_bytes(bytes(r), "big") for r in got] == PS.commit_on_layer(3, prev, cols)
+    ch, d, nd = PS.Channel(), _felt_bytes(0), 0
+    script = ["mix_root", "draw_secure_felts", "mix_felts", "draw_u32s", "mix_u64", "draw_secure_felts",
+              "mix_u32s", "draw_u32s", "draw_secure_felts"]
+    for op in script:
+        if op == "mix_root":
+            r = int.from_bytes(rng.bytes(32), "big") % PS.P
+            d, nd, _ = O.p252_channel_op(d, nd, op, data=_felt_bytes(r))
+            ch.mix_root(r)
+        elif op == "mix_u64":
+            v = int(rng.integers(0, 2 ** 63))
+            d, nd, _ = O.p252_channel_op(d, nd, op, v=v)
+            ch.mix_u64(v)
+        elif op == "mix_u32s":
+            w = [int(x) for x in rng.integers(0, 2 ** 32, 11, dtype=np.uint64)]
+            d, nd, _ = O.p252_channel_op(d, nd, op, words=w)
+            ch.mix_u32s(w)
+        elif op == "mix_felts":
+            f = [tuple(int(x) for x in rng.integers(0, PS.M31, 4)) for _ in range(5)]
+            d, nd, _ = O.p252_channel_op(d, nd, op, words=[x for q in f for x in q])
+            ch.mix_felts(f)
+        elif op == "draw_secure_felts":
+            d, nd, got = O.p252_channel_op(d, nd, op, n=3)
+            assert got == [x for q in ch.draw_secure_felts(3) for x in q]
+        else:
+            d, nd, got = O.p252_channel_op(d, nd, op, n=2)
+            assert got == ch.draw_u32s() + ch.draw_u32s()
+        assert int.from_bytes(d, "big") == ch.digest and nd == ch.n_draws, op
+    for bits in [0, 3, 8]:
+        nonce = O.p252_grind(d, bits)
+        assert nonce == PS.Channel(int.from_bytes(d, "big")).grind(bits)
+        assert O.p252_verify_pow(d, bits, nonce)
+
+
+def test_cpp_oracle_proves_with_poseidon252_channel():
+    """The oracle prover runs with Poseidon252MerkleChannel; the proof differs
+    from the Blake2s one and is deterministic."""
+    a = O.prove("wide_fibonacci", 6, n_cols=8, merkle_channel="poseidon252")
+    b = O.prove("wide_fibonacci", 6, n_cols=8, merkle_channel="poseidon252")
+    c = O.prove("wide_fibonacci", 6, n_cols=8)
+    assert a == b and a != c
