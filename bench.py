@@ -410,15 +410,17 @@ def run_kernels(args, world, rank, local):
 PROOF_SIZES = {"poseidon": 18, "wide_fibonacci": 16}
 
 
-def proof_metric(workload):
+def proof_metric(workload, channel="blake2s"):
+    suffix = "" if channel == "blake2s" else ", Poseidon252 channel"
     if workload == "poseidon":
-        return "Poseidon2 2^18 proof ms"
-    return "Wide-Fibonacci 2^16x100 proof ms"
+        return "Poseidon2 2^18 proof ms" + suffix
+    return "Wide-Fibonacci 2^16x100 proof ms" + suffix
 
 
-def proof_config(workload, log_n):
+def proof_config(workload, log_n, channel="blake2s"):
     base = {"pcs": "pow_bits=10, FriConfig(log_last_layer=0, log_blowup=1, n_queries=70, fold_step=1)",
-            "channel": "Blake2s", "inputs": "seeded uniform M31 states (mode 1)",
+            "channel": "Blake2s" if channel == "blake2s" else "Poseidon252 (Poseidon252MerkleChannel)",
+            "inputs": "seeded uniform M31 states (mode 1)",
             "l2": "each proof streams >1 GB through HBM (inputs larger than L2)"}
     if workload == "poseidon":
         base.update({"workload": "Poseidon2 AIR full proof, 2^%d instances (one per row), width 16, 8 full + 14 "
@@ -428,7 +430,7 @@ def proof_config(workload, log_n):
     return base
 
 
-def cpu_proof_sample(workload, threads, log_target):
+def cpu_proof_sample(workload, threads, log_target, channel="blake2s"):
     """Oracle (C++ restatement of the reference's CPU prover, all host
     threads): one proof of the full-size workload (about 2 s for Poseidon2
     2^18 on 16 threads). Returns (ms, desc)."""
@@ -437,9 +439,9 @@ def cpu_proof_sample(workload, threads, log_target):
     O.set_threads(threads)
     air = "poseidon" if workload == "poseidon" else "wide_fibonacci"
     t0 = time.perf_counter()
-    O.prove(air, log_target, n_cols=100, seed=0, input_mode=1)
+    O.prove(air, log_target, n_cols=100, seed=0, input_mode=1, merkle_channel=channel)
     dt = time.perf_counter() - t0
-    return 1e3 * dt, "oracle %s proof at 2^%d, full size (%.2f s)" % (air, log_target, dt)
+    return 1e3 * dt, "oracle %s proof at 2^%d (%s channel), full size (%.2f s)" % (air, log_target, channel, dt)
 
 
 def cpu_mix_sample(jobs, threads, budget_s=20.0):
@@ -471,10 +473,13 @@ def run_proof(args, world, rank, local):
     stream = torch.cuda.current_stream()
     tuning = fft_autotune(args, 22)
 
+    mc = args.merkle_channel
+
     def one(mode=G.INPUT_SEEDED, host=None):
         if wl == "poseidon":
-            return G.prove_poseidon(log_n, seed=rank, input_mode=mode, host_inputs=host, ctx=ctx)
-        return G.prove_wide_fibonacci(log_n, 100, seed=rank, input_mode=mode, host_inputs=host, ctx=ctx)
+            return G.prove_poseidon(log_n, seed=rank, input_mode=mode, host_inputs=host, ctx=ctx, merkle_channel=mc)
+        return G.prove_wide_fibonacci(log_n, 100, seed=rank, input_mode=mode, host_inputs=host, ctx=ctx,
+                                      merkle_channel=mc)
 
     for _ in range(args.warmup):
         proof = one()
@@ -525,15 +530,16 @@ def run_proof(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        ms, desc = cpu_proof_sample(wl, threads, log_n)
+        ms, desc = cpu_proof_sample(wl, threads, log_n, mc)
         cpu = {"value": round(ms, 1), "unit": "ms", "cores": threads, "kind": "port", "sample": desc}
     out = {
-        "metric": proof_metric(wl) if log_n == PROOF_SIZES[wl] else proof_metric(wl).replace(
+        "metric": proof_metric(wl, mc) if log_n == PROOF_SIZES[wl] else proof_metric(wl, mc).replace(
             str(PROOF_SIZES[wl]), str(log_n)),
         "value": round(value, 3), "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_per_step, 3), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 (M31/QM31 integer arithmetic)", "data": "synthetic: seeded uniform M31",
-        "config": dict(proof_config(wl, log_n), parallelism="independent proofs x%d" % world, fft_tuning=tuning),
+        "config": dict(proof_config(wl, log_n, mc), parallelism="independent proofs x%d" % world,
+                       fft_tuning=tuning),
         "proofs_per_s": round(1e3 / value, 2), "proof_bytes": len(proof),
         "latency_ms": {"p50": round(statistics.median(lat), 3), "max": round(max(lat), 3)},
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(host.nbytes),
@@ -543,7 +549,7 @@ def run_proof(args, world, rank, local):
     }
     if cpu:
         out["cpu_baseline"] = cpu
-    rl = proof_roofline(args, log_n, wl, ctx)
+    rl = proof_roofline(args, log_n, wl, ctx) if mc == "blake2s" else None
     if rl:
         out["roofline"] = rl
     return out
@@ -790,20 +796,21 @@ def run_reference(args, world, rank):
             "e2e": {"value": round(v, 3), "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
     log_n = args.log_n or PROOF_SIZES[args.workload]
+    mc = args.merkle_channel
     for _ in range(min(args.warmup, 1)):
-        cpu_proof_sample(args.workload, threads, log_n)
+        cpu_proof_sample(args.workload, threads, log_n, mc)
     vals, desc = [], ""
     steps = max(1, min(args.steps, 3))
     for _ in range(steps):
-        ms, desc = cpu_proof_sample(args.workload, threads, log_n)
+        ms, desc = cpu_proof_sample(args.workload, threads, log_n, mc)
         vals.append(ms)
     v = statistics.mean(vals)
     return {
-        "impl": "reference", "metric": proof_metric(args.workload), "value": round(v, 1), "unit": "ms",
+        "impl": "reference", "metric": proof_metric(args.workload, mc), "value": round(v, 1), "unit": "ms",
         "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": round(v, 1),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32 (M31/QM31 integer arithmetic)", "data": "synthetic: seeded uniform M31",
-        "config": dict(proof_config(args.workload, log_n), parallelism="cpu threads"),
+        "config": dict(proof_config(args.workload, log_n, mc), parallelism="cpu threads"),
         "cpu_baseline": {"value": round(v, 1), "unit": "ms", "cores": threads, "kind": "port", "sample": desc},
         "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -868,6 +875,8 @@ def main():
                     choices=["poseidon", "wide_fibonacci", "kernels", "batched", "served"])
     ap.add_argument("--workers", type=int, default=16, help="server workers (batched / served)")
     ap.add_argument("--load", type=float, default=2.0, help="served: arrival rate / sequential proof rate")
+    ap.add_argument("--merkle-channel", default="blake2s", choices=["blake2s", "poseidon252"],
+                    help="proof workloads: Blake2sMerkleChannel or Poseidon252MerkleChannel")
     ap.add_argument("--log-n", type=int, default=0, help="override the proof size (log instances / rows)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fft-autotune", default="on", choices=["on", "off"],

@@ -269,6 +269,31 @@ int gs_prove_poseidon(gs_ctx* ctx, uint32_t log_n_instances, uint64_t seed, uint
                       const uint32_t* host_inputs, uint32_t composition_log_split, const gs_pcs_config* config,
                       uint8_t* proof, size_t capacity, size_t* proof_len);
 
+/* The same two proofs over Poseidon252MerkleChannel: every Merkle tree hashed
+ * with Poseidon252MerkleHasher, the Fiat-Shamir transcript a
+ * Poseidon252Channel, the proof of work GrindOps<Poseidon252Channel>.
+ * cuda_prove_wide_fibonacci_poseidon (crates/examples/src/wide_fibonacci/
+ * mod.rs:335-379) and cuda_prove_poseidon_poseidon (crates/examples/src/
+ * poseidon/mod.rs:702-785). Arguments as above; hashes in the proof are the
+ * felt252 values as 32 big-endian bytes. */
+int gs_prove_wide_fibonacci_poseidon252(gs_ctx* ctx, uint32_t log_n_rows, uint32_t n_columns, uint64_t seed,
+                                        uint32_t input_mode, const uint32_t* host_inputs,
+                                        const gs_pcs_config* config, uint8_t* proof, size_t capacity,
+                                        size_t* proof_len);
+int gs_prove_poseidon_poseidon252(gs_ctx* ctx, uint32_t log_n_instances, uint64_t seed, uint32_t input_mode,
+                                  const uint32_t* host_inputs, uint32_t composition_log_split,
+                                  const gs_pcs_config* config, uint8_t* proof, size_t capacity, size_t* proof_len);
+
+/* Poseidon252Channel (core/channel/poseidon252.rs:18-155) on the host, the
+ * channel the Poseidon252 proofs use; no context and no device work. From
+ * the state (digest as 32 big-endian bytes, n_draws), op 0: mix_root(bytes,
+ * 32 bytes; Poseidon252MerkleChannel::mix_root), 1: mix_u64(value), 3:
+ * mix_felts(n QM31 values, 4n words), 4: draw_secure_felts(n) into out (4n
+ * words), 5: draw_u32s n times into out (7n words). Writes the new state. */
+int gs_poseidon252_channel_op(const uint8_t digest[32], uint32_t n_draws, uint32_t op, const uint8_t* bytes,
+                              uint64_t value, const uint32_t* words, size_t n, uint32_t* out, uint8_t digest_out[32],
+                              uint32_t* n_draws_out);
+
 /* ------------------------------------------------------------- serving */
 /* A proof server (no reference counterpart: the reference proves one proof at
  * a time on the default stream). n_workers threads, each with its own CUDA

@@ -417,11 +417,12 @@ static int run_prove(gs_ctx* ctx, prover::ProveRequest& req, const gs_pcs_config
   return OK;
 }
 
-int gs_prove_wide_fibonacci(gs_ctx* ctx, uint32_t log_n_rows, uint32_t n_columns, uint64_t seed, uint32_t input_mode,
-                            const uint32_t* host_inputs, const gs_pcs_config* config, uint8_t* proof,
-                            size_t capacity, size_t* proof_len) {
+static int prove_wf(gs_ctx* ctx, uint32_t log_n_rows, uint32_t n_columns, uint64_t seed, uint32_t input_mode,
+                    const uint32_t* host_inputs, const gs_pcs_config* config, uint8_t* proof, size_t capacity,
+                    size_t* proof_len, uint32_t merkle_channel) {
   prover::ProveRequest req;
   req.air = 0;
+  req.merkle_channel = merkle_channel;
   req.log_n = log_n_rows;
   req.n_cols = n_columns;
   req.seed = seed;
@@ -432,17 +433,79 @@ int gs_prove_wide_fibonacci(gs_ctx* ctx, uint32_t log_n_rows, uint32_t n_columns
   return run_prove(ctx, req, config, proof, capacity, proof_len);
 }
 
-int gs_prove_poseidon(gs_ctx* ctx, uint32_t log_n_instances, uint64_t seed, uint32_t input_mode,
-                      const uint32_t* host_inputs, uint32_t composition_log_split, const gs_pcs_config* config,
-                      uint8_t* proof, size_t capacity, size_t* proof_len) {
+static int prove_p2(gs_ctx* ctx, uint32_t log_n_instances, uint64_t seed, uint32_t input_mode,
+                    const uint32_t* host_inputs, uint32_t composition_log_split, const gs_pcs_config* config,
+                    uint8_t* proof, size_t capacity, size_t* proof_len, uint32_t merkle_channel) {
   prover::ProveRequest req;
   req.air = 1;
+  req.merkle_channel = merkle_channel;
   req.log_n = log_n_instances;
   req.seed = seed;
   req.input_mode = input_mode;
   req.host_inputs = host_inputs;
   req.split_log = composition_log_split;
   return run_prove(ctx, req, config, proof, capacity, proof_len);
+}
+
+int gs_prove_wide_fibonacci(gs_ctx* ctx, uint32_t log_n_rows, uint32_t n_columns, uint64_t seed, uint32_t input_mode,
+                            const uint32_t* host_inputs, const gs_pcs_config* config, uint8_t* proof,
+                            size_t capacity, size_t* proof_len) {
+  return prove_wf(ctx, log_n_rows, n_columns, seed, input_mode, host_inputs, config, proof, capacity, proof_len, 0);
+}
+int gs_prove_wide_fibonacci_poseidon252(gs_ctx* ctx, uint32_t log_n_rows, uint32_t n_columns, uint64_t seed,
+                                        uint32_t input_mode, const uint32_t* host_inputs,
+                                        const gs_pcs_config* config, uint8_t* proof, size_t capacity,
+                                        size_t* proof_len) {
+  return prove_wf(ctx, log_n_rows, n_columns, seed, input_mode, host_inputs, config, proof, capacity, proof_len, 1);
+}
+int gs_prove_poseidon(gs_ctx* ctx, uint32_t log_n_instances, uint64_t seed, uint32_t input_mode,
+                      const uint32_t* host_inputs, uint32_t composition_log_split, const gs_pcs_config* config,
+                      uint8_t* proof, size_t capacity, size_t* proof_len) {
+  return prove_p2(ctx, log_n_instances, seed, input_mode, host_inputs, composition_log_split, config, proof,
+                  capacity, proof_len, 0);
+}
+int gs_prove_poseidon_poseidon252(gs_ctx* ctx, uint32_t log_n_instances, uint64_t seed, uint32_t input_mode,
+                                  const uint32_t* host_inputs, uint32_t composition_log_split,
+                                  const gs_pcs_config* config, uint8_t* proof, size_t capacity, size_t* proof_len) {
+  return prove_p2(ctx, log_n_instances, seed, input_mode, host_inputs, composition_log_split, config, proof,
+                  capacity, proof_len, 1);
+}
+
+// Poseidon252Channel on the host (no device work): one operation from the
+// state (digest, n_draws).
+int gs_poseidon252_channel_op(const uint8_t digest[32], uint32_t n_draws, uint32_t op, const uint8_t* bytes,
+                              uint64_t value, const uint32_t* words, size_t n, uint32_t* out, uint8_t digest_out[32],
+                              uint32_t* n_draws_out) {
+  GS_REQUIRE(digest && digest_out && n_draws_out, "null digest");
+  GS_REQUIRE(op <= 5 && op != 2, "channel operation must be 0, 1, 3, 4 or 5");
+  GS_REQUIRE(op != 0 || bytes, "null root");
+  GS_REQUIRE(op != 3 || n == 0 || words, "null words");
+  GS_REQUIRE((op != 4 && op != 5) || n == 0 || out, "null output");
+  host::Channel ch;
+  ch.p252 = true;
+  memcpy(ch.digest.data(), digest, 32);
+  ch.n_draws = n_draws;
+  if (op == 0) {
+    host::Hash r;
+    memcpy(r.data(), bytes, 32);
+    ch.mix_root(r);
+  } else if (op == 1) {
+    ch.mix_u64(value);
+  } else if (op == 3) {
+    std::vector<qm31> f(n);
+    for (size_t i = 0; i < n; i++) f[i] = qm_make(words[4 * i], words[4 * i + 1], words[4 * i + 2], words[4 * i + 3]);
+    ch.mix_felts(f);
+  } else if (op == 4) {
+    auto f = ch.draw_felts(n);
+    for (size_t i = 0; i < n; i++) {
+      out[4 * i] = f[i].x.a; out[4 * i + 1] = f[i].x.b; out[4 * i + 2] = f[i].y.a; out[4 * i + 3] = f[i].y.b;
+    }
+  } else {
+    for (size_t i = 0; i < n; i++) ch.draw_words(out + 7 * i);
+  }
+  memcpy(digest_out, ch.digest.data(), 32);
+  *n_draws_out = ch.n_draws;
+  return OK;
 }
 
 // ------------------------------------------------------------ lifted Merkle

@@ -1,8 +1,10 @@
 // Host-side protocol pieces of the GPU prover: Blake2s hashing, the
-// Fiat-Shamir channel, circle points over QM31 and proof serialisation.
+// Fiat-Shamir channel (Blake2s, or Poseidon252 for Poseidon252MerkleChannel),
+// circle points over QM31 and proof serialisation.
 //
 // Semantics follow the reference:
 //   crates/stwo/src/core/channel/blake2s.rs:20-140   (channel: mix, draw, pow prefix)
+//   crates/stwo/src/core/channel/poseidon252.rs:18-155 (the Poseidon252 channel)
 //   crates/stwo/src/core/vcs/blake2_merkle.rs:53-58  (mix_root)
 //   crates/stwo/src/core/queries.rs:11-28            (draw_queries)
 //   crates/stwo/src/core/circle.rs:12-214            (points, random point, generators)
@@ -15,6 +17,7 @@
 #include <vector>
 #include "../blake2s.cuh"
 #include "../m31.cuh"
+#include "felt252_host.h"
 
 namespace gs {
 namespace host {
@@ -73,38 +76,77 @@ inline uint32_t word(const Hash& h, int i) {
   return (uint32_t)h[4 * i] | ((uint32_t)h[4 * i + 1] << 8) | ((uint32_t)h[4 * i + 2] << 16) | ((uint32_t)h[4 * i + 3] << 24);
 }
 
+// Blake2sChannel, or Poseidon252Channel when `p252` is set (then `digest`
+// holds the felt252 digest as 32 big-endian bytes).
 struct Channel {
   Hash digest{};
   uint32_t n_draws = 0;
+  bool p252 = false;
   void set(const Hash& d) { digest = d; n_draws = 0; }
-  void mix_root(const Hash& root) { Hasher s; s.update(digest.data(), 32); s.update(root.data(), 32); set(s.finish()); }
+  p252::F fdigest() const { return p252::from_bytes(digest.data()); }
+  void set_f(const p252::F& f) { set(p252::to_bytes(f)); }
+  void mix_root(const Hash& root) {
+    if (p252) return set_f(p252::hash2(fdigest(), p252::from_bytes(root.data())));
+    Hasher s; s.update(digest.data(), 32); s.update(root.data(), 32); set(s.finish());
+  }
   void mix_felts(const std::vector<qm31>& f) {
+    if (p252) {  // two QM31 per felt252: 1, then the 8 coordinates shifted in by 31 bits
+      std::vector<p252::F> res = {fdigest()};
+      for (size_t i = 0; i < f.size(); i += 2) {
+        uint64_t v[4] = {1, 0, 0, 0};
+        for (size_t k = i; k < i + 2 && k < f.size(); k++)
+          for (uint32_t c : {f[k].x.a, f[k].x.b, f[k].y.a, f[k].y.b}) {
+            for (int w = 3; w > 0; w--) v[w] = (v[w] << 31) | (v[w - 1] >> 33);
+            v[0] = (v[0] << 31) | c;
+          }
+        res.push_back(p252::from_int(v));
+      }
+      return set_f(p252::hash_many(res));
+    }
     Hasher s;
     s.update(digest.data(), 32);
     for (auto& q : f) { s.u32(q.x.a); s.u32(q.x.b); s.u32(q.y.a); s.u32(q.y.b); }
     set(s.finish());
   }
   void mix_u64(uint64_t v) {
+    if (p252) return set_f(p252::hash2(fdigest(), p252::from_u64(v)));
     Hasher s;
     s.update(digest.data(), 32);
     s.u32((uint32_t)v);
     s.u32((uint32_t)(v >> 32));
     set(s.finish());
   }
-  std::array<uint32_t, 8> draw_u32s() {
+  // Words of one draw: 8 (Blake2s) or 7 (Poseidon252, 32-bit chunks of the
+  // drawn felt252, low first); returns the count.
+  int draw_words(uint32_t out[8]) {
+    if (p252) {
+      uint64_t v[4];
+      p252::draw_int(fdigest(), n_draws++, v);
+      for (int i = 0; i < 7; i++) out[i] = (uint32_t)p252::take_bits(v, 32);
+      return 7;
+    }
     uint8_t in[37];
     memcpy(in, digest.data(), 32);
     for (int i = 0; i < 4; i++) in[32 + i] = (uint8_t)(n_draws >> (8 * i));
     in[36] = 0;
     n_draws++;
     Hash h = hash_bytes(in, 37);
-    std::array<uint32_t, 8> r;
-    for (int i = 0; i < 8; i++) r[i] = word(h, i);
-    return r;
+    for (int i = 0; i < 8; i++) out[i] = word(h, i);
+    return 8;
   }
   std::array<uint32_t, 8> draw_base() {
+    std::array<uint32_t, 8> u;
+    if (p252) {  // 31-bit chunks, each reduced mod P
+      uint64_t v[4];
+      p252::draw_int(fdigest(), n_draws++, v);
+      for (int i = 0; i < 8; i++) {
+        uint32_t x = (uint32_t)p252::take_bits(v, 31);
+        u[i] = x == P ? 0 : x;
+      }
+      return u;
+    }
     for (;;) {
-      auto u = draw_u32s();
+      draw_words(u.data());
       bool ok = true;
       for (auto x : u) ok = ok && x < 2 * P;
       if (ok) {
@@ -123,7 +165,7 @@ struct Channel {
     }
     return r;
   }
-  // H(POW_PREFIX, 0^12, digest, pow_bits) as 8 words (the grind kernel's input).
+  // H(POW_PREFIX, 0^12, digest, pow_bits) as 8 words (the Blake2s grind kernel's input).
   std::array<uint32_t, 8> pow_prefixed(uint32_t pow_bits) const {
     Hasher s;
     s.u32(0x12345678u);
@@ -142,10 +184,9 @@ inline std::vector<size_t> draw_queries(Channel& ch, uint32_t log_domain, size_t
   std::vector<size_t> r;
   uint32_t mask = (uint32_t)((1ull << log_domain) - 1);
   while (r.size() < n) {
-    auto w = ch.draw_u32s();
-    for (auto x : w) {
-      if (r.size() < n) r.push_back(x & mask);
-    }
+    uint32_t w[8];
+    int k = ch.draw_words(w);
+    for (int i = 0; i < k && r.size() < n; i++) r.push_back(w[i] & mask);
   }
   return r;
 }

@@ -7,6 +7,72 @@ namespace gs {
 void fft_set_columns_aligned(bool aligned);
 namespace prover {
 
+static int finish_last_layer(Prover& pv, const uint32_t* h, uint32_t log, std::vector<qm31>& last_coeffs);
+
+// FRI commit with Poseidon252MerkleChannel (prover/fri.rs:99-199 over
+// MerkleProver<Poseidon252MerkleHasher>): per layer, the leaves (the 4
+// coordinates packed into one felt252 each) and node layers of its tree, then
+// its root back to the host channel (mix_root, draw_secure_felt) for the fold
+// into the next layer.
+static int fri_commit_p252(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first,
+                           std::vector<FriLayerDev>& inner, std::vector<qm31>& last_coeffs,
+                           const std::function<void()>& while_busy) {
+  cudaStream_t st = pv.st;
+  const uint32_t last_log = pv.cfg.log_last_layer + pv.cfg.log_blowup;
+  GS_REQUIRE(lifting >= last_log + 1, "FRI: lifting domain below the last layer");
+  auto planes_of = [&](FriLayerDev& L, uint32_t log) -> int {
+    L.log = log;
+    for (int c = 0; c < 4; c++) GS_TRY(pv.A.alloc_n((size_t)1 << log, &L.planes[c]));
+    return OK;
+  };
+  bool busy_done = false;
+  auto commit_layer = [&](FriLayerDev& L) -> int {
+    L.layers.assign(L.log + 1, nullptr);
+    for (uint32_t k = 0; k <= L.log; k++) GS_TRY(pv.A.alloc_n((size_t)8 << k, &L.layers[k]));
+    std::vector<const uint32_t*> cols = {L.planes[0], L.planes[1], L.planes[2], L.planes[3]};
+    const uint32_t* const* tab = nullptr;
+    GS_TRY(pv.table(cols, &tab));
+    GS_TRY(poseidon252_commit_on_layer(st, L.log, nullptr, tab, 4, (uint8_t*)L.layers[L.log]));
+    for (int k = (int)L.log - 1; k >= 0; k--)
+      GS_TRY(poseidon252_commit_on_layer(st, (uint32_t)k, (const uint8_t*)L.layers[k + 1], nullptr, 0,
+                                         (uint8_t*)L.layers[k]));
+    if (!busy_done && while_busy) while_busy();  // overlaps the first tree
+    busy_done = true;
+    GS_TRY(pv.ctx.read_back(L.layers[0], 32, L.root.data()));
+    pv.ch.mix_root(L.root);
+    return OK;
+  };
+  first.log = lifting;
+  for (int c = 0; c < 4; c++) first.planes[c] = quot[c];
+  GS_TRY(commit_layer(first));
+  qm31 alpha = pv.ch.draw_felt();
+  FriLayerDev cur;
+  GS_TRY(planes_of(cur, lifting - 1));
+  for (int c = 0; c < 4; c++) GS_CUDA_TRY(cudaMemsetAsync(cur.planes[c], 0, (size_t)4 << cur.log, st));
+  GS_TRY(fold_circle_into_line_fused(st, CPlanes{{quot[0], quot[1], quot[2], quot[3]}}, lifting, alpha,
+                                     Planes{{cur.planes[0], cur.planes[1], cur.planes[2], cur.planes[3]}}, pv.itw,
+                                     pv.tw_log, nullptr));
+  while (cur.log > last_log) {
+    GS_TRY(commit_layer(cur));
+    alpha = pv.ch.draw_felt();
+    FriLayerDev next;
+    GS_TRY(planes_of(next, cur.log - 1));
+    GS_TRY(fold_line_fused(st, CPlanes{{cur.planes[0], cur.planes[1], cur.planes[2], cur.planes[3]}}, cur.log, alpha,
+                           Planes{{next.planes[0], next.planes[1], next.planes[2], next.planes[3]}}, pv.itw,
+                           pv.tw_log, nullptr));
+    inner.push_back(std::move(cur));
+    cur = std::move(next);
+  }
+  const size_t n = (size_t)1 << cur.log;
+  uint32_t* d_last = nullptr;
+  GS_TRY(pv.A.alloc_n(4 * n, &d_last));
+  for (int c = 0; c < 4; c++)
+    GS_CUDA_TRY(cudaMemcpyAsync(d_last + c * n, cur.planes[c], 4 * n, cudaMemcpyDeviceToDevice, st));
+  std::vector<uint32_t> h(4 * n);
+  GS_TRY(pv.ctx.read_back(d_last, 16 * n, h.data()));
+  return finish_last_layer(pv, h.data(), cur.log, last_coeffs);
+}
+
 // FRI commit (prover/fri.rs:99-199) on the combined quotient planes (2^lifting).
 //
 // The whole phase is enqueued without a host round trip: each layer's Merkle
@@ -19,6 +85,7 @@ namespace prover {
 int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first,
                       std::vector<FriLayerDev>& inner, std::vector<qm31>& last_coeffs,
                       const std::function<void()>& while_busy) {
+  if (pv.ch.p252) return fri_commit_p252(pv, quot, lifting, first, inner, last_coeffs, while_busy);
   cudaStream_t st = pv.st;
   const uint32_t last_log = pv.cfg.log_last_layer + pv.cfg.log_blowup;
   GS_REQUIRE(lifting >= last_log + 1, "FRI: lifting domain below the last layer");
@@ -142,13 +209,19 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
     if (r == 0) first.root = root;
     else inner[r - 1].root = root;
   }
-  // last layer: 2^last_log values -> line polynomial, degree check, mix
+  return finish_last_layer(pv, h.data(), cur.log, last_coeffs);
+}
+
+// The last FRI layer (4 planes of 2^log values, host memory) into the line
+// polynomial's coefficients: interpolation, degree check, mix into the channel.
+static int finish_last_layer(Prover& pv, const uint32_t* h, uint32_t log, std::vector<qm31>& last_coeffs) {
+  const size_t n = (size_t)1 << log;
   std::vector<qm31> vals(n);
   for (size_t i = 0; i < n; i++) vals[i] = qm_make(h[i], h[n + i], h[2 * n + i], h[3 * n + i]);
-  std::vector<qm31> coeffs = line_interpolate_host(vals, cur.log);
+  std::vector<qm31> coeffs = line_interpolate_host(vals, log);
   // into ordered coefficients (bit reverse), keep the degree bound, back
   std::vector<qm31> ordered(n);
-  for (size_t i = 0; i < n; i++) ordered[host::bitrev(i, cur.log)] = coeffs[i];
+  for (size_t i = 0; i < n; i++) ordered[host::bitrev(i, log)] = coeffs[i];
   size_t bound = (size_t)1 << pv.cfg.log_last_layer;
   for (size_t i = bound; i < n; i++)
     if (!qm_eq(ordered[i], qm_zero())) {
@@ -185,6 +258,8 @@ void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::
 int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_bytes, ProveStats* stats) {
   PcsConfig cfg = req.cfg;
   Prover pv(ctx, cfg);
+  GS_REQUIRE(req.merkle_channel <= 1, "merkle channel must be 0 (Blake2s) or 1 (Poseidon252)");
+  pv.ch.p252 = req.merkle_channel == 1;
   pv.mark("start");
   cudaStream_t st = ctx.stream;
   AirHost air;

@@ -14,6 +14,7 @@ struct ProveRequest {
   uint32_t input_mode = 0;   // 0 reference rule, 1 seeded, 2 host inputs
   const uint32_t* host_inputs = nullptr;  // mode 2: WF a,b columns; Poseidon 16 state columns
   uint32_t split_log = 1;    // composition split
+  uint32_t merkle_channel = 0;  // 0 Blake2sMerkleChannel, 1 Poseidon252MerkleChannel
   PcsConfig cfg;
   // Optional caller buffer: when the proof fits, it is serialised straight
   // into it (ProveStats::in_out_buf) and the string stays untouched.

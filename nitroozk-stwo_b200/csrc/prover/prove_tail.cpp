@@ -227,10 +227,17 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   std::vector<qm31> last;
   GS_TRY(fri_commit(pv, quot, lifting, first, inner, last, sanity));
   pv.mark("fri_commit");
-  auto pre = pv.ch.pow_prefixed(cfg.pow_bits);
   uint64_t nonce = 0;
-  GS_TRY(grind_blake2s(st, pre.data(), cfg.pow_bits, (uint32_t*)pv.ctx.d_small, &nonce,
-                       (uint32_t*)pv.ctx.h_small));
+  if (pv.ch.p252) {  // GrindOps<Poseidon252Channel>: the device derives the prefix from the digest
+    const void* d_digest = nullptr;
+    GS_TRY(pv.ctx.stage_bytes(pv.ch.digest.data(), 32, &d_digest));
+    GS_TRY(poseidon252_grind(st, (const uint8_t*)d_digest, cfg.pow_bits, pv.ctx.d_small, (uint32_t*)pv.ctx.h_small,
+                             &nonce));
+  } else {
+    auto pre = pv.ch.pow_prefixed(cfg.pow_bits);
+    GS_TRY(grind_blake2s(st, pre.data(), cfg.pow_bits, (uint32_t*)pv.ctx.d_small, &nonce,
+                         (uint32_t*)pv.ctx.h_small));
+  }
   pv.ch.mix_u64(nonce);
   pv.mark("grind");
   // queries

@@ -115,8 +115,15 @@ struct Prover {
     for (uint32_t c = 0; c < t.n_cols; c++) cols.push_back(t.eval_col(c));
     const uint32_t* const* tab = nullptr;
     GS_TRY(table(cols, &tab));
-    GS_TRY(commit_on_layer(st, t.eval_log, nullptr, tab, t.n_cols, t.layers[t.eval_log]));
-    GS_TRY(commit_node_layers(st, t.eval_log, t.layers.data(), ctx.tree_counters));
+    if (ch.p252) {  // Poseidon252MerkleHasher: one launch per layer
+      GS_TRY(poseidon252_commit_on_layer(st, t.eval_log, nullptr, tab, t.n_cols, (uint8_t*)t.layers[t.eval_log]));
+      for (int L = (int)t.eval_log - 1; L >= 0; L--)
+        GS_TRY(poseidon252_commit_on_layer(st, (uint32_t)L, (const uint8_t*)t.layers[L + 1], nullptr, 0,
+                                           (uint8_t*)t.layers[L]));
+    } else {
+      GS_TRY(commit_on_layer(st, t.eval_log, nullptr, tab, t.n_cols, t.layers[t.eval_log]));
+      GS_TRY(commit_node_layers(st, t.eval_log, t.layers.data(), ctx.tree_counters));
+    }
     uint32_t w[8];
     GS_TRY(ctx.read_back(t.layers[0], 32, w));
     t.root = host::hash_from_words(w);
@@ -163,7 +170,8 @@ struct Prover {
 
   int commit_empty() {
     Tree t;
-    t.root = host::hash_bytes(nullptr, 0);
+    // MerkleProver::commit of no columns: hash_node(None, []) of one node
+    t.root = ch.p252 ? host::p252::to_bytes(host::p252::hash_many({})) : host::hash_bytes(nullptr, 0);
     ch.mix_root(t.root);
     trees.push_back(std::move(t));
     return OK;

@@ -89,6 +89,12 @@ _PROTOS = {
     "gs_commit_plan_destroy": [C.c_void_p],
     "gs_prove_poseidon": [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint32, U32P, C.c_uint32, C.POINTER(PcsConfig),
                           C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
+    "gs_prove_wide_fibonacci_poseidon252": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, U32P,
+                                            C.POINTER(PcsConfig), C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
+    "gs_prove_poseidon_poseidon252": [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint32, U32P, C.c_uint32,
+                                      C.POINTER(PcsConfig), C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
+    "gs_poseidon252_channel_op": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64, U32P, C.c_size_t,
+                                  U32P, C.c_void_p, C.POINTER(C.c_uint32)],
 }
 _RESTYPE = {"gs_last_error": C.c_char_p, "gs_ctx_stream": C.c_void_p, "gs_launch_count": C.c_ulonglong}
 _OPTIONAL = set()

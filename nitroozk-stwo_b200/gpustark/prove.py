@@ -1,10 +1,13 @@
 """Full proofs of the two benchmark components on the GPU prover (C ABI
-gs_prove_wide_fibonacci / gs_prove_poseidon).
+gs_prove_wide_fibonacci / gs_prove_poseidon, and their Poseidon252MerkleChannel
+forms gs_prove_wide_fibonacci_poseidon252 / gs_prove_poseidon_poseidon252).
 
 Mirrors the reference's example drivers cuda_prove_wide_fibonacci
-(crates/examples/src/wide_fibonacci/mod.rs:140-184) and cuda_prove_poseidon
-(crates/examples/src/poseidon/mod.rs:617-700), which build the trace and call
-the generic prove(); the result is the serialised StarkProof.
+(crates/examples/src/wide_fibonacci/mod.rs:140-184), cuda_prove_poseidon
+(crates/examples/src/poseidon/mod.rs:617-700), cuda_prove_wide_fibonacci_poseidon
+(wide_fibonacci/mod.rs:335-379) and cuda_prove_poseidon_poseidon
+(poseidon/mod.rs:702-785), which build the trace and call the generic
+prove(); the result is the serialised StarkProof.
 """
 import ctypes as C
 import threading
@@ -16,6 +19,7 @@ from .backend import default_context
 
 INPUT_REFERENCE, INPUT_SEEDED, INPUT_HOST = 0, 1, 2
 GS_ERR_PROOF = 5
+MERKLE_CHANNELS = ("blake2s", "poseidon252")
 
 
 class ConstraintsNotSatisfied(L.GpuStarkError):
@@ -61,22 +65,30 @@ def _inputs(host_inputs):
     return a, a.ctypes.data_as(L.U32P)
 
 
+def _entry(name, merkle_channel):
+    if merkle_channel not in MERKLE_CHANNELS:
+        raise ValueError(f"merkle_channel must be one of {MERKLE_CHANNELS}")
+    return getattr(L.lib(), name + ("_poseidon252" if merkle_channel == "poseidon252" else ""))
+
+
 def prove_wide_fibonacci(log_n_rows, n_columns=100, seed=0, input_mode=INPUT_REFERENCE, host_inputs=None,
-                         config=None, ctx=None, capacity=1 << 21):
-    """host_inputs (INPUT_HOST): array (2, 2^log_n_rows) of columns 0 and 1."""
+                         config=None, ctx=None, capacity=1 << 21, merkle_channel="blake2s"):
+    """host_inputs (INPUT_HOST): array (2, 2^log_n_rows) of columns 0 and 1.
+    merkle_channel: 'blake2s' (Blake2sMerkleChannel) or 'poseidon252'."""
     ctx = ctx or default_context()
     keep, ptr = _inputs(host_inputs)
     cfg = config or pcs_config()
-    return _run(L.lib().gs_prove_wide_fibonacci,
+    return _run(_entry("gs_prove_wide_fibonacci", merkle_channel),
                 (ctx.handle, log_n_rows, n_columns, seed, input_mode, ptr, C.byref(cfg)), ctx, capacity)
 
 
 def prove_poseidon(log_n_instances, seed=0, input_mode=INPUT_REFERENCE, host_inputs=None, composition_log_split=2,
-                   config=None, ctx=None, capacity=1 << 21):
-    """host_inputs (INPUT_HOST): array (16, 2^log_n_instances) of initial states."""
+                   config=None, ctx=None, capacity=1 << 21, merkle_channel="blake2s"):
+    """host_inputs (INPUT_HOST): array (16, 2^log_n_instances) of initial states.
+    merkle_channel: 'blake2s' (Blake2sMerkleChannel) or 'poseidon252'."""
     ctx = ctx or default_context()
     keep, ptr = _inputs(host_inputs)
     cfg = config or pcs_config()
-    return _run(L.lib().gs_prove_poseidon,
+    return _run(_entry("gs_prove_poseidon", merkle_channel),
                 (ctx.handle, log_n_instances, seed, input_mode, ptr, composition_log_split, C.byref(cfg)), ctx,
                 capacity)

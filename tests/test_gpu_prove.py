@@ -70,3 +70,29 @@ def test_wide_fibonacci_config_size(G):
 def test_poseidon_config_size(G):
     """Poseidon2 2^18 instances, seeded inputs (the benchmark configuration)."""
     assert G.prove_poseidon(18, seed=0, input_mode=1) == O.prove("poseidon", 18, seed=0, input_mode=1)
+
+
+# ---------------------------------------------- Poseidon252MerkleChannel proofs
+@pytest.mark.parametrize("log_n,n_cols,mode", [(4, 8, 0), (7, 9, 1), (10, 100, 1)])
+def test_wide_fibonacci_poseidon252_proof_bytes(G, log_n, n_cols, mode):
+    """cuda_prove_wide_fibonacci_poseidon: every tree, the channel and the
+    proof of work over Poseidon252, byte-identical to the oracle."""
+    got = G.prove_wide_fibonacci(log_n, n_cols, seed=4, input_mode=mode, merkle_channel="poseidon252")
+    exp = O.prove("wide_fibonacci", log_n, n_cols=n_cols, seed=4, input_mode=mode, merkle_channel="poseidon252")
+    assert got == exp
+    assert got != G.prove_wide_fibonacci(log_n, n_cols, seed=4, input_mode=mode)
+
+
+@pytest.mark.parametrize("log_n,mode", [(4, 0), (8, 1)])
+def test_poseidon_poseidon252_proof_bytes(G, log_n, mode):
+    got = G.prove_poseidon(log_n, seed=6, input_mode=mode, merkle_channel="poseidon252")
+    exp = O.prove("poseidon", log_n, seed=6, input_mode=mode, merkle_channel="poseidon252")
+    assert got == exp
+
+
+def test_poseidon252_pcs_config(G):
+    cfg = G.pcs_config(pow_bits=6, log_blowup=2, log_last_layer=1, n_queries=11)
+    got = G.prove_wide_fibonacci(8, 12, seed=2, input_mode=1, config=cfg, merkle_channel="poseidon252")
+    exp = O.prove("wide_fibonacci", 8, n_cols=12, seed=2, input_mode=1, pow_bits=6, n_queries=11, log_blowup=2,
+                  log_last_layer=1, merkle_channel="poseidon252")
+    assert got == exp
