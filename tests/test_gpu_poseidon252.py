@@ -96,3 +96,27 @@ def test_grind_matches_oracle(B, pow_bits, salt):
     got = B.poseidon252_grind(ch.digest, pow_bits)
     assert got == ch.grind(pow_bits)
     assert ch.verify_pow_nonce(pow_bits, got)
+
+
+def test_large_layers_and_batches_match_the_oracle(B):
+    """Layers of 2^13..2^15 nodes (leaves with an all-(P-1) column, node-only
+    layers, two felts per leaf) and permutation batches of 300 and 20000
+    states (grid-stride loops) against the C++ oracle."""
+    import pyoracle as O
+    rng = np.random.default_rng(21)
+    for log_size, n_cols in [(13, 8), (14, 0), (15, 9)]:
+        n = 1 << log_size
+        cols = [rng.integers(0, PS.M31, n, dtype=np.int64).astype(np.uint32) for _ in range(n_cols)]
+        cols[-1:] = [np.full(n, PS.M31 - 1, np.uint32)] if n_cols else []
+        prev = None
+        if n_cols == 0:
+            prev = np.frombuffer(b"".join(PS.to_bytes_be(int.from_bytes(rng.bytes(32), "big") % PS.P)
+                                          for _ in range(2 * n)), np.uint8)
+        got = B.poseidon252_commit_on_layer(log_size, torch.tensor(prev, device="cuda") if prev is not None else None,
+                                            [col(c) for c in cols])
+        want = O.p252_commit_on_layer(log_size, prev, cols)
+        assert np.array_equal(got.cpu().numpy().reshape(-1, 32), want), (log_size, n_cols)
+    for n in [300, 20000]:
+        raw = b"".join(PS.to_bytes_be(int.from_bytes(rng.bytes(32), "big") % PS.P) for _ in range(3 * n))
+        got = B.poseidon252_permute(torch.tensor(np.frombuffer(raw, np.uint8).copy(), device="cuda"))
+        assert bytes(got.cpu().numpy()) == O.p252_permute(raw), n
