@@ -98,6 +98,83 @@ __global__ void __launch_bounds__(256) eap_chunk_kernel(const uint32_t* const* _
   }
 }
 
+// K polynomials per block for chunks of exactly 2^12 coefficients: each
+// weight W[j] (16 bytes, read through L1) serves K coefficients, so L1
+// traffic per coefficient drops from 20 to 4 + 16/K bytes (the one-polynomial
+// kernel above is L1-bound). Thread t owns coefficients 4t + 1024q + e
+// (q, e < 4): 16-byte coefficient loads, a warp reading 512 contiguous bytes
+// per polynomial; the fold schedule is static (after every third
+// coefficient: three products of < 2^62 on a folded value < 2^34 fit 64 bits).
+constexpr uint32_t EAP_MULTI_LOG = 12;
+template <int K>
+__global__ void __launch_bounds__(256) eap_chunk_multi_kernel(const uint32_t* const* __restrict__ polys,
+                                                              uint32_t n_polys, uint32_t log_n,
+                                                              const uint32_t* __restrict__ w, Factors fs,
+                                                              uint32_t* partials) {
+  __shared__ uint32_t red[K][4][8];
+  const uint32_t chunk = blockIdx.x, p0 = blockIdx.y * K;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint4* wv = reinterpret_cast<const uint4*>(w);
+  const uint4* cp[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const uint32_t p = p0 + k < n_polys ? p0 + k : n_polys - 1;  // tail rows recompute the last poly
+    cp[k] = reinterpret_cast<const uint4*>(polys[p] + ((size_t)chunk << EAP_MULTI_LOG));
+  }
+  uint64_t acc[K][4];
+#pragma unroll
+  for (int k = 0; k < K; k++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) acc[k][c] = 0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const uint32_t j = 4 * threadIdx.x + 1024 * q;
+    uint4 cv[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) cv[k] = __ldg(cp[k] + (j >> 2));
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const uint4 wj = __ldg(wv + j + e);
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const uint32_t v = e == 0 ? cv[k].x : e == 1 ? cv[k].y : e == 2 ? cv[k].z : cv[k].w;
+        acc[k][0] += (uint64_t)wj.x * v;
+        acc[k][1] += (uint64_t)wj.y * v;
+        acc[k][2] += (uint64_t)wj.z * v;
+        acc[k][3] += (uint64_t)wj.w * v;
+      }
+      if ((4 * q + e) % 3 == 2)
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+          for (int c = 0; c < 4; c++) acc[k][c] = fold64e(acc[k][c]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K; k++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      uint32_t r = reduce64(acc[k][c]);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) r = add(r, __shfl_down_sync(0xffffffffu, r, off));
+      if (lane == 0) red[k][c][warp] = r;
+    }
+  __syncthreads();
+  if (threadIdx.x < K && p0 + threadIdx.x < n_polys) {
+    const uint32_t k = threadIdx.x;
+    uint32_t t[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+#pragma unroll
+      for (int q = 0; q < 8; q++) t[c] = add(t[c], red[k][c][q]);
+    qm31 sum = qm_make(t[0], t[1], t[2], t[3]);
+    for (uint32_t b = 0; EAP_MULTI_LOG + b < log_n; b++)
+      if ((chunk >> b) & 1u) sum = qm_mul(sum, fs.f[EAP_MULTI_LOG + b]);
+    uint32_t* o = partials + 4 * ((size_t)(p0 + k) * gridDim.x + chunk);
+    o[0] = sum.x.a; o[1] = sum.x.b; o[2] = sum.y.a; o[3] = sum.y.b;
+  }
+}
+
 // One block of 128 threads per polynomial: strided partial sums, then a
 // shuffle and shared-memory reduction (field additions are exact, so the
 // order does not change the result).
@@ -163,8 +240,15 @@ int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_
   eap_weights_kernel<<<((1u << s) + 255) / 256, 256, 0, st>>>(fs, s, w);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
-  dim3 grid(chunks, n_polys);
-  eap_chunk_kernel<<<grid, 256, 0, st>>>(d_polys, log_n, s, w, fs, partials, vec);
+  if (vec && s == EAP_MULTI_LOG) {
+    // four polynomials per block (two: L1-bound again, 84 µs on the Poseidon2
+    // 2^18 trace; eight: register-bound, 75 µs; four: 54 µs)
+    dim3 grid(chunks, (n_polys + 3) / 4);
+    eap_chunk_multi_kernel<4><<<grid, 256, 0, st>>>(d_polys, n_polys, log_n, w, fs, partials);
+  } else {
+    dim3 grid(chunks, n_polys);
+    eap_chunk_kernel<<<grid, 256, 0, st>>>(d_polys, log_n, s, w, fs, partials, vec);
+  }
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   eap_finalize_kernel<<<n_polys, 128, 0, st>>>(partials, chunks, n_polys, d_out);
