@@ -614,10 +614,11 @@ def job_mix(kind, seed):
     return jobs
 
 
-def serving_metric(kind):
+def serving_metric(kind, channel="blake2s"):
+    suffix = "" if channel == "blake2s" else ", Poseidon252 channel"
     if kind == "batched":
-        return "batched vs sequential proofs/s (64 Wide-Fibonacci proofs, 2^10..2^16 rows)"
-    return "served proofs/s with p50/p99 latency (Poisson mix of Poseidon2 2^12..2^18, WF 2^12..2^20)"
+        return "batched vs sequential proofs/s (64 Wide-Fibonacci proofs, 2^10..2^16 rows)" + suffix
+    return "served proofs/s with p50/p99 latency (Poisson mix of Poseidon2 2^12..2^18, WF 2^12..2^20)" + suffix
 
 
 def run_serving(args, world, rank, local):
@@ -629,11 +630,12 @@ def run_serving(args, world, rank, local):
     ctx = Context(torch.cuda.current_stream())
     tuning = fft_autotune(args, 23)
     jobs = job_mix(args.workload, 1 + rank)
+    mc = args.merkle_channel
 
     def single(a, n, c, sd):
         if a == 0:
-            return G.prove_wide_fibonacci(n, c, seed=sd, input_mode=G.INPUT_SEEDED, ctx=ctx)
-        return G.prove_poseidon(n, seed=sd, input_mode=G.INPUT_SEEDED, ctx=ctx)
+            return G.prove_wide_fibonacci(n, c, seed=sd, input_mode=G.INPUT_SEEDED, ctx=ctx, merkle_channel=mc)
+        return G.prove_poseidon(n, seed=sd, input_mode=G.INPUT_SEEDED, ctx=ctx, merkle_channel=mc)
 
     # warm-up: every distinct shape once (pool growth, twiddle trees, pinned buffers)
     for shape in sorted({(a, n, c) for a, n, c, _ in jobs}):
@@ -656,12 +658,12 @@ def run_serving(args, world, rank, local):
         # tables and pool growth happen once per context): `workers` copies
         # of each shape in flight at once
         for a, n, c in sorted({(a, n, c) for a, n, c, _ in jobs}):
-            for i in [sv.submit(a, n, c or 100, 0) for _ in range(workers)]:
+            for i in [sv.submit(a, n, c or 100, 0, merkle_channel=mc) for _ in range(workers)]:
                 sv.wait(i)
         barrier(world)
         t0 = time.perf_counter()
         if args.workload == "batched":
-            ids = [sv.submit(a, n, c or 100, sd) for a, n, c, sd in jobs]
+            ids = [sv.submit(a, n, c or 100, sd, merkle_channel=mc) for a, n, c, sd in jobs]
         else:
             # Poisson arrivals at `load` x the sequential proof rate (seeded)
             rate = args.load * len(jobs) / seq_s
@@ -672,7 +674,7 @@ def run_serving(args, world, rank, local):
                 now = time.perf_counter() - t0
                 if at > now:
                     time.sleep(at - now)
-                ids.append(sv.submit(a, n, c or 100, sd))
+                ids.append(sv.submit(a, n, c or 100, sd, merkle_channel=mc))
         res = [sv.wait(i) for i in ids]
         srv_s = time.perf_counter() - t0
     identical = all(p == q for (p, _), q in zip(res, seq_proofs))
@@ -683,7 +685,7 @@ def run_serving(args, world, rank, local):
     seq_pps = world * len(jobs) / seq_s
     q = lambda v, f: float(np.percentile(np.asarray(v), f))
     out = {
-        "metric": serving_metric(args.workload),
+        "metric": serving_metric(args.workload, mc),
         "value": round(pps, 2), "unit": "proofs/s", "n_gpus": world, "steps": 1, "warmup": 1,
         "ms_per_step": round(1e3 * srv_s, 2), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32 (M31/QM31 integer arithmetic)", "data": "synthetic: seeded uniform M31",
@@ -699,7 +701,7 @@ def run_serving(args, world, rank, local):
     }
     if arrivals is not None:
         out["arrival_rate_per_s"] = round(args.load * len(jobs) / seq_s, 2)
-    if args.workload == "batched":
+    if args.workload == "batched" and mc == "blake2s":
         out["commit"] = run_batched_commit(ctx, 1 + rank)
     return out
 

@@ -307,6 +307,10 @@ typedef struct gs_server gs_server;
 int gs_server_create(uint32_t n_workers, size_t hbm_budget_bytes, gs_server** out);
 int gs_server_submit(gs_server* server, uint32_t air, uint32_t log_n, uint32_t n_columns, uint64_t seed,
                      uint32_t composition_log_split, const gs_pcs_config* config, uint64_t* job_id);
+/* The same job proved over Poseidon252MerkleChannel (as
+ * gs_prove_wide_fibonacci_poseidon252 / gs_prove_poseidon_poseidon252). */
+int gs_server_submit_poseidon252(gs_server* server, uint32_t air, uint32_t log_n, uint32_t n_columns, uint64_t seed,
+                                 uint32_t composition_log_split, const gs_pcs_config* config, uint64_t* job_id);
 int gs_server_wait(gs_server* server, uint64_t job_id, uint8_t* proof, size_t capacity, size_t* proof_len,
                    double* latency_ms);
 int gs_server_destroy(gs_server* server);

@@ -129,12 +129,14 @@ int gs_server_create(uint32_t n_workers, size_t hbm_budget_bytes, gs_server** ou
   return OK;
 }
 
-int gs_server_submit(gs_server* sv, uint32_t air, uint32_t log_n, uint32_t n_columns, uint64_t seed,
-                     uint32_t composition_log_split, const gs_pcs_config* config, uint64_t* job_id) {
+static int submit_job(gs_server* sv, uint32_t air, uint32_t log_n, uint32_t n_columns, uint64_t seed,
+                      uint32_t composition_log_split, const gs_pcs_config* config, uint32_t merkle_channel,
+                      uint64_t* job_id) {
   GS_REQUIRE(sv && job_id, "null argument");
   GS_REQUIRE(air <= 1, "unknown component");
   Job j;
   j.req.air = air;
+  j.req.merkle_channel = merkle_channel;
   j.req.log_n = log_n;
   j.req.n_cols = n_columns;
   j.req.seed = seed;
@@ -157,6 +159,15 @@ int gs_server_submit(gs_server* sv, uint32_t air, uint32_t log_n, uint32_t n_col
   }
   sv->s.cv_jobs.notify_one();
   return OK;
+}
+
+int gs_server_submit(gs_server* sv, uint32_t air, uint32_t log_n, uint32_t n_columns, uint64_t seed,
+                     uint32_t composition_log_split, const gs_pcs_config* config, uint64_t* job_id) {
+  return submit_job(sv, air, log_n, n_columns, seed, composition_log_split, config, 0, job_id);
+}
+int gs_server_submit_poseidon252(gs_server* sv, uint32_t air, uint32_t log_n, uint32_t n_columns, uint64_t seed,
+                                 uint32_t composition_log_split, const gs_pcs_config* config, uint64_t* job_id) {
+  return submit_job(sv, air, log_n, n_columns, seed, composition_log_split, config, 1, job_id);
 }
 
 int gs_server_wait(gs_server* sv, uint64_t job_id, uint8_t* proof, size_t capacity, size_t* proof_len,

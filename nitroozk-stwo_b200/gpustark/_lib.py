@@ -78,6 +78,8 @@ _PROTOS = {
     "gs_server_create": [C.c_uint32, C.c_size_t, C.POINTER(C.c_void_p)],
     "gs_server_submit": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
                          C.POINTER(PcsConfig), C.POINTER(C.c_uint64)],
+    "gs_server_submit_poseidon252": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
+                                     C.POINTER(PcsConfig), C.POINTER(C.c_uint64)],
     "gs_server_wait": [C.c_void_p, C.c_uint64, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t),
                        C.POINTER(C.c_double)],
     "gs_server_destroy": [C.c_void_p],

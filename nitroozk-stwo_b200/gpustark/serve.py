@@ -19,14 +19,19 @@ class ProofServer:
         L.check(L.lib().gs_server_create(n_workers, hbm_budget_bytes, C.byref(h)), "gs_server_create")
         self.handle = h
 
-    def submit(self, air, log_n, n_columns=100, seed=0, composition_log_split=None, config=None):
-        """air: WIDE_FIBONACCI or POSEIDON; returns a job id."""
+    def submit(self, air, log_n, n_columns=100, seed=0, composition_log_split=None, config=None,
+               merkle_channel="blake2s"):
+        """air: WIDE_FIBONACCI or POSEIDON; merkle_channel: 'blake2s' or
+        'poseidon252'; returns a job id."""
         if composition_log_split is None:
             composition_log_split = 1 if air == WIDE_FIBONACCI else 2
+        if merkle_channel not in ("blake2s", "poseidon252"):
+            raise ValueError("merkle_channel must be 'blake2s' or 'poseidon252'")
+        fn = L.lib().gs_server_submit_poseidon252 if merkle_channel == "poseidon252" else L.lib().gs_server_submit
         cfg = config or pcs_config()
         jid = C.c_uint64()
-        L.check(L.lib().gs_server_submit(self.handle, air, log_n, n_columns, seed, composition_log_split,
-                                         C.byref(cfg), C.byref(jid)), "gs_server_submit")
+        L.check(fn(self.handle, air, log_n, n_columns, seed, composition_log_split, C.byref(cfg), C.byref(jid)),
+                fn.__name__)
         return jid.value
 
     def wait(self, job_id, capacity=1 << 20):

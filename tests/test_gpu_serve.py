@@ -43,3 +43,20 @@ def test_server_reports_errors(mods):
         with pytest.raises(prove.ConstraintsNotSatisfied):
             sv.wait(bad)
         assert sv.wait(good)[0] == alone(prove, 0, 6, 10, 1)
+
+
+def test_served_poseidon252_jobs_match_single_proofs(mods):
+    """Poseidon252-channel jobs mixed with Blake2s ones: each job's proof is
+    the one proved alone over its channel."""
+    prove, serve = mods
+    jobs = [(0, 8, 20, 1, "poseidon252"), (1, 6, 0, 2, "poseidon252"), (0, 9, 30, 3, "blake2s"),
+            (0, 10, 100, 4, "poseidon252")]
+    with serve.ProofServer(3) as sv:
+        ids = [sv.submit(a, n, c or 100, s, merkle_channel=mc) for a, n, c, s, mc in jobs]
+        got = [sv.wait(i)[0] for i in ids]
+    for (a, n, c, s, mc), proof in zip(jobs, got):
+        if a == 0:
+            want = prove.prove_wide_fibonacci(n, c, seed=s, input_mode=prove.INPUT_SEEDED, merkle_channel=mc)
+        else:
+            want = prove.prove_poseidon(n, seed=s, input_mode=prove.INPUT_SEEDED, merkle_channel=mc)
+        assert proof == want
