@@ -96,3 +96,17 @@ def test_poseidon252_pcs_config(G):
     exp = O.prove("wide_fibonacci", 8, n_cols=12, seed=2, input_mode=1, pow_bits=6, n_queries=11, log_blowup=2,
                   log_last_layer=1, merkle_channel="poseidon252")
     assert got == exp
+
+
+@pytest.mark.slow
+def test_wide_fibonacci_poseidon252_config_size(G):
+    """The Wide-Fibonacci 2^16 x 100 benchmark proof over the Poseidon252
+    channel, byte-identical to the oracle's."""
+    assert G.prove_wide_fibonacci(16, 100, seed=0, input_mode=1, merkle_channel="poseidon252") == \
+        O.prove("wide_fibonacci", 16, n_cols=100, seed=0, input_mode=1, merkle_channel="poseidon252")
+
+
+@pytest.mark.slow
+def test_poseidon_poseidon252_2e14(G):
+    assert G.prove_poseidon(14, seed=3, input_mode=1, merkle_channel="poseidon252") == \
+        O.prove("poseidon", 14, seed=3, input_mode=1, merkle_channel="poseidon252")
