@@ -165,46 +165,98 @@ int fold_circle_into_line_dev_alpha(cudaStream_t st, CPlanes src, uint32_t log_n
 }
 
 // Fused tail of the FRI commit phase: every layer of log size <= 11 in one
-// launch of one 8-CTA thread-block cluster. For layer k (log size log0 - k,
-// leaves already hashed): its Merkle node layers (each CTA its eighth of the
-// tree, then CTA 0 the last three levels), the channel step on its root (one
-// thread), then fold_line into layer k + 1 with that layer's leaf hashes,
-// split over the cluster — the same steps the per-layer kernels run, with
-// cluster barriers in place of kernel boundaries. Data written inside the
-// kernel by another CTA is read at L2 (__ldcg) after a cluster barrier.
-__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(1024) fri_tail_kernel(FriTail a, uint32_t* state,
-                                                                                  const uint32_t* __restrict__ itw,
-                                                                                  uint32_t tw_len) {
-  __shared__ uint4 buf[2][256];
-  cg::cluster_group cluster = cg::this_cluster();
-  const uint32_t gtid = cluster.block_rank() * blockDim.x + threadIdx.x;
-  const uint32_t gthreads = 8 * blockDim.x;
+// launch of one 1024-thread CTA. For layer k (log size log0 - k, leaves
+// already hashed): its Merkle node levels (at most 1024 nodes each, one per
+// thread), the channel step on its root (one thread), then fold_line into
+// layer k + 1 with that layer's leaf hashes — the steps the per-layer kernels
+// run, with the data in shared memory and `__syncthreads` between them. The
+// tail is a chain of about a hundred dependent steps, most of them one
+// Blake2s compression long; an earlier 8-CTA cluster version spent more on
+// cluster barriers and L2 re-reads than it gained in width (164 µs against
+// 132 µs for the Poseidon2 2^18 proof's tail).
+// Shared memory (uint4): two node-hash buffers of 1024 hashes, the current
+// layer's leaves (1024 hashes), the current and next layer values (1024
+// QM31 each): 128 KiB.
+constexpr uint32_t TAIL_CTA_SMEM = 8192 * 16;
+__global__ void __launch_bounds__(1024) fri_tail_cta_kernel(FriTail a, uint32_t* state,
+                                                            const uint32_t* __restrict__ itw, uint32_t tw_len) {
+  extern __shared__ uint4 tsm[];
+  __shared__ uint32_t alpha_s[4];
+  uint4* nb[2] = {tsm, tsm + 2048};
+  uint4* leaves = tsm + 4096;
+  uint4* vals[2] = {tsm + 6144, tsm + 7168};
+  const uint32_t tid = threadIdx.x;
   for (uint32_t k = 0; k < a.n; k++) {
     const uint32_t log = a.log0 - k;
-    cluster_tree_levels(log, a.tree[k], k > 0, buf, cluster);
-    if (cluster.block_rank() == 0 && threadIdx.x == 0)
-      channel_mix_root_draw_dev(state, a.tree[k][0], a.roots + 8 * k, a.felts + 8 * k);
-    cluster.sync();
-    const uint32_t* f = a.felts + 8 * k;
-    const qm31 alpha = qm_make(__ldcg(f), __ldcg(f + 1), __ldcg(f + 2), __ldcg(f + 3));
-    const uint32_t half = 1u << (log - 1);
-    const uint32_t* lvl = itw + (tw_len - (1u << log));
-    uint32_t* const* sp = a.planes[k];
-    uint32_t* const* dp = a.planes[k + 1];
-    uint32_t* leaves = (k + 1 < a.n) ? a.tree[k + 1][log - 1] : nullptr;
-    for (uint32_t i = gtid; i < half; i += gthreads) {
-      // layer 0's planes come from the previous kernel; later ones from this one
-      qm31 fx = qm_make(__ldcg(sp[0] + 2 * i), __ldcg(sp[1] + 2 * i), __ldcg(sp[2] + 2 * i), __ldcg(sp[3] + 2 * i));
-      qm31 fnx = qm_make(__ldcg(sp[0] + 2 * i + 1), __ldcg(sp[1] + 2 * i + 1), __ldcg(sp[2] + 2 * i + 1),
-                         __ldcg(sp[3] + 2 * i + 1));
-      uint32_t xinv = __ldg(lvl + i);
-      qm31 f0 = qm_add(fx, fnx);
-      qm31 f1 = qm_mul_m31(qm_sub(fx, fnx), xinv);
-      qm31 r = qm_add(f0, qm_mul(alpha, f1));
-      dp[0][i] = r.x.a; dp[1][i] = r.x.b; dp[2][i] = r.y.a; dp[3][i] = r.y.b;
-      if (leaves) leaf_hash4(leaves, i, r);
+    uint32_t* const* tree = a.tree[k];
+    int cur = 0;
+    for (int L = (int)log - 1; L >= 0; L--) {
+      if (tid < (1u << L)) {
+        uint4 c[4];
+        if (L == (int)log - 1) {
+          if (k == 0) {  // leaves hashed by the previous kernel
+            const uint4* src = reinterpret_cast<const uint4*>(tree[log]) + 4 * (size_t)tid;
+#pragma unroll
+            for (int q = 0; q < 4; q++) c[q] = __ldg(src + q);
+          } else {
+#pragma unroll
+            for (int q = 0; q < 4; q++) c[q] = leaves[4 * tid + q];
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; q++) c[q] = nb[cur ^ 1][4 * tid + q];
+        }
+        uint32_t h[8];
+        hash_children16(c, h);
+        tail_store_hash(tree[L], tid, h);
+        nb[cur][2 * tid] = make_uint4(h[0], h[1], h[2], h[3]);
+        nb[cur][2 * tid + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+      }
+      __syncthreads();
+      cur ^= 1;
     }
-    cluster.sync();
+    if (tid == 0) {  // the root sits in the buffer of the last level
+      const uint32_t* f = a.felts + 8 * k;
+      channel_mix_root_draw_dev(state, reinterpret_cast<const uint32_t*>(nb[cur ^ 1]), a.roots + 8 * k,
+                                a.felts + 8 * k);
+#pragma unroll
+      for (int j = 0; j < 4; j++) alpha_s[j] = f[j];
+    }
+    __syncthreads();
+    const qm31 alpha = qm_make(alpha_s[0], alpha_s[1], alpha_s[2], alpha_s[3]);
+    const uint32_t half = 1u << (log - 1);
+    if (tid < half) {
+      qm31 fx, fnx;
+      if (k == 0) {  // layer 0's values come from the previous kernel
+        uint32_t* const* sp = a.planes[0];
+        fx = qm_make(__ldg(sp[0] + 2 * tid), __ldg(sp[1] + 2 * tid), __ldg(sp[2] + 2 * tid), __ldg(sp[3] + 2 * tid));
+        fnx = qm_make(__ldg(sp[0] + 2 * tid + 1), __ldg(sp[1] + 2 * tid + 1), __ldg(sp[2] + 2 * tid + 1),
+                      __ldg(sp[3] + 2 * tid + 1));
+      } else {
+        const uint4 u = vals[k & 1][2 * tid], v = vals[k & 1][2 * tid + 1];
+        fx = qm_make(u.x, u.y, u.z, u.w);
+        fnx = qm_make(v.x, v.y, v.z, v.w);
+      }
+      const uint32_t xinv = __ldg(itw + (tw_len - (1u << log)) + tid);
+      const qm31 f0 = qm_add(fx, fnx);
+      const qm31 f1 = qm_mul_m31(qm_sub(fx, fnx), xinv);
+      const qm31 r = qm_add(f0, qm_mul(alpha, f1));
+      uint32_t* const* dp = a.planes[k + 1];
+      dp[0][tid] = r.x.a; dp[1][tid] = r.x.b; dp[2][tid] = r.y.a; dp[3][tid] = r.y.b;
+      vals[(k + 1) & 1][tid] = make_uint4(r.x.a, r.x.b, r.y.a, r.y.b);
+      if (k + 1 < a.n) {  // the next layer's leaf
+        uint32_t h[8], m[16];
+        blake2s_init(h);
+        m[0] = r.x.a; m[1] = r.x.b; m[2] = r.y.a; m[3] = r.y.b;
+#pragma unroll
+        for (int j = 4; j < 16; j++) m[j] = 0;
+        blake2s_compress(h, m, 16, true);
+        tail_store_hash(a.tree[k + 1][log - 1], tid, h);
+        leaves[2 * tid] = make_uint4(h[0], h[1], h[2], h[3]);
+        leaves[2 * tid + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -212,7 +264,10 @@ int fri_tail(cudaStream_t st, const FriTail& a, uint32_t* d_state, const uint32_
   GS_REQUIRE(a.n >= 1 && a.n <= FRI_TAIL_MAX && a.log0 <= FRI_TAIL_MAX - 1 && a.log0 >= a.n,
              "FRI tail: layer sizes out of range");
   GS_REQUIRE(a.log0 <= tw_log, "FRI tail: line domain must fit the twiddle tree");
-  fri_tail_kernel<<<8, 1024, 0, st>>>(a, d_state, d_itw, 1u << tw_log);
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(fri_tail_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_CTA_SMEM);
+  GS_CUDA_TRY(attr);
+  fri_tail_cta_kernel<<<1, 1024, TAIL_CTA_SMEM, st>>>(a, d_state, d_itw, 1u << tw_log);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;
