@@ -56,7 +56,8 @@ def line_coeffs(point8, value4, alpha4):
     return qmul(alpha4, a), qmul(alpha4, b), qmul(alpha4, c)
 
 
-@pytest.mark.parametrize("log_size,n_cols,n_entries", [(3, 2, 2), (8, 5, 7), (12, 17, 17), (16, 100, 108)])
+@pytest.mark.parametrize("log_size,n_cols,n_entries", [(3, 2, 2), (8, 5, 7), (10, 3, 4), (10, 6, 6), (11, 7, 7),
+                                                       (12, 17, 17), (16, 100, 108)])
 def test_accumulate_numerators(B, log_size, n_cols, n_entries):
     rng = np.random.default_rng(log_size * 1000 + n_cols)
     cols = [rand(rng, 1 << log_size) for _ in range(n_cols)]
@@ -97,7 +98,7 @@ def test_lift_and_accumulate(B, sizes):
     assert np.array_equal(np.stack([host(t) for t in got], 1), exp)
 
 
-@pytest.mark.parametrize("log_n,n_polys", [(0, 2), (1, 3), (5, 4), (10, 3), (11, 2), (18, 5)])
+@pytest.mark.parametrize("log_n,n_polys", [(0, 2), (1, 3), (5, 4), (10, 3), (11, 2), (12, 4), (13, 9), (18, 5)])
 def test_batch_eval_at_point(B, log_n, n_polys):
     rng = np.random.default_rng(log_n * 7 + n_polys)
     polys = [rand(rng, 1 << log_n) for _ in range(n_polys)]
