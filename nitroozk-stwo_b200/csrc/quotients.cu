@@ -149,18 +149,15 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // entries (k = g, g + EG, ...). In a round the RG warps of an entry group
 // read 512·RG contiguous bytes of one column, which keeps HBM pages open.
 template <int EG>
-__global__ void __launch_bounds__(256) accumulate_numerators_split_kernel(const NumEntry* __restrict__ entries,
-                                                                          uint32_t n_entries, qm31 b_sum,
-                                                                          uint32_t log_size, Planes out) {
+__global__ void __launch_bounds__(256, 4) accumulate_numerators_split_kernel(const NumEntry* __restrict__ entries,
+                                                                             uint32_t n_entries, qm31 b_sum,
+                                                                             uint32_t log_size, Planes out) {
   constexpr uint32_t RG = 8 / EG, TILE = 128 * RG, STRIDE = EG * ACC_ROUND;
-  __shared__ NumEntry se[ACC_MAX_SMEM_ENTRIES];
   extern __shared__ uint4 dyn[];  // [warp][slot][entry][lane] in the loop; part[group][q][row] after it
   uint32_t* part = reinterpret_cast<uint32_t*>(dyn);
-  const bool staged = n_entries <= ACC_MAX_SMEM_ENTRIES;
-  if (staged)
-    for (uint32_t k = threadIdx.x; k < n_entries; k += blockDim.x) se[k] = entries[k];
-  __syncthreads();
-  const NumEntry* E = staged ? se : entries;
+  // entries are read where they lie (every thread of a warp reads the same
+  // entry, an L1 broadcast): without a shared copy, 4 blocks fit on an SM
+  const NumEntry* E = entries;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t eg = warp / RG, rg = warp % RG;
   uint4* wbuf = dyn + (size_t)warp * 2 * ACC_ROUND * 32;
