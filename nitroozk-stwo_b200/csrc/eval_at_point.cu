@@ -14,8 +14,6 @@
 
 namespace gs {
 
-constexpr uint32_t EAP_S = 12;                 // default low bits per chunk: 4096 coefficients
-
 struct Factors { qm31 f[31]; };
 
 // W[j] = prod over set bits b < s of j of F_b, for j < 2^s (one thread each).
