@@ -470,14 +470,17 @@ __global__ void __launch_bounds__(P252_GRIND_STEP) poseidon252_grind_kernel(cons
 }
 
 int poseidon252_grind(cudaStream_t st, const uint8_t* d_digest, uint32_t pow_bits, uint8_t* d_scratch,
-                      uint32_t* h_word, uint64_t* nonce_out) {
+                      uint32_t* h_word, uint64_t* nonce_out, bool digest_is_prefixed) {
   GS_REQUIRE(pow_bits <= 128, "pow_bits > 128 is not supported");
   GS_REQUIRE(((uintptr_t)d_digest & 15) == 0 && ((uintptr_t)d_scratch & 15) == 0, "buffers must be 16-byte aligned");
-  uint8_t* d_pre = d_scratch;                                                          // 32 bytes
+  const uint8_t* d_pre = d_digest;
   unsigned long long* d_res = reinterpret_cast<unsigned long long*>(d_scratch + 32);  // 8 bytes
-  poseidon252_pow_prefix_kernel<<<1, 32, 0, st>>>(d_digest, pow_bits, d_pre);
-  note_launch();
-  GS_CUDA_TRY(cudaGetLastError());
+  if (!digest_is_prefixed) {  // one thread, two permutations
+    d_pre = d_scratch;        // 32 bytes
+    poseidon252_pow_prefix_kernel<<<1, 32, 0, st>>>(d_digest, pow_bits, d_scratch);
+    note_launch();
+    GS_CUDA_TRY(cudaGetLastError());
+  }
   // high words per launch: about twice the expected number of chunks
   // (2^(pow_bits - 14) each), 1 to 64
   const uint32_t e = pow_bits > P252_GRIND_LOW_LOG ? pow_bits - P252_GRIND_LOW_LOG + 1 : 0;

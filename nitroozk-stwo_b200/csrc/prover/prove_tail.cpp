@@ -228,11 +228,13 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   GS_TRY(fri_commit(pv, quot, lifting, first, inner, last, sanity));
   pv.mark("fri_commit");
   uint64_t nonce = 0;
-  if (pv.ch.p252) {  // GrindOps<Poseidon252Channel>: the device derives the prefix from the digest
-    const void* d_digest = nullptr;
-    GS_TRY(pv.ctx.stage_bytes(pv.ch.digest.data(), 32, &d_digest));
-    GS_TRY(poseidon252_grind(st, (const uint8_t*)d_digest, cfg.pow_bits, pv.ctx.d_small, (uint32_t*)pv.ctx.h_small,
-                             &nonce));
+  if (pv.ch.p252) {  // GrindOps<Poseidon252Channel>; the prefix hash on the host
+    namespace f = host::p252;
+    const auto pre = f::to_bytes(f::hash_many({f::from_u64(0x12345678u), pv.ch.fdigest(), f::from_u64(cfg.pow_bits)}));
+    const void* d_pre = nullptr;
+    GS_TRY(pv.ctx.stage_bytes(pre.data(), 32, &d_pre));
+    GS_TRY(poseidon252_grind(st, (const uint8_t*)d_pre, cfg.pow_bits, pv.ctx.d_small, (uint32_t*)pv.ctx.h_small,
+                             &nonce, true));
   } else {
     auto pre = pv.ch.pow_prefixed(cfg.pow_bits);
     GS_TRY(grind_blake2s(st, pre.data(), cfg.pow_bits, (uint32_t*)pv.ctx.d_small, &nonce,

@@ -170,8 +170,10 @@ int poseidon252_commit_on_layer(cudaStream_t st, uint32_t log_size, const uint8_
                                 const uint32_t* const* d_cols, uint32_t n_cols, uint8_t* d_out);
 int poseidon252_permute(cudaStream_t st, const uint8_t* d_in, uint32_t n, uint8_t* d_out);
 // d_scratch: 48 bytes of device memory; h_word: 8 bytes of pinned host memory.
+// digest_is_prefixed: d_digest already holds poseidon_hash_many([POW_PREFIX,
+// digest, pow_bits]) (computed by a host that has the channel).
 int poseidon252_grind(cudaStream_t st, const uint8_t* d_digest, uint32_t pow_bits, uint8_t* d_scratch,
-                      uint32_t* h_word, uint64_t* nonce_out);
+                      uint32_t* h_word, uint64_t* nonce_out, bool digest_is_prefixed = false);
 
 // FRI layers of log size <= 11 in one launch (fri.cu): layer k has log size
 // log0 - k; layers 0..n-1 are committed (tree[k][L] = their Merkle layers,
