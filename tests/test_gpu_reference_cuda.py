@@ -238,6 +238,14 @@ def test_timing_against_reference_cuda(ref, B):
     ours = _time(lambda: B.fold_line(planes, 22, [1, 2, 3, 4], tw))
     theirs = _time(lambda: ref_fold_line(ref, planes, 22, [1, 2, 3, 4], tw, folded))
     rows.append(("fold_line 2^22", ours, theirs))
+    epolys = [to_device(rng.integers(0, P, 1 << 18, dtype=np.int64).astype(np.uint32)) for _ in range(160)]
+    epoint = [int(v) for v in rng.integers(0, P, 8)]
+    etable = torch.tensor([p.data_ptr() for p in epolys], dtype=torch.int64, device="cuda")
+    eres = (QM31 * 160)()
+    ours = _time(lambda: B.batch_eval_at_point(epolys, epoint), reps=3)
+    theirs = _time(lambda: ref.batch_eval_at_points(etable.data_ptr(), 1 << 18, 160, QM31(*epoint[:4]),
+                                                   QM31(*epoint[4:]), eres), reps=3)
+    rows.append(("OODS 160 polys x 2^18", ours, theirs))
     pcols = [to_device(rng.integers(0, P, 1 << 18, dtype=np.int64).astype(np.uint32)) for _ in range(8)]
     pout = torch.empty((1 << 18) * 32, dtype=torch.uint8, device="cuda")
     ours = _time(lambda: B.poseidon252_commit_on_layer(18, None, pcols, out=pout), reps=3)
