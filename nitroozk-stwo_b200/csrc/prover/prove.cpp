@@ -239,7 +239,7 @@ static int finish_last_layer(Prover& pv, const uint32_t* h, uint32_t log, std::v
 // compute_decommitment_positions_and_witness_evals (prover/fri.rs:301-330),
 // fold step 1: positions are both members of each queried pair; the witness
 // values are the pair members that were not queried.
-void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::vector<bool>& is_witness) {
+void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::vector<uint8_t>& is_witness) {
   size_t i = 0;
   while (i < q.size()) {
     size_t start = (q[i] >> 1) << 1;
@@ -248,8 +248,8 @@ void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::
     size_t k = i;
     for (size_t p = start; p < start + 2; p++) {
       pos.push_back(p);
-      if (k < j && q[k] == p) { k++; is_witness.push_back(false); }
-      else is_witness.push_back(true);
+      if (k < j && q[k] == p) { k++; is_witness.push_back(0); }
+      else is_witness.push_back(1);
     }
     i = j;
   }

@@ -10,7 +10,7 @@ namespace prover {
 
 int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first, std::vector<FriLayerDev>& inner,
                std::vector<qm31>& last_coeffs, const std::function<void()>& while_busy);
-void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::vector<bool>& is_witness);
+void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::vector<uint8_t>& is_witness);
 
 struct ColSamples {
   std::vector<ptq> points;
@@ -253,7 +253,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   g.clear();
   struct FriPlan {
     std::vector<size_t> pos;
-    std::vector<bool> wit;
+    std::vector<uint8_t> wit;  // 1: the position is a witness value
     size_t val_base = 0;
     MerkleDecommitPlan merkle;
   };
