@@ -107,12 +107,27 @@ __host__ __device__ __forceinline__ void p2_external(uint32_t* s) {
     for (int i = 0; i < 4; i++) s[4 * i + j] = add(s[4 * i + j], t);
   }
 }
+// x * 2^k mod p for canonical x and 1 <= k <= 30: the 31-bit rotation of x
+// left by k, which is canonical again (a rotation of a word that is not all
+// ones is not all ones). On the device: one wide multiply by 2^(k+1), whose
+// high word x >> (31 - k) and halved low word (x << k) mod 2^31 occupy
+// disjoint bits, then one shift-add; no reduction step.
+__host__ __device__ __forceinline__ uint32_t mul_pow2(uint32_t x, int k) {
+#ifdef __CUDA_ARCH__
+  uint64_t w = (uint64_t)x * (2u << k);
+  return (uint32_t)(w >> 32) + ((uint32_t)w >> 1);
+#else
+  return ((x << k) & P) | (x >> (31 - k));
+#endif
+}
+// The internal round matrix: s_i * 2^(i+1) + sum (the reference multiplies
+// by the constant, poseidon/mod.rs:132-146).
 __host__ __device__ __forceinline__ void p2_internal(uint32_t* s) {
   uint32_t sum = s[0];
 #pragma unroll
   for (int i = 1; i < 16; i++) sum = add(sum, s[i]);
 #pragma unroll
-  for (int i = 0; i < 16; i++) s[i] = add(mul(s[i], 1u << (i + 1)), sum);
+  for (int i = 0; i < 16; i++) s[i] = add(mul_pow2(s[i], i + 1), sum);
 }
 __host__ __device__ __forceinline__ uint32_t pow5(uint32_t x) { uint32_t x2 = sqr(x); return mul(sqr(x2), x); }
 
@@ -163,7 +178,12 @@ __device__ __forceinline__ qm31 combine16(const LookupParams& lp, const uint32_t
     uint32_t x = __ldg(v + (size_t)i * stride + r);
     const uint32_t* a = lp.alpha_pow + 4 * i;
 #pragma unroll
-    for (int q = 0; q < 4; q++) acc[q] = fold64a(acc[q] + (uint64_t)a[q] * x);
+    for (int q = 0; q < 4; q++) acc[q] += (uint64_t)a[q] * x;
+    // three products (< 2^62 each) and a folded accumulator (< 2^34) fit in 64 bits
+    if (i % 3 == 2 || i == 15) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[q] = fold64a(acc[q]);
+    }
   }
   qm31 s = qm_make(reduce64(acc[0]), reduce64(acc[1]), reduce64(acc[2]), reduce64(acc[3]));
   return qm_sub(s, qm_make(lp.z[0], lp.z[1], lp.z[2], lp.z[3]));

@@ -169,19 +169,43 @@ def test_grind(B, pow_bits, salt):
 
 
 # ---------------------------------------------------------------- full sizes
-@pytest.mark.parametrize("log_n", [22, 24, 26])
-def test_fft_roundtrip_full_size(B, log_n):
-    """interpolate(evaluate(c)) == c and the LDE restricted to the even rows of
-    CanonicCoset(n+1) ... is checked by sampled points against the oracle."""
+def bit_reverse_index(i, log_n):
+    return int(format(i, f"0{log_n}b")[::-1], 2) if log_n else i
+
+
+def canonic_domain_point(log_n, i):
+    """CanonicCoset(log_n).circle_domain().at(i) (core/poly/circle/domain.rs:
+    57-68) as an M31 point: the half coset half_odds(log_n - 1) then its
+    conjugate."""
+    half = 1 << (log_n - 1)
+    init, step = 1 << (31 - (log_n + 1)), 1 << (31 - (log_n - 1))
+    idx = (init + step * (i % half)) % (1 << 31)
+    if i >= half:
+        idx = (-idx) % (1 << 31)
+    xy = np.zeros(2, np.uint32)
+    O.lib().oracle_index_to_point(idx, xy.ctypes.data_as(O.U32P))
+    return int(xy[0]), int(xy[1])
+
+
+@pytest.mark.parametrize("log_n,n_points", [(22, 4), (24, 3), (26, 2)])
+def test_fft_full_size_against_oracle_points(B, log_n, n_points):
+    """The kernel sweep's top sizes: evaluate on CanonicCoset(n) and check
+    sampled rows against the oracle's direct evaluation of the coefficient
+    polynomial at those domain points (fold over the circle FFT basis,
+    independent of any twiddle table), then interpolate back and require the
+    original coefficients. The reference's own CUDA FFT is compared at the
+    same sizes in test_gpu_reference_cuda.py."""
     rng = np.random.default_rng(600 + log_n)
     c = rand_m31(rng, 1 << log_n)
     tw = B.precompute_twiddles(log_n)
     ev = B.evaluate_polynomials([dev(c)], log_n, tw)[0]
+    ev_h = host(ev)
+    for j in rng.integers(0, 1 << log_n, n_points):
+        x, y = canonic_domain_point(log_n, bit_reverse_index(int(j), log_n))
+        want = O.eval_at_point(c, np.array([x, 0, 0, 0, y, 0, 0, 0], np.uint32))
+        assert list(want) == [int(ev_h[j]), 0, 0, 0], f"row {j}"
     B.interpolate_columns([ev], log_n, tw)
     assert np.array_equal(host(ev), c)
-    # sampled evaluation points against the oracle's basis definition
-    lde = B.evaluate_polynomials([dev(c[: 1 << 12].copy())], 13, B.precompute_twiddles(12))[0]
-    assert np.array_equal(host(lde), O.evaluate(c[: 1 << 12], 13, root_log=12))
 
 
 def test_merkle_64x2p20_root(B):

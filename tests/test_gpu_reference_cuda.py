@@ -79,7 +79,7 @@ def ref_interpolate(ref, cols, log, tw):
     ref.ntt_b2n_column(arr, log, len(cols), tw.itwiddles.data_ptr(), 1 << (log - 1), 1 << (log - 1))
 
 
-@pytest.mark.parametrize("log,n_cols", [(13, 3), (16, 2), (19, 1), (20, 4), (24, 1)])
+@pytest.mark.parametrize("log,n_cols", [(13, 3), (16, 2), (19, 1), (20, 4), (24, 1), (25, 1), (26, 1)])
 def test_fft_matches_reference_cuda(ref, B, log, n_cols):
     from gpustark.backend import to_device
     rng = np.random.default_rng(log)
@@ -127,7 +127,7 @@ def test_fold_line_matches_reference_cuda(ref, B, log):
         assert torch.equal(a, b)
 
 
-@pytest.mark.parametrize("log", [4, 13, 21])
+@pytest.mark.parametrize("log", [4, 13, 21, 23])
 def test_fold_circle_into_line_matches_reference_cuda(ref, B, log):
     from gpustark.backend import to_device
     rng = np.random.default_rng(300 + log)
