@@ -43,6 +43,10 @@ def _declare(L):
         fn.argtypes = list(args)
 
     f("oracle_set_threads", None, C.c_int)
+    f("oracle_verify", C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, U32P, C.c_uint32, U32P, U8P,
+      C.c_size_t, C.c_char_p, C.c_size_t)
+    f("oracle_verify_lookup_elements", C.c_int, C.c_uint32, U8P, C.c_size_t, U32P, U32P)
+    f("oracle_poseidon_claimed_sum", None, C.c_uint32, C.c_uint64, C.c_uint32, U32P, U32P, U32P, U32P)
     f("oracle_max_threads", C.c_int)
     f("oracle_m31_reduce", C.c_uint32, C.c_uint64)
     f("oracle_m31_partial_reduce", C.c_uint32, C.c_uint32)
@@ -370,3 +374,68 @@ def prove(air, log_n, n_cols=100, seed=0, input_mode=0, pow_bits=10, n_queries=7
 
 def seeded_m31(seed, col, row):
     return lib().oracle_seeded_m31(seed, col, row)
+
+
+# ------------------------------------------------------------------ verifier
+VERIFY_ERRORS = {1: "InvalidStructure", 2: "Merkle", 3: "OodsNotMatching", 4: "Fri", 5: "ProofOfWork"}
+
+
+class VerificationError(RuntimeError):
+    """The verifier rejected the proof; ``kind`` is the reference's
+    VerificationError variant (core/verifier.rs:124-139)."""
+
+    def __init__(self, code, msg):
+        self.kind = VERIFY_ERRORS.get(code, str(code))
+        super().__init__(f"{self.kind}: {msg}")
+
+
+def _bytes_ptr(data):
+    buf = (C.c_uint8 * max(1, len(data))).from_buffer_copy(data if data else b"\0")
+    return buf, C.cast(buf, U8P)
+
+
+def poseidon_claimed_sum(proof, log_n, seed=0, input_mode=0, host_inputs=None, merkle_channel="blake2s"):
+    """The logup claimed sum of the Poseidon2 trace the proof was made for
+    (the statement the prover reports beside the proof): lookup elements
+    drawn from the proof's first two commitments, then the sum over rows of
+    1/combine(initial) - 1/combine(final)."""
+    L = lib()
+    buf, bp = _bytes_ptr(proof)
+    z = np.zeros(4, np.uint32)
+    a = np.zeros(4, np.uint32)
+    if L.oracle_verify_lookup_elements(1 if merkle_channel == "poseidon252" else 0, bp, len(proof),
+                                       z.ctypes.data_as(U32P), a.ctypes.data_as(U32P)):
+        raise VerificationError(1, "proof bytes do not parse")
+    out = np.zeros(4, np.uint32)
+    hp = None
+    if host_inputs is not None:
+        h = np.ascontiguousarray(host_inputs, dtype=np.uint32)
+        hp = h.ctypes.data_as(U32P)
+    L.oracle_poseidon_claimed_sum(log_n, seed, input_mode, hp, z.ctypes.data_as(U32P), a.ctypes.data_as(U32P),
+                                  out.ctypes.data_as(U32P))
+    return out
+
+
+def verify(proof, air, log_n, n_cols=100, split_log=None, claimed_sum=None, merkle_channel="blake2s", config=None):
+    """Runs the verifier (verifier.h) on serialised proof bytes; returns True
+    or raises VerificationError. Poseidon2 needs the claimed sum. config: the
+    verifier's PcsConfig as (pow_bits, log_blowup, log_last_layer, n_queries,
+    line_fold_step), or None to use the one serialised in the proof."""
+    if split_log is None:
+        split_log = default_split(air)
+    L = lib()
+    buf, bp = _bytes_ptr(proof)
+    cs = None
+    if claimed_sum is not None:
+        c = np.ascontiguousarray(claimed_sum, dtype=np.uint32)
+        cs = c.ctypes.data_as(U32P)
+    cfg = None
+    if config is not None:
+        cw = np.array(config, np.uint32)
+        cfg = cw.ctypes.data_as(U32P)
+    msg = C.create_string_buffer(256)
+    code = L.oracle_verify(0 if air == "wide_fibonacci" else 1, log_n, n_cols, split_log, cs,
+                           1 if merkle_channel == "poseidon252" else 0, cfg, bp, len(proof), msg, 256)
+    if code:
+        raise VerificationError(code, msg.value.decode())
+    return True
