@@ -215,14 +215,106 @@ int gs_batch_eval_at_point(gs_ctx* ctx, const uint32_t* const* polys, uint32_t n
  * gs_batch_eval_at_point, results identical, but allocating nothing: no
  * context, no cudaMalloc/cudaFree, no pinned staging. Its device scratch is
  * one file-scope __device__ array of 4 MiB + 22 KiB per device, whose address
- * is looked up with cudaGetSymbolAddress on the first call on each device
- * (make that first call before any stream capture). Limits, checked before
+ * is looked up with cudaGetSymbolAddress on the first call under each CUDA
+ * context (with the device's primary context, the usual case, once per
+ * device; make that first call before any stream capture) and cached per
+ * context. Limits, checked before
  * any launch (ERR_INVALID otherwise): n_polys <= 256 and
  * n_polys * 2^max(log_size - 10, 0) <= 2^18. Runs on `stream` (a
  * cudaStream_t; NULL = the default stream) and synchronises it. Calls that
  * overlap in time on one device race on the shared array: serialise them. */
 int gs_batch_eval_at_point_noalloc(void* stream, const uint32_t* const* polys, uint32_t n_polys, uint32_t log_size,
                                    gs_point_qm31 point, gs_qm31* out);
+
+/* ------------------------------------------------- column gathers (decommit) */
+/* cuda_batch_gather_multi_uint32 (bindings.rs:314-320); Column::
+ * batch_at_multi (prover/backend/mod.rs:73-89; CUDA prover/backend/cuda/
+ * column.rs:198): the values of n_cols device columns (each at least col_len
+ * words) at n_indices positions, written to host memory row-major:
+ * out[i * n_cols + c] = cols[c][indices[i]]. Indices >= col_len are rejected
+ * (ERR_INVALID) before any device work. Synchronises. */
+int gs_batch_gather_multi_uint32(gs_ctx* ctx, const uint32_t* const* cols, uint32_t n_cols, size_t col_len,
+                                 const uint32_t* indices, uint32_t n_indices, uint32_t* out);
+/* cuda_batch_get_blake_2s_hash (bindings.rs:300-305); Column<Blake2sHash>::
+ * batch_at for MerkleProver::decommit (prover/vcs/prover.rs:84-217): hashes of
+ * one device layer of n_hashes (16-byte aligned) at the indices, 8 words
+ * each, written to host memory. Synchronises. */
+int gs_batch_get_blake2s_hash(gs_ctx* ctx, const uint32_t* layer, size_t n_hashes, const uint32_t* indices,
+                              uint32_t n_indices, uint32_t* out);
+
+/* ---------------------------------------------------- barycentric OODS */
+/* barycentric_weights_cuda (bindings.rs:141-151); PolyOps::
+ * barycentric_weights (prover/poly/circle/ops.rs:64-68; CPU prover/backend/
+ * cpu/circle.rs:101-132): the weights of CanonicCoset(log_size) at `point`,
+ * 2^log_size QM31 values in bit-reversed domain order, written to 4 device
+ * planes. The point must not lie on the domain. */
+int gs_barycentric_weights(gs_ctx* ctx, uint32_t log_size, gs_point_qm31 point, uint32_t* const weights[4]);
+/* barycentric_eval_at_point_cuda (bindings.rs:153-158); PolyOps::
+ * barycentric_eval_at_point (ops.rs:73-77; cpu/circle.rs:134-141): the sum of
+ * evals[i] * weights[i] over 2^log_size bit-reversed evaluations (device), to
+ * host memory. Synchronises. */
+int gs_barycentric_eval_at_point(gs_ctx* ctx, const uint32_t* evals, const uint32_t* const weights[4],
+                                 uint32_t log_size, gs_qm31* out);
+
+/* ---------------------------------------------- example trace generation */
+/* generate_wide_fibonacci_trace (bindings.rs:426-433; CUDA
+ * evaluate_wide_fibonacci.cu:127-179): trace[0] = input_a, trace[1] =
+ * input_b, trace[k] = trace[k-2]^2 + trace[k-1]^2 over 2^log_size rows;
+ * inputs and the n_columns trace columns are device buffers. */
+int gs_generate_wide_fibonacci_trace(gs_ctx* ctx, const uint32_t* input_a, const uint32_t* input_b,
+                                     uint32_t log_size, uint32_t* const* traces, uint32_t n_columns);
+/* generate_poseidon_traces (bindings.rs:435-440; CUDA
+ * evaluate_poseidon_constraint.cu:270-363): the 158 Poseidon2 trace columns
+ * of 2^log_size rows with the reference's inputs (row r, lane i: r + i), and
+ * the 16 initial- and final-state columns the lookup uses (device). */
+int gs_generate_poseidon_traces(gs_ctx* ctx, uint32_t* const* traces, uint32_t* const* lookup_init,
+                                uint32_t* const* lookup_final, uint32_t log_size);
+/* generate_poseidon_interaction_traces (bindings.rs:442-449; CUDA
+ * evaluate_poseidon_constraint.cu:365-600; semantics crates/examples/src/
+ * poseidon/mod.rs:305-335): the logup interaction column (4 device planes,
+ * the shifted prefix sum in coset order) of the fractions 1/combine(init) -
+ * 1/combine(final), and the claimed sum (4 words, host memory; the
+ * reference writes it to device memory). lookup_elements: the #[repr(C)]
+ * LookupElements<16> { z, alpha, alpha_powers[16] }, QM31 as 4 words.
+ * Synchronises. */
+int gs_generate_poseidon_interaction_traces(gs_ctx* ctx, const void* lookup_elements,
+                                            const uint32_t* const* lookup_init, const uint32_t* const* lookup_final,
+                                            uint32_t log_size, uint32_t* const interaction_traces[4],
+                                            uint32_t claimed_sum[4]);
+
+/* ------------------------------------------------- constraint accumulation */
+/* AccumulationOps::generate_secure_powers (prover/air/accumulation.rs:127-145;
+ * the reference's CUDA backend computes it on the host, prover/backend/cuda/
+ * accumulation.rs:20-22): out[i] = felt^i for i < n, 4 device planes. */
+int gs_generate_secure_powers(gs_ctx* ctx, gs_qm31 felt, size_t n, uint32_t* const out[4]);
+/* evaluate_constraint_quotients_on_domain (bindings.rs:469-490), called by
+ * ComponentProver<CudaBackend>::evaluate_constraint_quotients_on_domain
+ * (constraint-framework/src/prover/component_prover.rs:249-498): per row of
+ * the evaluation domain, sum_k random_coeff_powers[k] * C_k(row) times
+ * denominator_inverses[row >> domain_log_size], written to (or, with
+ * should_accumulate, added to) the 4 quotient planes. trace0/1/2: host arrays
+ * of device columns on the evaluation domain (preprocessed, trace,
+ * interaction); random_coeff_powers: n_constraints QM31 values in the order
+ * the constraints are added (the reversed accumulator powers) and
+ * denominator_inverses: 2^(eval_domain_log_size - domain_log_size) words,
+ * both HOST arrays (the reference uploads them first). eval: the buffer the
+ * reference's ComponentProver builds, eval_id (FNV-1a of
+ * FrameworkEval::cuda_eval_name) followed by the component's #[repr(C)] Eval
+ * struct, eval_len bytes. Supported ids: "fibonacci_example" (WideFibonacciEval,
+ * trace1 = n_constraints + 2 columns) and "poseidon_example" (PoseidonEval,
+ * 158 trace and 4 interaction columns, 143 constraints); any other id
+ * returns GS_ERR_UNSUPPORTED (the reference returns false and falls back to
+ * the CPU; this library has no CPU path). cumsum_shift = claimed_sum /
+ * 2^domain_log_size; logup_counts is accepted and unused. */
+int gs_evaluate_constraint_quotients_on_domain(gs_ctx* ctx, uint32_t* const quotients[4],
+                                               const uint32_t* const* trace0, uint32_t trace0_len,
+                                               const uint32_t* const* trace1, uint32_t trace1_len,
+                                               const uint32_t* const* trace2, uint32_t trace2_len,
+                                               const gs_qm31* random_coeff_powers,
+                                               const uint32_t* denominator_inverses, uint32_t domain_log_size,
+                                               uint32_t eval_domain_log_size, uint32_t n_constraints,
+                                               uint32_t logup_counts, const void* eval, size_t eval_len,
+                                               gs_qm31 cumsum_shift, int should_accumulate);
 
 /* --------------------------------------------------------------- GrindOps */
 /* grind_blake2s (bindings.rs:615); GrindOps<Blake2sChannel>::grind

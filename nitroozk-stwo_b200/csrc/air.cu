@@ -58,15 +58,53 @@ __global__ void wf_trace_kernel(uint32_t* cols, uint32_t log_n, uint32_t n_cols,
 
 __device__ __forceinline__ uint64_t fold64a(uint64_t x) { return (x & P) + (x >> 31); }
 
-__global__ void __launch_bounds__(256) wf_constraints_kernel(const uint32_t* __restrict__ cols, uint32_t n_cols,
-                                                             uint32_t eval_log, uint32_t trace_log, ConstraintParams prm,
-                                                             Planes out) {
+// Column access of the constraint kernels: a tree's columns as one
+// contiguous buffer (the prover's layout: column c at base + c * n), or a
+// device table of column pointers (callers of the C ABI, whose columns are
+// separate allocations). cursor(c, r) walks row r of columns c, c+1, ...
+struct ContigCols {
+  const uint32_t* base;
+  size_t n;
+  struct Cursor {
+    const uint32_t* p;
+    size_t n;
+    __device__ __forceinline__ uint32_t next() {
+      uint32_t v = __ldg(p);
+      p += n;
+      return v;
+    }
+  };
+  __device__ __forceinline__ const uint32_t* col(uint32_t c) const { return base + (size_t)c * n; }
+  __device__ __forceinline__ Cursor cursor(uint32_t c, size_t r) const { return Cursor{col(c) + r, n}; }
+};
+struct TableCols {
+  const uint32_t* const* tab;
+  struct Cursor {
+    const uint32_t* const* t;
+    size_t r;
+    __device__ __forceinline__ uint32_t next() { return __ldg(*t++ + r); }
+  };
+  __device__ __forceinline__ const uint32_t* col(uint32_t c) const { return tab[c]; }
+  __device__ __forceinline__ Cursor cursor(uint32_t c, size_t r) const { return Cursor{tab + c, r}; }
+};
+
+// Writes (accumulate == 0) or adds to (accumulate != 0) the output planes.
+__device__ __forceinline__ void store_quotient(const Planes& out, size_t r, const uint32_t v[4], uint32_t accumulate) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) out.p[q][r] = accumulate ? add(out.p[q][r], v[q]) : v[q];
+}
+
+template <class Cols>
+__global__ void __launch_bounds__(256) wf_constraints_kernel(Cols cols, uint32_t n_cols, uint32_t eval_log,
+                                                             uint32_t trace_log, ConstraintParams prm, Planes out,
+                                                             uint32_t accumulate) {
   const size_t n = (size_t)1 << eval_log;
   for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
-    uint32_t a = __ldg(cols + r), b = __ldg(cols + n + r);
+    auto cur = cols.cursor(0, r);
+    uint32_t a = cur.next(), b = cur.next();
     uint64_t acc[4] = {0, 0, 0, 0};
     for (uint32_t k = 2; k < n_cols; k++) {
-      uint32_t c = __ldg(cols + (size_t)k * n + r);
+      uint32_t c = cur.next();
       uint32_t cons = sub(c, add(sqr(a), sqr(b)));
       const uint32_t* p = prm.powers + 4 * (k - 2);
 #pragma unroll
@@ -75,8 +113,10 @@ __global__ void __launch_bounds__(256) wf_constraints_kernel(const uint32_t* __r
       b = c;
     }
     uint32_t dinv = prm.denom_inv[r >> trace_log];
+    uint32_t v[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) out.p[q][r] = mul(reduce64(acc[q]), dinv);
+    for (int q = 0; q < 4; q++) v[q] = mul(reduce64(acc[q]), dinv);
+    store_quotient(out, r, v, accumulate);
   }
 }
 
@@ -171,11 +211,13 @@ __global__ void poseidon_trace_kernel(uint32_t* cols, uint32_t log_n, uint64_t s
   }
 }
 
-__device__ __forceinline__ qm31 combine16(const LookupParams& lp, const uint32_t* v, size_t stride, size_t r) {
+// LookupElements::combine of 16 columns (c0 .. c0 + 15) at row r.
+template <class Cols>
+__device__ __forceinline__ qm31 combine16(const LookupParams& lp, const Cols& cols, uint32_t c0, size_t r) {
   uint64_t acc[4] = {0, 0, 0, 0};
 #pragma unroll
   for (int i = 0; i < 16; i++) {
-    uint32_t x = __ldg(v + (size_t)i * stride + r);
+    uint32_t x = __ldg(cols.col(c0 + i) + r);
     const uint32_t* a = lp.alpha_pow + 4 * i;
 #pragma unroll
     for (int q = 0; q < 4; q++) acc[q] += (uint64_t)a[q] * x;
@@ -195,13 +237,16 @@ __device__ __forceinline__ uint32_t coset_index(uint32_t i, uint32_t log_n) {
   return j < n / 2 ? 2 * j : 2 * (n - 1 - j) + 1;
 }
 
-// Per row: (1/d0 - 1/d1) written at its coset-order position.
-__global__ void logup_fraction_kernel(const uint32_t* __restrict__ cols, uint32_t log_n, LookupParams lp,
-                                      uint4* __restrict__ coset_vals) {
+// Per row: (1/d0 - 1/d1) written at its coset-order position; d0 / d1 the
+// lookup combination of the initial / final state (16 columns each, from
+// column c_init of `init` and c_final of `fin`).
+template <class InitCols, class FinalCols>
+__global__ void logup_fraction_kernel(InitCols init, uint32_t c_init, FinalCols fin, uint32_t c_final, uint32_t log_n,
+                                      LookupParams lp, uint4* __restrict__ coset_vals) {
   const size_t n = (size_t)1 << log_n;
   for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
-    qm31 d0 = combine16(lp, cols, n, r);
-    qm31 d1 = combine16(lp, cols + (size_t)(158 - 16) * n, n, r);
+    qm31 d0 = combine16(lp, init, c_init, r);
+    qm31 d1 = combine16(lp, fin, c_final, r);
     qm31 v = qm_mul(qm_sub(d1, d0), qm_inv(qm_mul(d0, d1)));
     coset_vals[coset_index((uint32_t)r, log_n)] = make_uint4(v.x.a, v.x.b, v.y.a, v.y.b);
   }
@@ -214,16 +259,16 @@ struct AddQM {
 };
 
 // out_c[i] = S_c[k] - (k + 1) * shift_c at k = coset position of storage row i.
-__global__ void logup_finalize_kernel(const uint4* __restrict__ scan, uint32_t log_n, qm31 shift, uint32_t* out) {
+__global__ void logup_finalize_kernel(const uint4* __restrict__ scan, uint32_t log_n, qm31 shift, Planes out) {
   const size_t n = (size_t)1 << log_n;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     uint32_t k = coset_index((uint32_t)i, log_n);
     uint4 s = scan[k];
     uint32_t m = (k + 1) % P;
-    out[i] = sub(s.x, mul(shift.x.a, m));
-    out[n + i] = sub(s.y, mul(shift.x.b, m));
-    out[2 * n + i] = sub(s.z, mul(shift.y.a, m));
-    out[3 * n + i] = sub(s.w, mul(shift.y.b, m));
+    out.p[0][i] = sub(s.x, mul(shift.x.a, m));
+    out.p[1][i] = sub(s.y, mul(shift.x.b, m));
+    out.p[2][i] = sub(s.z, mul(shift.y.a, m));
+    out.p[3][i] = sub(s.w, mul(shift.y.b, m));
   }
 }
 
@@ -242,10 +287,11 @@ __device__ __forceinline__ uint32_t prev_row(uint32_t i, uint32_t trace_log, uin
 // 2^34, so three terms fit in 64 bits between folds; a fold follows every
 // third term of a round and the round's last term. The round loops stay
 // rolled: unrolled, the kernel outgrows the instruction cache.
-__global__ void __launch_bounds__(128) poseidon_constraints_kernel(const uint32_t* __restrict__ trace,
-                                                                   const uint32_t* __restrict__ inter, uint32_t eval_log,
+template <class TraceCols, class InterCols>
+__global__ void __launch_bounds__(128) poseidon_constraints_kernel(TraceCols trace, InterCols inter, uint32_t eval_log,
                                                                    uint32_t trace_log, ConstraintParams prm,
-                                                                   LookupParams lp, qm31 cumsum_shift, Planes out) {
+                                                                   LookupParams lp, qm31 cumsum_shift, Planes out,
+                                                                   uint32_t accumulate) {
   const size_t n = (size_t)1 << eval_log;
   for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
     uint64_t acc[4] = {0, 0, 0, 0};
@@ -261,11 +307,10 @@ __global__ void __launch_bounds__(128) poseidon_constraints_kernel(const uint32_
       }
       k++;
     };
-    const uint32_t* col = trace + r;
+    auto col = trace.cursor(0, r);
     uint32_t s[16];
 #pragma unroll
-    for (int i = 0; i < 16; i++) s[i] = __ldg(col + (size_t)i * n);
-    col += 16 * n;
+    for (int i = 0; i < 16; i++) s[i] = col.next();
 #pragma unroll 1
     for (int round = 0; round < 4; round++) {
 #pragma unroll
@@ -273,8 +318,7 @@ __global__ void __launch_bounds__(128) poseidon_constraints_kernel(const uint32_
       p2_external(s);
 #pragma unroll
       for (int i = 0; i < 16; i++) {
-        uint32_t m = __ldg(col);
-        col += n;
+        uint32_t m = col.next();
         add_cons(sub(pow5(s[i]), m), i, 15);
         s[i] = m;
       }
@@ -283,8 +327,7 @@ __global__ void __launch_bounds__(128) poseidon_constraints_kernel(const uint32_
     for (int round = 0; round < 14; round++) {
       s[0] = add(s[0], PN_RC);
       p2_internal(s);
-      uint32_t m = __ldg(col);
-      col += n;
+      uint32_t m = col.next();
       add_cons(sub(pow5(s[0]), m), 0, 0);
       s[0] = m;
     }
@@ -295,27 +338,26 @@ __global__ void __launch_bounds__(128) poseidon_constraints_kernel(const uint32_
       p2_external(s);
 #pragma unroll
       for (int i = 0; i < 16; i++) {
-        uint32_t m = __ldg(col);
-        col += n;
+        uint32_t m = col.next();
         add_cons(sub(pow5(s[i]), m), i, 15);
         s[i] = m;
       }
     }
     // logup: frac = 1/d0 - 1/d1 as (d1 - d0) / (d0 d1); constraint
     // (cur - prev + shift) * d0 d1 - (d1 - d0)
-    qm31 d0 = combine16(lp, trace, n, r);
-    qm31 d1 = combine16(lp, trace + (size_t)(158 - 16) * n, n, r);
+    qm31 d0 = combine16(lp, trace, 0, r);
+    qm31 d1 = combine16(lp, trace, 158 - 16, r);
     uint32_t pr = prev_row((uint32_t)r, trace_log, eval_log);
-    qm31 cur = qm_make(__ldg(inter + r), __ldg(inter + n + r), __ldg(inter + 2 * n + r), __ldg(inter + 3 * n + r));
-    qm31 prv = qm_make(__ldg(inter + pr), __ldg(inter + n + pr), __ldg(inter + 2 * n + pr), __ldg(inter + 3 * n + pr));
+    qm31 cur = qm_make(__ldg(inter.col(0) + r), __ldg(inter.col(1) + r), __ldg(inter.col(2) + r),
+                       __ldg(inter.col(3) + r));
+    qm31 prv = qm_make(__ldg(inter.col(0) + pr), __ldg(inter.col(1) + pr), __ldg(inter.col(2) + pr),
+                       __ldg(inter.col(3) + pr));
     qm31 lc = qm_sub(qm_mul(qm_add(qm_sub(cur, prv), cumsum_shift), qm_mul(d0, d1)), qm_sub(d1, d0));
     qm31 pl = qm_make(prm.powers[4 * k], prm.powers[4 * k + 1], prm.powers[4 * k + 2], prm.powers[4 * k + 3]);
     qm31 res = qm_add(qm_make(reduce64(acc[0]), reduce64(acc[1]), reduce64(acc[2]), reduce64(acc[3])), qm_mul(pl, lc));
     uint32_t dinv = prm.denom_inv[r >> trace_log];
-    out.p[0][r] = mul(res.x.a, dinv);
-    out.p[1][r] = mul(res.x.b, dinv);
-    out.p[2][r] = mul(res.y.a, dinv);
-    out.p[3][r] = mul(res.y.b, dinv);
+    uint32_t v[4] = {mul(res.x.a, dinv), mul(res.x.b, dinv), mul(res.y.a, dinv), mul(res.y.b, dinv)};
+    store_quotient(out, r, v, accumulate);
   }
 }
 
@@ -336,8 +378,19 @@ int wf_trace(cudaStream_t st, uint32_t* cols, uint32_t log_n, uint32_t n_cols, u
 int wf_constraints(cudaStream_t st, const uint32_t* cols, uint32_t n_cols, uint32_t eval_log, uint32_t trace_log,
                    const ConstraintParams& prm, Planes out) {
   GS_REQUIRE(n_cols >= 3 && n_cols - 2 <= MAX_CONSTRAINTS, "bad wide fibonacci width");
-  wf_constraints_kernel<<<grid_rows((size_t)1 << eval_log, 256), 256, 0, st>>>(cols, n_cols, eval_log, trace_log, prm,
-                                                                                out);
+  wf_constraints_kernel<<<grid_rows((size_t)1 << eval_log, 256), 256, 0, st>>>(
+      ContigCols{cols, (size_t)1 << eval_log}, n_cols, eval_log, trace_log, prm, out, 0u);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+int wf_constraints_table(cudaStream_t st, const uint32_t* const* d_cols, uint32_t n_cols, uint32_t eval_log,
+                         uint32_t trace_log, const ConstraintParams& prm, Planes out, bool accumulate) {
+  GS_REQUIRE(n_cols >= 3 && n_cols - 2 <= MAX_CONSTRAINTS, "bad wide fibonacci width");
+  GS_REQUIRE(eval_log > trace_log && eval_log - trace_log <= 3 && eval_log <= 30, "bad domain sizes");
+  wf_constraints_kernel<<<grid_rows((size_t)1 << eval_log, 256), 256, 0, st>>>(
+      TableCols{d_cols}, n_cols, eval_log, trace_log, prm, out, accumulate ? 1u : 0u);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;
@@ -358,17 +411,20 @@ size_t logup_scratch_bytes(uint32_t log_n) {
   return 2 * n * sizeof(uint4) + ((temp + 255) & ~(size_t)255);
 }
 
-// Interaction column: writes the 4 coordinate columns (out, 4 x 2^log_n) and
-// the claimed sum (host). scratch: logup_scratch_bytes(log_n).
-int poseidon_interaction(cudaStream_t st, const uint32_t* trace, uint32_t log_n, const LookupParams& lp,
-                         uint32_t* out, void* scratch, qm31* claimed_sum, void* h_pinned) {
+// The interaction trace from the 16 initial- and final-state columns (given
+// as accessors), written to 4 planes, and the claimed sum (host). scratch:
+// logup_scratch_bytes(log_n).
+template <class InitCols, class FinalCols>
+static int interaction_impl(cudaStream_t st, InitCols init, uint32_t c_init, FinalCols fin, uint32_t c_final,
+                            uint32_t log_n, const LookupParams& lp, Planes out, void* scratch, qm31* claimed_sum,
+                            void* h_pinned) {
   size_t n = (size_t)1 << log_n;
   uint4* vals = (uint4*)scratch;
   uint4* scan = vals + n;
   void* temp = (void*)(scan + n);
   size_t temp_bytes = 0;
   cub::DeviceScan::InclusiveScan(nullptr, temp_bytes, (const uint4*)nullptr, (uint4*)nullptr, AddQM(), (int)n);
-  logup_fraction_kernel<<<grid_rows(n, 128), 128, 0, st>>>(trace, log_n, lp, vals);
+  logup_fraction_kernel<<<grid_rows(n, 128), 128, 0, st>>>(init, c_init, fin, c_final, log_n, lp, vals);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   GS_CUDA_TRY(cub::DeviceScan::InclusiveScan(temp, temp_bytes, (const uint4*)vals, scan, AddQM(), (int)n, st));
@@ -387,12 +443,124 @@ int poseidon_interaction(cudaStream_t st, const uint32_t* trace, uint32_t log_n,
   return OK;
 }
 
+// Interaction column: writes the 4 coordinate columns (out, 4 x 2^log_n) and
+// the claimed sum (host). scratch: logup_scratch_bytes(log_n).
+int poseidon_interaction(cudaStream_t st, const uint32_t* trace, uint32_t log_n, const LookupParams& lp,
+                         uint32_t* out, void* scratch, qm31* claimed_sum, void* h_pinned) {
+  const size_t n = (size_t)1 << log_n;
+  ContigCols t{trace, n};
+  return interaction_impl(st, t, 0, t, 158 - 16, log_n, lp, Planes{{out, out + n, out + 2 * n, out + 3 * n}},
+                          scratch, claimed_sum, h_pinned);
+}
+
+int poseidon_interaction_table(cudaStream_t st, const uint32_t* const* d_init, const uint32_t* const* d_final,
+                               uint32_t log_n, const LookupParams& lp, Planes out, void* scratch,
+                               qm31* claimed_sum) {
+  GS_REQUIRE(log_n >= 1 && log_n <= 28, "bad poseidon size");
+  return interaction_impl(st, TableCols{d_init}, 0, TableCols{d_final}, 0, log_n, lp, out, scratch, claimed_sum,
+                          nullptr);
+}
+
+// generate_wide_fibonacci_trace / generate_poseidon_traces (the reference's
+// CUDA trace generation, evaluate_wide_fibonacci.cu:127-179,
+// evaluate_poseidon_constraint.cu:270-363) into columns given by device
+// pointer tables: Wide-Fibonacci from the inputs a, b; Poseidon2 with the
+// reference's input rule (row + i), also writing the 16 initial- and
+// final-state lookup columns.
+__global__ void wf_trace_table_kernel(const uint32_t* __restrict__ in_a, const uint32_t* __restrict__ in_b, size_t n,
+                                      uint32_t* const* __restrict__ cols, uint32_t n_cols) {
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+    uint32_t a = __ldg(in_a + r), b = __ldg(in_b + r);
+    cols[0][r] = a;
+    cols[1][r] = b;
+    for (uint32_t k = 2; k < n_cols; k++) {
+      uint32_t c = add(sqr(a), sqr(b));
+      cols[k][r] = c;
+      a = b;
+      b = c;
+    }
+  }
+}
+
+__global__ void poseidon_trace_table_kernel(uint32_t* const* __restrict__ cols, uint32_t* const* __restrict__ init,
+                                            uint32_t* const* __restrict__ fin, size_t n) {
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+    uint32_t s[16];
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      s[i] = (uint32_t)((r + i) % P);
+      cols[c++][r] = s[i];
+      init[i][r] = s[i];
+    }
+    for (int round = 0; round < 4; round++) {
+#pragma unroll
+      for (int i = 0; i < 16; i++) s[i] = add(s[i], PN_RC);
+      p2_external(s);
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        s[i] = pow5(s[i]);
+        cols[c++][r] = s[i];
+      }
+    }
+    for (int round = 0; round < 14; round++) {
+      s[0] = add(s[0], PN_RC);
+      p2_internal(s);
+      s[0] = pow5(s[0]);
+      cols[c++][r] = s[0];
+    }
+    for (int round = 0; round < 4; round++) {
+#pragma unroll
+      for (int i = 0; i < 16; i++) s[i] = add(s[i], PN_RC);
+      p2_external(s);
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        s[i] = pow5(s[i]);
+        cols[c++][r] = s[i];
+        if (round == 3) fin[i][r] = s[i];
+      }
+    }
+  }
+}
+
+int wf_trace_table(cudaStream_t st, const uint32_t* in_a, const uint32_t* in_b, uint32_t log_n,
+                   uint32_t* const* d_cols, uint32_t n_cols) {
+  GS_REQUIRE(n_cols >= 2 && log_n <= 28, "bad wide fibonacci shape");
+  const size_t n = (size_t)1 << log_n;
+  wf_trace_table_kernel<<<grid_rows(n, 256), 256, 0, st>>>(in_a, in_b, n, d_cols, n_cols);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+int poseidon_trace_table(cudaStream_t st, uint32_t* const* d_cols, uint32_t* const* d_init, uint32_t* const* d_final,
+                         uint32_t log_n) {
+  GS_REQUIRE(log_n <= 28, "bad poseidon size");
+  const size_t n = (size_t)1 << log_n;
+  poseidon_trace_table_kernel<<<grid_rows(n, 128), 128, 0, st>>>(d_cols, d_init, d_final, n);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
 int poseidon_constraints(cudaStream_t st, const uint32_t* trace, const uint32_t* inter, uint32_t eval_log,
                          uint32_t trace_log, const ConstraintParams& prm, const LookupParams& lp, qm31 cumsum_shift,
                          Planes out) {
   GS_REQUIRE(eval_log > trace_log, "poseidon constraints need an extended domain");
-  poseidon_constraints_kernel<<<grid_rows((size_t)1 << eval_log, 128), 128, 0, st>>>(trace, inter, eval_log, trace_log,
-                                                                                      prm, lp, cumsum_shift, out);
+  const size_t n = (size_t)1 << eval_log;
+  poseidon_constraints_kernel<<<grid_rows(n, 128), 128, 0, st>>>(ContigCols{trace, n}, ContigCols{inter, n}, eval_log,
+                                                                  trace_log, prm, lp, cumsum_shift, out, 0u);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+int poseidon_constraints_table(cudaStream_t st, const uint32_t* const* d_trace, const uint32_t* const* d_inter,
+                               uint32_t eval_log, uint32_t trace_log, const ConstraintParams& prm,
+                               const LookupParams& lp, qm31 cumsum_shift, Planes out, bool accumulate) {
+  GS_REQUIRE(eval_log > trace_log && eval_log - trace_log <= 3 && eval_log <= 30, "bad domain sizes");
+  poseidon_constraints_kernel<<<grid_rows((size_t)1 << eval_log, 128), 128, 0, st>>>(
+      TableCols{d_trace}, TableCols{d_inter}, eval_log, trace_log, prm, lp, cumsum_shift, out, accumulate ? 1u : 0u);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;

@@ -24,6 +24,23 @@ struct LookupParams {
 int wf_trace(cudaStream_t st, uint32_t* cols, uint32_t log_n, uint32_t n_cols, uint64_t seed, uint32_t mode);
 int wf_constraints(cudaStream_t st, const uint32_t* cols, uint32_t n_cols, uint32_t eval_log, uint32_t trace_log,
                    const ConstraintParams& prm, Planes out);
+// The same kernels over columns given by a device table of pointers (the C
+// ABI's evaluate_constraint_quotients_on_domain); accumulate: add to the
+// output planes instead of writing them.
+int wf_constraints_table(cudaStream_t st, const uint32_t* const* d_cols, uint32_t n_cols, uint32_t eval_log,
+                         uint32_t trace_log, const ConstraintParams& prm, Planes out, bool accumulate);
+int poseidon_constraints_table(cudaStream_t st, const uint32_t* const* d_trace, const uint32_t* const* d_inter,
+                               uint32_t eval_log, uint32_t trace_log, const ConstraintParams& prm,
+                               const LookupParams& lp, qm31 cumsum_shift, Planes out, bool accumulate);
+// The trace kernels of the C ABI (the reference's generate_* bindings):
+// columns, initial and final lookup states as device pointer tables.
+int wf_trace_table(cudaStream_t st, const uint32_t* in_a, const uint32_t* in_b, uint32_t log_n,
+                   uint32_t* const* d_cols, uint32_t n_cols);
+int poseidon_trace_table(cudaStream_t st, uint32_t* const* d_cols, uint32_t* const* d_init, uint32_t* const* d_final,
+                         uint32_t log_n);
+int poseidon_interaction_table(cudaStream_t st, const uint32_t* const* d_init, const uint32_t* const* d_final,
+                               uint32_t log_n, const LookupParams& lp, Planes out, void* scratch,
+                               qm31* claimed_sum);
 int poseidon_trace(cudaStream_t st, uint32_t* cols, uint32_t log_n, uint64_t seed, uint32_t mode);
 size_t logup_scratch_bytes(uint32_t log_n);
 int poseidon_interaction(cudaStream_t st, const uint32_t* trace, uint32_t log_n, const LookupParams& lp,

@@ -1,6 +1,7 @@
 // C ABI (include/gpustark.h) over the internal launch interface.
 #include "../../include/gpustark.h"
 #include "runtime.cuh"
+#include "air.cuh"
 #include "prover/prove_api.h"
 #include <cstring>
 #include <algorithm>
@@ -377,6 +378,225 @@ int gs_batch_eval_at_point(gs_ctx* ctx, const uint32_t* const* polys, uint32_t n
   return OK;
 }
 
+// ------------------------------------------------------ per-trait operations
+int gs_batch_gather_multi_uint32(gs_ctx* ctx, const uint32_t* const* cols, uint32_t n_cols, size_t col_len,
+                                 const uint32_t* indices, uint32_t n_indices, uint32_t* out) {
+  CTX_REQUIRED(ctx);
+  if (n_cols == 0 || n_indices == 0) return OK;
+  GS_REQUIRE(cols && indices && out, "null argument");
+  for (uint32_t c = 0; c < n_cols; c++) GS_REQUIRE(cols[c] != nullptr, "null column");
+  for (uint32_t i = 0; i < n_indices; i++) GS_REQUIRE(indices[i] < col_len, "gather index out of range");
+  GS_REQUIRE((size_t)n_cols * n_indices <= ((size_t)1 << 30), "gather too large");
+  const void* const* d_cols = nullptr;
+  const void* d_idx = nullptr;
+  GS_TRY(ctx->c.stage_ptrs((const void* const*)cols, n_cols, &d_cols));
+  GS_TRY(ctx->c.stage_bytes(indices, 4 * (size_t)n_indices, &d_idx));
+  size_t bytes = 4 * (size_t)n_cols * n_indices;
+  void* d_out = nullptr;
+  GS_TRY(ctx->c.get_scratch(bytes, &d_out));
+  GS_TRY(gather_multi(ctx->c.stream, (const uint32_t* const*)d_cols, n_cols, (const uint32_t*)d_idx, n_indices,
+                      (uint32_t*)d_out));
+  return ctx->c.read_back(d_out, bytes, out);
+}
+
+int gs_batch_get_blake2s_hash(gs_ctx* ctx, const uint32_t* layer, size_t n_hashes, const uint32_t* indices,
+                              uint32_t n_indices, uint32_t* out) {
+  CTX_REQUIRED(ctx);
+  if (n_indices == 0) return OK;
+  GS_REQUIRE(layer && indices && out, "null argument");
+  GS_REQUIRE(((uintptr_t)layer & 15) == 0, "hash layer must be 16-byte aligned");
+  for (uint32_t i = 0; i < n_indices; i++) GS_REQUIRE(indices[i] < n_hashes, "hash index out of range");
+  const void* d_idx = nullptr;
+  GS_TRY(ctx->c.stage_bytes(indices, 4 * (size_t)n_indices, &d_idx));
+  size_t bytes = 32 * (size_t)n_indices;
+  void* d_out = nullptr;
+  GS_TRY(ctx->c.get_scratch(bytes, &d_out));
+  GS_TRY(gather_hashes(ctx->c.stream, layer, (const uint32_t*)d_idx, n_indices, (uint32_t*)d_out));
+  return ctx->c.read_back(d_out, bytes, out);
+}
+
+int gs_barycentric_weights(gs_ctx* ctx, uint32_t log_size, gs_point_qm31 point, uint32_t* const weights[4]) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(log_size >= 2 && log_size <= 30, "log size out of range");
+  for (int q = 0; q < 4; q++) GS_REQUIRE(weights[q] != nullptr, "null weight plane");
+  DomainTables dt;
+  GS_TRY(ctx->c.domain_tables(log_size, &dt));
+  ptq p = {to_qm(point.x), to_qm(point.y)};
+  return barycentric_weights(ctx->c.stream, dt, p, Planes{{weights[0], weights[1], weights[2], weights[3]}});
+}
+
+int gs_barycentric_eval_at_point(gs_ctx* ctx, const uint32_t* evals, const uint32_t* const weights[4],
+                                 uint32_t log_size, gs_qm31* out) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(evals && out, "null argument");
+  GS_REQUIRE(log_size <= 30, "log size out of range");
+  for (int q = 0; q < 4; q++) GS_REQUIRE(weights[q] != nullptr, "null weight plane");
+  const size_t n = (size_t)1 << log_size;
+  size_t words = barycentric_scratch_words(n) + 4;
+  void* scratch = nullptr;
+  GS_TRY(ctx->c.get_scratch(4 * words, &scratch));
+  uint32_t* d_out = (uint32_t*)scratch + barycentric_scratch_words(n);
+  GS_TRY(barycentric_eval(ctx->c.stream, evals, CPlanes{{weights[0], weights[1], weights[2], weights[3]}}, n,
+                          (uint32_t*)scratch, d_out));
+  uint32_t v[4];
+  GS_TRY(ctx->c.read_back(d_out, 16, v));
+  *out = gs_qm31{v[0], v[1], v[2], v[3]};
+  return OK;
+}
+
+int gs_generate_secure_powers(gs_ctx* ctx, gs_qm31 felt, size_t n, uint32_t* const out[4]) {
+  CTX_REQUIRED(ctx);
+  if (n == 0) return OK;
+  for (int q = 0; q < 4; q++) GS_REQUIRE(out[q] != nullptr, "null output plane");
+  return secure_powers(ctx->c.stream, to_qm(felt), n, Planes{{out[0], out[1], out[2], out[3]}});
+}
+
+int gs_generate_wide_fibonacci_trace(gs_ctx* ctx, const uint32_t* input_a, const uint32_t* input_b,
+                                     uint32_t log_size, uint32_t* const* traces, uint32_t n_columns) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(input_a && input_b && traces, "null argument");
+  GS_REQUIRE(n_columns >= 2 && n_columns <= 1024 && log_size <= 28, "bad wide fibonacci shape");
+  for (uint32_t c = 0; c < n_columns; c++) GS_REQUIRE(traces[c] != nullptr, "null trace column");
+  const void* const* d = nullptr;
+  GS_TRY(ctx->c.stage_ptrs((const void* const*)traces, n_columns, &d));
+  return wf_trace_table(ctx->c.stream, input_a, input_b, log_size, (uint32_t* const*)d, n_columns);
+}
+
+int gs_generate_poseidon_traces(gs_ctx* ctx, uint32_t* const* traces, uint32_t* const* lookup_init,
+                                uint32_t* const* lookup_final, uint32_t log_size) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(traces && lookup_init && lookup_final, "null argument");
+  GS_REQUIRE(log_size <= 28, "log size out of range");
+  for (int c = 0; c < 158; c++) GS_REQUIRE(traces[c] != nullptr, "null trace column");
+  for (int c = 0; c < 16; c++) GS_REQUIRE(lookup_init[c] && lookup_final[c], "null lookup column");
+  const void* const* dt = nullptr;
+  const void* const* di = nullptr;
+  const void* const* df = nullptr;
+  GS_TRY(ctx->c.stage_ptrs((const void* const*)traces, 158, &dt));
+  GS_TRY(ctx->c.stage_ptrs((const void* const*)lookup_init, 16, &di));
+  GS_TRY(ctx->c.stage_ptrs((const void* const*)lookup_final, 16, &df));
+  return poseidon_trace_table(ctx->c.stream, (uint32_t* const*)dt, (uint32_t* const*)di, (uint32_t* const*)df,
+                              log_size);
+}
+
+int gs_generate_poseidon_interaction_traces(gs_ctx* ctx, const void* lookup_elements,
+                                            const uint32_t* const* lookup_init, const uint32_t* const* lookup_final,
+                                            uint32_t log_size, uint32_t* const interaction_traces[4],
+                                            uint32_t claimed_sum[4]) {
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(lookup_elements && lookup_init && lookup_final && claimed_sum, "null argument");
+  GS_REQUIRE(log_size >= 1 && log_size <= 28, "log size out of range");
+  for (int c = 0; c < 16; c++) GS_REQUIRE(lookup_init[c] && lookup_final[c], "null lookup column");
+  for (int c = 0; c < 4; c++) GS_REQUIRE(interaction_traces[c] != nullptr, "null interaction column");
+  // LookupElements<16> { z, alpha, alpha_powers[16] }, QM31 as 4 words
+  LookupParams lp;
+  memcpy(lp.z, lookup_elements, 16);
+  memcpy(lp.alpha_pow, (const uint8_t*)lookup_elements + 32, 16 * 16);
+  const void* const* di = nullptr;
+  const void* const* df = nullptr;
+  GS_TRY(ctx->c.stage_ptrs((const void* const*)lookup_init, 16, &di));
+  GS_TRY(ctx->c.stage_ptrs((const void* const*)lookup_final, 16, &df));
+  void* scratch = nullptr;
+  GS_TRY(ctx->c.get_scratch(logup_scratch_bytes(log_size), &scratch));
+  qm31 cs;
+  GS_TRY(poseidon_interaction_table(
+      ctx->c.stream, (const uint32_t* const*)di, (const uint32_t* const*)df, log_size, lp,
+      Planes{{interaction_traces[0], interaction_traces[1], interaction_traces[2], interaction_traces[3]}},
+      scratch, &cs));
+  claimed_sum[0] = cs.x.a;
+  claimed_sum[1] = cs.x.b;
+  claimed_sum[2] = cs.y.a;
+  claimed_sum[3] = cs.y.b;
+  return OK;
+}
+
+// FrameworkEval::cuda_eval_name ids (constraint-framework/src/lib.rs:353-363).
+static constexpr uint32_t fnv1a(const char* s) {
+  uint32_t h = 0x811C9DC5u;
+  while (*s) {
+    h ^= (uint8_t)*s++;
+    h *= 0x01000193u;
+  }
+  return h;
+}
+static constexpr uint32_t EVAL_ID_WIDE_FIBONACCI = fnv1a("fibonacci_example");
+static constexpr uint32_t EVAL_ID_POSEIDON = fnv1a("poseidon_example");
+
+int gs_evaluate_constraint_quotients_on_domain(gs_ctx* ctx, uint32_t* const quotients[4],
+                                               const uint32_t* const* trace0, uint32_t trace0_len,
+                                               const uint32_t* const* trace1, uint32_t trace1_len,
+                                               const uint32_t* const* trace2, uint32_t trace2_len,
+                                               const gs_qm31* random_coeff_powers,
+                                               const uint32_t* denominator_inverses, uint32_t domain_log_size,
+                                               uint32_t eval_domain_log_size, uint32_t n_constraints,
+                                               uint32_t logup_counts, const void* eval, size_t eval_len,
+                                               gs_qm31 cumsum_shift, int should_accumulate) {
+  (void)trace0;
+  (void)logup_counts;
+  CTX_REQUIRED(ctx);
+  GS_REQUIRE(eval != nullptr && eval_len >= 12, "eval: eval_id followed by the component's Eval struct");
+  for (int q = 0; q < 4; q++) GS_REQUIRE(quotients[q] != nullptr, "null quotient plane");
+  GS_REQUIRE(random_coeff_powers && denominator_inverses, "null argument");
+  GS_REQUIRE(eval_domain_log_size > domain_log_size && eval_domain_log_size - domain_log_size <= 3 &&
+                 eval_domain_log_size <= 30,
+             "evaluation domain must be 2 to 8 times the trace domain");
+  GS_REQUIRE(trace0_len == 0, "the example components have no preprocessed columns");
+  GS_REQUIRE(n_constraints >= 1 && n_constraints <= (uint32_t)MAX_CONSTRAINTS, "constraint count out of range");
+  uint32_t w[3];
+  memcpy(w, eval, 12);  // eval_id, then the Eval struct: its own eval_id, log_n_rows
+  const uint32_t eval_id = w[0], log_n_rows = w[2];
+  GS_REQUIRE(log_n_rows == domain_log_size, "Eval.log_n_rows differs from the trace domain");
+  ConstraintParams prm;
+  memset(&prm, 0, sizeof(prm));
+  for (uint32_t k = 0; k < n_constraints; k++) {
+    const gs_qm31& p = random_coeff_powers[k];
+    prm.powers[4 * k] = p.a;
+    prm.powers[4 * k + 1] = p.b;
+    prm.powers[4 * k + 2] = p.c;
+    prm.powers[4 * k + 3] = p.d;
+  }
+  for (uint32_t i = 0; i < (1u << (eval_domain_log_size - domain_log_size)); i++)
+    prm.denom_inv[i] = denominator_inverses[i];
+  Planes out{{quotients[0], quotients[1], quotients[2], quotients[3]}};
+  const void* const* d_t1 = nullptr;
+  if (eval_id == EVAL_ID_WIDE_FIBONACCI) {
+    // WideFibonacciEval { eval_id, log_n_rows } (examples/src/wide_fibonacci/mod.rs:34-37);
+    // constraints c_k - (c_{k-2}^2 + c_{k-1}^2), k >= 2
+    GS_REQUIRE(eval_domain_log_size == domain_log_size + 1, "wide fibonacci evaluates on the doubled domain");
+    GS_REQUIRE(trace1_len == n_constraints + 2 && trace2_len == 0, "wide fibonacci: n_constraints + 2 columns");
+    for (uint32_t c = 0; c < trace1_len; c++) GS_REQUIRE(trace1[c] != nullptr, "null trace column");
+    GS_TRY(ctx->c.stage_ptrs((const void* const*)trace1, trace1_len, &d_t1));
+    return wf_constraints_table(ctx->c.stream, (const uint32_t* const*)d_t1, trace1_len, eval_domain_log_size,
+                                domain_log_size, prm, out, should_accumulate != 0);
+  }
+  if (eval_id == EVAL_ID_POSEIDON) {
+    // PoseidonEval { eval_id, log_n_rows, lookup_elements: LookupElements<16> { z, alpha,
+    // alpha_powers[16] }, claimed_sum } (examples/src/poseidon/mod.rs:57-64,
+    // constraint-framework/src/logup.rs:60-66), all #[repr(C)], QM31 as 4 words
+    constexpr size_t QW = 16;
+    GS_REQUIRE(eval_len >= 12 + QW * 19, "poseidon: Eval struct too short");
+    GS_REQUIRE(eval_domain_log_size == domain_log_size + 2, "poseidon evaluates on the 4x domain");
+    GS_REQUIRE(trace1_len == 158 && trace2_len == 4 && n_constraints == 143,
+               "poseidon: 158 trace columns, 4 interaction columns, 143 constraints");
+    for (uint32_t c = 0; c < trace1_len; c++) GS_REQUIRE(trace1[c] != nullptr, "null trace column");
+    for (uint32_t c = 0; c < trace2_len; c++) GS_REQUIRE(trace2[c] != nullptr, "null interaction column");
+    const uint8_t* e = (const uint8_t*)eval + 12;
+    LookupParams lp;
+    memcpy(lp.z, e, QW);
+    memcpy(lp.alpha_pow, e + 2 * QW, 16 * QW);
+    const void* const* d_t2 = nullptr;
+    GS_TRY(ctx->c.stage_ptrs((const void* const*)trace1, trace1_len, &d_t1));
+    GS_TRY(ctx->c.stage_ptrs((const void* const*)trace2, trace2_len, &d_t2));
+    return poseidon_constraints_table(ctx->c.stream, (const uint32_t* const*)d_t1, (const uint32_t* const*)d_t2,
+                                      eval_domain_log_size, domain_log_size, prm, lp, to_qm(cumsum_shift), out,
+                                      should_accumulate != 0);
+  }
+  char msg[96];
+  snprintf(msg, sizeof msg, "no device kernel for eval id 0x%08x", eval_id);
+  set_error(msg);
+  return ERR_UNSUPPORTED;
+}
+
 int gs_grind_blake2s(gs_ctx* ctx, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint64_t* nonce) {
   CTX_REQUIRED(ctx);
   GS_REQUIRE(prefixed_digest != nullptr, "null digest");
@@ -395,9 +615,7 @@ static int run_prove(gs_ctx* ctx, prover::ProveRequest& req, const gs_pcs_config
     req.cfg.n_queries = config->n_queries;
     req.cfg.fold_step = config->line_fold_step;
   }
-  GS_REQUIRE(req.input_mode <= 2, "unknown input mode");
-  GS_REQUIRE(req.input_mode != 2 || req.host_inputs != nullptr, "host inputs required");
-  GS_REQUIRE(req.cfg.pow_bits <= 32 && req.cfg.n_queries >= 1 && req.cfg.log_last_layer <= 10, "bad PCS config");
+  GS_TRY(prover::validate_request(req));
   // serialised straight into the caller's buffer when it fits; the string
   // (reused per thread) only holds a proof that does not, for its length
   static thread_local std::string bytes;
@@ -429,7 +647,6 @@ static int prove_wf(gs_ctx* ctx, uint32_t log_n_rows, uint32_t n_columns, uint64
   req.input_mode = input_mode;
   req.host_inputs = host_inputs;
   req.split_log = 1;
-  GS_REQUIRE(n_columns >= 3 && n_columns <= 160, "wide fibonacci needs 3..160 columns");
   return run_prove(ctx, req, config, proof, capacity, proof_len);
 }
 

@@ -255,4 +255,118 @@ int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_
   return OK;
 }
 
+// ------------------------------------------------------------ barycentric
+// PolyOps::barycentric_weights for CanonicCoset(log) (crates/stwo/src/
+// prover/backend/cpu/circle.rs:101-132): for the domain point q_i at
+// bit-reversed position i,
+//   w_i = V(p) / (s_i * v_i(p)),  V(p) = coset_vanishing(CanonicCoset(log), p),
+//   s_i = -2 q_i.y * coset_vanishing_derivative(log, q_i)
+//       = -2 * 4^(log-1) * q_i.y * prod_{j=1}^{log-1} pi^(j-1)(q_i.x),
+//   v_i(p) = point_vanishing(q_i, p) = h.y / (1 + h.x),  h = p - q_i,
+// because the vanishing polynomial of CanonicCoset(j) at a point is
+// pi^(j-1) of its x (core/constraints.rs:12-55, 87-93). So
+//   w_i = V(p) (1 + h.x) / (s_i h.y)
+// with one QM31 inversion per point. c0 = -2 * 4^(log-1).
+__global__ void barycentric_weights_kernel(DomainTables dt, uint32_t log_n, ptq p, qm31 vn_p, uint32_t c0,
+                                           Planes out) {
+  const size_t n = (size_t)1 << log_n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    pt31 q = domain_point_bitrev(dt, (uint32_t)i);
+    uint32_t prod = 1, x = q.x;
+    for (uint32_t j = 1; j < log_n; j++) {
+      prod = mul(prod, x);
+      x = double_x(x);
+    }
+    uint32_t si = mul(mul(c0, q.y), prod);
+    // h = p + conj(q): (p.x q.x + p.y q.y, p.y q.x - p.x q.y)
+    qm31 hx = qm_add(qm_mul_m31(p.x, q.x), qm_mul_m31(p.y, q.y));
+    qm31 hy = qm_sub(qm_mul_m31(p.y, q.x), qm_mul_m31(p.x, q.y));
+    qm31 w = qm_mul(qm_mul(vn_p, qm_add_m31(hx, 1)), qm_inv(qm_mul_m31(hy, si)));
+    out.p[0][i] = w.x.a;
+    out.p[1][i] = w.x.b;
+    out.p[2][i] = w.y.a;
+    out.p[3][i] = w.y.b;
+  }
+}
+
+// PolyOps::barycentric_eval_at_point (cpu/circle.rs:134-141): sum_i evals[i]
+// * w_i. Each block folds its rows into 64-bit accumulators (three products
+// between folds) and writes one partial QM31; one block adds the partials.
+constexpr int BARY_THREADS = 256;
+__global__ void barycentric_dot_kernel(const uint32_t* __restrict__ evals, CPlanes w, size_t n, uint32_t* partials) {
+  uint64_t acc[4] = {0, 0, 0, 0};
+  int k = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t e = __ldg(evals + i);
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[q] += (uint64_t)e * __ldg(w.p[q] + i);
+    if (++k == 3) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[q] = (acc[q] & P) + (acc[q] >> 31);
+      k = 0;
+    }
+  }
+  __shared__ uint32_t red[4][BARY_THREADS];
+#pragma unroll
+  for (int q = 0; q < 4; q++) red[q][threadIdx.x] = reduce64(acc[q]);
+  __syncthreads();
+  for (int half = BARY_THREADS / 2; half > 0; half >>= 1) {
+    if ((int)threadIdx.x < half)
+#pragma unroll
+      for (int q = 0; q < 4; q++) red[q][threadIdx.x] = add(red[q][threadIdx.x], red[q][threadIdx.x + half]);
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) partials[4 * blockIdx.x + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void barycentric_sum_kernel(const uint32_t* partials, uint32_t n_partials, uint32_t* out) {
+  __shared__ uint32_t red[4][BARY_THREADS];
+  uint32_t a[4] = {0, 0, 0, 0};
+  for (uint32_t b = threadIdx.x; b < n_partials; b += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < 4; q++) a[q] = add(a[q], partials[4 * b + q]);
+#pragma unroll
+  for (int q = 0; q < 4; q++) red[q][threadIdx.x] = a[q];
+  __syncthreads();
+  for (int half = BARY_THREADS / 2; half > 0; half >>= 1) {
+    if ((int)threadIdx.x < half)
+#pragma unroll
+      for (int q = 0; q < 4; q++) red[q][threadIdx.x] = add(red[q][threadIdx.x], red[q][threadIdx.x + half]);
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[threadIdx.x] = red[threadIdx.x][0];
+}
+
+int barycentric_weights(cudaStream_t st, const DomainTables& dt, ptq p, Planes out) {
+  const uint32_t log_n = dt.lift;
+  GS_REQUIRE(log_n >= 2 && log_n <= 30, "domain log size out of range");
+  // V(p) = pi^(log-1)(p.x), c0 = -2 * 4^(log-1)
+  qm31 vn = p.x;
+  for (uint32_t j = 1; j < log_n; j++) vn = qm_double_x(vn);
+  uint32_t c0 = neg(2);
+  for (uint32_t j = 1; j < log_n; j++) c0 = mul(c0, 4);
+  const size_t n = (size_t)1 << log_n;
+  size_t blocks = (n + 255) / 256, cap = (size_t)num_sms() * 8;
+  barycentric_weights_kernel<<<(unsigned)(blocks < cap ? blocks : cap), 256, 0, st>>>(dt, log_n, p, vn, c0, out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+size_t barycentric_scratch_words(size_t n) { return 4 * (size_t)num_sms() * 2 + 4; }
+
+int barycentric_eval(cudaStream_t st, const uint32_t* d_evals, CPlanes w, size_t n, uint32_t* d_scratch,
+                     uint32_t* d_out) {
+  size_t blocks = (n + BARY_THREADS - 1) / BARY_THREADS, cap = (size_t)num_sms() * 2;
+  if (blocks > cap) blocks = cap;
+  if (blocks == 0) blocks = 1;
+  barycentric_dot_kernel<<<(unsigned)blocks, BARY_THREADS, 0, st>>>(d_evals, w, n, d_scratch);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  barycentric_sum_kernel<<<1, BARY_THREADS, 0, st>>>(d_scratch, (uint32_t)blocks, d_out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
 }  // namespace gs

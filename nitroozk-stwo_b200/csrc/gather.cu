@@ -53,4 +53,47 @@ int gather_hash_runs(cudaStream_t st, const HashRun* d_runs, uint32_t n_runs, co
   return OK;
 }
 
+// Column::batch_at_multi (crates/stwo/src/prover/backend/mod.rs:73-89):
+// out[i * n_cols + c] = cols[c][idx[i]], row-major over the indices.
+__global__ void gather_multi_kernel(const uint32_t* const* __restrict__ cols, uint32_t n_cols,
+                                    const uint32_t* __restrict__ idx, uint32_t n_idx, uint32_t* __restrict__ out) {
+  const size_t total = (size_t)n_cols * n_idx;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    uint32_t i = (uint32_t)(t / n_cols), c = (uint32_t)(t - (size_t)i * n_cols);
+    out[t] = __ldg(cols[c] + __ldg(idx + i));
+  }
+}
+
+// Hashes of one Merkle layer at a list of indices, 32 bytes each.
+__global__ void gather_hashes_kernel(const uint4* __restrict__ layer, const uint32_t* __restrict__ idx, uint32_t n_idx,
+                                     uint4* __restrict__ out) {
+  const size_t total = 2 * (size_t)n_idx;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x)
+    out[t] = __ldg(layer + 2 * (size_t)__ldg(idx + (t >> 1)) + (t & 1));
+}
+
+static unsigned gather_blocks(size_t items) {
+  size_t b = (items + 255) / 256;
+  size_t cap = (size_t)num_sms() * 8;
+  return (unsigned)(b < cap ? (b ? b : 1) : cap);
+}
+
+int gather_multi(cudaStream_t st, const uint32_t* const* d_cols, uint32_t n_cols, const uint32_t* d_idx,
+                 uint32_t n_idx, uint32_t* d_out) {
+  if (n_cols == 0 || n_idx == 0) return OK;
+  gather_multi_kernel<<<gather_blocks((size_t)n_cols * n_idx), 256, 0, st>>>(d_cols, n_cols, d_idx, n_idx, d_out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+int gather_hashes(cudaStream_t st, const uint32_t* d_layer, const uint32_t* d_idx, uint32_t n_idx, uint32_t* d_out) {
+  if (n_idx == 0) return OK;
+  gather_hashes_kernel<<<gather_blocks(2 * (size_t)n_idx), 256, 0, st>>>((const uint4*)d_layer, d_idx, n_idx,
+                                                                          (uint4*)d_out);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
 }  // namespace gs

@@ -21,20 +21,6 @@
 
 namespace gs {
 
-__device__ __forceinline__ pt31 ld_pt(const pt31* p) {
-  uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
-  return {v.x, v.y};
-}
-
-__device__ __forceinline__ pt31 domain_point_bitrev(const DomainTables& t, uint32_t row) {
-  uint32_t j = __brev(row) >> (32 - t.lift);
-  uint32_t half = 1u << (t.lift - 1);
-  bool second = j >= half;
-  if (second) j -= half;
-  pt31 p = pt_add(ld_pt(t.hi + (j >> t.s)), ld_pt(t.lo + (j & ((1u << t.s) - 1))));
-  return second ? pt_conj(p) : p;
-}
-
 // ------------------------------------------------------------ numerators
 __device__ __forceinline__ uint64_t fold64(uint64_t x) { return (x & P) + (x >> 31); }
 
@@ -429,6 +415,33 @@ int accumulate(cudaStream_t st, Planes a, CPlanes b, size_t n) {
   if (blocks > cap) blocks = cap;
   if (blocks == 0) return OK;
   accumulate_kernel<<<(unsigned)blocks, 256, 0, st>>>(a, b, n);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+// AccumulationOps::generate_secure_powers (crates/stwo/src/prover/air/
+// accumulation.rs:127-145; the reference's CUDA backend computes it on the
+// host, prover/backend/cuda/accumulation.rs:20-22): out[i] = felt^i, i < n.
+// Each thread raises felt to its index by squaring and multiplying.
+__global__ void secure_powers_kernel(qm31 felt, size_t n, Planes out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    qm31 r = qm_one(), b = felt;
+    for (size_t e = i; e; e >>= 1) {
+      if (e & 1) r = qm_mul(r, b);
+      b = qm_sqr(b);
+    }
+    out.p[0][i] = r.x.a;
+    out.p[1][i] = r.x.b;
+    out.p[2][i] = r.y.a;
+    out.p[3][i] = r.y.b;
+  }
+}
+
+int secure_powers(cudaStream_t st, qm31 felt, size_t n, Planes out) {
+  if (n == 0) return OK;
+  size_t blocks = (n + 255) / 256, cap = (size_t)num_sms() * 8;
+  secure_powers_kernel<<<(unsigned)(blocks < cap ? blocks : cap), 256, 0, st>>>(felt, n, out);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;

@@ -62,6 +62,22 @@ struct DomainTables {
   uint32_t lift;
 };
 
+#ifdef __CUDACC__
+__device__ __forceinline__ pt31 ld_pt(const pt31* p) {
+  uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+  return {v.x, v.y};
+}
+// CanonicCoset(lift).circle_domain().at(bit_reverse(row)).
+__device__ __forceinline__ pt31 domain_point_bitrev(const DomainTables& t, uint32_t row) {
+  uint32_t j = __brev(row) >> (32 - t.lift);
+  uint32_t half = 1u << (t.lift - 1);
+  bool second = j >= half;
+  if (second) j -= half;
+  pt31 p = pt_add(ld_pt(t.hi + (j >> t.s)), ld_pt(t.lo + (j & ((1u << t.s) - 1))));
+  return second ? pt_conj(p) : p;
+}
+#endif
+
 // Waits for `st`. By default CUDA's own stream synchronisation (the lowest
 // latency for one proof at a time). A thread that installs a blocking-sync
 // event (the proof server's workers, many threads sharing one device and the
@@ -224,6 +240,19 @@ struct LiftCol { const uint32_t* p[4]; uint32_t log_size; uint32_t pad; };
 size_t eval_at_point_scratch_bytes(uint32_t n_polys, uint32_t log_n, uint32_t chunk_log = 12);
 int batch_eval_at_point(cudaStream_t st, const uint32_t* const* d_polys, uint32_t n_polys, uint32_t log_n, ptq point,
                         uint32_t* d_out, uint32_t* d_scratch, uint32_t chunk_log = 12, bool vec = false);
+
+// barycentric weights on CanonicCoset(dt.lift) (4 planes) and evaluation
+// (d_scratch: barycentric_scratch_words(n) words; d_out: 4 words)
+int barycentric_weights(cudaStream_t st, const DomainTables& dt, ptq p, Planes out);
+size_t barycentric_scratch_words(size_t n);
+int barycentric_eval(cudaStream_t st, const uint32_t* d_evals, CPlanes w, size_t n, uint32_t* d_scratch,
+                     uint32_t* d_out);
+// quotients.cu: out[i] = felt^i
+int secure_powers(cudaStream_t st, qm31 felt, size_t n, Planes out);
+// gather.cu: Column::batch_at_multi (row-major) and hashes of one layer
+int gather_multi(cudaStream_t st, const uint32_t* const* d_cols, uint32_t n_cols, const uint32_t* d_idx,
+                 uint32_t n_idx, uint32_t* d_out);
+int gather_hashes(cudaStream_t st, const uint32_t* d_layer, const uint32_t* d_idx, uint32_t n_idx, uint32_t* d_out);
 
 // grind.cu
 int grind_blake2s(cudaStream_t st, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint32_t* d_scratch,

@@ -95,6 +95,17 @@ _PROTOS = {
                                             C.POINTER(PcsConfig), C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
     "gs_prove_poseidon_poseidon252": [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint32, U32P, C.c_uint32,
                                       C.POINTER(PcsConfig), C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
+    "gs_batch_gather_multi_uint32": [C.c_void_p, VPP, C.c_uint32, C.c_size_t, U32P, C.c_uint32, U32P],
+    "gs_batch_get_blake2s_hash": [C.c_void_p, C.c_void_p, C.c_size_t, U32P, C.c_uint32, U32P],
+    "gs_barycentric_weights": [C.c_void_p, C.c_uint32, PointQM31, VPP],
+    "gs_barycentric_eval_at_point": [C.c_void_p, C.c_void_p, VPP, C.c_uint32, C.POINTER(QM31)],
+    "gs_generate_secure_powers": [C.c_void_p, QM31, C.c_size_t, VPP],
+    "gs_evaluate_constraint_quotients_on_domain": [C.c_void_p, VPP, VPP, C.c_uint32, VPP, C.c_uint32, VPP, C.c_uint32,
+                                                   C.c_void_p, U32P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                                   C.c_void_p, C.c_size_t, QM31, C.c_int],
+    "gs_generate_wide_fibonacci_trace": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, VPP, C.c_uint32],
+    "gs_generate_poseidon_traces": [C.c_void_p, VPP, VPP, VPP, C.c_uint32],
+    "gs_generate_poseidon_interaction_traces": [C.c_void_p, C.c_void_p, VPP, VPP, C.c_uint32, VPP, U32P],
     "gs_poseidon252_channel_op": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64, U32P, C.c_size_t,
                                   U32P, C.c_void_p, C.POINTER(C.c_uint32)],
 }

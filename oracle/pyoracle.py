@@ -43,6 +43,11 @@ def _declare(L):
         fn.argtypes = list(args)
 
     f("oracle_set_threads", None, C.c_int)
+    f("oracle_barycentric_weights", None, C.c_uint32, U32P, PP)
+    f("oracle_barycentric_eval", None, U32P, PP, C.c_uint32, U32P)
+    f("oracle_secure_powers", None, U32P, C.c_size_t, PP)
+    f("oracle_constraint_quotients", None, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, PP, PP, U32P, C.c_uint32,
+      U32P, U32P, U32P, U32P, PP)
     f("oracle_verify", C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, U32P, C.c_uint32, U32P, U8P,
       C.c_size_t, C.c_char_p, C.c_size_t)
     f("oracle_verify_lookup_elements", C.c_int, C.c_uint32, U8P, C.c_size_t, U32P, U32P)
@@ -439,3 +444,49 @@ def verify(proof, air, log_n, n_cols=100, split_log=None, claimed_sum=None, merk
     if code:
         raise VerificationError(code, msg.value.decode())
     return True
+
+
+# ------------------------------------------------------- per-trait operations
+def barycentric_weights(log_size, point8):
+    """PolyOps::barycentric_weights(CanonicCoset(log_size), p): 4 planes."""
+    out = [np.zeros(1 << log_size, np.uint32) for _ in range(4)]
+    pt, ptp = u32(point8)
+    pp, keep = ptr_array(out)
+    lib().oracle_barycentric_weights(log_size, ptp, pp)
+    return out
+
+
+def barycentric_eval(evals, weights):
+    e, ep = u32(evals)
+    wp, keep = ptr_array([np.ascontiguousarray(w, np.uint32) for w in weights])
+    out = np.zeros(4, np.uint32)
+    lib().oracle_barycentric_eval(ep, wp, int(len(e)).bit_length() - 1, out.ctypes.data_as(U32P))
+    return out
+
+
+def secure_powers(felt4, n):
+    out = [np.zeros(max(n, 1), np.uint32) for _ in range(4)]
+    f, fp = u32(felt4)
+    pp, keep = ptr_array(out)
+    lib().oracle_secure_powers(fp, n, pp)
+    return [o[:n] for o in out]
+
+
+def constraint_quotients(air, trace, inter, trace_log, eval_log, powers, denom_inv, z=None, alpha=None, shift=None,
+                         n_cols=None):
+    """Constraint quotients over the evaluation domain (component_prover.rs:177-245):
+    row_res * denom_inv[row >> trace_log]; powers: (n_constraints, 4) words."""
+    n = 1 << eval_log
+    out = [np.zeros(n, np.uint32) for _ in range(4)]
+    tp, keep_t = ptr_array([np.ascontiguousarray(c, np.uint32) for c in trace])
+    ip, keep_i = ptr_array([np.ascontiguousarray(c, np.uint32) for c in inter] or [np.zeros(1, np.uint32)])
+    pw = np.ascontiguousarray(powers, np.uint32).reshape(-1)
+    dn = np.ascontiguousarray(denom_inv, np.uint32)
+    zz = np.ascontiguousarray(z if z is not None else np.zeros(4), np.uint32)
+    aa = np.ascontiguousarray(alpha if alpha is not None else np.zeros(4), np.uint32)
+    sh = np.ascontiguousarray(shift if shift is not None else np.zeros(4), np.uint32)
+    op, keep_o = ptr_array(out)
+    lib().oracle_constraint_quotients(0 if air == "wide_fibonacci" else 1, n_cols or len(trace), trace_log, eval_log,
+                                      tp, ip, pw.ctypes.data_as(U32P), len(pw) // 4, dn.ctypes.data_as(U32P),
+                                      zz.ctypes.data_as(U32P), aa.ctypes.data_as(U32P), sh.ctypes.data_as(U32P), op)
+    return out
