@@ -12,12 +12,19 @@
 // Every word a kernel reads is written earlier in the same call on the same
 // stream, so nothing needs clearing between calls.
 //
-// The array's device address is looked up once per device with
-// cudaGetSymbolAddress (the first call on a device does that lookup, which
-// also loads this library's kernels onto the device). There is one array per
-// device: calls that overlap in time on one device race on it, whatever their
-// streams or threads.
+// The array's device address belongs to a CUDA context. It is looked up with
+// cudaGetSymbolAddress the first time a call runs under a context (for the
+// usual case, the device's primary context, once per device; that first call
+// also loads this library's kernels onto the device) and cached per context.
+// The current context is read through the runtime's driver entry point for
+// cuCtxGetCurrent, so the library does not link the driver library; should
+// that entry point be unavailable, every call looks the address up again.
+// There is one array per context: calls that overlap in time under one
+// context race on it, whatever their streams or threads.
+#include <cuda.h>
 #include <mutex>
+#include <utility>
+#include <vector>
 #include "../../include/gpustark.h"
 #include "runtime.cuh"
 
@@ -39,15 +46,41 @@ __global__ void eaps_table_kernel(PolyTable t, uint32_t n, const uint32_t** dst)
 }
 
 static std::mutex g_eaps_mu;
-static void* g_eaps_addr[128];
+static std::vector<std::pair<CUcontext, void*>> g_eaps_addr;  // address of the array per context
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+static CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (CtxGetCurrentFn)p;
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
 
 static int eaps_base(uint8_t** out) {
-  int dev = 0;
-  GS_CUDA_TRY(cudaGetDevice(&dev));
-  GS_REQUIRE(dev >= 0 && dev < 128, "device ordinal out of range");
+  CtxGetCurrentFn fn = ctx_get_current();
+  CUcontext ctx = nullptr;
+  if (fn && fn(&ctx) != CUDA_SUCCESS) ctx = nullptr;
   std::lock_guard<std::mutex> lk(g_eaps_mu);
-  if (!g_eaps_addr[dev]) GS_CUDA_TRY(cudaGetSymbolAddress(&g_eaps_addr[dev], g_eap_static));
-  *out = (uint8_t*)g_eaps_addr[dev];
+  if (ctx)
+    for (auto& e : g_eaps_addr)
+      if (e.first == ctx) {
+        *out = (uint8_t*)e.second;
+        return OK;
+      }
+  // the lookup makes the device's primary context current when no context is
+  void* a = nullptr;
+  GS_CUDA_TRY(cudaGetSymbolAddress(&a, g_eap_static));
+  if (fn && !ctx && fn(&ctx) != CUDA_SUCCESS) ctx = nullptr;
+  if (ctx) g_eaps_addr.push_back({ctx, a});
+  *out = (uint8_t*)a;
   return OK;
 }
 

@@ -15,10 +15,22 @@
 // step (a plain read, nothing waits), so a search that hits early costs a
 // few thousand compressions instead of 2^20, and the answer is still the
 // smallest hit: steps are skipped only when a smaller hit exists.
+#include <cstdlib>
 #include "runtime.cuh"
 #include "blake2s.cuh"
 
 namespace gs {
+
+// High words searched before giving up: 2^12, or GS_GRIND_MAX_HI (1..4096,
+// read once per process), which tests set low to reach the error path.
+static uint32_t grind_max_hi() {
+  static const uint32_t v = [] {
+    const char* e = getenv("GS_GRIND_MAX_HI");
+    long x = e ? strtol(e, nullptr, 10) : 0;
+    return (uint32_t)(x >= 1 && x <= 4096 ? x : 4096);
+  }();
+  return v;
+}
 
 struct Digest8 { uint32_t w[8]; };
 
@@ -58,7 +70,8 @@ int grind_blake2s(cudaStream_t st, const uint32_t prefixed_digest[8], uint32_t p
   const uint64_t want = ((uint64_t)1 << (pow_bits < 24 ? pow_bits : 24)) * 16 / GRIND_STEP;
   const uint64_t lo_b = (uint64_t)num_sms(), hi_b = 8 * (uint64_t)num_sms();
   const unsigned blocks = (unsigned)(want < lo_b ? lo_b : want > hi_b ? hi_b : want);
-  for (uint32_t hi = 0; hi < (1u << 12); hi++) {
+  const uint32_t max_hi = grind_max_hi();
+  for (uint32_t hi = 0; hi < max_hi; hi++) {
     GS_CUDA_TRY(cudaMemsetAsync(d_scratch, 0xff, 4, st));
     grind_kernel<<<blocks, GRIND_STEP, 0, st>>>(d, hi, pow_bits, d_scratch);
     note_launch();

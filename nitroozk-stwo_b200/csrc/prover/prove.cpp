@@ -255,6 +255,16 @@ void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::
   }
 }
 
+int validate_request(const ProveRequest& r) {
+  GS_REQUIRE(r.air <= 1, "unknown component");
+  GS_REQUIRE(r.merkle_channel <= 1, "merkle channel must be 0 (Blake2s) or 1 (Poseidon252)");
+  GS_REQUIRE(r.input_mode <= 2, "unknown input mode");
+  GS_REQUIRE(r.input_mode != 2 || r.host_inputs != nullptr, "host inputs required");
+  GS_REQUIRE(r.cfg.pow_bits <= 32 && r.cfg.n_queries >= 1 && r.cfg.log_last_layer <= 10, "bad PCS config");
+  GS_REQUIRE(r.air != 0 || (r.n_cols >= 3 && r.n_cols <= 160), "wide fibonacci needs 3..160 columns");
+  return OK;
+}
+
 int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_bytes, ProveStats* stats) {
   PcsConfig cfg = req.cfg;
   Prover pv(ctx, cfg);

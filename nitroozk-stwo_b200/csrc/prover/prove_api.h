@@ -30,6 +30,10 @@ struct ProveStats {
 
 struct Prover;
 struct AirHost;
+// The checks every proof request passes before any device work (direct
+// gs_prove_* calls and proof-server submissions alike): component, channel,
+// input mode, PcsConfig ranges, Wide-Fibonacci width. ERR_INVALID otherwise.
+int validate_request(const ProveRequest& r);
 int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_bytes, ProveStats* stats);
 int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_bytes, ProveStats* stats,
                uint8_t* out_buf = nullptr, size_t out_cap = 0);

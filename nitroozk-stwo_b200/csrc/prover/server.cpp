@@ -71,10 +71,12 @@ struct Server {
       Job job;
       {
         std::unique_lock<std::mutex> lk(mu);
+        // admission by footprint holds while the server drains at shutdown too
         cv_jobs.wait(lk, [&] {
-          return stopping || (!queue.empty() && (in_flight == 0 || in_flight + queue.front().footprint <= budget));
+          return (stopping && queue.empty()) ||
+                 (!queue.empty() && (in_flight == 0 || in_flight + queue.front().footprint <= budget));
         });
-        if (stopping && queue.empty()) break;
+        if (queue.empty()) break;
         job = std::move(queue.front());
         queue.pop_front();
         in_flight += job.footprint;
@@ -133,7 +135,6 @@ static int submit_job(gs_server* sv, uint32_t air, uint32_t log_n, uint32_t n_co
                       uint32_t composition_log_split, const gs_pcs_config* config, uint32_t merkle_channel,
                       uint64_t* job_id) {
   GS_REQUIRE(sv && job_id, "null argument");
-  GS_REQUIRE(air <= 1, "unknown component");
   Job j;
   j.req.air = air;
   j.req.merkle_channel = merkle_channel;
@@ -149,6 +150,7 @@ static int submit_job(gs_server* sv, uint32_t air, uint32_t log_n, uint32_t n_co
     j.req.cfg.n_queries = config->n_queries;
     j.req.cfg.fold_step = config->line_fold_step;
   }
+  GS_TRY(validate_request(j.req));
   j.footprint = proof_footprint(j.req);
   j.submitted = std::chrono::steady_clock::now();
   {

@@ -299,6 +299,15 @@ class GpuBackend:
         return out
 
     @staticmethod
+    def accumulate(a_planes, b_planes, ctx=None):
+        """AccumulationOps::accumulate: a += b coordinate-wise (4 planes each), in place."""
+        ctx = ctx or default_context()
+        ap, k1 = L.ptr_array([t.data_ptr() for t in a_planes])
+        bp, k2 = L.ptr_array([t.data_ptr() for t in b_planes])
+        L.check(L.lib().gs_accumulate(ctx.handle, ap, bp, a_planes[0].numel()), "accumulate")
+        return a_planes
+
+    @staticmethod
     def batch_eval_at_point(polys, point, ctx=None):
         """Values of coefficient polynomials at a QM31 circle point (ops.rs:51-59)."""
         ctx = ctx or default_context()
@@ -315,10 +324,12 @@ class GpuBackend:
         most 256 polynomials and 256 * 2^10 coefficients per polynomial at
         that count). Runs on `stream` (torch's current stream by default)."""
         if stream is None:
-            import torch
             stream = torch.cuda.current_stream()
         if log_size is None:
             log_size = polys[0].numel().bit_length() - 1 if polys else 0
+        for p in polys:
+            if not (p.is_cuda and p.dtype == torch.int32 and p.is_contiguous() and p.numel() == 1 << log_size):
+                raise ValueError(f"every polynomial must be a contiguous int32 CUDA tensor of 2^{log_size} words")
         pp, k = L.ptr_array([p.data_ptr() for p in polys])
         out = (L.QM31 * max(len(polys), 1))()
         pt = L.PointQM31(qm31(point[:4]), qm31(point[4:]))
@@ -326,6 +337,131 @@ class GpuBackend:
         L.check(L.lib().gs_batch_eval_at_point_noalloc(handle, pp, len(polys), log_size, pt, out),
                 "batch_eval_at_point_noalloc")
         return [[o.a, o.b, o.c, o.d] for o in out[:len(polys)]]
+
+    # ------------------------------------------------------- Column gathers
+    @staticmethod
+    def batch_at_multi(columns, indices, ctx=None):
+        """Column::batch_at_multi (prover/backend/mod.rs:73-89): values of every
+        column at every index, row-major (index-major), as a uint32 array of
+        len(indices) * len(columns)."""
+        ctx = ctx or default_context()
+        idx = np.ascontiguousarray(indices, dtype=np.uint32)
+        out = np.zeros(max(len(idx) * len(columns), 1), np.uint32)
+        col_len = min(c.numel() for c in columns) if columns else 0
+        pp, k = L.ptr_array([c.data_ptr() for c in columns])
+        L.check(L.lib().gs_batch_gather_multi_uint32(ctx.handle, pp, len(columns), col_len,
+                                                     idx.ctypes.data_as(L.U32P), len(idx),
+                                                     out.ctypes.data_as(L.U32P)), "batch_at_multi")
+        return out[: len(idx) * len(columns)]
+
+    @staticmethod
+    def batch_get_hashes(layer, indices, ctx=None):
+        """Column<Blake2sHash>::batch_at: the hashes of one Merkle layer at the
+        indices, as (len(indices), 32) bytes."""
+        ctx = ctx or default_context()
+        idx = np.ascontiguousarray(indices, dtype=np.uint32)
+        out = np.zeros(max(8 * len(idx), 8), np.uint32)
+        L.check(L.lib().gs_batch_get_blake2s_hash(ctx.handle, _p(layer), layer.numel() // 8,
+                                                  idx.ctypes.data_as(L.U32P), len(idx),
+                                                  out.ctypes.data_as(L.U32P)), "batch_get_hashes")
+        return out[: 8 * len(idx)].view(np.uint8).reshape(-1, 32)
+
+    # ----------------------------------------------------- barycentric OODS
+    @staticmethod
+    def barycentric_weights(log_size, point, ctx=None):
+        """PolyOps::barycentric_weights(CanonicCoset(log_size), p) (ops.rs:64-68): 4 planes."""
+        ctx = ctx or default_context()
+        out = [torch.empty(1 << log_size, dtype=torch.int32, device="cuda") for _ in range(4)]
+        op, k = L.ptr_array([t.data_ptr() for t in out])
+        pt = L.PointQM31(qm31(point[:4]), qm31(point[4:]))
+        L.check(L.lib().gs_barycentric_weights(ctx.handle, log_size, pt, op), "barycentric_weights")
+        return out
+
+    @staticmethod
+    def barycentric_eval_at_point(evals, weights, ctx=None):
+        """PolyOps::barycentric_eval_at_point (ops.rs:73-77): sum_i evals[i] * weights[i]."""
+        ctx = ctx or default_context()
+        wp, k = L.ptr_array([t.data_ptr() for t in weights])
+        out = L.QM31()
+        L.check(L.lib().gs_barycentric_eval_at_point(ctx.handle, _p(evals), wp, evals.numel().bit_length() - 1,
+                                                     C.byref(out)), "barycentric_eval_at_point")
+        return [out.a, out.b, out.c, out.d]
+
+    # ------------------------------------------------- constraint evaluation
+    @staticmethod
+    def generate_secure_powers(felt, n, ctx=None):
+        """AccumulationOps::generate_secure_powers: felt^i for i < n, 4 planes."""
+        ctx = ctx or default_context()
+        out = [torch.empty(max(n, 1), dtype=torch.int32, device="cuda") for _ in range(4)]
+        op, k = L.ptr_array([t.data_ptr() for t in out])
+        L.check(L.lib().gs_generate_secure_powers(ctx.handle, qm31(felt), n, op), "generate_secure_powers")
+        return [t[:n] for t in out]
+
+    @staticmethod
+    def evaluate_constraint_quotients_on_domain(quotients, trace0, trace1, trace2, random_coeff_powers,
+                                                denominator_inverses, domain_log_size, eval_domain_log_size,
+                                                n_constraints, eval_bytes, cumsum_shift=(0, 0, 0, 0),
+                                                should_accumulate=True, logup_counts=0, ctx=None):
+        """ComponentProver<CudaBackend>::evaluate_constraint_quotients_on_domain's
+        FFI call (component_prover.rs:447-470): eval_bytes is eval_id followed
+        by the component's #[repr(C)] Eval struct (eval_blob_* below)."""
+        ctx = ctx or default_context()
+        qp, k0 = L.ptr_array([t.data_ptr() for t in quotients])
+        t0, k1 = L.ptr_array([t.data_ptr() for t in trace0])
+        t1, k2 = L.ptr_array([t.data_ptr() for t in trace1])
+        t2, k3 = L.ptr_array([t.data_ptr() for t in trace2])
+        pw = (L.QM31 * max(len(random_coeff_powers), 1))(*[qm31(p) for p in random_coeff_powers])
+        dn = np.ascontiguousarray(denominator_inverses, dtype=np.uint32)
+        eb = (C.c_uint8 * len(eval_bytes)).from_buffer_copy(eval_bytes)
+        L.check(L.lib().gs_evaluate_constraint_quotients_on_domain(
+            ctx.handle, qp, t0, len(trace0), t1, len(trace1), t2, len(trace2), pw, dn.ctypes.data_as(L.U32P),
+            domain_log_size, eval_domain_log_size, n_constraints, logup_counts, eb, len(eval_bytes),
+            qm31(cumsum_shift), 1 if should_accumulate else 0), "evaluate_constraint_quotients_on_domain")
+        return quotients
+
+    # ----------------------------------------------- example trace generation
+    @staticmethod
+    def generate_wide_fibonacci_trace(input_a, input_b, n_columns, ctx=None):
+        """generate_wide_fibonacci_trace: n_columns device columns from inputs a, b."""
+        ctx = ctx or default_context()
+        n = input_a.numel()
+        cols = [torch.empty(n, dtype=torch.int32, device="cuda") for _ in range(n_columns)]
+        cp, k = L.ptr_array([c.data_ptr() for c in cols])
+        L.check(L.lib().gs_generate_wide_fibonacci_trace(ctx.handle, _p(input_a), _p(input_b), n.bit_length() - 1, cp,
+                                                         n_columns), "generate_wide_fibonacci_trace")
+        return cols
+
+    @staticmethod
+    def generate_poseidon_traces(log_size, ctx=None):
+        """generate_poseidon_traces: (158 trace columns, 16 initial-state, 16 final-state columns)."""
+        ctx = ctx or default_context()
+        mk = lambda k: [torch.empty(1 << log_size, dtype=torch.int32, device="cuda") for _ in range(k)]
+        trace, init, fin = mk(158), mk(16), mk(16)
+        tp, k1 = L.ptr_array([c.data_ptr() for c in trace])
+        ip, k2 = L.ptr_array([c.data_ptr() for c in init])
+        fp, k3 = L.ptr_array([c.data_ptr() for c in fin])
+        L.check(L.lib().gs_generate_poseidon_traces(ctx.handle, tp, ip, fp, log_size), "generate_poseidon_traces")
+        return trace, init, fin
+
+    @staticmethod
+    def generate_poseidon_interaction_traces(z, alpha, init, fin, ctx=None):
+        """generate_poseidon_interaction_traces: (4 interaction planes, claimed sum)."""
+        ctx = ctx or default_context()
+        log_size = init[0].numel().bit_length() - 1
+        powers, cur = [], [1, 0, 0, 0]
+        for _ in range(16):
+            powers.append(cur)
+            cur = _qm_mul(cur, alpha)
+        words = list(z) + list(alpha) + [w for p in powers for w in p]
+        le = (C.c_uint32 * len(words))(*[int(w) for w in words])
+        out = [torch.empty(1 << log_size, dtype=torch.int32, device="cuda") for _ in range(4)]
+        ip, k1 = L.ptr_array([c.data_ptr() for c in init])
+        fp, k2 = L.ptr_array([c.data_ptr() for c in fin])
+        op, k3 = L.ptr_array([c.data_ptr() for c in out])
+        cs = (C.c_uint32 * 4)()
+        L.check(L.lib().gs_generate_poseidon_interaction_traces(ctx.handle, le, ip, fp, log_size, op, cs),
+                "generate_poseidon_interaction_traces")
+        return out, list(cs)
 
     # ------------------------------------------------------------- GrindOps
     @staticmethod
@@ -389,3 +525,49 @@ class CommitPlan:
             self.close()
         except Exception:
             pass
+
+
+def fnv1a_eval_id(name: str) -> int:
+    """fnv1a_eval_id_gen (crates/constraint-framework/src/lib.rs:353-363)."""
+    h = 0x811C9DC5
+    for b in name.encode():
+        h = ((h ^ b) * 0x01000193) & 0xFFFFFFFF
+    return h
+
+
+def eval_blob_wide_fibonacci(log_n_rows):
+    """The bytes ComponentProver passes for WideFibonacciEval: eval_id, then
+    #[repr(C)] WideFibonacciEval { eval_id, log_n_rows }
+    (crates/examples/src/wide_fibonacci/mod.rs:32-37)."""
+    i = fnv1a_eval_id("fibonacci_example")
+    return struct.pack("<3I", i, i, log_n_rows)
+
+
+def eval_blob_poseidon(log_n_rows, z, alpha, claimed_sum):
+    """The bytes for PoseidonEval: eval_id, then #[repr(C)] PoseidonEval {
+    eval_id, log_n_rows, lookup_elements { z, alpha, alpha_powers[16] },
+    claimed_sum } (crates/examples/src/poseidon/mod.rs:57-64), QM31 as 4 words."""
+    def mul(a, b):  # QM31 product on the host
+        return _qm_mul(a, b)
+    i = fnv1a_eval_id("poseidon_example")
+    powers, cur = [], [1, 0, 0, 0]
+    for _ in range(16):
+        powers.append(cur)
+        cur = mul(cur, alpha)
+    words = [i, i, log_n_rows] + list(z) + list(alpha) + [w for p in powers for w in p] + list(claimed_sum)
+    return struct.pack(f"<{len(words)}I", *[int(w) for w in words])
+
+
+def _cm_mul(a, b):
+    return ((a[0] * b[0] - a[1] * b[1]) % P, (a[0] * b[1] + a[1] * b[0]) % P)
+
+
+def _qm_mul(p, q):
+    """QM31 (a + b i) + (c + d i) u with u^2 = 2 + i (core/fields/qm31.rs), on Python ints."""
+    p, q = [int(x) for x in p], [int(x) for x in q]
+    x0, y0, x1, y1 = (p[0], p[1]), (p[2], p[3]), (q[0], q[1]), (q[2], q[3])
+    xx, yy = _cm_mul(x0, x1), _cm_mul(y0, y1)
+    r_yy = _cm_mul((2, 1), yy)
+    re = ((xx[0] + r_yy[0]) % P, (xx[1] + r_yy[1]) % P)
+    a, b = _cm_mul(x0, y1), _cm_mul(y0, x1)
+    return [re[0], re[1], (a[0] + b[0]) % P, (a[1] + b[1]) % P]

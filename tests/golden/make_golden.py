@@ -5,7 +5,7 @@ The reference is a Rust crate that cannot be built in this container, so its
 own test files are read as text and the literal expected values are copied
 out. Run from the repository root, in the container that holds the reference:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 Sources (paths inside the reference checkout):
   crates/stwo/src/core/vcs/blake2_hash.rs      single_hash_test   (Blake2s of b"a")
@@ -117,4 +117,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <reference checkout>")
+    main(sys.argv[1])
