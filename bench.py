@@ -621,6 +621,35 @@ def serving_metric(kind, channel="blake2s"):
     return "served proofs/s with p50/p99 latency (Poisson mix of Poseidon2 2^12..2^18, WF 2^12..2^20)" + suffix
 
 
+def gpu_busy_fraction(fn):
+    """Fraction of fn's wall time during which at least one kernel ran on
+    the device (kernel intervals from a CUPTI trace via torch.profiler,
+    merged); fn runs once, outside any timed region."""
+    import torch
+    from torch.profiler import profile, ProfilerActivity
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    iv = []
+    for e in prof.events():
+        if e.device_type == torch.autograd.DeviceType.CUDA and "Memcpy" not in e.name and "Memset" not in e.name:
+            iv.append((e.time_range.start, e.time_range.end))
+    if not iv:
+        return None
+    iv.sort()
+    busy, cur_s, cur_e = 0.0, iv[0][0], iv[0][1]
+    for a, b in iv[1:]:
+        if a > cur_e:
+            busy += cur_e - cur_s
+            cur_s, cur_e = a, b
+        else:
+            cur_e = max(cur_e, b)
+    busy += cur_e - cur_s
+    span = max(b for _, b in iv) - iv[0][0]
+    return round(busy / span, 3) if span > 0 else None
+
+
 def run_serving(args, world, rank, local):
     import torch
     from gpustark import prove as G
@@ -631,6 +660,7 @@ def run_serving(args, world, rank, local):
     tuning = fft_autotune(args, 23)
     jobs = job_mix(args.workload, 1 + rank)
     mc = args.merkle_channel
+    steps, warmup = max(1, args.steps), max(0, args.warmup)
 
     def single(a, n, c, sd):
         if a == 0:
@@ -641,63 +671,83 @@ def run_serving(args, world, rank, local):
     for shape in sorted({(a, n, c) for a, n, c, _ in jobs}):
         single(*shape, 0)
     torch.cuda.synchronize()
-    # sequential: one proof at a time on one stream
+    # sequential: one proof at a time on one stream, the same job list `steps` times
     barrier(world)
+    seq_lat, seq_proofs = [], None
     t0 = time.perf_counter()
-    seq_lat = []
-    seq_proofs = []
-    for j in jobs:
-        ts = time.perf_counter()
-        seq_proofs.append(single(*j))
-        seq_lat.append(1e3 * (time.perf_counter() - ts))
-    seq_s = time.perf_counter() - t0
-    workers = args.workers
+    for _ in range(steps):
+        proofs = []
+        for j in jobs:
+            ts = time.perf_counter()
+            proofs.append(single(*j))
+            seq_lat.append(1e3 * (time.perf_counter() - ts))
+        seq_proofs = seq_proofs or proofs
+    seq_s = (time.perf_counter() - t0) / steps
+    workers, fibers = args.workers, args.fibers
     arrivals = None
-    with S.ProofServer(workers, 96 << 30) as sv:
-        # warm every worker's context on every shape (twiddle trees, domain
-        # tables and pool growth happen once per context): `workers` copies
-        # of each shape in flight at once
+    lat, identical, busy = [], True, None
+    with S.ProofServer(workers, 96 << 30, fibers_per_worker=fibers) as sv:
+        # warm every context on every shape (twiddle trees, domain tables and
+        # pool growth happen once per context): `workers * fibers` copies of
+        # each shape in flight at once, then `warmup` whole batches
+        conc = workers * fibers
         for a, n, c in sorted({(a, n, c) for a, n, c, _ in jobs}):
-            for i in [sv.submit(a, n, c or 100, 0, merkle_channel=mc) for _ in range(workers)]:
+            for i in [sv.submit(a, n, c or 100, 0, merkle_channel=mc) for _ in range(conc)]:
                 sv.wait(i)
-        barrier(world)
-        t0 = time.perf_counter()
-        if args.workload == "batched":
-            ids = [sv.submit(a, n, c or 100, sd, merkle_channel=mc) for a, n, c, sd in jobs]
-        else:
+
+        def batch(record):
+            t_start = time.perf_counter()
+            if args.workload == "batched":
+                ids = [sv.submit(a, n, c or 100, sd, merkle_channel=mc) for a, n, c, sd in jobs]
+            else:
+                ids = []
+                for (a, n, c, sd), at in zip(jobs, arrivals):
+                    now = time.perf_counter() - t_start
+                    if at > now:
+                        time.sleep(at - now)
+                    ids.append(sv.submit(a, n, c or 100, sd, merkle_channel=mc))
+            res = [sv.wait(i) for i in ids]
+            if record:
+                lat.extend(l for _, l in res)
+            return res
+
+        if args.workload == "served":
             # Poisson arrivals at `load` x the sequential proof rate (seeded)
             rate = args.load * len(jobs) / seq_s
             gaps = np.random.default_rng(7 + rank).exponential(1.0 / rate, len(jobs))
             arrivals = np.cumsum(gaps)
-            ids = []
-            for (a, n, c, sd), at in zip(jobs, arrivals):
-                now = time.perf_counter() - t0
-                if at > now:
-                    time.sleep(at - now)
-                ids.append(sv.submit(a, n, c or 100, sd, merkle_channel=mc))
-        res = [sv.wait(i) for i in ids]
-        srv_s = time.perf_counter() - t0
-    identical = all(p == q for (p, _), q in zip(res, seq_proofs))
-    lat = sorted(l for _, l in res)
+        for _ in range(warmup):
+            batch(False)
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            res = batch(True)
+            identical = identical and all(p == q for (p, _), q in zip(res, seq_proofs))
+        srv_s = (time.perf_counter() - t0) / steps
+        busy = gpu_busy_fraction(lambda: batch(False))
+    lat = sorted(lat)
     srv_s = max_over_ranks(srv_s, world, "cuda")
     seq_s = max_over_ranks(seq_s, world, "cuda")
     pps = world * len(jobs) / srv_s
     seq_pps = world * len(jobs) / seq_s
     q = lambda v, f: float(np.percentile(np.asarray(v), f))
+    mode = ("%d host threads x %d proof fibers (one CUDA stream each)" % (workers, fibers) if fibers > 1
+            else "%d workers (one CUDA stream each)" % workers)
     out = {
         "metric": serving_metric(args.workload, mc),
-        "value": round(pps, 2), "unit": "proofs/s", "n_gpus": world, "steps": 1, "warmup": 1,
+        "value": round(pps, 2), "unit": "proofs/s", "n_gpus": world, "steps": steps, "warmup": warmup,
         "ms_per_step": round(1e3 * srv_s, 2), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32 (M31/QM31 integer arithmetic)", "data": "synthetic: seeded uniform M31",
-        "config": {"workload": "%s: %d jobs, %d workers (one CUDA stream each), admission by HBM footprint"
-                               % (args.workload, len(jobs), workers),
+        "config": {"workload": "%s: %d jobs per step, %s, admission by HBM footprint"
+                               % (args.workload, len(jobs), mode),
                    "parallelism": "replicas x%d" % world, "fft_tuning": tuning},
         "sequential_proofs_per_s": round(seq_pps, 2), "speedup_vs_sequential": round(pps / seq_pps, 2),
         "latency_ms": {"p50": round(q(lat, 50), 2), "p99": round(q(lat, 99), 2)},
         "sequential_latency_ms": {"p50": round(q(seq_lat, 50), 2), "p99": round(q(seq_lat, 99), 2)},
         "proofs_identical_to_sequential": identical,
+        "gpu_busy_fraction": busy,
         "e2e": {"value": round(pps, 2), "unit": "proofs/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": int(sum(len(p) for p, _ in res))},
+                "d2h_bytes_per_step": int(sum(len(p) for p in seq_proofs))},
     }
     if arrivals is not None:
         out["arrival_rate_per_s"] = round(args.load * len(jobs) / seq_s, 2)
@@ -799,17 +849,23 @@ def run_reference(args, world, rank):
         }
     log_n = args.log_n or PROOF_SIZES[args.workload]
     mc = args.merkle_channel
-    for _ in range(min(args.warmup, 1)):
+    # the same step count as the GPU arm, unless that would run past about
+    # 150 s of CPU proving (sized from the one warm-up proof)
+    warm = min(args.warmup, 1)
+    est = None
+    for _ in range(warm):
+        t0 = time.perf_counter()
         cpu_proof_sample(args.workload, threads, log_n, mc)
+        est = time.perf_counter() - t0
     vals, desc = [], ""
-    steps = max(1, min(args.steps, 3))
+    steps = max(1, args.steps if est is None or est * args.steps <= 150 else int(150 / est))
     for _ in range(steps):
         ms, desc = cpu_proof_sample(args.workload, threads, log_n, mc)
         vals.append(ms)
     v = statistics.mean(vals)
     return {
         "impl": "reference", "metric": proof_metric(args.workload, mc), "value": round(v, 1), "unit": "ms",
-        "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": round(v, 1),
+        "n_gpus": world, "steps": steps, "warmup": warm, "ms_per_step": round(v, 1),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32 (M31/QM31 integer arithmetic)", "data": "synthetic: seeded uniform M31",
         "config": dict(proof_config(args.workload, log_n, mc), parallelism="cpu threads"),
@@ -875,7 +931,9 @@ def main():
     ap.add_argument("--impl", default="gpustark", choices=["gpustark", "reference"])
     ap.add_argument("--workload", default="poseidon",
                     choices=["poseidon", "wide_fibonacci", "kernels", "batched", "served"])
-    ap.add_argument("--workers", type=int, default=16, help="server workers (batched / served)")
+    ap.add_argument("--workers", type=int, default=2, help="server host threads (batched / served)")
+    ap.add_argument("--fibers", type=int, default=8,
+                    help="batched / served: proofs per server thread as cooperative fibers (1 = one proof per thread)")
     ap.add_argument("--load", type=float, default=2.0, help="served: arrival rate / sequential proof rate")
     ap.add_argument("--merkle-channel", default="blake2s", choices=["blake2s", "poseidon252"],
                     help="proof workloads: Blake2sMerkleChannel or Poseidon252MerkleChannel")

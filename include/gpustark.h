@@ -397,6 +397,14 @@ int gs_poseidon252_channel_op(const uint8_t digest[32], uint32_t n_draws, uint32
  * proof and reports the submit-to-done latency. */
 typedef struct gs_server gs_server;
 int gs_server_create(uint32_t n_workers, size_t hbm_budget_bytes, gs_server** out);
+/* The same server with n_threads host threads, each driving
+ * fibers_per_thread proofs at once as cooperative fibers (one CUDA stream
+ * and context per fiber): a proof's wait on its stream yields to the other
+ * proofs of its thread instead of blocking it, so a few threads keep many
+ * proofs' launches queued. Results and admission are as above;
+ * gs_server_create(n, b) is gs_server_create_fibers(n, 1, b). */
+int gs_server_create_fibers(uint32_t n_threads, uint32_t fibers_per_thread, size_t hbm_budget_bytes,
+                            gs_server** out);
 int gs_server_submit(gs_server* server, uint32_t air, uint32_t log_n, uint32_t n_columns, uint64_t seed,
                      uint32_t composition_log_split, const gs_pcs_config* config, uint64_t* job_id);
 /* The same job proved over Poseidon252MerkleChannel (as

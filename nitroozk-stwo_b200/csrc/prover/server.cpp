@@ -17,6 +17,7 @@
 #include <mutex>
 #include <thread>
 #include "../../../include/gpustark.h"
+#include "fiber.h"
 #include "prove_api.h"
 
 namespace gs {
@@ -56,8 +57,82 @@ struct Server {
   uint64_t next_id = 1;
   bool stopping = false;
   int device = 0;
+  uint32_t fibers = 1;  // proofs per host thread (fiber mode when > 1)
+
+  bool admissible() const {
+    return !queue.empty() && (in_flight == 0 || in_flight + queue.front().footprint <= budget);
+  }
+
+  // Proves one job on a context and publishes the result.
+  void serve(Context& ctx, cudaStream_t st, int init, Job& job) {
+    Done d;
+    auto t0 = std::chrono::steady_clock::now();
+    if (init != OK) {
+      d.status = init;
+      d.error = "context initialisation failed";
+    } else {
+      d.status = prove_component(ctx, job.req, &d.proof, nullptr);
+      if (d.status != OK) d.error = last_error();
+      stream_sync(st);
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    d.service_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    d.latency_ms = std::chrono::duration<double, std::milli>(t1 - job.submitted).count();
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      in_flight -= job.footprint;
+      done[job.id] = std::move(d);
+    }
+    cv_done.notify_all();
+    cv_jobs.notify_all();
+  }
+
+  // Fiber mode: `fibers` proof loops on this host thread, each with its own
+  // stream and context; a loop with no admissible job yields, and the thread
+  // sleeps on the job queue only when every loop is idle.
+  void fiber_worker() {
+    cudaSetDevice(device);
+    std::vector<std::function<void()>> bodies;
+    for (uint32_t k = 0; k < fibers; k++) {
+      bodies.push_back([this] {
+        cudaStream_t st;
+        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        Context ctx;
+        int init = ctx.init(st);
+        for (;;) {
+          Job job;
+          bool got = false, quit = false;
+          {
+            std::lock_guard<std::mutex> lk(mu);
+            if (admissible()) {
+              job = std::move(queue.front());
+              queue.pop_front();
+              in_flight += job.footprint;
+              got = true;
+            } else if (stopping && queue.empty()) {
+              quit = true;
+            }
+          }
+          if (quit) break;
+          if (!got) {
+            FiberScheduler::yield_idle();
+            continue;
+          }
+          serve(ctx, st, init, job);
+        }
+        ctx.destroy();
+        cudaStreamDestroy(st);
+      });
+    }
+    FiberScheduler sched;
+    sched.run(std::move(bodies), [this] {
+      std::unique_lock<std::mutex> lk(mu);
+      cv_jobs.wait_for(lk, std::chrono::milliseconds(2), [&] { return stopping || admissible(); });
+    });
+  }
 
   void worker() {
+    if (fibers > 1) return fiber_worker();
     cudaSetDevice(device);
     cudaStream_t st;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
@@ -72,35 +147,13 @@ struct Server {
       {
         std::unique_lock<std::mutex> lk(mu);
         // admission by footprint holds while the server drains at shutdown too
-        cv_jobs.wait(lk, [&] {
-          return (stopping && queue.empty()) ||
-                 (!queue.empty() && (in_flight == 0 || in_flight + queue.front().footprint <= budget));
-        });
+        cv_jobs.wait(lk, [&] { return (stopping && queue.empty()) || admissible(); });
         if (queue.empty()) break;
         job = std::move(queue.front());
         queue.pop_front();
         in_flight += job.footprint;
       }
-      Done d;
-      auto t0 = std::chrono::steady_clock::now();
-      if (init != OK) {
-        d.status = init;
-        d.error = last_error();
-      } else {
-        d.status = prove_component(ctx, job.req, &d.proof, nullptr);
-        if (d.status != OK) d.error = last_error();
-        stream_sync(st);
-      }
-      auto t1 = std::chrono::steady_clock::now();
-      d.service_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-      d.latency_ms = std::chrono::duration<double, std::milli>(t1 - job.submitted).count();
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        in_flight -= job.footprint;
-        done[job.id] = std::move(d);
-      }
-      cv_done.notify_all();
-      cv_jobs.notify_all();
+      serve(ctx, st, init, job);
     }
     set_thread_wait_event(nullptr);
     ctx.destroy();
@@ -122,11 +175,18 @@ struct gs_server {
 extern "C" {
 
 int gs_server_create(uint32_t n_workers, size_t hbm_budget_bytes, gs_server** out) {
-  GS_REQUIRE(out != nullptr && n_workers >= 1 && n_workers <= 64, "bad server arguments");
+  return gs_server_create_fibers(n_workers, 1, hbm_budget_bytes, out);
+}
+
+int gs_server_create_fibers(uint32_t n_threads, uint32_t fibers_per_thread, size_t hbm_budget_bytes,
+                            gs_server** out) {
+  GS_REQUIRE(out != nullptr && n_threads >= 1 && n_threads <= 64, "bad server arguments");
+  GS_REQUIRE(fibers_per_thread >= 1 && fibers_per_thread <= 64, "fibers per thread must be in [1, 64]");
   gs_server* sv = new gs_server();
   sv->s.budget = hbm_budget_bytes;
+  sv->s.fibers = fibers_per_thread;
   cudaGetDevice(&sv->s.device);
-  for (uint32_t i = 0; i < n_workers; i++) sv->s.workers.emplace_back([sv] { sv->s.worker(); });
+  for (uint32_t i = 0; i < n_threads; i++) sv->s.workers.emplace_back([sv] { sv->s.worker(); });
   *out = sv;
   return OK;
 }

@@ -25,7 +25,11 @@ static double wait_spin_us() {
   }();
   return us;
 }
+static thread_local int (*g_sync_hook)(cudaStream_t) = nullptr;
+void set_thread_sync_hook(int (*hook)(cudaStream_t)) { g_sync_hook = hook; }
+
 int stream_sync(cudaStream_t st) {
+  if (g_sync_hook) return g_sync_hook(st);
   if (g_wait_ev) {
     GS_CUDA_TRY(cudaEventRecord(g_wait_ev, st));
     const double limit = wait_spin_us();

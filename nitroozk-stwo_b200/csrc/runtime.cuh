@@ -86,6 +86,9 @@ __device__ __forceinline__ pt31 domain_point_bitrev(const DomainTables& t, uint3
 // would lengthen), then sleeps on it.
 int stream_sync(cudaStream_t st);
 void set_thread_wait_event(cudaEvent_t ev);
+// Replaces stream_sync's wait on the calling thread (the proof server's
+// fiber scheduler installs one; nullptr restores the default).
+void set_thread_sync_hook(int (*hook)(cudaStream_t));
 
 // Number of SMs of the current device (cached).
 int num_sms();

@@ -76,6 +76,7 @@ _PROTOS = {
     "gs_prove_wide_fibonacci": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, U32P,
                                 C.POINTER(PcsConfig), C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
     "gs_server_create": [C.c_uint32, C.c_size_t, C.POINTER(C.c_void_p)],
+    "gs_server_create_fibers": [C.c_uint32, C.c_uint32, C.c_size_t, C.POINTER(C.c_void_p)],
     "gs_server_submit": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
                          C.POINTER(PcsConfig), C.POINTER(C.c_uint64)],
     "gs_server_submit_poseidon252": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,

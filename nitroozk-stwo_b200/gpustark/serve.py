@@ -14,9 +14,12 @@ WIDE_FIBONACCI, POSEIDON = 0, 1
 
 
 class ProofServer:
-    def __init__(self, n_workers=4, hbm_budget_bytes=64 << 30):
+    def __init__(self, n_workers=4, hbm_budget_bytes=64 << 30, fibers_per_worker=1):
+        """n_workers host threads; fibers_per_worker > 1 runs that many proofs
+        per thread as cooperative fibers (gs_server_create_fibers)."""
         h = C.c_void_p()
-        L.check(L.lib().gs_server_create(n_workers, hbm_budget_bytes, C.byref(h)), "gs_server_create")
+        L.check(L.lib().gs_server_create_fibers(n_workers, fibers_per_worker, hbm_budget_bytes, C.byref(h)),
+                "gs_server_create_fibers")
         self.handle = h
 
     def submit(self, air, log_n, n_columns=100, seed=0, composition_log_split=None, config=None,

@@ -60,3 +60,33 @@ def test_served_poseidon252_jobs_match_single_proofs(mods):
         else:
             want = prove.prove_poseidon(n, seed=s, input_mode=prove.INPUT_SEEDED, merkle_channel=mc)
         assert proof == want
+
+
+@pytest.mark.parametrize("threads,fibers,budget", [(1, 8, 64 << 30), (2, 6, 64 << 30), (2, 4, 1 << 20)])
+def test_fiber_server_results_match_single_proofs(mods, threads, fibers, budget):
+    """Fiber mode: several proofs per host thread, each waiting by yielding
+    to the others; every proof is the one proved alone, also when the
+    budget admits one job at a time."""
+    prove, serve = mods
+    with serve.ProofServer(threads, budget, fibers_per_worker=fibers) as sv:
+        ids = [sv.submit(a, n, c or 100, s) for a, n, c, s in JOBS * 2]
+        got = [sv.wait(i) for i in ids]
+    for (a, n, c, s), (proof, lat) in zip(JOBS * 2, got):
+        assert proof == alone(prove, a, n, c or 100, s)
+        assert lat > 0
+
+
+def test_fiber_server_mixed_channels_and_errors(mods):
+    prove, serve = mods
+    with serve.ProofServer(1, fibers_per_worker=4) as sv:
+        bad = sv.submit(serve.POSEIDON, 6, composition_log_split=1)
+        ids = [sv.submit(0, 8, 20, 1, merkle_channel="poseidon252"), sv.submit(1, 6, 0, 2),
+               sv.submit(0, 9, 30, 3, merkle_channel="poseidon252")]
+        with pytest.raises(prove.ConstraintsNotSatisfied):
+            sv.wait(bad)
+        got = [sv.wait(i)[0] for i in ids]
+    assert got[0] == prove.prove_wide_fibonacci(8, 20, seed=1, input_mode=prove.INPUT_SEEDED,
+                                                merkle_channel="poseidon252")
+    assert got[1] == alone(prove, 1, 6, 0, 2)
+    assert got[2] == prove.prove_wide_fibonacci(9, 30, seed=3, input_mode=prove.INPUT_SEEDED,
+                                                merkle_channel="poseidon252")
