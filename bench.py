@@ -549,17 +549,35 @@ def run_proof(args, world, rank, local):
     }
     if cpu:
         out["cpu_baseline"] = cpu
-    rl = proof_roofline(args, log_n, wl, ctx) if mc == "blake2s" else None
+    rl = proof_roofline(args, log_n, wl, ctx, clk) if mc == "blake2s" else None
     if rl:
         out["roofline"] = rl
     return out
 
 
-def proof_roofline(args, log_n, wl, ctx):
+def int_roof(counts, ms, clk):
+    """The integer-instruction ceiling of a kernel whose instruction counts ncu
+    measured: each SM issues at most one warp instruction per cycle on each of
+    its 4 schedulers and two per cycle on the integer ALU pipe, so the launch
+    cannot end before max(inst / 4, alu / 2) / n_SM cycles. Taken at the SM
+    clock sampled during the timed region; frac = that time / measured time."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965
+    issue = counts["warp_inst"] / (4.0 * sms)
+    alu = counts["alu_warp_inst"] / (2.0 * sms)
+    roof_ms = max(issue, alu) / (mhz * 1e3)
+    return {"bound": "issue" if issue >= alu else "int_alu", "roof_ms": round(roof_ms, 4),
+            "frac": round(roof_ms / ms, 4), "sm_mhz": mhz, "warp_inst": counts["warp_inst"],
+            "alu_warp_inst": counts["alu_warp_inst"], "n_sm": sms}
+
+
+def proof_roofline(args, log_n, wl, ctx, clk=None):
     """Roofline of the proof's dominant kernel, timed live on the proof's shape:
     the low-degree extension of the committed trace (evaluate_polynomials,
     CanonicCoset(log_n) coefficients -> 2^(log_n + 2) for Poseidon's constraint
-    domain, 2^(log_n + 1) for Wide-Fibonacci)."""
+    domain, 2^(log_n + 1) for Wide-Fibonacci). Beside the HBM line it reports
+    the integer-issue ceiling (int_roof), the bound the kernel actually meets."""
     import torch
     from gpustark.backend import GpuBackend as B
     hbm_peak, peak_kind = load_peaks()
@@ -586,17 +604,22 @@ def proof_roofline(args, log_n, wl, ctx):
     ms = statistics.mean(times)
     alg = 4 * cols * ((1 << log_n) + (1 << target))   # LDE n -> n+b: 4(2^n + 2^(n+b)) bytes per column
     achieved = alg / (ms / 1e3) / 1e9
-    traffic = None
+    traffic = inst = None
     tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get("lde_%s_%d" % (wl, log_n))
+            recs = json.load(open(tpath))
+            traffic = recs.get("lde_%s_%d" % (wl, log_n))
+            inst = recs.get("inst_lde_%s_%d" % (wl, log_n))
         except Exception:
-            traffic = None
-    return {"kernel": "fft_tile_kernel (LDE %d cols 2^%d -> 2^%d, 2 launches)" % (cols, log_n, target), "bound": "hbm",
-            "achieved": round(achieved, 1), "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
-            "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "algorithmic_bytes": alg,
-            "avg_ms": round(ms, 4)}
+            traffic = inst = None
+    out = {"kernel": "fft_tile_kernel (LDE %d cols 2^%d -> 2^%d, 2 launches)" % (cols, log_n, target), "bound": "hbm",
+           "achieved": round(achieved, 1), "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
+           "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "algorithmic_bytes": alg,
+           "avg_ms": round(ms, 4)}
+    if inst:
+        out["int_roof"] = int_roof(inst, ms, clk)
+    return out
 
 
 # ------------------------------------------------------------ batched / served

@@ -49,12 +49,13 @@ int poseidon_constraints(cudaStream_t st, const uint32_t* trace, const uint32_t*
                          uint32_t trace_log, const ConstraintParams& prm, const LookupParams& lp, qm31 cumsum_shift,
                          Planes out);
 
-// gather.cu: hash witnesses as runs read from one Merkle layer each; item i
-// (out hash i) is hash idx[i] of its run's layer, the items of a run
-// consecutive from `first`.
+// gather.cu: hash witnesses as runs read from one Merkle layer each; item k
+// of a run is hash idx[first + k] of its layer, written to output hash
+// out + k (runs may share index ranges).
 struct HashRun {
   const uint32_t* src;
   uint32_t first, count;
+  uint32_t out, pad;
 };
 int gather_hash_runs(cudaStream_t st, const HashRun* d_runs, uint32_t n_runs, const uint32_t* d_idx,
                      uint32_t* d_out);

@@ -12,9 +12,8 @@ __global__ void gather_hash_runs_kernel(const HashRun* __restrict__ runs, const 
                                         uint32_t* __restrict__ out) {
   const HashRun r = runs[blockIdx.x];
   for (uint32_t k = threadIdx.x; k < r.count; k += blockDim.x) {
-    const size_t i = (size_t)r.first + k;
-    const uint4* s = reinterpret_cast<const uint4*>(r.src + 8 * (size_t)__ldg(idx + i));
-    uint4* o = reinterpret_cast<uint4*>(out + 8 * i);
+    const uint4* s = reinterpret_cast<const uint4*>(r.src + 8 * (size_t)__ldg(idx + (size_t)r.first + k));
+    uint4* o = reinterpret_cast<uint4*>(out + 8 * ((size_t)r.out + k));
     o[0] = __ldg(s);
     o[1] = __ldg(s + 1);
   }

@@ -240,19 +240,23 @@ static int finish_last_layer(Prover& pv, const uint32_t* h, uint32_t log, std::v
 // fold step 1: positions are both members of each queried pair; the witness
 // values are the pair members that were not queried.
 void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::vector<uint8_t>& is_witness) {
-  size_t i = 0;
-  while (i < q.size()) {
-    size_t start = (q[i] >> 1) << 1;
-    size_t j = i;
-    while (j < q.size() && (q[j] >> 1) == (q[i] >> 1)) j++;
-    size_t k = i;
-    for (size_t p = start; p < start + 2; p++) {
-      pos.push_back(p);
-      if (k < j && q[k] == p) { k++; is_witness.push_back(0); }
-      else is_witness.push_back(1);
-    }
-    i = j;
+  // q is sorted and unique: a pair holds one or two queries
+  const size_t n = q.size();
+  pos.resize(2 * n);
+  is_witness.resize(2 * n);
+  size_t o = 0;
+  for (size_t i = 0; i < n;) {
+    const size_t start = q[i] & ~(size_t)1;
+    const bool both = i + 1 < n && q[i + 1] == start + 1;
+    pos[o] = start;
+    pos[o + 1] = start + 1;
+    is_witness[o] = q[i] != start;
+    is_witness[o + 1] = !both && q[i] == start;
+    o += 2;
+    i += both ? 2 : 1;
   }
+  pos.resize(o);
+  is_witness.resize(o);
 }
 
 int validate_request(const ProveRequest& r) {

@@ -257,14 +257,22 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     size_t val_base = 0;
     MerkleDecommitPlan merkle;
   };
-  auto plan_fri = [&](FriLayerDev& L, const std::vector<size_t>& q, FriPlan& fp) -> int {
+  // the witness lists of every level of the query set, shared by the FRI
+  // layers and the lifting-size trees
+  static thread_local SharedWitness sw;
+  sw.build(g, queries, lifting);
+  // FRI layer i (the first layer is i = 0) is queried at S_i, its leaves
+  // decommitted as the pairs of S_i
+  auto plan_fri = [&](FriLayerDev& L, const std::vector<size_t>& q, size_t i, FriPlan& fp) -> int {
     fri_positions(q, fp.pos, fp.wit);
     std::vector<const uint32_t*> cols = {L.planes[0], L.planes[1], L.planes[2], L.planes[3]};
     GS_TRY(g.add_cols(cols, fp.pos, &fp.val_base));
+    if (L.layers.size() == (size_t)lifting - i + 1)
+      return fp.merkle.plan_shared(g, L.layers, cols, fp.pos, sw, (int)L.layers.size() - 3, i + 1, false);
     return fp.merkle.plan(g, L.layers, cols, fp.pos, false);
   };
   FriPlan first_plan;
-  GS_TRY(plan_fri(first, queries, first_plan));
+  GS_TRY(plan_fri(first, queries, 0, first_plan));
   std::vector<FriPlan> inner_plans(inner.size());
   std::vector<size_t> lq = queries;
   for (size_t i = 0; i < inner.size(); i++) {
@@ -272,7 +280,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     for (size_t q : lq)
       if (f.empty() || f.back() != (q >> 1)) f.push_back(q >> 1);
     lq = f;
-    GS_TRY(plan_fri(inner[i], lq, inner_plans[i]));
+    GS_TRY(plan_fri(inner[i], lq, i + 1, inner_plans[i]));
   }
   pv.mark("fri_plans");
   std::vector<MerkleDecommitPlan> tree_plans(n_trees);
@@ -282,7 +290,10 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     std::vector<size_t> pos = prepare_positions(queries, lifting, tr.max_log());
     std::vector<const uint32_t*> cols;
     for (uint32_t c = 0; c < tr.n_cols; c++) cols.push_back(tr.eval_col(c));
-    GS_TRY(tree_plans[t].plan(g, tr.layers, cols, pos));
+    if (tr.layers.size() == (size_t)lifting + 1 && pos == sw.s0)
+      GS_TRY(tree_plans[t].plan_shared(g, tr.layers, cols, pos, sw, (int)lifting - 1, 0));
+    else
+      GS_TRY(tree_plans[t].plan(g, tr.layers, cols, pos));
   }
   pv.mark("decommit_plan");
   GS_TRY(g.run(pv.ctx, pv.A));

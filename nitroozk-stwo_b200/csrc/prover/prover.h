@@ -72,6 +72,7 @@ struct GatherPlan {
   std::vector<uint32_t> hidx;    // hash index of every witness, in output order
   std::vector<uint8_t> packed;   // the upload: blocks | positions | runs | hidx
   size_t n_words = 0;
+  size_t n_hash_out = 0;         // hashes the runs write, in run order
   uint32_t max_items = 0;
   // results, in the context's pinned read-back buffer (valid until its next
   // read-back): gathered words, then 8 words per hash
@@ -84,10 +85,11 @@ struct GatherPlan {
     runs.clear();
     hidx.clear();
     n_words = 0;
+    n_hash_out = 0;
     max_items = 0;
     word_out = hash_out = nullptr;
   }
-  size_t n_hashes() const { return hidx.size(); }
+  size_t n_hashes() const { return n_hash_out; }
   // Values of `cols` at `pos`, position-major; returns the first output word.
   // More than 4 columns must be equally spaced (one tree's columns are).
   int add_cols(const std::vector<const uint32_t*>& cols, const std::vector<size_t>& pos, size_t* first) {
@@ -104,16 +106,20 @@ struct GatherPlan {
       for (uint32_t c = 2; c < b.n_cols; c++)
         GS_REQUIRE((uint64_t)(cols[c] - cols[0]) == c * b.stride, "decommitted columns are not equally spaced");
     }
-    for (size_t p : pos) positions.push_back((uint32_t)p);
+    const size_t p0 = positions.size();
+    positions.resize(p0 + pos.size());
+    for (size_t i = 0; i < pos.size(); i++) positions[p0 + i] = (uint32_t)pos[i];
     *first = n_words;
     n_words += (size_t)b.n_cols * b.n_pos;
     max_items = std::max<uint32_t>(max_items, b.n_cols * b.n_pos);
     if (b.n_cols && b.n_pos) blocks.push_back(b);
     return OK;
   }
-  // Witnesses hidx[first, first + count) read from the layer at `src`.
+  // Witnesses hidx[first, first + count) read from the layer at `src`; they
+  // take the next `count` output hashes.
   void add_run(const uint32_t* src, size_t first, size_t count) {
-    runs.push_back(HashRun{src, (uint32_t)first, (uint32_t)count});
+    runs.push_back(HashRun{src, (uint32_t)first, (uint32_t)count, (uint32_t)n_hash_out, 0});
+    n_hash_out += count;
   }
   int run(Context& ctx, Arena& A) {
     cudaStream_t st = ctx.stream;
@@ -144,7 +150,7 @@ struct GatherPlan {
     // hashes are written as 16-byte vectors: their region starts at a
     // multiple of 4 words
     const size_t hbase = (n_words + 3) & ~(size_t)3;
-    const size_t out_words = hbase + 8 * nh;
+    const size_t out_words = hbase + 8 * n_hash_out;
     uint32_t* d_out = nullptr;
     GS_TRY(A.alloc_n(out_words + 4, &d_out));
     GS_TRY(gather_cols(st, (const ColGather*)d_in, (uint32_t)blocks.size(), max_items, (const uint32_t*)(d_in + o_pos),
@@ -167,6 +173,8 @@ struct GatherPlan {
 // queried values are node-major / column-minor at the leaves, the hash witness
 // lists, layer by layer from the leaves up, the children that the verifier
 // cannot recompute. Pass 1 queues the gathers, pass 2 assembles.
+struct SharedWitness;
+
 struct MerkleDecommitPlan {
   size_t n_positions = 0;
   size_t value_base = 0, n_cols = 0;
@@ -212,6 +220,14 @@ struct MerkleDecommitPlan {
     n_hashes = g.n_hashes() - hash_begin;
     return OK;
   }
+  // The same plan from shared witness lists: the tree's level just above
+  // layers[top_L + 1] holds the positions S_m0, the next S_(m0 + 1), and so
+  // on (top_L = layers.size() - 2 when the leaves are S_0; a FRI layer's
+  // leaves are the complete pairs of S_i, which reveal no hash, so it starts
+  // one level up with top_L = layers.size() - 3 and m0 = i + 1).
+  int plan_shared(GatherPlan& g, const std::vector<uint32_t*>& layers, const std::vector<const uint32_t*>& cols,
+                  const std::vector<size_t>& pos, const SharedWitness& sw, int top_L, size_t m0,
+                  bool with_values = true);
   // The witnesses stay in the gather's read-back buffer; `d` refers to them.
   void assemble(const GatherPlan& g, std::vector<uint32_t>& queried, host::Decommitment& d) const {
     queried.assign(g.word_out + value_base, g.word_out + value_base + n_positions * n_cols);
@@ -219,6 +235,64 @@ struct MerkleDecommitPlan {
     d.n_witness = n_hashes;
   }
 };
+
+// Witness index lists shared by every tree decommitted at the same query
+// positions. Level m of the query set is S_m = {q >> m} (sorted, unique); at a
+// Merkle level whose positions are S_m a decommitment reveals W(S_m), the
+// siblings that are not in S_m, in order. The trees with leaves at S_0 (every
+// tree of the lifting size) and every FRI layer (leaves = the pairs of S_i,
+// level above = S_(i+1)) reveal W(S_m) at their levels, so each list is
+// computed and uploaded once and read by one hash run per tree.
+struct SharedWitness {
+  std::vector<size_t> s0;            // S_0
+  std::vector<size_t> first, count;  // W(S_m) = g.hidx[first[m], first[m] + count[m])
+  void build(GatherPlan& g, const std::vector<size_t>& queries, size_t levels) {
+    s0 = queries;
+    first.assign(levels, 0);
+    count.assign(levels, 0);
+    static thread_local std::vector<size_t> prev, next;
+    prev.assign(queries.begin(), queries.end());
+    for (size_t m = 0; m < levels; m++) {
+      const size_t n = prev.size();
+      const size_t base = g.hidx.size();
+      g.hidx.resize(base + n);
+      uint32_t* w = g.hidx.data() + base;
+      next.resize(n);
+      size_t nw = 0, nn = 0, last_parent = ~(size_t)0;
+      for (size_t i = 0; i < n; i++) {
+        const size_t q = prev[i];
+        const bool sib = (q & 1) ? (i > 0 && prev[i - 1] == q - 1) : (i + 1 < n && prev[i + 1] == q + 1);
+        w[nw] = (uint32_t)(q ^ 1);
+        nw += sib ? 0 : 1;
+        const size_t par = q >> 1;
+        next[nn] = par;
+        nn += par != last_parent ? 1 : 0;
+        last_parent = par;
+      }
+      g.hidx.resize(base + nw);
+      first[m] = base;
+      count[m] = nw;
+      next.resize(nn);
+      prev.swap(next);
+    }
+  }
+};
+
+inline int MerkleDecommitPlan::plan_shared(GatherPlan& g, const std::vector<uint32_t*>& layers,
+                                           const std::vector<const uint32_t*>& cols, const std::vector<size_t>& pos,
+                                           const SharedWitness& sw, int top_L, size_t m0, bool with_values) {
+  GS_REQUIRE(top_L < (int)layers.size() - 1 && m0 + (size_t)(top_L + 1) <= sw.first.size(),
+             "shared witness lists too short for the tree");
+  n_positions = pos.size();
+  n_cols = with_values ? cols.size() : 0;
+  if (with_values) GS_TRY(g.add_cols(cols, pos, &value_base));
+  hash_begin = g.n_hashes();
+  size_t m = m0;
+  for (int L = top_L; L >= 0; L--, m++)
+    if (sw.count[m]) g.add_run(layers[L + 1], sw.first[m], sw.count[m]);
+  n_hashes = g.n_hashes() - hash_begin;
+  return OK;
+}
 
 }  // namespace prover
 }  // namespace gs
