@@ -954,8 +954,8 @@ def main():
     ap.add_argument("--impl", default="gpustark", choices=["gpustark", "reference"])
     ap.add_argument("--workload", default="poseidon",
                     choices=["poseidon", "wide_fibonacci", "kernels", "batched", "served"])
-    ap.add_argument("--workers", type=int, default=2, help="server host threads (batched / served)")
-    ap.add_argument("--fibers", type=int, default=8,
+    ap.add_argument("--workers", type=int, default=4, help="server host threads (batched / served)")
+    ap.add_argument("--fibers", type=int, default=6,
                     help="batched / served: proofs per server thread as cooperative fibers (1 = one proof per thread)")
     ap.add_argument("--load", type=float, default=2.0, help="served: arrival rate / sequential proof rate")
     ap.add_argument("--merkle-channel", default="blake2s", choices=["blake2s", "poseidon252"],

@@ -258,9 +258,13 @@ struct AddQM {
   }
 };
 
-// out_c[i] = S_c[k] - (k + 1) * shift_c at k = coset position of storage row i.
-__global__ void logup_finalize_kernel(const uint4* __restrict__ scan, uint32_t log_n, qm31 shift, Planes out) {
+// out_c[i] = S_c[k] - (k + 1) * shift_c at k = coset position of storage row i,
+// shift = S[n - 1] / n (the claimed sum over n, inv_n = 1/n mod p), read here
+// so that the host need not wait for the sum first.
+__global__ void logup_finalize_kernel(const uint4* __restrict__ scan, uint32_t log_n, uint32_t inv_n, Planes out) {
   const size_t n = (size_t)1 << log_n;
+  const uint4 total = scan[n - 1];
+  const qm31 shift = qm_mul_m31(qm_make(total.x, total.y, total.z, total.w), inv_n);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     uint32_t k = coset_index((uint32_t)i, log_n);
     uint4 s = scan[k];
@@ -411,9 +415,14 @@ size_t logup_scratch_bytes(uint32_t log_n) {
   return 2 * n * sizeof(uint4) + ((temp + 255) & ~(size_t)255);
 }
 
+const void* logup_claimed_sum_ptr(const void* scratch, uint32_t log_n) {
+  return (const uint4*)scratch + 2 * ((size_t)1 << log_n) - 1;
+}
+
 // The interaction trace from the 16 initial- and final-state columns (given
-// as accessors), written to 4 planes, and the claimed sum (host). scratch:
-// logup_scratch_bytes(log_n).
+// as accessors), written to 4 planes, and the claimed sum (host; with
+// claimed_sum null it is left on the device, at logup_claimed_sum_ptr).
+// scratch: logup_scratch_bytes(log_n).
 template <class InitCols, class FinalCols>
 static int interaction_impl(cudaStream_t st, InitCols init, uint32_t c_init, FinalCols fin, uint32_t c_final,
                             uint32_t log_n, const LookupParams& lp, Planes out, void* scratch, qm31* claimed_sum,
@@ -429,17 +438,17 @@ static int interaction_impl(cudaStream_t st, InitCols init, uint32_t c_init, Fin
   GS_CUDA_TRY(cudaGetLastError());
   GS_CUDA_TRY(cub::DeviceScan::InclusiveScan(temp, temp_bytes, (const uint4*)vals, scan, AddQM(), (int)n, st));
   note_launch();
-  uint4 local;
-  uint4* ht = h_pinned ? (uint4*)h_pinned : &local;  // pinned when the caller has a mailbox
-  GS_CUDA_TRY(cudaMemcpyAsync(ht, scan + (n - 1), sizeof(uint4), cudaMemcpyDeviceToHost, st));
-  GS_TRY(stream_sync(st));
-  uint4 total = *ht;
-  qm31 cs = qm_make(total.x, total.y, total.z, total.w);
-  *claimed_sum = cs;
-  qm31 shift = qm_mul_m31(cs, inv((uint32_t)(n % P)));
-  logup_finalize_kernel<<<grid_rows(n, 256), 256, 0, st>>>(scan, log_n, shift, out);
+  logup_finalize_kernel<<<grid_rows(n, 256), 256, 0, st>>>(scan, log_n, inv((uint32_t)(n % P)), out);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
+  if (claimed_sum) {
+    uint4 local;
+    uint4* ht = h_pinned ? (uint4*)h_pinned : &local;  // pinned when the caller has a mailbox
+    GS_CUDA_TRY(cudaMemcpyAsync(ht, scan + (n - 1), sizeof(uint4), cudaMemcpyDeviceToHost, st));
+    GS_TRY(stream_sync(st));
+    const uint4 total = *ht;
+    *claimed_sum = qm_make(total.x, total.y, total.z, total.w);
+  }
   return OK;
 }
 

@@ -43,6 +43,9 @@ int poseidon_interaction_table(cudaStream_t st, const uint32_t* const* d_init, c
                                qm31* claimed_sum);
 int poseidon_trace(cudaStream_t st, uint32_t* cols, uint32_t log_n, uint64_t seed, uint32_t mode);
 size_t logup_scratch_bytes(uint32_t log_n);
+// Device address of the claimed sum (one QM31 as 4 words) inside the scratch
+// of an interaction computed with claimed_sum = null.
+const void* logup_claimed_sum_ptr(const void* scratch, uint32_t log_n);
 int poseidon_interaction(cudaStream_t st, const uint32_t* trace, uint32_t log_n, const LookupParams& lp,
                          uint32_t* out, void* scratch, qm31* claimed_sum, void* h_pinned = nullptr);
 int poseidon_constraints(cudaStream_t st, const uint32_t* trace, const uint32_t* inter, uint32_t eval_log,

@@ -27,13 +27,18 @@ void FiberScheduler::yield_idle() {
   swapcontext(&f->uc, t_main);
 }
 
-int FiberScheduler::wait_stream(cudaStream_t st) {
+int FiberScheduler::wait_device(cudaStream_t st, cudaEvent_t ev) {
   Fiber* f = (Fiber*)t_current;
   if (!f) {
-    GS_CUDA_TRY(cudaStreamSynchronize(st));
+    if (ev) GS_CUDA_TRY(cudaEventSynchronize(ev));
+    else GS_CUDA_TRY(cudaStreamSynchronize(st));
     return OK;
   }
-  GS_CUDA_TRY(cudaEventRecord(f->ev, st));
+  if (!ev) {
+    GS_CUDA_TRY(cudaEventRecord(f->ev, st));
+    ev = f->ev;
+  }
+  f->waiting_on = ev;
   f->state = WAITING;
   swapcontext(&f->uc, t_main);
   if (f->status != OK) {
@@ -62,7 +67,7 @@ void FiberScheduler::run(std::vector<std::function<void()>> bodies, const std::f
   ucontext_t* prev_main = t_main;
   t_sched = this;
   t_main = &main_uc_;
-  set_thread_sync_hook(&FiberScheduler::wait_stream);
+  set_thread_sync_hook(&FiberScheduler::wait_device);
   size_t live = fibers_.size();
   while (live > 0) {
     bool progress = false, waiting = false;
@@ -70,7 +75,7 @@ void FiberScheduler::run(std::vector<std::function<void()>> bodies, const std::f
       Fiber* f = fp.get();
       if (f->state == DONE) continue;
       if (f->state == WAITING) {
-        const cudaError_t q = cudaEventQuery(f->ev);
+        const cudaError_t q = cudaEventQuery(f->waiting_on);
         if (q == cudaErrorNotReady) {
           waiting = true;
           continue;

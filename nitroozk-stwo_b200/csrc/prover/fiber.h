@@ -30,9 +30,10 @@ class FiberScheduler {
            size_t stack_bytes = 1u << 20);
   // Inside a fiber: there is no work now; resume me on the next round.
   static void yield_idle();
-  // The stream_sync hook: inside a fiber, record an event on st and yield
-  // until it has completed; elsewhere, synchronise the stream.
-  static int wait_stream(cudaStream_t st);
+  // The stream_sync / event_sync hook: inside a fiber, yield until `ev` (or,
+  // when ev is null, an event recorded now on st) has completed; elsewhere,
+  // synchronise the stream or the event.
+  static int wait_device(cudaStream_t st, cudaEvent_t ev);
 
  private:
   enum State { READY, WAITING, IDLE, DONE };
@@ -41,7 +42,8 @@ class FiberScheduler {
     std::unique_ptr<char[]> stack;
     std::function<void()> body;
     State state = READY;
-    cudaEvent_t ev = nullptr;
+    cudaEvent_t ev = nullptr;       // the fiber's own event, recorded on its stream
+    cudaEvent_t waiting_on = nullptr;  // the event the fiber waits for
     int status = 0;
   };
   static void entry();

@@ -313,7 +313,12 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
     GS_TRY(poseidon_trace(st, trace, T, req.seed, req.input_mode));
   }
   pv.mark("trace");
-  GS_TRY(pv.commit_evals(trace, air.n_trace_cols(), T));
+  // The trace's extension to the constraint domain (Poseidon2: 2^(T+2), the
+  // largest FFT of the proof) depends on no channel draw: it runs while the
+  // trace root travels to the host, so the device does not wait for the
+  // host's lookup draw there.
+  const uint32_t n_trace = air.n_trace_cols();
+  GS_TRY(pv.commit_evals(trace, n_trace, T, [&](Tree& t) { return pv.extend(t, E, n_trace); }));
   pv.mark("trace_commit");
   if (air.kind == AirKind::Poseidon) {
     auto z = pv.ch.draw_felts(2);
@@ -328,14 +333,21 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
     GS_TRY(pv.A.alloc(logup_scratch_bytes(T), &scratch));
     uint32_t* inter = nullptr;
     GS_TRY(pv.A.alloc_n((size_t)4 << T, &inter));
-    GS_TRY(poseidon_interaction(st, trace, T, air.lookup, inter, scratch, &air.claimed_sum, pv.ctx.h_small));
+    // the claimed sum stays on the device (the finalize kernel reads it) and
+    // comes back through mailbox slot 1 while the interaction is committed
+    GS_TRY(poseidon_interaction(st, trace, T, air.lookup, inter, scratch, nullptr));
+    GS_TRY(pv.ctx.mail_start(1, logup_claimed_sum_ptr(scratch, T), 16));
     pv.mark("interaction");
-    GS_TRY(pv.commit_evals(inter, 4, T));
+    GS_TRY(pv.commit_evals(inter, 4, T, [&](Tree& t) { return pv.extend(t, E, t.n_cols); }));
+    const void* h = nullptr;
+    GS_TRY(pv.ctx.mail_wait(1, &h));
+    const uint32_t* cs = (const uint32_t*)h;
+    air.claimed_sum = qm_make(cs[0], cs[1], cs[2], cs[3]);
     pv.mark("interaction_commit");
   }
   int rc = prove_tail(pv, air, split, proof_bytes, stats, req.out_buf, req.out_cap);
   pv.mark("end");
-  pv.phases.report();
+  pv.phases.report(pv.A.ptrs.size(), pv.A.n_requests);
   return rc;
 }
 

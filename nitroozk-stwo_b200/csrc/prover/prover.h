@@ -26,11 +26,17 @@ struct PcsConfig {
 struct Arena {
   cudaStream_t st = nullptr;
   cudaMemPool_t pool = nullptr;  // the context's pool (default pool if null)
-  std::vector<void*> ptrs;
-  int alloc(size_t bytes, void** out) {
+  std::vector<void*> ptrs;       // pool allocations, freed by release()
+  // Requests below SMALL bytes are carved, 256-byte aligned, from chunks of
+  // the pool (2 MiB, doubling to 16 MiB): a proof makes a few hundred small
+  // allocations (every level of every Merkle tree), and one pool call each
+  // costs host time on every proof.
+  static constexpr size_t SMALL = (size_t)1 << 20;
+  uint8_t* chunk = nullptr;
+  size_t chunk_left = 0, next_chunk = (size_t)2 << 20;
+  int pool_alloc(size_t bytes, void** out) {
     void* p = nullptr;
-    cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, pool, st)
-                         : cudaMallocAsync(&p, bytes ? bytes : 16, st);
+    cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, st) : cudaMallocAsync(&p, bytes, st);
     if (e != cudaSuccess) {
       cudaGetLastError();
       set_error(std::string("device allocation failed: ") + cudaGetErrorString(e));
@@ -40,10 +46,30 @@ struct Arena {
     *out = p;
     return OK;
   }
+  size_t n_requests = 0;
+  int alloc(size_t bytes, void** out) {
+    n_requests++;
+    const size_t need = ((bytes ? bytes : 16) + 255) & ~(size_t)255;
+    if (need >= SMALL) return pool_alloc(need, out);
+    if (need > chunk_left) {
+      void* c = nullptr;
+      GS_TRY(pool_alloc(next_chunk, &c));
+      chunk = (uint8_t*)c;
+      chunk_left = next_chunk;
+      if (next_chunk < ((size_t)16 << 20)) next_chunk *= 2;
+    }
+    *out = chunk;
+    chunk += need;
+    chunk_left -= need;
+    return OK;
+  }
   template <class T> int alloc_n(size_t n, T** out) { return alloc(n * sizeof(T), (void**)out); }
   void release() {
     for (void* p : ptrs) cudaFreeAsync(p, st);
     ptrs.clear();
+    chunk = nullptr;
+    chunk_left = 0;
+    next_chunk = (size_t)2 << 20;
   }
   ~Arena() { release(); }
 };
@@ -58,6 +84,11 @@ struct Tree {
   std::vector<const uint32_t*> coeff_ptrs;    // host copies of the column pointers
   std::vector<uint32_t*> layers;              // layers[L]: 2^L hashes; empty tree: none
   host::Hash root{};
+  // evaluations on the constraint domain (2^ext_log rows per column), filled
+  // column range by column range as the prover finds idle device time
+  uint32_t* ext = nullptr;
+  uint32_t ext_log = 0;
+  uint32_t ext_done = 0;  // columns [0, ext_done) extended
   uint32_t max_log() const { return layers.empty() ? 0 : (uint32_t)layers.size() - 1; }
   const uint32_t* eval_col(uint32_t c) const { return evals + ((size_t)c << eval_log); }
 };

@@ -1,4 +1,5 @@
 #pragma once
+#include <functional>
 // GPU prover (see prover.h): commitment trees, composition polynomial,
 // out-of-domain sampling, DEEP quotients, FRI, proof of work, decommitment.
 #include "prover.h"
@@ -49,7 +50,7 @@ struct PhaseLog {
     ev.push_back(x);
     host.push_back(std::chrono::steady_clock::now());
   }
-  void report() {
+  void report(size_t pool_allocs = 0, size_t requests = 0) {
     if (!on || ev.size() < 2) return;
     cudaEventSynchronize(ev.back());
     std::string js = "{\"phases\": [";
@@ -64,8 +65,9 @@ struct PhaseLog {
     float tot = 0;
     cudaEventElapsedTime(&tot, ev.front(), ev.back());
     double htot = std::chrono::duration<double, std::milli>(host.back() - host.front()).count();
-    char buf[96];
-    snprintf(buf, sizeof buf, "], \"device_ms\": %.3f, \"host_ms\": %.3f}\n", tot, htot);
+    char buf[160];
+    snprintf(buf, sizeof buf, "], \"device_ms\": %.3f, \"host_ms\": %.3f, \"pool_allocs\": %zu, \"requests\": %zu}\n",
+             tot, htot, pool_allocs, requests);
     js += buf;
     fputs(js.c_str(), stderr);
     for (auto x : ev) cudaEventDestroy(x);
@@ -124,14 +126,36 @@ struct Prover {
       GS_TRY(commit_on_layer(st, t.eval_log, nullptr, tab, t.n_cols, t.layers[t.eval_log]));
       GS_TRY(commit_node_layers(st, t.eval_log, t.layers.data(), ctx.tree_counters));
     }
-    uint32_t w[8];
-    GS_TRY(ctx.read_back(t.layers[0], 32, w));
-    t.root = host::hash_from_words(w);
+    // the root comes back through mailbox slot 0; commit_coeffs waits for it
+    return ctx.mail_start(0, t.layers[0], 32);
+  }
+
+  // Extends columns [t.ext_done, c_end) of a committed tree to the constraint
+  // domain 2^E (the composition needs every column there; the work depends
+  // on nothing the channel draws, so it can fill a wait for the host).
+  int extend(Tree& t, uint32_t E, uint32_t c_end) {
+    if (t.eval_log == E || c_end <= t.ext_done) return OK;
+    if (!t.ext) {
+      GS_TRY(A.alloc_n((size_t)t.n_cols << E, &t.ext));
+      t.ext_log = E;
+    }
+    std::vector<const uint32_t*> src(t.coeff_ptrs.begin() + t.ext_done, t.coeff_ptrs.begin() + c_end);
+    std::vector<const uint32_t*> dst;
+    for (uint32_t c = t.ext_done; c < c_end; c++) dst.push_back(t.ext + ((size_t)c << E));
+    const uint32_t* const* stab = nullptr;
+    const uint32_t* const* dtab = nullptr;
+    GS_TRY(table(src, &stab));
+    GS_TRY(table(dst, &dtab));
+    GS_TRY(evaluate_columns(st, stab, t.coeff_log, (uint32_t* const*)dtab, c_end - t.ext_done, E, tw, tw_log));
+    t.ext_done = c_end;
     return OK;
   }
 
-  // TreeBuilder::commit on coefficient columns (given by pointer).
-  int commit_coeffs(const std::vector<const uint32_t*>& coeffs, uint32_t coeff_log) {
+  // TreeBuilder::commit on coefficient columns (given by pointer). `overlap`
+  // enqueues device work that needs neither this root nor anything drawn
+  // after it; it runs while the root is on its way to the host.
+  int commit_coeffs(const std::vector<const uint32_t*>& coeffs, uint32_t coeff_log,
+                    const std::function<int(Tree&)>& overlap = nullptr) {
     Tree t;
     t.n_cols = (uint32_t)coeffs.size();
     t.coeff_log = coeff_log;
@@ -145,6 +169,10 @@ struct Prover {
     GS_TRY(table(dst, &dtab));
     GS_TRY(evaluate_columns(st, t.coeff_tab, coeff_log, (uint32_t* const*)dtab, t.n_cols, t.eval_log, tw, tw_log));
     GS_TRY(merkle(t));
+    if (overlap) GS_TRY(overlap(t));
+    const void* h = nullptr;
+    GS_TRY(ctx.mail_wait(0, &h));
+    t.root = host::hash_from_words((const uint32_t*)h);
     ch.mix_root(t.root);
     trees.push_back(std::move(t));
     return OK;
@@ -152,7 +180,8 @@ struct Prover {
 
   // TreeBuilder::extend_evals + commit: contiguous evaluations on
   // CanonicCoset(log) (bit-reversed) are interpolated into new buffers.
-  int commit_evals(const uint32_t* evals, uint32_t n_cols, uint32_t log) {
+  int commit_evals(const uint32_t* evals, uint32_t n_cols, uint32_t log,
+                   const std::function<int(Tree&)>& overlap = nullptr) {
     uint32_t* coeffs = nullptr;
     GS_TRY(A.alloc_n((size_t)n_cols << log, &coeffs));
     std::vector<const uint32_t*> src, dst;
@@ -165,7 +194,7 @@ struct Prover {
     GS_TRY(table(src, &stab));
     GS_TRY(table(dst, &dtab));
     GS_TRY(interpolate_columns_to(st, stab, (uint32_t* const*)dtab, n_cols, log, itw, tw_log));
-    return commit_coeffs(dst, log);
+    return commit_coeffs(dst, log, overlap);
   }
 
   int commit_empty() {
@@ -185,14 +214,8 @@ struct Prover {
     for (size_t t = 1; t < trees.size(); t++) {
       Tree& tr = trees[t];
       if (tr.eval_log == E) { on_domain[t] = tr.evals; continue; }
-      uint32_t* ext = nullptr;
-      GS_TRY(A.alloc_n((size_t)tr.n_cols << E, &ext));
-      std::vector<const uint32_t*> dst;
-      for (uint32_t c = 0; c < tr.n_cols; c++) dst.push_back(ext + ((size_t)c << E));
-      const uint32_t* const* dtab = nullptr;
-      GS_TRY(table(dst, &dtab));
-      GS_TRY(evaluate_columns(st, tr.coeff_tab, tr.coeff_log, (uint32_t* const*)dtab, tr.n_cols, E, tw, tw_log));
-      on_domain[t] = ext;
+      GS_TRY(extend(tr, E, tr.n_cols));  // the columns not extended earlier
+      on_domain[t] = tr.ext;
     }
     ConstraintParams prm;
     memset(&prm, 0, sizeof(prm));

@@ -25,25 +25,37 @@ static double wait_spin_us() {
   }();
   return us;
 }
-static thread_local int (*g_sync_hook)(cudaStream_t) = nullptr;
-void set_thread_sync_hook(int (*hook)(cudaStream_t)) { g_sync_hook = hook; }
+static thread_local int (*g_sync_hook)(cudaStream_t, cudaEvent_t) = nullptr;
+void set_thread_sync_hook(int (*hook)(cudaStream_t, cudaEvent_t)) { g_sync_hook = hook; }
+
+// Polls ev for the spin time, then blocks on it.
+static int spin_then_wait(cudaEvent_t ev) {
+  const double limit = wait_spin_us();
+  const auto t0 = std::chrono::steady_clock::now();
+  while (limit > 0) {
+    const cudaError_t q = cudaEventQuery(ev);
+    if (q == cudaSuccess) return OK;
+    if (q != cudaErrorNotReady) GS_CUDA_TRY(q);
+    if (std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count() > limit) break;
+  }
+  GS_CUDA_TRY(cudaEventSynchronize(ev));
+  return OK;
+}
 
 int stream_sync(cudaStream_t st) {
-  if (g_sync_hook) return g_sync_hook(st);
+  if (g_sync_hook) return g_sync_hook(st, nullptr);
   if (g_wait_ev) {
     GS_CUDA_TRY(cudaEventRecord(g_wait_ev, st));
-    const double limit = wait_spin_us();
-    const auto t0 = std::chrono::steady_clock::now();
-    while (limit > 0) {
-      const cudaError_t q = cudaEventQuery(g_wait_ev);
-      if (q == cudaSuccess) return OK;
-      if (q != cudaErrorNotReady) GS_CUDA_TRY(q);
-      if (std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count() > limit) break;
-    }
-    GS_CUDA_TRY(cudaEventSynchronize(g_wait_ev));
-  } else {
-    GS_CUDA_TRY(cudaStreamSynchronize(st));
+    return spin_then_wait(g_wait_ev);
   }
+  GS_CUDA_TRY(cudaStreamSynchronize(st));
+  return OK;
+}
+
+int event_sync(cudaEvent_t ev) {
+  if (g_sync_hook) return g_sync_hook(nullptr, ev);
+  if (g_wait_ev) return spin_then_wait(ev);
+  GS_CUDA_TRY(cudaEventSynchronize(ev));
   return OK;
 }
 
@@ -82,7 +94,9 @@ int Context::init(void* user_stream) {
   GS_CUDA_TRY(cudaMalloc((void**)&d_ring, ring_cap));
   small_cap = 4096;
   GS_CUDA_TRY(cudaMalloc((void**)&d_small, small_cap));
-  GS_CUDA_TRY(cudaMallocHost((void**)&h_small, small_cap));
+  GS_CUDA_TRY(cudaMallocHost((void**)&h_small, small_cap + MAIL_SLOTS * MAIL_BYTES));
+  h_mail = h_small + small_cap;
+  for (int i = 0; i < MAIL_SLOTS; i++) GS_CUDA_TRY(cudaEventCreateWithFlags(&mail_ev[i], cudaEventDisableTiming));
   GS_CUDA_TRY(cudaMalloc((void**)&tree_counters, 4 * TREE_COUNTERS));
   GS_CUDA_TRY(cudaMemsetAsync(tree_counters, 0, 4 * TREE_COUNTERS, stream));
   return OK;
@@ -108,6 +122,11 @@ void Context::destroy() {
   if (tree_counters) cudaFree(tree_counters);
   tree_counters = nullptr;
   if (h_small) cudaFreeHost(h_small);
+  for (int i = 0; i < MAIL_SLOTS; i++) {
+    if (mail_ev[i]) cudaEventDestroy(mail_ev[i]);
+    mail_ev[i] = nullptr;
+  }
+  h_mail = nullptr;
   if (h_read) cudaFreeHost(h_read);
   h_read = nullptr;
   read_cap = 0;
@@ -163,6 +182,20 @@ int Context::read_back(const void* d_src, size_t bytes, void* host_dst) {
   GS_CUDA_TRY(cudaMemcpyAsync(h, d_src, bytes, cudaMemcpyDeviceToHost, stream));
   GS_TRY(stream_sync(stream));
   memcpy(host_dst, h, bytes);
+  return OK;
+}
+
+int Context::mail_start(int slot, const void* d_src, size_t bytes) {
+  GS_REQUIRE(slot >= 0 && slot < MAIL_SLOTS && bytes <= MAIL_BYTES, "mailbox read out of range");
+  GS_CUDA_TRY(cudaMemcpyAsync(h_mail + slot * MAIL_BYTES, d_src, bytes, cudaMemcpyDeviceToHost, stream));
+  GS_CUDA_TRY(cudaEventRecord(mail_ev[slot], stream));
+  return OK;
+}
+
+int Context::mail_wait(int slot, const void** host) {
+  GS_REQUIRE(slot >= 0 && slot < MAIL_SLOTS, "mailbox slot out of range");
+  GS_TRY(event_sync(mail_ev[slot]));
+  *host = h_mail + slot * MAIL_BYTES;
   return OK;
 }
 

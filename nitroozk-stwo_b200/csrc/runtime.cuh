@@ -85,10 +85,12 @@ __device__ __forceinline__ pt31 domain_point_bitrev(const DomainTables& t, uint3
 // default 50 µs: most waits are short read-backs, which a sleep and wake-up
 // would lengthen), then sleeps on it.
 int stream_sync(cudaStream_t st);
+// Waits for an event recorded earlier (through the thread's hook if one is set).
+int event_sync(cudaEvent_t ev);
 void set_thread_wait_event(cudaEvent_t ev);
 // Replaces stream_sync's wait on the calling thread (the proof server's
 // fiber scheduler installs one; nullptr restores the default).
-void set_thread_sync_hook(int (*hook)(cudaStream_t));
+void set_thread_sync_hook(int (*hook)(cudaStream_t, cudaEvent_t));
 
 // Number of SMs of the current device (cached).
 int num_sms();
@@ -117,6 +119,16 @@ struct Context {
   int alloc_async(size_t bytes, void** out);
   // Small device-to-host read through the pinned mailbox, then synchronise.
   int read_back(const void* d_src, size_t bytes, void* host_dst);
+  // Reads that the host waits for later: mail_start enqueues a copy of at
+  // most MAIL_BYTES into slot `slot` of a pinned area of its own and records
+  // the slot's event; work enqueued after it runs on meanwhile, and
+  // mail_wait(slot) waits for that event only (not for the stream).
+  static constexpr int MAIL_SLOTS = 4;
+  static constexpr size_t MAIL_BYTES = 256;
+  uint8_t* h_mail = nullptr;
+  cudaEvent_t mail_ev[MAIL_SLOTS] = {nullptr};
+  int mail_start(int slot, const void* d_src, size_t bytes);
+  int mail_wait(int slot, const void** host);
   // growable pinned host buffer for read-backs (decommitment values)
   uint8_t* h_read = nullptr;
   size_t read_cap = 0;
