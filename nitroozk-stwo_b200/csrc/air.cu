@@ -56,7 +56,6 @@ __global__ void wf_trace_kernel(uint32_t* cols, uint32_t log_n, uint32_t n_cols,
   }
 }
 
-__device__ __forceinline__ uint64_t fold64a(uint64_t x) { return (x & P) + (x >> 31); }
 
 // Column access of the constraint kernels: a tree's columns as one
 // contiguous buffer (the prover's layout: column c at base + c * n), or a
@@ -108,7 +107,7 @@ __global__ void __launch_bounds__(256) wf_constraints_kernel(Cols cols, uint32_t
       uint32_t cons = sub(c, add(sqr(a), sqr(b)));
       const uint32_t* p = prm.powers + 4 * (k - 2);
 #pragma unroll
-      for (int q = 0; q < 4; q++) acc[q] = fold64a(acc[q] + (uint64_t)p[q] * cons);
+      for (int q = 0; q < 4; q++) acc[q] = fold64h(acc[q] + (uint64_t)p[q] * cons);
       a = b;
       b = c;
     }
@@ -224,7 +223,7 @@ __device__ __forceinline__ qm31 combine16(const LookupParams& lp, const Cols& co
     // three products (< 2^62 each) and a folded accumulator (< 2^34) fit in 64 bits
     if (i % 3 == 2 || i == 15) {
 #pragma unroll
-      for (int q = 0; q < 4; q++) acc[q] = fold64a(acc[q]);
+      for (int q = 0; q < 4; q++) acc[q] = fold64h(acc[q]);
     }
   }
   qm31 s = qm_make(reduce64(acc[0]), reduce64(acc[1]), reduce64(acc[2]), reduce64(acc[3]));
@@ -307,7 +306,7 @@ __global__ void __launch_bounds__(128) poseidon_constraints_kernel(TraceCols tra
       for (int q = 0; q < 4; q++) acc[q] += (uint64_t)p[q] * c;
       if (i % 3 == 2 || i == last) {
 #pragma unroll
-        for (int q = 0; q < 4; q++) acc[q] = fold64a(acc[q]);
+        for (int q = 0; q < 4; q++) acc[q] = fold64h(acc[q]);
       }
       k++;
     };

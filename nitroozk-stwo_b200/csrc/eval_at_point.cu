@@ -26,7 +26,6 @@ __global__ void eap_weights_kernel(Factors fs, uint32_t s, uint32_t* w /* [j][4]
   w[4 * j + 0] = acc.x.a; w[4 * j + 1] = acc.x.b; w[4 * j + 2] = acc.y.a; w[4 * j + 3] = acc.y.b;
 }
 
-__device__ __forceinline__ uint64_t fold64e(uint64_t x) { return (x & P) + (x >> 31); }
 
 // grid: (chunks per poly, n_polys). Each block handles one chunk of 2^s
 // coefficients of one poly, 2^(s-8) per thread: products of M31 by the QM31
@@ -59,7 +58,7 @@ __global__ void __launch_bounds__(256) eap_chunk_kernel(const uint32_t* const* _
           uint4 wj = __ldg(reinterpret_cast<const uint4*>(w) + jb + e);
           const uint32_t v = vv[e];
           a0 += (uint64_t)wj.x * v; a1 += (uint64_t)wj.y * v; a2 += (uint64_t)wj.z * v; a3 += (uint64_t)wj.w * v;
-          if (++cnt == 3) { a0 = fold64e(a0); a1 = fold64e(a1); a2 = fold64e(a2); a3 = fold64e(a3); cnt = 0; }
+          if (++cnt == 3) { a0 = fold64h(a0); a1 = fold64h(a1); a2 = fold64h(a2); a3 = fold64h(a3); cnt = 0; }
         }
       }
     }
@@ -68,7 +67,7 @@ __global__ void __launch_bounds__(256) eap_chunk_kernel(const uint32_t* const* _
       uint32_t v = __ldg(c + j);
       uint4 wj = __ldg(reinterpret_cast<const uint4*>(w) + j);
       a0 += (uint64_t)wj.x * v; a1 += (uint64_t)wj.y * v; a2 += (uint64_t)wj.z * v; a3 += (uint64_t)wj.w * v;
-      if (++cnt == 3) { a0 = fold64e(a0); a1 = fold64e(a1); a2 = fold64e(a2); a3 = fold64e(a3); cnt = 0; }
+      if (++cnt == 3) { a0 = fold64h(a0); a1 = fold64h(a1); a2 = fold64h(a2); a3 = fold64h(a3); cnt = 0; }
     }
   }
   uint32_t r0 = reduce64(a0), r1 = reduce64(a1), r2 = reduce64(a2), r3 = reduce64(a3);
@@ -145,7 +144,7 @@ __global__ void __launch_bounds__(256) eap_chunk_multi_kernel(const uint32_t* co
 #pragma unroll
         for (int k = 0; k < K; k++)
 #pragma unroll
-          for (int c = 0; c < 4; c++) acc[k][c] = fold64e(acc[k][c]);
+          for (int c = 0; c < 4; c++) acc[k][c] = fold64h(acc[k][c]);
     }
   }
 #pragma unroll

@@ -93,6 +93,15 @@ GS_HD uint32_t mul(uint32_t a, uint32_t b) {
   return umin32(r, r - P);
 #endif
 }
+// Fold of a 64-bit lazy accumulator of products to below 2^34, congruent
+// mod p but not reduced: x = hi * 2^32 + lo and 2^32 = 2 (mod p), so x = 2 hi
+// + lo (mod p), one wide multiply-add on the device. Three more products of
+// two values below 2^31 fit after it (3 * 2^62 + 2^34 < 2^64).
+__device__ __forceinline__ uint64_t fold64h(uint64_t x) {
+  uint64_t r;
+  asm("mad.wide.u32 %0, %1, 2, %2;" : "=l"(r) : "r"((uint32_t)(x >> 32)), "l"(x & 0xffffffffull));
+  return r;
+}
 // Reduce any 64-bit value (used for lazily accumulated sums of products).
 GS_HD uint32_t reduce64(uint64_t v) {
   // v = h * 2^62 + m * 2^31 + l  ->  h + m + l (mod p), each part < 2^31

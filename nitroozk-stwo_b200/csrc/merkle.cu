@@ -178,19 +178,21 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(1024) merkle_tail_ke
 // one launch per level before.
 struct TreePtrs { uint32_t* p[TREE_MAX_LOG + 1]; };
 
-__global__ void __launch_bounds__(256, 4) merkle_tree_kernel(uint32_t top, TreePtrs layers, uint32_t* counters,
-                                                             uint32_t* state, uint32_t* root_copy, uint32_t* felt) {
-  __shared__ uint4 buf[2][512];
+template <int U>
+__global__ void __launch_bounds__(1 << (U - 1), 4)
+    merkle_tree_kernel(uint32_t top, TreePtrs layers, uint32_t* counters, uint32_t* state, uint32_t* root_copy,
+                       uint32_t* felt) {
+  __shared__ uint4 buf[2][1 << U];
   __shared__ uint32_t last;
   const uint32_t tid = threadIdx.x;
   uint32_t in_log = top;
   uint32_t u = blockIdx.x;
   uint32_t cnt_off = 0;
   for (;;) {
-    const uint32_t out_log = in_log > 9 ? in_log - 9 : 0;
+    const uint32_t out_log = in_log > U ? in_log - U : 0;
     int cur = 0;
     for (int L = (int)in_log - 1; L >= (int)out_log; L--) {
-      const uint32_t n = 1u << (L - (int)out_log);  // this unit's nodes on level L (<= 256)
+      const uint32_t n = 1u << (L - (int)out_log);  // this unit's nodes on level L (<= 2^(U-1))
       if (tid < n) {
         const size_t node = ((size_t)u << (L - (int)out_log)) + tid;
         uint4 c[4];
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(256, 4) merkle_tree_kernel(uint32_t top, TreeP
       cur ^= 1;
     }
     if (out_log == 0) break;  // this block wrote the root
-    const uint32_t group_log = out_log > 9 ? 9u : out_log;
+    const uint32_t group_log = out_log > U ? (uint32_t)U : out_log;
     const uint32_t next_u = u >> group_log;
     if (tid == 0) {
       __threadfence();  // this unit's root (written by thread 0) before the ticket
@@ -237,8 +239,8 @@ int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layer
   return commit_node_layers_ch(st, top_log, layers, d_counters, nullptr, nullptr, nullptr);
 }
 
-// Stage-1 units of a tree of top_log <= TREE_MAX_LOG use at most 2^9 + 1
-// counters (TREE_COUNTERS).
+// A tree of top_log <= TREE_MAX_LOG uses at most 2^(27 - 2U) + 2^(27 - 3U) + 1
+// ticket counters for units of 2^U children (checked against TREE_COUNTERS).
 int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters,
                           uint32_t* d_state, uint32_t* d_root_copy, uint32_t* d_felt) {
   GS_REQUIRE(top_log <= 30, "layer log size out of range");
@@ -262,8 +264,21 @@ int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* la
       GS_REQUIRE(((uintptr_t)layers[k] & 15) == 0, "hash buffers must be 16-byte aligned");
       tp.p[k] = layers[k];
     }
-    const uint32_t blocks = top > 9 ? 1u << (top - 9) : 1u;
-    merkle_tree_kernel<<<blocks, 256, 0, st>>>(top, tp, d_counters, d_state, d_root_copy, d_felt);
+    // units of 2^9 children (256 threads): 2^8 (440 -> 464 us of tree
+    // kernels per Poseidon2 2^18 proof), 2^7 (854 us) and 2^10 (449 us) were
+    // slower
+    constexpr int unit = 9;
+    {  // ticket counters the continuation stages use
+      size_t need = 0;
+      for (uint32_t in = top; in > (uint32_t)unit;) {
+        const uint32_t out = in - unit, g = out > (uint32_t)unit ? (uint32_t)unit : out;
+        need += (size_t)1 << (out - g);
+        in = out;
+      }
+      GS_REQUIRE(need <= TREE_COUNTERS, "tree too large for the ticket counters");
+    }
+    const uint32_t blocks = top > (uint32_t)unit ? 1u << (top - unit) : 1u;
+    merkle_tree_kernel<unit><<<blocks, 1u << (unit - 1), 0, st>>>(top, tp, d_counters, d_state, d_root_copy, d_felt);
     note_launch();
     GS_CUDA_TRY(cudaGetLastError());
     return OK;

@@ -22,7 +22,6 @@
 namespace gs {
 
 // ------------------------------------------------------------ numerators
-__device__ __forceinline__ uint64_t fold64(uint64_t x) { return (x & P) + (x >> 31); }
 
 // The batch's entries are staged in shared memory once per block. VEC: four
 // consecutive rows per thread, each column read as one 16-byte load (all
@@ -76,7 +75,7 @@ __global__ void __launch_bounds__(256) accumulate_numerators_kernel(const NumEnt
           acc_term(acc[r], E[k + j], v[j][r]);
           if (j == 2 || j == 5)
 #pragma unroll
-            for (int q = 0; q < 4; q++) acc[r][q] = fold64(acc[r][q]);
+            for (int q = 0; q < 4; q++) acc[r][q] = fold64h(acc[r][q]);
         }
       }
     }
@@ -90,7 +89,7 @@ __global__ void __launch_bounds__(256) accumulate_numerators_kernel(const NumEnt
 #pragma unroll
         for (int r = 0; r < R; r++)
 #pragma unroll
-          for (int q = 0; q < 4; q++) acc[r][q] = fold64(acc[r][q]);
+          for (int q = 0; q < 4; q++) acc[r][q] = fold64h(acc[r][q]);
       }
     }
     uint32_t o[4][R];
@@ -177,7 +176,7 @@ __global__ void __launch_bounds__(256, 4) accumulate_numerators_split_kernel(con
           acc_term(acc[rr], E[k + EG * j], v[rr]);
           if (j == 2 || j == 5)
 #pragma unroll
-            for (int q = 0; q < 4; q++) acc[rr][q] = fold64(acc[rr][q]);
+            for (int q = 0; q < 4; q++) acc[rr][q] = fold64h(acc[rr][q]);
         }
       }
     }
@@ -192,7 +191,7 @@ __global__ void __launch_bounds__(256, 4) accumulate_numerators_split_kernel(con
 #pragma unroll
         for (int rr = 0; rr < 4; rr++)
 #pragma unroll
-          for (int q = 0; q < 4; q++) acc[rr][q] = fold64(acc[rr][q]);
+          for (int q = 0; q < 4; q++) acc[rr][q] = fold64h(acc[rr][q]);
       }
     }
     if (EG == 1) {  // this warp holds its rows' whole sums
