@@ -269,8 +269,28 @@ int validate_request(const ProveRequest& r) {
   return OK;
 }
 
+// The context's proof streams for one proof: entered after the caller's
+// stream, left (side work joined, the caller's stream ordered after) when
+// the proof returns on any path. Declared before the Prover, so the Prover's
+// buffers are released on the work stream first.
+struct ProofStreams {
+  Context& c;
+  bool on = false;
+  explicit ProofStreams(Context& x) : c(x) {}
+  int begin() {
+    GS_TRY(c.begin_proof());
+    on = true;
+    return OK;
+  }
+  ~ProofStreams() {
+    if (on) c.end_proof();
+  }
+};
+
 int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_bytes, ProveStats* stats) {
   PcsConfig cfg = req.cfg;
+  ProofStreams streams(ctx);
+  GS_TRY(streams.begin());
   Prover pv(ctx, cfg);
   GS_REQUIRE(req.merkle_channel <= 1, "merkle channel must be 0 (Blake2s) or 1 (Poseidon252)");
   pv.ch.p252 = req.merkle_channel == 1;
@@ -314,11 +334,13 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
   }
   pv.mark("trace");
   // The trace's extension to the constraint domain (Poseidon2: 2^(T+2), the
-  // largest FFT of the proof) depends on no channel draw: it runs while the
-  // trace root travels to the host, so the device does not wait for the
-  // host's lookup draw there.
+  // largest FFT of the proof) depends on no channel draw: it is enqueued on
+  // the low-priority side stream as soon as the trace is committed, and its
+  // blocks fill the SMs that the latency-bound work up to the composition
+  // (tree-kernel tails, the interaction phase, the host's draws) leaves
+  // idle; the composition joins it.
   const uint32_t n_trace = air.n_trace_cols();
-  GS_TRY(pv.commit_evals(trace, n_trace, T, [&](Tree& t) { return pv.extend(t, E, n_trace); }));
+  GS_TRY(pv.commit_evals(trace, n_trace, T, [&](Tree& t) { return pv.extend(t, E, n_trace, true); }));
   pv.mark("trace_commit");
   if (air.kind == AirKind::Poseidon) {
     auto z = pv.ch.draw_felts(2);

@@ -132,8 +132,10 @@ struct Prover {
 
   // Extends columns [t.ext_done, c_end) of a committed tree to the constraint
   // domain 2^E (the composition needs every column there; the work depends
-  // on nothing the channel draws, so it can fill a wait for the host).
-  int extend(Tree& t, uint32_t E, uint32_t c_end) {
+  // on nothing the channel draws, so it can fill a wait for the host). With
+  // on_side it runs on the context's low-priority side stream, joined
+  // before the composition reads it.
+  int extend(Tree& t, uint32_t E, uint32_t c_end, bool on_side = false) {
     if (t.eval_log == E || c_end <= t.ext_done) return OK;
     if (!t.ext) {
       GS_TRY(A.alloc_n((size_t)t.n_cols << E, &t.ext));
@@ -146,7 +148,12 @@ struct Prover {
     const uint32_t* const* dtab = nullptr;
     GS_TRY(table(src, &stab));
     GS_TRY(table(dst, &dtab));
-    GS_TRY(evaluate_columns(st, stab, t.coeff_log, (uint32_t* const*)dtab, c_end - t.ext_done, E, tw, tw_log));
+    cudaStream_t s = st;
+    if (on_side && ctx.side) {
+      GS_TRY(ctx.fork_side());
+      s = ctx.side;
+    }
+    GS_TRY(evaluate_columns(s, stab, t.coeff_log, (uint32_t* const*)dtab, c_end - t.ext_done, E, tw, tw_log));
     t.ext_done = c_end;
     return OK;
   }
@@ -217,6 +224,7 @@ struct Prover {
       GS_TRY(extend(tr, E, tr.n_cols));  // the columns not extended earlier
       on_domain[t] = tr.ext;
     }
+    GS_TRY(ctx.join_side());
     ConstraintParams prm;
     memset(&prm, 0, sizeof(prm));
     const uint32_t nc = air.n_constraints();

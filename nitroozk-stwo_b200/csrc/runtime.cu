@@ -104,6 +104,17 @@ int Context::init(void* user_stream) {
 
 void Context::destroy() {
   if (stream) cudaStreamSynchronize(stream);
+  if (work) {
+    cudaStreamSynchronize(work);
+    cudaStreamSynchronize(side);
+    cudaStreamDestroy(work);
+    cudaStreamDestroy(side);
+    cudaEventDestroy(ev_enter);
+    cudaEventDestroy(ev_fork);
+    cudaEventDestroy(ev_join);
+    work = side = nullptr;
+    ev_enter = ev_fork = ev_join = nullptr;
+  }
   if (scratch) {
     cudaFreeAsync(scratch, stream);
     cudaStreamSynchronize(stream);
@@ -137,13 +148,67 @@ void Context::destroy() {
   stream = nullptr;
 }
 
+int Context::begin_proof() {
+  if (!work) {
+    int least = 0, greatest = 0;
+    GS_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    GS_CUDA_TRY(cudaStreamCreateWithPriority(&work, cudaStreamNonBlocking, greatest));
+    GS_CUDA_TRY(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, least));
+    GS_CUDA_TRY(cudaEventCreateWithFlags(&ev_enter, cudaEventDisableTiming));
+    GS_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    GS_CUDA_TRY(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+  }
+  GS_REQUIRE(!in_proof, "proof already in progress on this context");
+  GS_CUDA_TRY(cudaEventRecord(ev_enter, stream));
+  GS_CUDA_TRY(cudaStreamWaitEvent(work, ev_enter, 0));
+  caller = stream;
+  stream = work;
+  in_proof = true;
+  return OK;
+}
+
+int Context::end_proof() {
+  if (!in_proof) return OK;
+  // the caller's stream is restored on every path, also when a wait fails
+  int rc = OK;
+  if (side_pending) rc = join_side();
+  if (rc == OK && cudaEventRecord(ev_enter, work) == cudaSuccess &&
+      cudaStreamWaitEvent(caller, ev_enter, 0) == cudaSuccess) {
+  } else {
+    cudaStreamSynchronize(side);
+    cudaStreamSynchronize(work);
+  }
+  stream = caller;
+  caller = nullptr;
+  in_proof = false;
+  return rc;
+}
+
+int Context::fork_side() {
+  GS_REQUIRE(side != nullptr, "side stream outside a proof");
+  GS_CUDA_TRY(cudaEventRecord(ev_fork, stream));
+  GS_CUDA_TRY(cudaStreamWaitEvent(side, ev_fork, 0));
+  side_pending = true;
+  return OK;
+}
+
+int Context::join_side() {
+  if (!side_pending) return OK;
+  GS_CUDA_TRY(cudaEventRecord(ev_join, side));
+  GS_CUDA_TRY(cudaStreamWaitEvent(stream, ev_join, 0));
+  side_pending = false;
+  return OK;
+}
+
 int Context::stage_bytes(const void* host, size_t len, const void** out) {
   size_t bytes = (len + 255) & ~(size_t)255;
   GS_REQUIRE(bytes <= ring_cap, "staged argument block too large");
   if (ring_off + bytes > ring_cap) {
-    // Wrap: earlier copies out of the pinned ring must have completed before
+    // Wrap: earlier copies out of the pinned ring, and the kernels reading
+    // their device copies (on either stream), must have completed before
     // their slots are rewritten.
     GS_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (side_pending) GS_CUDA_TRY(cudaStreamSynchronize(side));
     ring_off = 0;
   }
   memcpy(h_ring + ring_off, host, len);

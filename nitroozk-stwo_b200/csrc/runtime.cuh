@@ -101,6 +101,20 @@ struct Context {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int device = 0;
+  // A proof runs on `work`, a stream of the device's greatest priority
+  // (ordered after the caller's stream on entry); `side`, of the lowest
+  // priority, carries work that the protocol's next steps do not need yet,
+  // so its blocks take only the SMs that latency-bound work on `work`
+  // leaves idle. Both are created on first use (begin_proof).
+  cudaStream_t work = nullptr, side = nullptr;
+  cudaStream_t caller = nullptr;  // may be the legacy default stream (null)
+  bool in_proof = false;
+  cudaEvent_t ev_enter = nullptr, ev_fork = nullptr, ev_join = nullptr;
+  bool side_pending = false;
+  int begin_proof();  // stream := work, after the caller's stream
+  int end_proof();    // the caller's stream after work; stream := caller
+  int fork_side();    // side waits for the work enqueued on `stream` so far
+  int join_side();    // `stream` waits for the side work enqueued so far
   // pointer-table staging: pinned host ring -> device ring, stream ordered
   uint8_t* h_ring = nullptr;
   uint8_t* d_ring = nullptr;

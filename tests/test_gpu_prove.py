@@ -110,3 +110,26 @@ def test_wide_fibonacci_poseidon252_config_size(G):
 def test_poseidon_poseidon252_2e14(G):
     assert G.prove_poseidon(14, seed=3, input_mode=1, merkle_channel="poseidon252") == \
         O.prove("poseidon", 14, seed=3, input_mode=1, merkle_channel="poseidon252")
+
+
+def test_context_stream_restored_after_proof(G):
+    """A proof runs on the context's own prioritised streams and hands the
+    caller's stream back when it returns, also when that stream is the legacy
+    default stream (a null handle): work the caller then enqueues on its
+    stream and passes to the library stays ordered. Pattern: a proof (Poseidon2,
+    which uses the side stream), then torch clones of an evaluation consumed
+    at once by an in-place interpolation on the same context."""
+    import torch
+    from gpustark.backend import GpuBackend as B, to_device
+    assert G.prove_poseidon(6, seed=3, input_mode=G.INPUT_SEEDED)
+    rng = np.random.default_rng(77)
+    log, blowup = 17, 2
+    tw = B.precompute_twiddles(log + blowup - 1)
+    coeffs = [to_device(rng.integers(0, O.P, 1 << log, dtype=np.int64).astype(np.uint32)) for _ in range(2)]
+    for _ in range(3):
+        ev = B.evaluate_polynomials(coeffs, log + blowup, tw)
+        back = [e.clone() for e in ev]
+        B.interpolate_columns(back, log + blowup, tw)
+        torch.cuda.synchronize()
+        for b, c in zip(back, coeffs):
+            assert torch.equal(b[: c.numel()], c) and not torch.any(b[c.numel():])
