@@ -166,7 +166,7 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(1024) merkle_tail_ke
 }
 
 // Every node layer of a tree in one launch. A unit is a 512-child subtree:
-// a block of 256 threads hashes its 256 parents, then each level above
+// a block of 128 threads hashes its 256 parents, then each level above
 // through shared memory, down to the unit's root (9 levels), writing every
 // level to its global layer. Stage 1 has one block per unit of the input
 // layer. The block that finishes last among the units under one next-stage
@@ -177,9 +177,14 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(1024) merkle_tail_ke
 // optional channel step. Critical path: one compression per level, against
 // one launch per level before.
 struct TreePtrs { uint32_t* p[TREE_MAX_LOG + 1]; };
+// Threads per 512-child unit: 128, each hashing two nodes of the unit's first
+// level (452 us of tree kernels per Poseidon2 2^18 proof, against 464 us
+// with 256 threads and 568 us with 64): half the warps wait at the barriers
+// of the upper levels, and twice as many units fit on an SM.
+constexpr int TREE_THREADS = 128;
 
-template <int U>
-__global__ void __launch_bounds__(1 << (U - 1), 4)
+template <int U, int TH>
+__global__ void __launch_bounds__(TH, TH >= 256 ? 4 : 8)
     merkle_tree_kernel(uint32_t top, TreePtrs layers, uint32_t* counters, uint32_t* state, uint32_t* root_copy,
                        uint32_t* felt) {
   __shared__ uint4 buf[2][1 << U];
@@ -193,8 +198,8 @@ __global__ void __launch_bounds__(1 << (U - 1), 4)
     int cur = 0;
     for (int L = (int)in_log - 1; L >= (int)out_log; L--) {
       const uint32_t n = 1u << (L - (int)out_log);  // this unit's nodes on level L (<= 2^(U-1))
-      if (tid < n) {
-        const size_t node = ((size_t)u << (L - (int)out_log)) + tid;
+      for (uint32_t i = tid; i < n; i += TH) {
+        const size_t node = ((size_t)u << (L - (int)out_log)) + i;
         uint4 c[4];
         if (L == (int)in_log - 1) {
           // written before the launch, or by other blocks of this launch:
@@ -204,13 +209,13 @@ __global__ void __launch_bounds__(1 << (U - 1), 4)
           for (int q = 0; q < 4; q++) c[q] = __ldcg(src + q);
         } else {
 #pragma unroll
-          for (int q = 0; q < 4; q++) c[q] = buf[cur ^ 1][4 * tid + q];
+          for (int q = 0; q < 4; q++) c[q] = buf[cur ^ 1][4 * i + q];
         }
         uint32_t h[8];
         hash_children16(c, h);
         tail_store_hash(layers.p[L], node, h);
-        buf[cur][2 * tid] = make_uint4(h[0], h[1], h[2], h[3]);
-        buf[cur][2 * tid + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+        buf[cur][2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
+        buf[cur][2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
       }
       __syncthreads();
       cur ^= 1;
@@ -278,7 +283,8 @@ int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* la
       GS_REQUIRE(need <= TREE_COUNTERS, "tree too large for the ticket counters");
     }
     const uint32_t blocks = top > (uint32_t)unit ? 1u << (top - unit) : 1u;
-    merkle_tree_kernel<unit><<<blocks, 1u << (unit - 1), 0, st>>>(top, tp, d_counters, d_state, d_root_copy, d_felt);
+    merkle_tree_kernel<unit, TREE_THREADS><<<blocks, TREE_THREADS, 0, st>>>(top, tp, d_counters, d_state,
+                                                                           d_root_copy, d_felt);
     note_launch();
     GS_CUDA_TRY(cudaGetLastError());
     return OK;
