@@ -335,12 +335,13 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
   pv.mark("trace");
   // The trace's extension to the constraint domain (Poseidon2: 2^(T+2), the
   // largest FFT of the proof) depends on no channel draw: it is enqueued on
-  // the low-priority side stream as soon as the trace is committed, and its
-  // blocks fill the SMs that the latency-bound work up to the composition
-  // (tree-kernel tails, the interaction phase, the host's draws) leaves
-  // idle; the composition joins it.
+  // the low-priority side stream as soon as the trace's coefficients exist,
+  // and its blocks fill the SMs that the work up to the composition leaves
+  // idle (the tails of the trace's own evaluation and hashing, the tree
+  // kernel's upper levels, the interaction phase, the host's draws); the
+  // composition joins it.
   const uint32_t n_trace = air.n_trace_cols();
-  GS_TRY(pv.commit_evals(trace, n_trace, T, [&](Tree& t) { return pv.extend(t, E, n_trace, true); }));
+  GS_TRY(pv.commit_evals(trace, n_trace, T, nullptr, [&](Tree& t) { return pv.extend(t, E, n_trace, true); }));
   pv.mark("trace_commit");
   if (air.kind == AirKind::Poseidon) {
     auto z = pv.ch.draw_felts(2);

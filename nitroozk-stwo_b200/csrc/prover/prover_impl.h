@@ -161,13 +161,18 @@ struct Prover {
   // TreeBuilder::commit on coefficient columns (given by pointer). `overlap`
   // enqueues device work that needs neither this root nor anything drawn
   // after it; it runs while the root is on its way to the host.
+  // `early` runs as soon as the coefficients are known, before the tree's
+  // own evaluation and hashing are enqueued (for side-stream work that can
+  // then fill the gaps of all of them).
   int commit_coeffs(const std::vector<const uint32_t*>& coeffs, uint32_t coeff_log,
-                    const std::function<int(Tree&)>& overlap = nullptr) {
+                    const std::function<int(Tree&)>& overlap = nullptr,
+                    const std::function<int(Tree&)>& early = nullptr) {
     Tree t;
     t.n_cols = (uint32_t)coeffs.size();
     t.coeff_log = coeff_log;
     t.eval_log = coeff_log + cfg.log_blowup;
     t.coeff_ptrs = coeffs;
+    if (early) GS_TRY(early(t));
     GS_TRY(table(coeffs, &t.coeff_tab));
     GS_TRY(A.alloc_n((size_t)t.n_cols << t.eval_log, &t.evals));
     std::vector<const uint32_t*> dst;
@@ -188,7 +193,8 @@ struct Prover {
   // TreeBuilder::extend_evals + commit: contiguous evaluations on
   // CanonicCoset(log) (bit-reversed) are interpolated into new buffers.
   int commit_evals(const uint32_t* evals, uint32_t n_cols, uint32_t log,
-                   const std::function<int(Tree&)>& overlap = nullptr) {
+                   const std::function<int(Tree&)>& overlap = nullptr,
+                   const std::function<int(Tree&)>& early = nullptr) {
     uint32_t* coeffs = nullptr;
     GS_TRY(A.alloc_n((size_t)n_cols << log, &coeffs));
     std::vector<const uint32_t*> src, dst;
@@ -201,7 +207,7 @@ struct Prover {
     GS_TRY(table(src, &stab));
     GS_TRY(table(dst, &dtab));
     GS_TRY(interpolate_columns_to(st, stab, (uint32_t* const*)dtab, n_cols, log, itw, tw_log));
-    return commit_coeffs(dst, log, overlap);
+    return commit_coeffs(dst, log, overlap, early);
   }
 
   int commit_empty() {
