@@ -361,7 +361,7 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
     GS_TRY(poseidon_interaction(st, trace, T, air.lookup, inter, scratch, nullptr));
     GS_TRY(pv.ctx.mail_start(1, logup_claimed_sum_ptr(scratch, T), 16));
     pv.mark("interaction");
-    GS_TRY(pv.commit_evals(inter, 4, T, [&](Tree& t) { return pv.extend(t, E, t.n_cols); }));
+    GS_TRY(pv.commit_evals(inter, 4, T, nullptr, [&](Tree& t) { return pv.extend(t, E, t.n_cols, true); }));
     const void* h = nullptr;
     GS_TRY(pv.ctx.mail_wait(1, &h));
     const uint32_t* cs = (const uint32_t*)h;

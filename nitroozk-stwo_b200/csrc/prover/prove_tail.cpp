@@ -68,14 +68,29 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     void* scratch = nullptr;
     GS_TRY(pv.A.alloc_n(4 * n_vals + 4, &d_vals));
     GS_TRY(pv.A.alloc(scratch_bytes + 16, &scratch));
-    for (auto& r : reqs) {
+    // the largest evaluation (the trace's) runs on the side stream with a
+    // scratch of its own, next to the small ones on the work stream
+    size_t big = 0;
+    auto cost = [&](const SampleReq& r) { return (size_t)pv.trees[r.t].n_cols << pv.trees[r.t].coeff_log; };
+    for (size_t i = 1; i < reqs.size(); i++)
+      if (cost(reqs[i]) > cost(reqs[big])) big = i;
+    const bool split_streams = reqs.size() > 1 && pv.ctx.side != nullptr;
+    void* scratch_big = scratch;
+    if (split_streams) {
+      GS_TRY(pv.A.alloc(scratch_bytes + 16, &scratch_big));
+      GS_TRY(pv.ctx.fork_side());
+    }
+    for (size_t i = 0; i < reqs.size(); i++) {
+      const SampleReq& r = reqs[i];
       Tree& tr = pv.trees[r.t];
       bool vec = true;
       for (auto* c : tr.coeff_ptrs) vec = vec && ((uintptr_t)c & 15) == 0;
-      GS_TRY(batch_eval_at_point(st, tr.coeff_tab, tr.n_cols, tr.coeff_log,
+      const bool side = split_streams && i == big;
+      GS_TRY(batch_eval_at_point(side ? pv.ctx.side : st, tr.coeff_tab, tr.n_cols, tr.coeff_log,
                                  host::ptq_rep_double(r.p, lifting - tr.eval_log), d_vals + 4 * r.slot,
-                                 (uint32_t*)scratch, 12, vec));
+                                 (uint32_t*)(side ? scratch_big : scratch), 12, vec));
     }
+    GS_TRY(pv.ctx.join_side());
     std::vector<uint32_t> h(4 * n_vals);
     GS_TRY(pv.ctx.read_back(d_vals, h.size() * 4, h.data()));
     for (auto& r : reqs) {
