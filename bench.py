@@ -897,13 +897,74 @@ def run_reference(args, world, rank):
     }
 
 
+def proof_timeline(air, log_n, reps):
+    """Device timeline of `reps` proofs after warm-up, from a CUPTI activity trace
+    (torch.profiler, CUDA activities only): per proof the span from the first to
+    the last device event, the time at least one kernel or copy runs (the union
+    of their intervals: kernels of the work and side streams overlap), and the
+    idle time split by what borders each gap (kernel or copy on either side)."""
+    import json as js
+    import tempfile
+    import torch
+    from torch.profiler import profile, ProfilerActivity
+    from gpustark import prove as G
+    fn = ((lambda: G.prove_poseidon(log_n, seed=7, input_mode=G.INPUT_SEEDED)) if air == "poseidon" else
+          (lambda: G.prove_wide_fibonacci(log_n, 100, seed=7, input_mode=G.INPUT_SEEDED)))
+    for _ in range(4):
+        fn()
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _ in range(reps):
+            fn()
+            torch.cuda.synchronize()
+    path = os.path.join(tempfile.mkdtemp(), "trace.json")
+    prof.export_chrome_trace(path)
+    ev = [e for e in js.load(open(path))["traceEvents"]
+          if e.get("ph") == "X" and e.get("cat") in ("kernel", "gpu_memcpy", "gpu_memset")]
+    ev.sort(key=lambda e: e["ts"])
+    # split into proofs at the host-side gaps between them (the largest reps - 1 gaps)
+    ends, end = [], ev[0]["ts"]
+    for i, e in enumerate(ev):
+        if i and e["ts"] > end:
+            ends.append((e["ts"] - end, i))
+        end = max(end, e["ts"] + e["dur"])
+    cuts = sorted(i for _, i in sorted(ends, reverse=True)[:reps - 1])
+    rows, lo = [], 0
+    for hi in cuts + [len(ev)]:
+        part = ev[lo:hi]
+        lo = hi
+        t0 = part[0]["ts"]
+        end, busy, prev = t0, 0.0, None
+        idle = {"kernel->kernel": 0.0, "kernel->copy": 0.0, "copy->kernel": 0.0, "copy->copy": 0.0}
+        for e in part:
+            s, d = e["ts"], e["dur"]
+            if s > end and prev is not None:
+                k = ("kernel" if prev["cat"] == "kernel" else "copy") + "->" + ("kernel" if e["cat"] == "kernel" else "copy")
+                idle[k] += s - end
+            busy += max(0.0, s + d - max(s, end))
+            if s + d > end:
+                end, prev = s + d, e
+        rows.append((end - t0, busy, idle, sum(1 for e in part if e["cat"] == "kernel")))
+    n = len(rows)
+    span = sum(r[0] for r in rows) / n
+    busy = sum(r[1] for r in rows) / n
+    idle = {k: round(sum(r[2][k] for r in rows) / n, 1) for k in rows[0][2]}
+    print(js.dumps({"air": air, "log_n": log_n, "proofs": n, "span_us": round(span, 1), "busy_us": round(busy, 1),
+                    "busy_frac": round(busy / span, 3), "idle_us": idle,
+                    "kernels_per_proof": round(sum(r[3] for r in rows) / n, 1)}))
+
+
 def run_case(args):
     """One op on a small case, for ncu captures: `--case fft:26`, `--case lde:18:162:2` (extension
     of 162 columns from 2^18 to 2^20), `--case merkle:20:64`, `--case fold:22`, `--case p252:18:8`
-    (Poseidon252 Merkle leaves of 8 columns x 2^18 rows, then the node layer above them)."""
+    (Poseidon252 Merkle leaves of 8 columns x 2^18 rows, then the node layer above them);
+    `--case timeline:poseidon:18` prints the device timeline of proofs (busy and idle time)."""
     import torch
     from gpustark.backend import GpuBackend as B, to_device, Context
     kind, *params = args.case.split(":")
+    if kind == "timeline":
+        proof_timeline(params[0], int(params[1]), max(2, args.steps))
+        return
     rng = np.random.default_rng(7)
     ctx = Context(torch.cuda.current_stream())
     if kind == "fft":
