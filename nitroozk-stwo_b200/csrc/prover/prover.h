@@ -26,7 +26,10 @@ struct PcsConfig {
 struct Arena {
   cudaStream_t st = nullptr;
   cudaMemPool_t pool = nullptr;  // the context's pool (default pool if null)
-  std::vector<void*> ptrs;       // pool allocations, freed by release()
+  std::vector<void*> ptrs;       // pool allocations, freed (or kept) by release()
+  std::vector<size_t> sizes;     // their sizes
+  // previous allocations of the same context to take back first (null: none)
+  std::vector<std::pair<size_t, void*>>* spare = nullptr;
   // Requests below SMALL bytes are carved, 256-byte aligned, from chunks of
   // the pool (2 MiB, doubling to 16 MiB): a proof makes a few hundred small
   // allocations (every level of every Merkle tree), and one pool call each
@@ -35,14 +38,31 @@ struct Arena {
   uint8_t* chunk = nullptr;
   size_t chunk_left = 0, next_chunk = (size_t)2 << 20;
   int pool_alloc(size_t bytes, void** out) {
+    if (spare)
+      for (size_t i = 0; i < spare->size(); i++)
+        if ((*spare)[i].first == bytes) {
+          *out = (*spare)[i].second;
+          (*spare)[i] = spare->back();
+          spare->pop_back();
+          ptrs.push_back(*out);
+          sizes.push_back(bytes);
+          return OK;
+        }
     void* p = nullptr;
     cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, st) : cudaMallocAsync(&p, bytes, st);
+    if (e != cudaSuccess && spare && !spare->empty()) {  // give the kept buffers back and retry
+      cudaGetLastError();
+      for (auto& b : *spare) cudaFreeAsync(b.second, st);
+      spare->clear();
+      e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, st) : cudaMallocAsync(&p, bytes, st);
+    }
     if (e != cudaSuccess) {
       cudaGetLastError();
       set_error(std::string("device allocation failed: ") + cudaGetErrorString(e));
       return ERR_OOM;
     }
     ptrs.push_back(p);
+    sizes.push_back(bytes);
     *out = p;
     return OK;
   }
@@ -64,9 +84,18 @@ struct Arena {
     return OK;
   }
   template <class T> int alloc_n(size_t n, T** out) { return alloc(n * sizeof(T), (void**)out); }
+  // With a spare list: the spare buffers not taken back are freed and this
+  // arena's allocations become the spare list; else every allocation is freed.
   void release() {
-    for (void* p : ptrs) cudaFreeAsync(p, st);
+    if (spare) {
+      for (auto& b : *spare) cudaFreeAsync(b.second, st);
+      spare->clear();
+      for (size_t i = 0; i < ptrs.size(); i++) spare->push_back({sizes[i], ptrs[i]});
+    } else {
+      for (void* p : ptrs) cudaFreeAsync(p, st);
+    }
     ptrs.clear();
+    sizes.clear();
     chunk = nullptr;
     chunk_left = 0;
     next_chunk = (size_t)2 << 20;

@@ -93,6 +93,7 @@ struct Prover {
   Prover(Context& c, const PcsConfig& p) : ctx(c), st(c.stream), cfg(p) {
     A.st = st;
     A.pool = c.pool;
+    if (c.keep_buffers) A.spare = &c.spare;
     phases.init(st);
   }
   void mark(const char* name) { phases.mark(name); }

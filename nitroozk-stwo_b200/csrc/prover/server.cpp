@@ -99,6 +99,7 @@ struct Server {
         cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
         Context ctx;
         int init = ctx.init(st);
+        ctx.keep_buffers = false;
         for (;;) {
           Job job;
           bool got = false, quit = false;
@@ -138,6 +139,7 @@ struct Server {
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     Context ctx;
     int init = ctx.init(st);
+    ctx.keep_buffers = false;
     // waits of this worker: poll briefly, then sleep
     cudaEvent_t wait_ev = nullptr;
     if (cudaEventCreateWithFlags(&wait_ev, cudaEventBlockingSync | cudaEventDisableTiming) == cudaSuccess)

@@ -104,6 +104,9 @@ int Context::init(void* user_stream) {
 
 void Context::destroy() {
   if (stream) cudaStreamSynchronize(stream);
+  for (auto& b : spare) cudaFreeAsync(b.second, stream);
+  spare.clear();
+  if (stream) cudaStreamSynchronize(stream);
   if (work) {
     cudaStreamSynchronize(work);
     cudaStreamSynchronize(side);

@@ -131,6 +131,14 @@ struct Context {
   // reusing freed memory never inserts a dependency on another stream.
   cudaMemPool_t pool = nullptr;
   int alloc_async(size_t bytes, void** out);
+  // The last proof's pool allocations (size, pointer), kept for the next
+  // proof on this context: a proof of the same shape makes the same requests
+  // and takes them back in stream order without a pool call, and the last
+  // proof's frees do not delay its return. Buffers the next proof does not
+  // take are freed when it ends. Off (keep_buffers = false) for the proof
+  // server's contexts, whose HBM budget counts only the proofs in flight.
+  bool keep_buffers = true;
+  std::vector<std::pair<size_t, void*>> spare;
   // Small device-to-host read through the pinned mailbox, then synchronise.
   int read_back(const void* d_src, size_t bytes, void* host_dst);
   // Reads that the host waits for later: mail_start enqueues a copy of at
