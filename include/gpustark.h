@@ -12,7 +12,11 @@
  *   - column lists are HOST arrays of DEVICE pointers (the library stages
  *     them), QM31 columns are 4 device coordinate planes;
  *   - work is stream-ordered on the context's stream; only the calls that
- *     return host values (roots, nonces, proofs) synchronise.
+ *     return host values (roots, nonces, proofs) synchronise. A whole proof
+ *     (gs_prove_*) runs on two streams of the context's own, a high-priority
+ *     one and a low-priority one for work the protocol needs only later,
+ *     entered after the context's stream and left with the context's stream
+ *     ordered after them, so callers see the same ordering.
  * Field values are canonical M31 words (< 2^31 - 1). Hashes are 32 bytes
  * (8 little-endian uint32 words) and hash buffers must be 16-byte aligned.
  */
