@@ -180,6 +180,20 @@ struct Channel {
   }
 };
 
+// GrindOps::grind's acceptance test: the first little-endian word of
+// Blake2s(prefixed_digest || nonce (8 B, LE)) has at least pow_bits trailing
+// zeros.
+inline bool pow_passes(const std::array<uint32_t, 8>& prefixed, uint64_t nonce, uint32_t pow_bits) {
+  Hasher s;
+  for (uint32_t w : prefixed) s.u32(w);
+  s.u32((uint32_t)nonce);
+  s.u32((uint32_t)(nonce >> 32));
+  const Hash h = s.finish();
+  const uint32_t w0 = word(h, 0);
+  const uint32_t tz = w0 == 0 ? 32u : (uint32_t)__builtin_ctz(w0);
+  return tz >= pow_bits;
+}
+
 inline std::vector<size_t> draw_queries(Channel& ch, uint32_t log_domain, size_t n) {
   std::vector<size_t> r;
   uint32_t mask = (uint32_t)((1ull << log_domain) - 1);
@@ -242,134 +256,36 @@ inline size_t bitrev(size_t i, uint32_t log) {
 }
 
 // ------------------------------------------------------------- proof
-struct Decommitment {
-  std::vector<Hash> hash_witness;
-  // further witnesses held elsewhere (8 words each), serialised after
-  // hash_witness: the prover points into its gather read-back
-  const uint32_t* witness_words = nullptr;
-  size_t n_witness = 0;
-  std::vector<uint32_t> column_witness;
-};
-struct FriLayerProof {
-  std::vector<qm31> fri_witness;
-  Decommitment decommitment;
-  Hash commitment{};
-};
-struct Proof {
-  uint32_t pow_bits = 10, log_blowup = 1, log_last_layer = 0, n_queries = 70, fold_step = 1;
-  std::vector<Hash> commitments;
-  std::vector<std::vector<std::vector<qm31>>> sampled_values;
-  std::vector<Decommitment> decommitments;
-  std::vector<std::vector<uint32_t>> queried_values;
-  uint64_t proof_of_work = 0;
-  FriLayerProof fri_first;
-  std::vector<FriLayerProof> fri_inner;
-  std::vector<qm31> last_layer;
-  uint32_t last_layer_log = 0;
-};
-
 // bincode-1.x style: little-endian fixed width, u64 sequence lengths,
 // Option as a 1-byte tag, hash = 32 raw bytes, QM31 = 4 x u32; field order of
 // CommitmentSchemeProof (config, commitments, sampled_values, decommitments,
 // queried_values, proof_of_work, fri_proof).
 static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "proof serialization assumes a little-endian host");
-// Two passes over the proof: the first only counts bytes, the second writes
-// them into an output string sized once (callers that reuse the string keep
-// its pages from proof to proof).
+// A proof is written in passes over one layout: a counting pass (no output),
+// then a pass of the bytes the host holds (`fixed`) and a pass of the bytes
+// gathered on the device (`gathered`), each advancing over the other kind,
+// so the first can run while the gather is still on its way.
 struct Writer {
   char* out = nullptr;  // null: counting pass
   size_t len = 0;
+  bool fixed = false, gathered = false;
   void put(const void* p, size_t n) {
-    if (out) memcpy(out + len, p, n);
+    if (out && fixed) memcpy(out + len, p, n);
+    len += n;
+  }
+  void put_gathered(const void* p, size_t n) {
+    if (out && gathered && n) memcpy(out + len, p, n);
     len += n;
   }
   void u8(uint8_t v) { put(&v, 1); }
   void u32(uint32_t v) { put(&v, 4); }
   void u64(uint64_t v) { put(&v, 8); }
   void hash(const Hash& h) { put(h.data(), 32); }
-  void qm(const qm31& q) { u32(q.x.a); u32(q.x.b); u32(q.y.a); u32(q.y.b); }
-  void dec(const Decommitment& d) {
-    u64(d.hash_witness.size() + d.n_witness);
-    static_assert(sizeof(Hash) == 32, "Hash is 32 contiguous bytes");
-    if (!d.hash_witness.empty()) put(d.hash_witness.data(), 32 * d.hash_witness.size());
-    if (d.n_witness) put(d.witness_words, 32 * d.n_witness);
-    u64(d.column_witness.size());
-    if (!d.column_witness.empty()) put(d.column_witness.data(), 4 * d.column_witness.size());
-  }
-  void layer(const FriLayerProof& l) {
-    u64(l.fri_witness.size());
-    for (auto& q : l.fri_witness) qm(q);
-    dec(l.decommitment);
-    hash(l.commitment);
+  void qm(const qm31& q) {
+    const uint32_t w[4] = {q.x.a, q.x.b, q.y.a, q.y.b};
+    put(w, 16);
   }
 };
-
-inline void write_proof(Writer& w, const Proof& p) {
-  w.u32(p.pow_bits);
-  w.u32(p.log_blowup);
-  w.u32(p.log_last_layer);
-  w.u64(p.n_queries);
-  w.u32(p.fold_step);
-  w.u8(0);  // lifting_log_size: None
-  w.u64(p.commitments.size());
-  for (auto& h : p.commitments) w.hash(h);
-  w.u64(p.sampled_values.size());
-  for (auto& t : p.sampled_values) {
-    w.u64(t.size());
-    for (auto& c : t) {
-      w.u64(c.size());
-      for (auto& q : c) w.qm(q);
-    }
-  }
-  w.u64(p.decommitments.size());
-  for (auto& d : p.decommitments) w.dec(d);
-  w.u64(p.queried_values.size());
-  for (auto& t : p.queried_values) {
-    w.u64(t.size());
-    if (!t.empty()) w.put(t.data(), 4 * t.size());
-  }
-  w.u64(p.proof_of_work);
-  w.layer(p.fri_first);
-  w.u64(p.fri_inner.size());
-  for (auto& l : p.fri_inner) w.layer(l);
-  w.u64(p.last_layer.size());
-  for (auto& q : p.last_layer) w.qm(q);
-  w.u32(p.last_layer_log);
-}
-
-inline void serialize_into(const Proof& p, std::string& out) {
-  Writer count;
-  write_proof(count, p);
-  out.resize(count.len);
-  Writer w;
-  w.out = count.len ? &out[0] : nullptr;
-  write_proof(w, p);
-}
-
-// Into `buf` when the proof fits its `cap` bytes (returns true), else into
-// `out`; *len receives the proof's length either way.
-inline bool serialize_to(const Proof& p, uint8_t* buf, size_t cap, std::string& out, size_t* len) {
-  Writer count;
-  write_proof(count, p);
-  *len = count.len;
-  if (buf && count.len <= cap) {
-    Writer w;
-    w.out = (char*)buf;
-    write_proof(w, p);
-    return true;
-  }
-  out.resize(count.len);
-  Writer w;
-  w.out = count.len ? &out[0] : nullptr;
-  write_proof(w, p);
-  return false;
-}
-
-inline std::string serialize(const Proof& p) {
-  std::string s;
-  serialize_into(p, s);
-  return s;
-}
 
 }  // namespace host
 }  // namespace gs

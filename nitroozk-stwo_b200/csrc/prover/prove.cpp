@@ -82,14 +82,22 @@ static int fri_commit_p252(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriL
 // on the roots and checks every challenge.
 // `while_busy` runs on the host after every FRI launch is enqueued and before
 // the one blocking read-back, overlapping host work with the device's.
+// With the Blake2s channel and a last layer of at most 2^FRI_POW_MAX_LOG
+// values, the proof of work follows on the device too (the last layer's
+// coefficients mixed into the device channel, the prefixed digest, the
+// grind's first chunk of nonces) and comes back in the same read: *nonce
+// is then set and *have_nonce true; the host checks the channel digest, the
+// prefixed digest and the nonce against its own.
 int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first,
                       std::vector<FriLayerDev>& inner, std::vector<qm31>& last_coeffs,
-                      const std::function<void()>& while_busy) {
+                      const std::function<void()>& while_busy, uint64_t* nonce, bool* have_nonce) {
+  *have_nonce = false;
   if (pv.ch.p252) return fri_commit_p252(pv, quot, lifting, first, inner, last_coeffs, while_busy);
   cudaStream_t st = pv.st;
   const uint32_t last_log = pv.cfg.log_last_layer + pv.cfg.log_blowup;
   GS_REQUIRE(lifting >= last_log + 1, "FRI: lifting domain below the last layer");
   const uint32_t n_roots = lifting - last_log;  // the first layer and the committed line layers
+  const bool dev_pow = last_log <= FRI_POW_MAX_LOG && pv.cfg.log_last_layer <= 3 && pv.cfg.pow_bits <= 32;
   // one allocation for every FRI buffer, carved at 256-byte boundaries
   auto up = [](size_t w) { return (w + 63) & ~(size_t)63; };
   auto tree_words = [&](uint32_t log) {
@@ -97,8 +105,10 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
     for (uint32_t k = 0; k <= log; k++) w += up((size_t)8 << k);
     return w;
   };
-  // channel state, roots, challenges, then a copy of the last layer
-  const size_t ctl_used = 16 + 16 * (size_t)n_roots + 4 * ((size_t)1 << last_log);
+  // channel state, roots, challenges, a copy of the last layer, then the
+  // proof of work's words
+  const size_t pow_off = 16 + 16 * (size_t)n_roots + 4 * ((size_t)1 << last_log);
+  const size_t ctl_used = pow_off + (dev_pow ? fri_last_layer_pow_words(pv.cfg.log_last_layer) : 0);
   const size_t ctl_words = up(ctl_used);
   size_t words = ctl_words + tree_words(lifting);
   for (uint32_t lg = lifting - 1;; lg--) {
@@ -192,6 +202,7 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
   uint32_t* d_last = ctl + 16 + 16 * (size_t)n_roots;
   for (int c = 0; c < 4; c++)
     GS_CUDA_TRY(cudaMemcpyAsync(d_last + c * n, cur.planes[c], 4 * n, cudaMemcpyDeviceToDevice, st));
+  if (dev_pow) GS_TRY(fri_last_layer_pow(st, d_last, cur.log, pv.cfg.log_last_layer, pv.cfg.pow_bits, ctl, ctl + pow_off));
   std::vector<uint32_t> hc(ctl_used);
   if (while_busy) while_busy();
   GS_TRY(pv.ctx.read_back(ctl, hc.size() * 4, hc.data()));
@@ -209,7 +220,30 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
     if (r == 0) first.root = root;
     else inner[r - 1].root = root;
   }
-  return finish_last_layer(pv, h.data(), cur.log, last_coeffs);
+  GS_TRY(finish_last_layer(pv, h.data(), cur.log, last_coeffs));
+  if (!dev_pow) return OK;
+  // the device's mixed digest and prefixed digest against the host channel's
+  const size_t nc = (size_t)4 << pv.cfg.log_last_layer;
+  const uint32_t* pw = hc.data() + pow_off;
+  const auto pre = pv.ch.pow_prefixed(pv.cfg.pow_bits);
+  for (int j = 0; j < 8; j++)
+    if (pw[nc + j] != host::word(pv.ch.digest, j) || pw[nc + 8 + j] != pre[j]) {
+      set_error("device channel diverged from the host channel (last FRI layer)");
+      return ERR_CUDA;
+    }
+  const uint32_t best = pw[nc + 16];
+  if (best == 0xffffffffu) {  // no nonce below 2^20: the search goes on from the next chunk
+    GS_TRY(grind_blake2s(st, pre.data(), pv.cfg.pow_bits, (uint32_t*)pv.ctx.d_small, nonce, (uint32_t*)pv.ctx.h_small,
+                         1));
+  } else {
+    if (!host::pow_passes(pre, best, pv.cfg.pow_bits)) {
+      set_error("device grind returned a nonce that does not pass");
+      return ERR_CUDA;
+    }
+    *nonce = best;
+  }
+  *have_nonce = true;
+  return OK;
 }
 
 // The last FRI layer (4 planes of 2^log values, host memory) into the line

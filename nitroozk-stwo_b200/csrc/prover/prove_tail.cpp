@@ -9,13 +9,9 @@ namespace gs {
 namespace prover {
 
 int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first, std::vector<FriLayerDev>& inner,
-               std::vector<qm31>& last_coeffs, const std::function<void()>& while_busy);
+               std::vector<qm31>& last_coeffs, const std::function<void()>& while_busy, uint64_t* nonce,
+               bool* have_nonce);
 void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::vector<uint8_t>& is_witness);
-
-struct ColSamples {
-  std::vector<ptq> points;
-  std::vector<qm31> values;
-};
 
 int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_bytes, ProveStats* stats,
                uint8_t* out_buf, size_t out_cap) {
@@ -38,9 +34,11 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   ptq oods = host::random_point(pv.ch);
   const uint32_t lifting = pv.trees.back().max_log();
   const uint32_t max_ldb = lifting - cfg.log_blowup;
-  // sample points and values per tree / column
+  // sample points and values per tree / column: the points of tree t are
+  // those of requests [req0[t], req0[t] + n_pts[t]); every column of a tree is
+  // sampled at all of them, the values staying in the read-back array
   const size_t n_trees = pv.trees.size();
-  std::vector<std::vector<ColSamples>> samples(n_trees);
+  std::vector<size_t> req0(n_trees, 0), n_pts(n_trees, 0);
   pt31 step = host::index_point(host::canonic_step_index(max_ldb));
   // every (tree, mask point) evaluation is enqueued, then read back once
   struct SampleReq {
@@ -52,7 +50,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   size_t n_vals = 0, scratch_bytes = 0;
   for (size_t t = 0; t < n_trees; t++) {
     Tree& tr = pv.trees[t];
-    samples[t].resize(tr.n_cols);
+    req0[t] = reqs.size();
     if (tr.n_cols == 0) continue;
     std::vector<ptq> pts;  // mask points of every column of this tree
     if (t + 1 == n_trees || t == 1) pts = {oods};
@@ -62,7 +60,14 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
       n_vals += tr.n_cols;
       scratch_bytes = std::max(scratch_bytes, eval_at_point_scratch_bytes(tr.n_cols, tr.coeff_log));
     }
+    n_pts[t] = pts.size();
   }
+  std::vector<uint32_t> h(4 * n_vals);
+  auto sample_point = [&](size_t t, size_t k) -> const ptq& { return reqs[req0[t] + k].p; };
+  auto sample_value = [&](size_t t, uint32_t c, size_t k) {
+    const uint32_t* v = h.data() + 4 * (reqs[req0[t] + k].slot + c);
+    return qm_make(v[0], v[1], v[2], v[3]);
+  };
   {
     uint32_t* d_vals = nullptr;
     void* scratch = nullptr;
@@ -91,31 +96,28 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
                                  (uint32_t*)(side ? scratch_big : scratch), 12, vec));
     }
     GS_TRY(pv.ctx.join_side());
-    std::vector<uint32_t> h(4 * n_vals);
     GS_TRY(pv.ctx.read_back(d_vals, h.size() * 4, h.data()));
-    for (auto& r : reqs) {
-      Tree& tr = pv.trees[r.t];
-      for (uint32_t c = 0; c < tr.n_cols; c++) {
-        const uint32_t* v = h.data() + 4 * (r.slot + c);
-        samples[r.t][c].points.push_back(r.p);
-        samples[r.t][c].values.push_back(qm_make(v[0], v[1], v[2], v[3]));
-      }
-    }
   }
+  // mixed tree by tree, column by column, point by point
   std::vector<qm31> flat;
-  for (auto& tr : samples)
-    for (auto& c : tr) flat.insert(flat.end(), c.values.begin(), c.values.end());
+  flat.reserve(n_vals);
+  for (size_t t = 0; t < n_trees; t++)
+    for (uint32_t c = 0; c < pv.trees[t].n_cols; c++)
+      for (size_t k = 0; k < n_pts[t]; k++) flat.push_back(sample_value(t, c, k));
   pv.ch.mix_felts(flat);
   pv.mark("oods_mix");
   pv.mark("oods_sample");
   // Sanity check (composition at the OODS point vs the constraints evaluated
   // from the mask values), run on this thread while the device works on the
   // FRI layers (fri_commit calls it before its read-back).
-  std::vector<std::vector<std::vector<qm31>>> sv(n_trees);
-  for (size_t t = 0; t < n_trees; t++)
-    for (auto& cs : samples[t]) sv[t].push_back(cs.values);
   bool sane = false;
-  auto sanity = [&air, &sv, &sane, split, oods, E, max_ldb, random_coeff]() {
+  auto sanity = [&, split, oods, E, max_ldb, random_coeff]() {
+    std::vector<std::vector<std::vector<qm31>>> sv(n_trees);
+    for (size_t t = 0; t < n_trees; t++) {
+      sv[t].resize(pv.trees[t].n_cols);
+      for (uint32_t c = 0; c < pv.trees[t].n_cols; c++)
+        for (size_t k = 0; k < n_pts[t]; k++) sv[t][c].push_back(sample_value(t, c, k));
+    }
     auto& cv = sv.back();
     qm31 total = qm_zero();
     for (uint32_t t = 0; t < (1u << split); t++) {
@@ -143,35 +145,43 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   pt31 lift_step = host::index_point(host::canonic_step_index(lifting));
   for (size_t t = 0; t < n_trees; t++) {
     Tree& tr = pv.trees[t];
-    for (uint32_t c = 0; c < tr.n_cols; c++) {
-      auto& cs = samples[t][c];
-      if (cs.points.empty()) continue;
-      std::vector<std::pair<ptq, qm31>> pv_list;
-      if (cs.points.size() == 2) {
-        pt31 period = lift_step;
-        for (uint32_t k = 0; k < tr.eval_log; k++) period = pt_add(period, period);
-        pv_list.push_back({ptq_add(cs.points[1], host::to_ptq(period)), cs.values[1]});
-      }
-      for (size_t k = 0; k < cs.points.size(); k++) pv_list.push_back({cs.points[k], cs.values[k]});
-      for (auto& [p, v] : pv_list) {
+    if (tr.n_cols == 0 || n_pts[t] == 0) continue;
+    // the terms of each column: with two points, the second point shifted by
+    // the tree's period first (its value repeated), then every point; all
+    // columns of a tree share the points, hence the batches
+    ptq pts[3];
+    size_t src[3], n_terms = 0;
+    if (n_pts[t] == 2) {
+      pt31 period = lift_step;
+      for (uint32_t k = 0; k < tr.eval_log; k++) period = pt_add(period, period);
+      pts[n_terms] = ptq_add(sample_point(t, 1), host::to_ptq(period));
+      src[n_terms++] = 1;
+    }
+    for (size_t k = 0; k < n_pts[t]; k++) {
+      pts[n_terms] = sample_point(t, k);
+      src[n_terms++] = k;
+    }
+    size_t bidx[3];
+    for (size_t j = 0; j < n_terms; j++) {
+      bidx[j] = batches.size();
+      for (size_t x = 0; x < batches.size(); x++)
+        if (batches[x].log == tr.eval_log && pt_eq(batches[x].point, pts[j])) bidx[j] = x;
+      if (bidx[j] == batches.size()) batches.push_back(Batch{pts[j], tr.eval_log, {}, qm_zero(), qm_zero()});
+      batches[bidx[j]].entries.reserve(batches[bidx[j]].entries.size() + tr.n_cols);
+    }
+    for (uint32_t c = 0; c < tr.n_cols; c++)
+      for (size_t j = 0; j < n_terms; j++) {
         qm31 a, b, cc;
-        line_coeffs(p, v, pw, a, b, cc);
+        line_coeffs(pts[j], sample_value(t, c, src[j]), pw, a, b, cc);
         pw = qm_mul(pw, qrc);
-        Batch* bt = nullptr;
-        for (auto& x : batches)
-          if (x.log == tr.eval_log && pt_eq(x.point, p)) bt = &x;
-        if (!bt) {
-          batches.push_back(Batch{p, tr.eval_log, {}, qm_zero(), qm_zero()});
-          bt = &batches.back();
-        }
+        Batch& bt = batches[bidx[j]];
         NumEntry e;
         e.col = tr.eval_col(c);
         e.c[0] = cc.x.a; e.c[1] = cc.x.b; e.c[2] = cc.y.a; e.c[3] = cc.y.b;
-        bt->entries.push_back(e);
-        bt->b_sum = qm_add(bt->b_sum, b);
-        bt->a_sum = qm_add(bt->a_sum, a);
+        bt.entries.push_back(e);
+        bt.b_sum = qm_add(bt.b_sum, b);
+        bt.a_sum = qm_add(bt.a_sum, a);
       }
-    }
   }
   pv.mark("quot_plan");
   struct PointAcc2 {
@@ -240,10 +250,13 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   FriLayerDev first;
   std::vector<FriLayerDev> inner;
   std::vector<qm31> last;
-  GS_TRY(fri_commit(pv, quot, lifting, first, inner, last, sanity));
-  pv.mark("fri_commit");
   uint64_t nonce = 0;
-  if (pv.ch.p252) {  // GrindOps<Poseidon252Channel>; the prefix hash on the host
+  bool have_nonce = false;
+  GS_TRY(fri_commit(pv, quot, lifting, first, inner, last, sanity, &nonce, &have_nonce));
+  pv.mark("fri_commit");
+  if (have_nonce) {
+    // found by the device right after the FRI layers (Blake2s channel)
+  } else if (pv.ch.p252) {  // GrindOps<Poseidon252Channel>; the prefix hash on the host
     namespace f = host::p252;
     const auto pre = f::to_bytes(f::hash_many({f::from_u64(0x12345678u), pv.ch.fdigest(), f::from_u64(cfg.pow_bits)}));
     const void* d_pre = nullptr;
@@ -264,11 +277,15 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   queries.erase(std::unique(queries.begin(), queries.end()), queries.end());
   pv.mark("queries");
   // plan all gathers of the decommitment
-  static thread_local GatherPlan g;  // keeps its capacity across proofs
+  // The plan keeps its capacity across proofs; proofs on fibers of one
+  // thread interleave at every wait, so nothing of it is read after launch
+  // (the results are this proof's GatherOut).
+  static thread_local GatherPlan g;
   g.clear();
   struct FriPlan {
     std::vector<size_t> pos;
     std::vector<uint8_t> wit;  // 1: the position is a witness value
+    std::vector<size_t> wpos;  // the witness positions: only their values are gathered
     size_t val_base = 0;
     MerkleDecommitPlan merkle;
   };
@@ -280,8 +297,11 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   // decommitted as the pairs of S_i
   auto plan_fri = [&](FriLayerDev& L, const std::vector<size_t>& q, size_t i, FriPlan& fp) -> int {
     fri_positions(q, fp.pos, fp.wit);
+    fp.wpos.clear();
+    for (size_t k = 0; k < fp.pos.size(); k++)
+      if (fp.wit[k]) fp.wpos.push_back(fp.pos[k]);
     std::vector<const uint32_t*> cols = {L.planes[0], L.planes[1], L.planes[2], L.planes[3]};
-    GS_TRY(g.add_cols(cols, fp.pos, &fp.val_base));
+    GS_TRY(g.add_cols(cols, fp.wpos, &fp.val_base));
     if (L.layers.size() == (size_t)lifting - i + 1)
       return fp.merkle.plan_shared(g, L.layers, cols, fp.pos, sw, (int)L.layers.size() - 3, i + 1, false);
     return fp.merkle.plan(g, L.layers, cols, fp.pos, false);
@@ -311,51 +331,84 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
       GS_TRY(tree_plans[t].plan(g, tr.layers, cols, pos));
   }
   pv.mark("decommit_plan");
-  GS_TRY(g.run(pv.ctx, pv.A));
-  pv.mark("decommit_gather");
-  // assemble the proof
-  host::Proof P;
-  P.pow_bits = cfg.pow_bits;
-  P.log_blowup = cfg.log_blowup;
-  P.log_last_layer = cfg.log_last_layer;
-  P.n_queries = cfg.n_queries;
-  P.fold_step = cfg.fold_step;
-  auto fri_layer_proof = [&](const FriPlan& fp, const FriLayerDev& L, host::FriLayerProof& out) {
-    for (size_t k = 0; k < fp.pos.size(); k++)
-      if (fp.wit[k]) {
-        const uint32_t* w = g.word_out + fp.val_base + 4 * k;
-        out.fri_witness.push_back(qm_make(w[0], w[1], w[2], w[3]));
-      }
-    std::vector<uint32_t> unused;
-    fp.merkle.assemble(g, unused, out.decommitment);
-    out.commitment = L.root;
+  GatherOut go;
+  GS_TRY(g.launch(pv.ctx, pv.A, &go));
+  // The proof, written straight from the plans: every size is known now, so
+  // the bytes the host holds are written while the gather runs, the gathered
+  // ones after it lands.
+  uint32_t last_layer_log = 0;
+  while ((1u << last_layer_log) < last.size()) last_layer_log++;
+  auto fri_layer = [&](host::Writer& w, const FriPlan& fp, const FriLayerDev& L) {
+    // the witness values (4 coordinates each), consecutive in the gather
+    w.u64(fp.wpos.size());
+    w.put_gathered(w.gathered ? go.word_out + fp.val_base : nullptr, 16 * fp.wpos.size());
+    fp.merkle.write_decommitment(w, go);
+    w.hash(L.root);
   };
-  fri_layer_proof(first_plan, first, P.fri_first);
-  P.fri_inner.resize(inner.size());
-  for (size_t i = 0; i < inner.size(); i++) fri_layer_proof(inner_plans[i], inner[i], P.fri_inner[i]);
-  P.last_layer = last;
-  P.last_layer_log = 0;
-  while ((1u << P.last_layer_log) < last.size()) P.last_layer_log++;
-  P.proof_of_work = nonce;
-  P.sampled_values.resize(n_trees);
-  P.decommitments.resize(n_trees);
-  P.queried_values.resize(n_trees);
-  for (size_t t = 0; t < n_trees; t++) {
-    Tree& tr = pv.trees[t];
-    P.commitments.push_back(tr.root);
-    for (auto& cs : samples[t]) P.sampled_values[t].push_back(cs.values);
-    if (tr.n_cols) tree_plans[t].assemble(g, P.queried_values[t], P.decommitments[t]);
-  }
-  if (stats) stats->constraint_check = sane ? 1.0 : 0.0;
-  pv.mark("assemble");
-  {
-    size_t len = 0;
-    const bool direct = host::serialize_to(P, out_buf, out_cap, *proof_bytes, &len);
-    if (stats) {
-      stats->proof_len = len;
-      stats->in_out_buf = direct;
+  auto write = [&](host::Writer& w) {
+    w.u32(cfg.pow_bits);
+    w.u32(cfg.log_blowup);
+    w.u32(cfg.log_last_layer);
+    w.u64(cfg.n_queries);
+    w.u32(cfg.fold_step);
+    w.u8(0);  // lifting_log_size: None
+    w.u64(n_trees);
+    for (auto& tr : pv.trees) w.hash(tr.root);
+    w.u64(n_trees);
+    for (size_t t = 0; t < n_trees; t++) {
+      w.u64(pv.trees[t].n_cols);
+      for (uint32_t c = 0; c < pv.trees[t].n_cols; c++) {
+        w.u64(n_pts[t]);
+        for (size_t k = 0; k < n_pts[t]; k++) w.qm(sample_value(t, c, k));
+      }
     }
+    w.u64(n_trees);
+    for (size_t t = 0; t < n_trees; t++) {
+      if (pv.trees[t].n_cols) {
+        tree_plans[t].write_decommitment(w, go);
+      } else {
+        w.u64(0);
+        w.u64(0);
+      }
+    }
+    w.u64(n_trees);
+    for (size_t t = 0; t < n_trees; t++) {
+      if (pv.trees[t].n_cols) tree_plans[t].write_queried(w, go);
+      else w.u64(0);
+    }
+    w.u64(nonce);
+    fri_layer(w, first_plan, first);
+    w.u64(inner.size());
+    for (size_t i = 0; i < inner.size(); i++) fri_layer(w, inner_plans[i], inner[i]);
+    w.u64(last.size());
+    for (auto& q : last) w.qm(q);
+    w.u32(last_layer_log);
+  };
+  host::Writer count;
+  write(count);
+  const size_t len = count.len;
+  const bool direct = out_buf && len <= out_cap;
+  char* dst = (char*)out_buf;
+  if (!direct) {
+    proof_bytes->resize(len);
+    dst = len ? &(*proof_bytes)[0] : nullptr;
   }
+  host::Writer fixed;
+  fixed.out = dst;
+  fixed.fixed = true;
+  write(fixed);
+  if (stats) {
+    stats->constraint_check = sane ? 1.0 : 0.0;
+    stats->proof_len = len;
+    stats->in_out_buf = direct;
+  }
+  pv.mark("assemble");
+  GS_TRY(go.wait(pv.ctx));
+  pv.mark("decommit_gather");
+  host::Writer gathered;
+  gathered.out = dst;
+  gathered.gathered = true;
+  write(gathered);
   pv.mark("serialize");
   if (!sane) {
     set_error("constraints not satisfied: composition OODS value differs from the constraints at the mask");

@@ -122,6 +122,14 @@ struct Tree {
   const uint32_t* eval_col(uint32_t c) const { return evals + ((size_t)c << eval_log); }
 };
 
+// Results of one launched gather, in the context's pinned read-back buffer
+// (valid until its next read-back): gathered words, then 8 words per hash.
+struct GatherOut {
+  const uint32_t* word_out = nullptr;
+  const uint32_t* hash_out = nullptr;
+  int wait(Context& ctx) { return stream_sync(ctx.stream); }
+};
+
 // Batched device gathers for decommitments: column values are described per
 // (column set, sorted positions) block and expanded on the device; hash
 // witnesses are (layer, index) items. One launch per kind, one read-back.
@@ -134,10 +142,6 @@ struct GatherPlan {
   size_t n_words = 0;
   size_t n_hash_out = 0;         // hashes the runs write, in run order
   uint32_t max_items = 0;
-  // results, in the context's pinned read-back buffer (valid until its next
-  // read-back): gathered words, then 8 words per hash
-  const uint32_t* word_out = nullptr;
-  const uint32_t* hash_out = nullptr;
   // Empties the plan, keeping its capacity (one plan serves many proofs).
   void clear() {
     blocks.clear();
@@ -147,7 +151,6 @@ struct GatherPlan {
     n_words = 0;
     n_hash_out = 0;
     max_items = 0;
-    word_out = hash_out = nullptr;
   }
   size_t n_hashes() const { return n_hash_out; }
   // Values of `cols` at `pos`, position-major; returns the first output word.
@@ -181,7 +184,10 @@ struct GatherPlan {
     runs.push_back(HashRun{src, (uint32_t)first, (uint32_t)count, (uint32_t)n_hash_out, 0});
     n_hash_out += count;
   }
-  int run(Context& ctx, Arena& A) {
+  // The upload, both gathers and the read-back, enqueued on the context's
+  // stream; `out` is valid after GatherOut::wait. The plan itself may be
+  // cleared and reused once launch returns (the upload has been taken).
+  int launch(Context& ctx, Arena& A, GatherOut* out) {
     cudaStream_t st = ctx.stream;
     const size_t nh = hidx.size();
     auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
@@ -220,12 +226,10 @@ struct GatherPlan {
     void* hr = nullptr;
     GS_TRY(ctx.read_buffer(out_words * 4, &hr));
     if (out_words) GS_CUDA_TRY(cudaMemcpyAsync(hr, d_out, out_words * 4, cudaMemcpyDeviceToHost, st));
-    GS_TRY(stream_sync(st));
-    word_out = (const uint32_t*)hr;
-    hash_out = word_out + hbase;
+    out->word_out = (const uint32_t*)hr;
+    out->hash_out = out->word_out + hbase;
     return OK;
   }
-  host::Hash hash(size_t slot) const { return host::hash_from_words(hash_out + 8 * slot); }
 };
 
 // Merkle decommitment of a tree whose columns all sit at the leaf layer
@@ -288,11 +292,16 @@ struct MerkleDecommitPlan {
   int plan_shared(GatherPlan& g, const std::vector<uint32_t*>& layers, const std::vector<const uint32_t*>& cols,
                   const std::vector<size_t>& pos, const SharedWitness& sw, int top_L, size_t m0,
                   bool with_values = true);
-  // The witnesses stay in the gather's read-back buffer; `d` refers to them.
-  void assemble(const GatherPlan& g, std::vector<uint32_t>& queried, host::Decommitment& d) const {
-    queried.assign(g.word_out + value_base, g.word_out + value_base + n_positions * n_cols);
-    d.witness_words = g.hash_out + 8 * hash_begin;
-    d.n_witness = n_hashes;
+  // Serialised MerkleDecommitment (hash witnesses, no column witness) and
+  // the queried values: gathered bytes, written by the writer's gathered pass.
+  void write_decommitment(host::Writer& w, const GatherOut& g) const {
+    w.u64(n_hashes);
+    w.put_gathered(w.gathered ? g.hash_out + 8 * hash_begin : nullptr, 32 * n_hashes);
+    w.u64(0);
+  }
+  void write_queried(host::Writer& w, const GatherOut& g) const {
+    w.u64(n_positions * n_cols);
+    w.put_gathered(w.gathered ? g.word_out + value_base : nullptr, 4 * n_positions * n_cols);
   }
 };
 

@@ -292,7 +292,21 @@ int gather_multi(cudaStream_t st, const uint32_t* const* d_cols, uint32_t n_cols
 int gather_hashes(cudaStream_t st, const uint32_t* d_layer, const uint32_t* d_idx, uint32_t n_idx, uint32_t* d_out);
 
 // grind.cu
+// hi0: the first high word searched (a search whose chunk hi = 0 already ran
+// on the device, as fri_last_layer_pow does, continues at 1)
 int grind_blake2s(cudaStream_t st, const uint32_t prefixed_digest[8], uint32_t pow_bits, uint32_t* d_scratch,
-                  uint64_t* nonce_out, uint32_t* h_word = nullptr);
+                  uint64_t* nonce_out, uint32_t* h_word = nullptr, uint32_t hi0 = 0);
+// The Blake2s channel's steps between the last FRI layer and the queries, on
+// the device: the last layer (4 planes of 2^log values at d_last) into its
+// LinePoly coefficients, mixed into the channel digest d_state[0, 8); the
+// proof of work's prefixed digest; and the grind's first chunk (nonces below
+// 2^20). d_out receives the 4 * 2^bound_log coefficient words, the mixed
+// digest (8 words), the prefixed digest (8 words) and the smallest passing
+// nonce of the chunk (1 word, all ones when none passed). Layers of at most
+// FRI_POW_MAX_LOG values' log and bound_log <= 3; the host checks every word.
+constexpr uint32_t FRI_POW_MAX_LOG = 5;
+size_t fri_last_layer_pow_words(uint32_t bound_log);
+int fri_last_layer_pow(cudaStream_t st, const uint32_t* d_last, uint32_t log, uint32_t bound_log, uint32_t pow_bits,
+                       const uint32_t* d_state, uint32_t* d_out);
 
 }  // namespace gs

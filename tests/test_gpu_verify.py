@@ -93,3 +93,21 @@ def test_poseidon_benchmark_gpu_proof_accepted_and_tamper_rejected(G):
                 O.verify(flip(p, off), "poseidon", log_n, **kw)
             n += 1
     assert n >= 60
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+def test_high_pow_bits_gpu_proofs_accepted(G, seed):
+    """pow_bits 22: the device's first chunk of nonces (below 2^20, searched
+    right after the FRI layers) holds a hit with probability about 0.22, so
+    these seeds take both the device nonce and the host-driven search of the
+    next chunks. Either way the proof is accepted; a nonce below 2^20 is the
+    smallest passing one, so the whole proof equals the oracle's."""
+    cfg = G.pcs_config(pow_bits=22, n_queries=5)
+    p = G.prove_wide_fibonacci(7, 12, seed=seed, input_mode=1, config=cfg)
+    assert O.verify(p, "wide_fibonacci", 7, n_cols=12, config=(22, 1, 0, 5, 1))
+    (s, _), = [(s, e) for name, s, e in sections(p) if name == "proof_of_work"]
+    nonce = int.from_bytes(p[s:s + 8], "little")
+    if nonce < (1 << 20):
+        assert p == O.prove("wide_fibonacci", 7, n_cols=12, seed=seed, input_mode=1, pow_bits=22, n_queries=5)
+    else:
+        assert nonce >> 32 >= 1 and (nonce & 0xFFFFFFFF) < (1 << 20)
