@@ -7,6 +7,7 @@ namespace gs {
 void fft_set_columns_aligned(bool aligned);
 namespace prover {
 
+static int last_layer_coeffs(Prover& pv, const uint32_t* h, uint32_t log, std::vector<qm31>& last_coeffs);
 static int finish_last_layer(Prover& pv, const uint32_t* h, uint32_t log, std::vector<qm31>& last_coeffs);
 
 // FRI commit with Poseidon252MerkleChannel (prover/fri.rs:99-199 over
@@ -86,12 +87,17 @@ static int fri_commit_p252(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriL
 // values, the proof of work follows on the device too (the last layer's
 // coefficients mixed into the device channel, the prefixed digest, the
 // grind's first chunk of nonces) and comes back in the same read: *nonce
-// is then set and *have_nonce true; the host checks the channel digest, the
-// prefixed digest and the nonce against its own.
+// is then set and *have_nonce true. The host channel then takes the device's
+// digest at once (the queries need it), and the replay of the layers' roots
+// and challenges, the last layer's mix and the comparison with the device's
+// digest go to *replay, which the caller runs before the proof is returned
+// (while the decommitment's gather is on the device).
 int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first,
                       std::vector<FriLayerDev>& inner, std::vector<qm31>& last_coeffs,
-                      const std::function<void()>& while_busy, uint64_t* nonce, bool* have_nonce) {
+                      const std::function<void()>& while_busy, uint64_t* nonce, bool* have_nonce,
+                      std::function<int()>* replay) {
   *have_nonce = false;
+  *replay = nullptr;
   if (pv.ch.p252) return fri_commit_p252(pv, quot, lifting, first, inner, last_coeffs, while_busy);
   cudaStream_t st = pv.st;
   const uint32_t last_log = pv.cfg.log_last_layer + pv.cfg.log_blowup;
@@ -206,8 +212,57 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
   std::vector<uint32_t> hc(ctl_used);
   if (while_busy) while_busy();
   GS_TRY(pv.ctx.read_back(ctl, hc.size() * 4, hc.data()));
-  std::vector<uint32_t> h(hc.begin() + 16 + 16 * (size_t)n_roots, hc.end());
+  std::vector<uint32_t> h(hc.begin() + 16 + 16 * (size_t)n_roots, hc.begin() + pow_off);
   GS_REQUIRE(hc[9] == 0, "device channel: no challenge within the draw bound");
+  if (dev_pow) {
+    for (uint32_t r = 0; r < n_roots; r++) {
+      host::Hash root = host::hash_from_words(hc.data() + 16 + 8 * r);
+      if (r == 0) first.root = root;
+      else inner[r - 1].root = root;
+    }
+    GS_TRY(last_layer_coeffs(pv, h.data(), cur.log, last_coeffs));
+    const size_t nc = (size_t)4 << pv.cfg.log_last_layer;
+    const uint32_t* pw = hc.data() + pow_off;
+    host::Channel before = pv.ch;
+    pv.ch.set(host::hash_from_words(pw + nc));  // the digest after the last layer's mix
+    const auto pre = pv.ch.pow_prefixed(pv.cfg.pow_bits);
+    for (int j = 0; j < 8; j++)
+      if (pw[nc + 8 + j] != pre[j]) {
+        set_error("device channel diverged from the host channel (proof-of-work prefix)");
+        return ERR_CUDA;
+      }
+    const uint32_t best = pw[nc + 16];
+    if (best == 0xffffffffu) {  // no nonce below 2^20: the search goes on from the next chunk
+      GS_TRY(grind_blake2s(st, pre.data(), pv.cfg.pow_bits, (uint32_t*)pv.ctx.d_small, nonce,
+                           (uint32_t*)pv.ctx.h_small, 1));
+    } else {
+      if (!host::pow_passes(pre, best, pv.cfg.pow_bits)) {
+        set_error("device grind returned a nonce that does not pass");
+        return ERR_CUDA;
+      }
+      *nonce = best;
+    }
+    *have_nonce = true;
+    *replay = [&pv, &first, &inner, &last_coeffs, before, hc = std::move(hc), n_roots,
+               digest = pv.ch.digest]() mutable -> int {
+      for (uint32_t r = 0; r < n_roots; r++) {
+        before.mix_root(r == 0 ? first.root : inner[r - 1].root);
+        const qm31 a = before.draw_felt();
+        const uint32_t* f = hc.data() + 16 + 8 * (size_t)n_roots + 8 * r;
+        if (!qm_eq(a, qm_make(f[0], f[1], f[2], f[3]))) {
+          set_error("device channel diverged from the host channel");
+          return ERR_CUDA;
+        }
+      }
+      before.mix_felts(last_coeffs);
+      if (before.digest != digest) {
+        set_error("device channel diverged from the host channel (last FRI layer)");
+        return ERR_CUDA;
+      }
+      return OK;
+    };
+    return OK;
+  }
   for (uint32_t r = 0; r < n_roots; r++) {
     host::Hash root = host::hash_from_words(hc.data() + 16 + 8 * r);
     pv.ch.mix_root(root);
@@ -220,35 +275,19 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
     if (r == 0) first.root = root;
     else inner[r - 1].root = root;
   }
-  GS_TRY(finish_last_layer(pv, h.data(), cur.log, last_coeffs));
-  if (!dev_pow) return OK;
-  // the device's mixed digest and prefixed digest against the host channel's
-  const size_t nc = (size_t)4 << pv.cfg.log_last_layer;
-  const uint32_t* pw = hc.data() + pow_off;
-  const auto pre = pv.ch.pow_prefixed(pv.cfg.pow_bits);
-  for (int j = 0; j < 8; j++)
-    if (pw[nc + j] != host::word(pv.ch.digest, j) || pw[nc + 8 + j] != pre[j]) {
-      set_error("device channel diverged from the host channel (last FRI layer)");
-      return ERR_CUDA;
-    }
-  const uint32_t best = pw[nc + 16];
-  if (best == 0xffffffffu) {  // no nonce below 2^20: the search goes on from the next chunk
-    GS_TRY(grind_blake2s(st, pre.data(), pv.cfg.pow_bits, (uint32_t*)pv.ctx.d_small, nonce, (uint32_t*)pv.ctx.h_small,
-                         1));
-  } else {
-    if (!host::pow_passes(pre, best, pv.cfg.pow_bits)) {
-      set_error("device grind returned a nonce that does not pass");
-      return ERR_CUDA;
-    }
-    *nonce = best;
-  }
-  *have_nonce = true;
-  return OK;
+  return finish_last_layer(pv, h.data(), cur.log, last_coeffs);
 }
 
 // The last FRI layer (4 planes of 2^log values, host memory) into the line
 // polynomial's coefficients: interpolation, degree check, mix into the channel.
 static int finish_last_layer(Prover& pv, const uint32_t* h, uint32_t log, std::vector<qm31>& last_coeffs) {
+  GS_TRY(last_layer_coeffs(pv, h, log, last_coeffs));
+  pv.ch.mix_felts(last_coeffs);
+  return OK;
+}
+
+// The interpolation and degree check of finish_last_layer, without the mix.
+static int last_layer_coeffs(Prover& pv, const uint32_t* h, uint32_t log, std::vector<qm31>& last_coeffs) {
   const size_t n = (size_t)1 << log;
   std::vector<qm31> vals(n);
   for (size_t i = 0; i < n; i++) vals[i] = qm_make(h[i], h[n + i], h[2 * n + i], h[3 * n + i]);
@@ -266,7 +305,6 @@ static int finish_last_layer(Prover& pv, const uint32_t* h, uint32_t log, std::v
   uint32_t blog = pv.cfg.log_last_layer;
   last_coeffs.assign(bound, qm_zero());
   for (size_t i = 0; i < bound; i++) last_coeffs[host::bitrev(i, blog)] = ordered[i];
-  pv.ch.mix_felts(last_coeffs);
   return OK;
 }
 

@@ -10,7 +10,7 @@ namespace prover {
 
 int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first, std::vector<FriLayerDev>& inner,
                std::vector<qm31>& last_coeffs, const std::function<void()>& while_busy, uint64_t* nonce,
-               bool* have_nonce);
+               bool* have_nonce, std::function<int()>* replay);
 void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::vector<uint8_t>& is_witness);
 
 int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_bytes, ProveStats* stats,
@@ -252,7 +252,8 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   std::vector<qm31> last;
   uint64_t nonce = 0;
   bool have_nonce = false;
-  GS_TRY(fri_commit(pv, quot, lifting, first, inner, last, sanity, &nonce, &have_nonce));
+  std::function<int()> replay;  // the FRI channel's host replay, when deferred
+  GS_TRY(fri_commit(pv, quot, lifting, first, inner, last, sanity, &nonce, &have_nonce, &replay));
   pv.mark("fri_commit");
   if (have_nonce) {
     // found by the device right after the FRI layers (Blake2s channel)
@@ -298,6 +299,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   auto plan_fri = [&](FriLayerDev& L, const std::vector<size_t>& q, size_t i, FriPlan& fp) -> int {
     fri_positions(q, fp.pos, fp.wit);
     fp.wpos.clear();
+    fp.wpos.reserve(fp.pos.size());
     for (size_t k = 0; k < fp.pos.size(); k++)
       if (fp.wit[k]) fp.wpos.push_back(fp.pos[k]);
     std::vector<const uint32_t*> cols = {L.planes[0], L.planes[1], L.planes[2], L.planes[3]};
@@ -310,11 +312,13 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   GS_TRY(plan_fri(first, queries, 0, first_plan));
   std::vector<FriPlan> inner_plans(inner.size());
   std::vector<size_t> lq = queries;
+  std::vector<size_t> f;
   for (size_t i = 0; i < inner.size(); i++) {
-    std::vector<size_t> f;
+    f.clear();
+    f.reserve(lq.size());
     for (size_t q : lq)
       if (f.empty() || f.back() != (q >> 1)) f.push_back(q >> 1);
-    lq = f;
+    lq.swap(f);
     GS_TRY(plan_fri(inner[i], lq, i + 1, inner_plans[i]));
   }
   pv.mark("fri_plans");
@@ -333,6 +337,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   pv.mark("decommit_plan");
   GatherOut go;
   GS_TRY(g.launch(pv.ctx, pv.A, &go));
+  if (replay) GS_TRY(replay());
   // The proof, written straight from the plans: every size is known now, so
   // the bytes the host holds are written while the gather runs, the gathered
   // ones after it lands.
