@@ -23,56 +23,212 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   uint32_t* comp[4];
   GS_TRY(pv.composition(air, random_coeff, comp));
   pv.mark("composition");
+  // The sample requests and the DEEP quotients' plan depend on the trees'
+  // shapes and on the sample points' offsets from the OODS point, not on the
+  // point itself (p + a = p + b exactly when a = b): both are built, and the
+  // plan uploaded, while the composition's root is on its way to the host.
+  // The points of tree t are oods + off for the requests [req0[t], req0[t] +
+  // n_pts[t]); every column of a tree is sampled at all of them, the values
+  // staying in the read-back array.
+  struct SampleReq {
+    size_t t;
+    pt31 off;
+    size_t slot;
+    ptq p;  // once the OODS point is drawn
+  };
+  std::vector<SampleReq> reqs;
+  std::vector<size_t> req0, n_pts;
+  size_t n_trees = 0, n_vals = 0, scratch_bytes = 0;
+  uint32_t lifting = 0, max_ldb = 0;
+  // DEEP quotients (compute_fri_quotients, prover/pcs/quotient_ops.rs): the
+  // terms (column, sample point) are grouped in batches of one column size
+  // and one point; each batch accumulates its numerators, each point lifts
+  // and combines its batches. One kernel computes the line coefficients and
+  // their sums once the random coefficient is drawn.
+  struct Batch {
+    pt31 off;
+    uint32_t log, point_id;
+    std::vector<NumEntry> entries;
+    std::vector<LineTerm> terms;
+    uint32_t* planes = nullptr;
+  };
+  std::vector<Batch> batches;
+  std::vector<pt31> qoffs;  // the distinct sample points' offsets
+  struct PointAcc {
+    std::vector<std::pair<uint32_t, uint32_t*>> parts;  // (log, planes base of 4 x 2^log)
+    const void* d_lift = nullptr;                       // LiftCol array when more than one part
+    uint32_t* res = nullptr;
+    uint32_t top = 0;
+  };
+  std::vector<PointAcc> per_point;
+  uint32_t* d_vals = nullptr;
+  void* eval_scratch = nullptr;
+  void* eval_scratch_big = nullptr;
+  NumEntry* d_entries = nullptr;
+  const LineTerm* d_terms = nullptr;
+  const uint32_t* d_bfirst = nullptr;
+  const uint32_t* d_bpoint = nullptr;
+  uint32_t* d_bsums = nullptr;
+  uint32_t* d_lscratch = nullptr;
+  std::vector<uint32_t> bfirst;
+  uint32_t n_terms = 0;
+  auto plan_samples = [&](Tree& comp_tree) -> int {
+    n_trees = pv.trees.size() + 1;
+    auto tree = [&](size_t t) -> Tree& { return t + 1 == n_trees ? comp_tree : pv.trees[t]; };
+    lifting = comp_tree.max_log();
+    max_ldb = lifting - cfg.log_blowup;
+    const pt31 step = host::index_point(host::canonic_step_index(max_ldb));
+    const pt31 zero = {1u, 0u};
+    req0.assign(n_trees, 0);
+    n_pts.assign(n_trees, 0);
+    for (size_t t = 0; t < n_trees; t++) {
+      Tree& tr = tree(t);
+      req0[t] = reqs.size();
+      if (tr.n_cols == 0) continue;
+      std::vector<pt31> offs;  // mask points of every column of this tree
+      if (t + 1 == n_trees || t == 1) offs = {zero};
+      else offs = {pt_conj(step), zero};  // interaction: offsets -1, 0
+      for (auto& o : offs) {
+        reqs.push_back({t, o, n_vals, {}});
+        n_vals += tr.n_cols;
+        scratch_bytes = std::max(scratch_bytes, eval_at_point_scratch_bytes(tr.n_cols, tr.coeff_log));
+      }
+      n_pts[t] = offs.size();
+    }
+    GS_TRY(pv.A.alloc_n(4 * n_vals + 4, &d_vals));
+    GS_TRY(pv.A.alloc(scratch_bytes + 16, &eval_scratch));
+    GS_TRY(pv.A.alloc(scratch_bytes + 16, &eval_scratch_big));
+    // the quotients' batches, in the order the terms are met
+    uint32_t kterm = 0;  // the random coefficient's power of the next term
+    const pt31 lift_step = host::index_point(host::canonic_step_index(lifting));
+    for (size_t t = 0; t < n_trees; t++) {
+      Tree& tr = tree(t);
+      if (tr.n_cols == 0 || n_pts[t] == 0) continue;
+      // the terms of each column: with two points, the second point shifted
+      // by the tree's period first (its value repeated), then every point;
+      // all columns of a tree share the points, hence the batches
+      pt31 offs[3];
+      size_t src[3], n_t = 0;
+      if (n_pts[t] == 2) {
+        pt31 period = lift_step;
+        for (uint32_t k = 0; k < tr.eval_log; k++) period = pt_add(period, period);
+        offs[n_t] = pt_add(reqs[req0[t] + 1].off, period);
+        src[n_t++] = 1;
+      }
+      for (size_t k = 0; k < n_pts[t]; k++) {
+        offs[n_t] = reqs[req0[t] + k].off;
+        src[n_t++] = k;
+      }
+      auto same = [](const pt31& a, const pt31& b) { return a.x == b.x && a.y == b.y; };
+      size_t bidx[3];
+      for (size_t j = 0; j < n_t; j++) {
+        bidx[j] = batches.size();
+        for (size_t x = 0; x < batches.size(); x++)
+          if (batches[x].log == tr.eval_log && same(batches[x].off, offs[j])) bidx[j] = x;
+        if (bidx[j] == batches.size()) {
+          uint32_t pid = (uint32_t)qoffs.size();
+          for (size_t q = 0; q < qoffs.size(); q++)
+            if (same(qoffs[q], offs[j])) pid = (uint32_t)q;
+          if (pid == qoffs.size()) qoffs.push_back(offs[j]);
+          batches.push_back(Batch{offs[j], tr.eval_log, pid, {}, {}, nullptr});
+        }
+        batches[bidx[j]].entries.reserve(batches[bidx[j]].entries.size() + tr.n_cols);
+        batches[bidx[j]].terms.reserve(batches[bidx[j]].terms.size() + tr.n_cols);
+      }
+      for (uint32_t c = 0; c < tr.n_cols; c++)
+        for (size_t j = 0; j < n_t; j++) {
+          Batch& bt = batches[bidx[j]];
+          NumEntry e{};
+          e.col = tr.eval_col(c);
+          bt.entries.push_back(e);
+          bt.terms.push_back(LineTerm{(uint32_t)(4 * (reqs[req0[t] + src[j]].slot + c)), bt.point_id, kterm++, 0});
+        }
+    }
+    GS_REQUIRE(batches.size() <= QUOT_MAX_BATCHES && qoffs.size() <= QUOT_MAX_POINTS,
+               "too many quotient batches or sample points");
+    // numerator planes per batch; per point the lifted sum of its batches
+    per_point.resize(qoffs.size());
+    for (auto& bt : batches) {
+      GS_TRY(pv.A.alloc_n((size_t)4 << bt.log, &bt.planes));
+      per_point[bt.point_id].parts.push_back({bt.log, bt.planes});
+    }
+    std::vector<std::vector<LiftCol>> lifts(qoffs.size());
+    for (size_t q = 0; q < qoffs.size(); q++) {
+      PointAcc& pa = per_point[q];
+      std::sort(pa.parts.begin(), pa.parts.end(), [](auto& x, auto& y) { return x.first < y.first; });
+      pa.top = pa.parts.back().first;
+      pa.res = pa.parts.back().second;
+      if (pa.parts.size() > 1) {
+        for (auto& [lg, base] : pa.parts) {
+          size_t nn = (size_t)1 << lg;
+          lifts[q].push_back(LiftCol{{base, base + nn, base + 2 * nn, base + 3 * nn}, lg, 0});
+        }
+        GS_TRY(pv.A.alloc_n((size_t)4 << pa.top, &pa.res));
+      }
+    }
+    // one upload: entries | terms | batch_first | batch_point | lift columns
+    std::vector<uint8_t> up;
+    auto put = [&up](const void* p, size_t n) {
+      const size_t o = up.size();
+      up.resize(o + ((n + 15) & ~(size_t)15));
+      if (n) memcpy(up.data() + o, p, n);
+      return o;
+    };
+    std::vector<uint32_t> bpoint;
+    bfirst.assign(1, 0);
+    for (auto& bt : batches) {
+      bfirst.push_back(bfirst.back() + (uint32_t)bt.entries.size());
+      bpoint.push_back(bt.point_id);
+    }
+    n_terms = bfirst.back();
+    std::vector<NumEntry> entries;
+    std::vector<LineTerm> terms;
+    entries.reserve(n_terms);
+    terms.reserve(n_terms);
+    for (auto& bt : batches) {
+      entries.insert(entries.end(), bt.entries.begin(), bt.entries.end());
+      terms.insert(terms.end(), bt.terms.begin(), bt.terms.end());
+    }
+    const size_t o_entries = put(entries.data(), entries.size() * sizeof(NumEntry));
+    const size_t o_terms = put(terms.data(), terms.size() * sizeof(LineTerm));
+    const size_t o_bfirst = put(bfirst.data(), bfirst.size() * 4);
+    const size_t o_bpoint = put(bpoint.data(), bpoint.size() * 4);
+    std::vector<size_t> o_lift(qoffs.size(), 0);
+    for (size_t q = 0; q < qoffs.size(); q++)
+      if (!lifts[q].empty()) o_lift[q] = put(lifts[q].data(), lifts[q].size() * sizeof(LiftCol));
+    const void* d = nullptr;
+    GS_TRY(pv.ctx.stage_bytes(up.data(), up.size(), &d));
+    const uint8_t* db = (const uint8_t*)d;
+    d_entries = (NumEntry*)(db + o_entries);  // the coefficient kernel writes c in place
+    d_terms = (const LineTerm*)(db + o_terms);
+    d_bfirst = (const uint32_t*)(db + o_bfirst);
+    d_bpoint = (const uint32_t*)(db + o_bpoint);
+    for (size_t q = 0; q < qoffs.size(); q++)
+      if (!lifts[q].empty()) per_point[q].d_lift = db + o_lift[q];
+    GS_TRY(pv.A.alloc_n(4 * batches.size() + 4, &d_bsums));
+    GS_TRY(pv.A.alloc_n(8 * (size_t)n_terms + 8, &d_lscratch));
+    return OK;
+  };
   {
     std::vector<const uint32_t*> parts;
     const uint32_t plog = E - split;
     for (uint32_t t = 0; t < (1u << split); t++)
       for (int c = 0; c < 4; c++) parts.push_back(comp[c] + ((size_t)t << plog));
-    GS_TRY(pv.commit_coeffs(parts, plog));
+    GS_TRY(pv.commit_coeffs(parts, plog, plan_samples));
   }
   pv.mark("composition_commit");
+  GS_REQUIRE(pv.trees.size() == n_trees, "sample plan out of step with the trees");
   ptq oods = host::random_point(pv.ch);
-  const uint32_t lifting = pv.trees.back().max_log();
-  const uint32_t max_ldb = lifting - cfg.log_blowup;
-  // sample points and values per tree / column: the points of tree t are
-  // those of requests [req0[t], req0[t] + n_pts[t]); every column of a tree is
-  // sampled at all of them, the values staying in the read-back array
-  const size_t n_trees = pv.trees.size();
-  std::vector<size_t> req0(n_trees, 0), n_pts(n_trees, 0);
-  pt31 step = host::index_point(host::canonic_step_index(max_ldb));
-  // every (tree, mask point) evaluation is enqueued, then read back once
-  struct SampleReq {
-    size_t t;
-    ptq p;
-    size_t slot;
-  };
-  std::vector<SampleReq> reqs;
-  size_t n_vals = 0, scratch_bytes = 0;
-  for (size_t t = 0; t < n_trees; t++) {
-    Tree& tr = pv.trees[t];
-    req0[t] = reqs.size();
-    if (tr.n_cols == 0) continue;
-    std::vector<ptq> pts;  // mask points of every column of this tree
-    if (t + 1 == n_trees || t == 1) pts = {oods};
-    else pts = {ptq_add(oods, host::to_ptq(pt_conj(step))), oods};  // interaction: offsets -1, 0
-    for (auto& p : pts) {
-      reqs.push_back({t, p, n_vals});
-      n_vals += tr.n_cols;
-      scratch_bytes = std::max(scratch_bytes, eval_at_point_scratch_bytes(tr.n_cols, tr.coeff_log));
-    }
-    n_pts[t] = pts.size();
-  }
+  for (auto& r : reqs) r.p = ptq_add(oods, host::to_ptq(r.off));
   std::vector<uint32_t> h(4 * n_vals);
-  auto sample_point = [&](size_t t, size_t k) -> const ptq& { return reqs[req0[t] + k].p; };
   auto sample_value = [&](size_t t, uint32_t c, size_t k) {
     const uint32_t* v = h.data() + 4 * (reqs[req0[t] + k].slot + c);
     return qm_make(v[0], v[1], v[2], v[3]);
   };
+  QuotAcc* d_qaccs = nullptr;
+  const ptq* d_qpoints = nullptr;
   {
-    uint32_t* d_vals = nullptr;
-    void* scratch = nullptr;
-    GS_TRY(pv.A.alloc_n(4 * n_vals + 4, &d_vals));
-    GS_TRY(pv.A.alloc(scratch_bytes + 16, &scratch));
+    // every (tree, mask point) evaluation is enqueued, then read back once;
     // the largest evaluation (the trace's) runs on the side stream with a
     // scratch of its own, next to the small ones on the work stream
     size_t big = 0;
@@ -80,11 +236,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     for (size_t i = 1; i < reqs.size(); i++)
       if (cost(reqs[i]) > cost(reqs[big])) big = i;
     const bool split_streams = reqs.size() > 1 && pv.ctx.side != nullptr;
-    void* scratch_big = scratch;
-    if (split_streams) {
-      GS_TRY(pv.A.alloc(scratch_bytes + 16, &scratch_big));
-      GS_TRY(pv.ctx.fork_side());
-    }
+    if (split_streams) GS_TRY(pv.ctx.fork_side());
     for (size_t i = 0; i < reqs.size(); i++) {
       const SampleReq& r = reqs[i];
       Tree& tr = pv.trees[r.t];
@@ -93,8 +245,31 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
       const bool side = split_streams && i == big;
       GS_TRY(batch_eval_at_point(side ? pv.ctx.side : st, tr.coeff_tab, tr.n_cols, tr.coeff_log,
                                  host::ptq_rep_double(r.p, lifting - tr.eval_log), d_vals + 4 * r.slot,
-                                 (uint32_t*)(side ? scratch_big : scratch), 12, vec));
+                                 (uint32_t*)(side ? eval_scratch_big : eval_scratch), 12, vec));
     }
+    // the sample points and the quotient accumulators (one upload)
+    std::vector<ptq> qpoints;
+    std::vector<QuotAcc> qaccs;
+    for (size_t q = 0; q < qoffs.size(); q++) {
+      const ptq pt = ptq_add(oods, host::to_ptq(qoffs[q]));
+      qpoints.push_back(pt);
+      const PointAcc& pa = per_point[q];
+      const size_t nn = (size_t)1 << pa.top;
+      QuotAcc qa{};
+      qa.p[0] = pa.res; qa.p[1] = pa.res + nn; qa.p[2] = pa.res + 2 * nn; qa.p[3] = pa.res + 3 * nn;
+      qa.log_size = pa.top;
+      qa.first_linear = qm_zero();  // written by the coefficient kernel
+      qa.prx = pt.x.x; qa.pix = pt.x.y; qa.pry = pt.y.x; qa.piy = pt.y.y;
+      qaccs.push_back(qa);
+    }
+    const size_t o_acc = ((qpoints.size() * sizeof(ptq)) + 15) & ~(size_t)15;
+    std::vector<uint8_t> up(o_acc + qaccs.size() * sizeof(QuotAcc));
+    memcpy(up.data(), qpoints.data(), qpoints.size() * sizeof(ptq));
+    memcpy(up.data() + o_acc, qaccs.data(), qaccs.size() * sizeof(QuotAcc));
+    const void* d = nullptr;
+    GS_TRY(pv.ctx.stage_bytes(up.data(), up.size(), &d));
+    d_qpoints = (const ptq*)d;
+    d_qaccs = (QuotAcc*)((uint8_t*)d + o_acc);
     GS_TRY(pv.ctx.join_side());
     GS_TRY(pv.ctx.read_back(d_vals, h.size() * 4, h.data()));
   }
@@ -131,119 +306,32 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     qm31 cons = eval_at_point(air, sv, random_coeff, dinv);
     sane = qm_eq(total, cons);
   };
-  // DEEP quotients: per (column size, point) batches of line-coefficient
-  // terms, lifted per point, combined over the lifting domain.
   qm31 qrc = pv.ch.draw_felt();
-  struct Batch {
-    ptq point;
-    uint32_t log;
-    std::vector<NumEntry> entries;
-    qm31 b_sum = qm_zero(), a_sum = qm_zero();
-  };
-  std::vector<Batch> batches;
-  qm31 pw = qm_one();
-  pt31 lift_step = host::index_point(host::canonic_step_index(lifting));
-  for (size_t t = 0; t < n_trees; t++) {
-    Tree& tr = pv.trees[t];
-    if (tr.n_cols == 0 || n_pts[t] == 0) continue;
-    // the terms of each column: with two points, the second point shifted by
-    // the tree's period first (its value repeated), then every point; all
-    // columns of a tree share the points, hence the batches
-    ptq pts[3];
-    size_t src[3], n_terms = 0;
-    if (n_pts[t] == 2) {
-      pt31 period = lift_step;
-      for (uint32_t k = 0; k < tr.eval_log; k++) period = pt_add(period, period);
-      pts[n_terms] = ptq_add(sample_point(t, 1), host::to_ptq(period));
-      src[n_terms++] = 1;
-    }
-    for (size_t k = 0; k < n_pts[t]; k++) {
-      pts[n_terms] = sample_point(t, k);
-      src[n_terms++] = k;
-    }
-    size_t bidx[3];
-    for (size_t j = 0; j < n_terms; j++) {
-      bidx[j] = batches.size();
-      for (size_t x = 0; x < batches.size(); x++)
-        if (batches[x].log == tr.eval_log && pt_eq(batches[x].point, pts[j])) bidx[j] = x;
-      if (bidx[j] == batches.size()) batches.push_back(Batch{pts[j], tr.eval_log, {}, qm_zero(), qm_zero()});
-      batches[bidx[j]].entries.reserve(batches[bidx[j]].entries.size() + tr.n_cols);
-    }
-    for (uint32_t c = 0; c < tr.n_cols; c++)
-      for (size_t j = 0; j < n_terms; j++) {
-        qm31 a, b, cc;
-        line_coeffs(pts[j], sample_value(t, c, src[j]), pw, a, b, cc);
-        pw = qm_mul(pw, qrc);
-        Batch& bt = batches[bidx[j]];
-        NumEntry e;
-        e.col = tr.eval_col(c);
-        e.c[0] = cc.x.a; e.c[1] = cc.x.b; e.c[2] = cc.y.a; e.c[3] = cc.y.b;
-        bt.entries.push_back(e);
-        bt.b_sum = qm_add(bt.b_sum, b);
-        bt.a_sum = qm_add(bt.a_sum, a);
-      }
-  }
+  GS_TRY(quot_line_coeffs(st, d_terms, n_terms, d_vals, d_qpoints, qrc, d_entries, d_bfirst, d_bpoint,
+                          (uint32_t)batches.size(), d_bsums, d_qaccs, (uint32_t)qoffs.size(), d_lscratch));
   pv.mark("quot_plan");
-  struct PointAcc2 {
-    ptq point;
-    std::vector<std::pair<uint32_t, uint32_t*>> parts;  // (log, planes base of 4 x 2^log)
-    qm31 flt = qm_zero();
-  };
-  std::vector<PointAcc2> per_point;
-  for (auto& bt : batches) {
-    uint32_t* planes = nullptr;
-    GS_TRY(pv.A.alloc_n((size_t)4 << bt.log, &planes));
-    const void* d_entries = nullptr;
-    GS_TRY(pv.ctx.stage_bytes(bt.entries.data(), bt.entries.size() * sizeof(NumEntry), &d_entries));
-    size_t nn = (size_t)1 << bt.log;
+  for (size_t b = 0; b < batches.size(); b++) {
+    const Batch& bt = batches[b];
+    const size_t nn = (size_t)1 << bt.log;
     bool vec = bt.log >= 2;  // tree columns and these planes sit at multiples of 2^log words
     for (auto& e : bt.entries) vec = vec && ((uintptr_t)e.col & 15) == 0;
-    GS_TRY(accumulate_numerators(st, d_entries, (uint32_t)bt.entries.size(), bt.b_sum, bt.log,
-                                 Planes{{planes, planes + nn, planes + 2 * nn, planes + 3 * nn}}, vec));
-    PointAcc2* pa = nullptr;
-    for (auto& x : per_point)
-      if (pt_eq(x.point, bt.point)) pa = &x;
-    if (!pa) {
-      per_point.push_back(PointAcc2{bt.point, {}, qm_zero()});
-      pa = &per_point.back();
-    }
-    pa->parts.push_back({bt.log, planes});
-    pa->flt = qm_add(pa->flt, bt.a_sum);
+    GS_TRY(accumulate_numerators(st, d_entries + bfirst[b], bfirst[b + 1] - bfirst[b], qm_zero(), bt.log,
+                                 Planes{{bt.planes, bt.planes + nn, bt.planes + 2 * nn, bt.planes + 3 * nn}}, vec,
+                                 d_bsums + 4 * b));
   }
-  std::vector<QuotAcc> qaccs;
-  for (auto& pa : per_point) {
-    std::sort(pa.parts.begin(), pa.parts.end(), [](auto& x, auto& y) { return x.first < y.first; });
-    uint32_t top = pa.parts.back().first;
-    uint32_t* res = pa.parts.back().second;
-    if (pa.parts.size() > 1) {
-      std::vector<LiftCol> lc;
-      for (auto& [lg, base] : pa.parts) {
-        size_t nn = (size_t)1 << lg;
-        lc.push_back(LiftCol{{base, base + nn, base + 2 * nn, base + 3 * nn}, lg, 0});
-      }
-      GS_TRY(pv.A.alloc_n((size_t)4 << top, &res));
-      const void* d = nullptr;
-      GS_TRY(pv.ctx.stage_bytes(lc.data(), lc.size() * sizeof(LiftCol), &d));
-      size_t nn = (size_t)1 << top;
-      GS_TRY(lift_and_accumulate(st, d, (uint32_t)lc.size(), top, Planes{{res, res + nn, res + 2 * nn, res + 3 * nn}}));
+  for (auto& pa : per_point)
+    if (pa.d_lift) {
+      size_t nn = (size_t)1 << pa.top;
+      GS_TRY(lift_and_accumulate(st, pa.d_lift, (uint32_t)pa.parts.size(), pa.top,
+                                 Planes{{pa.res, pa.res + nn, pa.res + 2 * nn, pa.res + 3 * nn}}));
     }
-    size_t nn = (size_t)1 << top;
-    QuotAcc q;
-    q.p[0] = res; q.p[1] = res + nn; q.p[2] = res + 2 * nn; q.p[3] = res + 3 * nn;
-    q.log_size = top;
-    q.pad = 0;
-    q.first_linear = pa.flt;
-    q.prx = pa.point.x.x; q.pix = pa.point.x.y; q.pry = pa.point.y.x; q.piy = pa.point.y.y;
-    qaccs.push_back(q);
-  }
   uint32_t* quot[4];
   for (int c = 0; c < 4; c++) GS_TRY(pv.A.alloc_n((size_t)1 << lifting, &quot[c]));
   {
     DomainTables dt;
     GS_TRY(pv.ctx.domain_tables(lifting, &dt));
-    const void* d = nullptr;
-    GS_TRY(pv.ctx.stage_bytes(qaccs.data(), qaccs.size() * sizeof(QuotAcc), &d));
-    GS_TRY(compute_quotients_and_combine(st, d, (uint32_t)qaccs.size(), dt, Planes{{quot[0], quot[1], quot[2], quot[3]}}));
+    GS_TRY(compute_quotients_and_combine(st, d_qaccs, (uint32_t)qoffs.size(), dt,
+                                         Planes{{quot[0], quot[1], quot[2], quot[3]}}));
   }
   pv.mark("quotients");
   // FRI commit, proof of work

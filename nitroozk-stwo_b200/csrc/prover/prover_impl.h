@@ -270,21 +270,6 @@ struct Prover {
   }
 };
 
-struct Sample {
-  ptq point;
-  qm31 value;
-};
-
-// complex_conjugate_line_coeffs (core/constraints.rs:119-134).
-static void line_coeffs(const ptq& p, qm31 v, qm31 alpha, qm31& a, qm31& b, qm31& c) {
-  qm31 aa = qm_sub(qm_conj(v), v);
-  qm31 cc = qm_sub(qm_conj(p.y), p.y);
-  qm31 bb = qm_sub(qm_mul(v, cc), qm_mul(aa, p.y));
-  a = qm_mul(alpha, aa);
-  b = qm_mul(alpha, bb);
-  c = qm_mul(alpha, cc);
-}
-
 static bool pt_eq(const ptq& a, const ptq& b) { return qm_eq(a.x, b.x) && qm_eq(a.y, b.y); }
 
 // Line interpolation of the last FRI layer (prover/line.rs:45-70) on

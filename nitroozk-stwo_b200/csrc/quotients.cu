@@ -52,7 +52,8 @@ __device__ __forceinline__ void load_rows(const uint32_t* col, size_t row0, uint
 template <int R>
 __global__ void __launch_bounds__(256) accumulate_numerators_kernel(const NumEntry* __restrict__ entries,
                                                                     uint32_t n_entries, qm31 b_sum, uint32_t log_size,
-                                                                    Planes out) {
+                                                                    Planes out, const uint32_t* __restrict__ bsum_dev) {
+  if (bsum_dev) b_sum = qm_make(bsum_dev[0], bsum_dev[1], bsum_dev[2], bsum_dev[3]);
   __shared__ NumEntry se[ACC_MAX_SMEM_ENTRIES];
   const bool staged = n_entries <= ACC_MAX_SMEM_ENTRIES;
   if (staged)
@@ -136,7 +137,9 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template <int EG>
 __global__ void __launch_bounds__(256, 4) accumulate_numerators_split_kernel(const NumEntry* __restrict__ entries,
                                                                              uint32_t n_entries, qm31 b_sum,
-                                                                             uint32_t log_size, Planes out) {
+                                                                             uint32_t log_size, Planes out,
+                                                                             const uint32_t* __restrict__ bsum_dev) {
+  if (bsum_dev) b_sum = qm_make(bsum_dev[0], bsum_dev[1], bsum_dev[2], bsum_dev[3]);
   constexpr uint32_t RG = 8 / EG, TILE = 128 * RG, STRIDE = EG * ACC_ROUND;
   extern __shared__ uint4 dyn[];  // [warp][slot][entry][lane] in the loop; part[group][q][row] after it
   uint32_t* part = reinterpret_cast<uint32_t*>(dyn);
@@ -223,7 +226,7 @@ __global__ void __launch_bounds__(256, 4) accumulate_numerators_split_kernel(con
 }
 
 int accumulate_numerators(cudaStream_t st, const void* d_entries, uint32_t n_entries, qm31 b_sum, uint32_t log_size,
-                          Planes out, bool vec) {
+                          Planes out, bool vec, const uint32_t* d_bsum) {
   GS_REQUIRE(log_size <= 30, "log size out of range");
   size_t n = (size_t)1 << log_size;
   int threads = 256;
@@ -243,13 +246,98 @@ int accumulate_numerators(cudaStream_t st, const void* d_entries, uint32_t n_ent
         accumulate_numerators_split_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ACC_DYN_SMEM);
     GS_CUDA_TRY(attr);
     accumulate_numerators_split_kernel<1><<<grid, 256, ACC_DYN_SMEM, st>>>((const NumEntry*)d_entries, n_entries,
-                                                                         b_sum, log_size, out);
+                                                                         b_sum, log_size, out, d_bsum);
   } else if (R == 4)
     accumulate_numerators_kernel<4><<<(unsigned)blocks, threads, 0, st>>>((const NumEntry*)d_entries, n_entries,
-                                                                         b_sum, log_size, out);
+                                                                         b_sum, log_size, out, d_bsum);
   else
     accumulate_numerators_kernel<1><<<(unsigned)blocks, threads, 0, st>>>((const NumEntry*)d_entries, n_entries,
-                                                                         b_sum, log_size, out);
+                                                                         b_sum, log_size, out, d_bsum);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
+// ------------------------------------------------------- line coefficients
+__device__ __forceinline__ qm31 qm_pow_dev(qm31 x, uint32_t k) {
+  qm31 r = qm_one();
+  while (k) {
+    if (k & 1u) r = qm_mul(r, x);
+    x = qm_mul(x, x);
+    k >>= 1;
+  }
+  return r;
+}
+
+__device__ __forceinline__ qm31 qm_ld(const uint32_t* p) { return qm_make(p[0], p[1], p[2], p[3]); }
+
+__device__ __forceinline__ qm31 qm_shfl_down(qm31 v, int d) {
+  return qm_make(__shfl_down_sync(0xffffffffu, v.x.a, d), __shfl_down_sync(0xffffffffu, v.x.b, d),
+                 __shfl_down_sync(0xffffffffu, v.y.a, d), __shfl_down_sync(0xffffffffu, v.y.b, d));
+}
+
+__global__ void __launch_bounds__(512) quot_line_coeffs_kernel(const LineTerm* __restrict__ terms, uint32_t n_terms,
+                                                               const uint32_t* __restrict__ vals,
+                                                               const ptq* __restrict__ points, qm31 alpha,
+                                                               NumEntry* entries, const uint32_t* batch_first,
+                                                               const uint32_t* batch_point, uint32_t n_batches,
+                                                               uint32_t* bsums, QuotAcc* accs, uint32_t n_points,
+                                                               uint32_t* scratch) {
+  __shared__ qm31 asum[QUOT_MAX_BATCHES];
+  for (uint32_t i = threadIdx.x; i < n_terms; i += blockDim.x) {
+    const LineTerm t = terms[i];
+    const qm31 v = qm_ld(vals + t.val);
+    const ptq p = points[t.point];
+    const qm31 pw = qm_pow_dev(alpha, t.k);
+    // complex_conjugate_line_coeffs: a = conj(v) - v, c = conj(p.y) - p.y,
+    // b = v c - a p.y, all three times alpha^k
+    const qm31 aa = qm_sub(qm_conj(v), v);
+    const qm31 cc = qm_sub(qm_conj(p.y), p.y);
+    const qm31 bb = qm_sub(qm_mul(v, cc), qm_mul(aa, p.y));
+    const qm31 a = qm_mul(pw, aa), b = qm_mul(pw, bb), c = qm_mul(pw, cc);
+    entries[i].c[0] = c.x.a; entries[i].c[1] = c.x.b; entries[i].c[2] = c.y.a; entries[i].c[3] = c.y.b;
+    uint32_t* s = scratch + 8 * (size_t)i;
+    s[0] = a.x.a; s[1] = a.x.b; s[2] = a.y.a; s[3] = a.y.b;
+    s[4] = b.x.a; s[5] = b.x.b; s[6] = b.y.a; s[7] = b.y.b;
+  }
+  __syncthreads();
+  // one warp per batch: the sums of a and b over its terms
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t bt = warp; bt < n_batches; bt += blockDim.x >> 5) {
+    qm31 sa = qm_zero(), sb = qm_zero();
+    for (uint32_t i = batch_first[bt] + lane; i < batch_first[bt + 1]; i += 32) {
+      sa = qm_add(sa, qm_ld(scratch + 8 * (size_t)i));
+      sb = qm_add(sb, qm_ld(scratch + 8 * (size_t)i + 4));
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+      sa = qm_add(sa, qm_shfl_down(sa, d));
+      sb = qm_add(sb, qm_shfl_down(sb, d));
+    }
+    if (lane == 0) {
+      asum[bt] = sa;
+      bsums[4 * bt] = sb.x.a; bsums[4 * bt + 1] = sb.x.b; bsums[4 * bt + 2] = sb.y.a; bsums[4 * bt + 3] = sb.y.b;
+    }
+  }
+  __syncthreads();
+  // per sample point, its batches' a sums, in batch order
+  for (uint32_t pt = threadIdx.x; pt < n_points; pt += blockDim.x) {
+    qm31 f = qm_zero();
+    for (uint32_t bt = 0; bt < n_batches; bt++)
+      if (batch_point[bt] == pt) f = qm_add(f, asum[bt]);
+    accs[pt].first_linear = f;
+  }
+}
+
+int quot_line_coeffs(cudaStream_t st, const LineTerm* d_terms, uint32_t n_terms, const uint32_t* d_vals,
+                     const ptq* d_points, qm31 alpha, NumEntry* d_entries, const uint32_t* d_batch_first,
+                     const uint32_t* d_batch_point, uint32_t n_batches, uint32_t* d_bsums, QuotAcc* d_accs,
+                     uint32_t n_points, uint32_t* d_scratch) {
+  GS_REQUIRE(n_batches <= QUOT_MAX_BATCHES && n_points <= QUOT_MAX_POINTS, "too many quotient batches or points");
+  GS_REQUIRE(n_terms == 0 || (d_terms && d_vals && d_points && d_entries && d_scratch), "null buffer");
+  GS_REQUIRE(d_batch_first && d_batch_point && d_bsums && d_accs, "null buffer");
+  quot_line_coeffs_kernel<<<1, 512, 0, st>>>(d_terms, n_terms, d_vals, d_points, alpha, d_entries, d_batch_first,
+                                             d_batch_point, n_batches, d_bsums, d_accs, n_points, d_scratch);
   note_launch();
   GS_CUDA_TRY(cudaGetLastError());
   return OK;

@@ -254,8 +254,10 @@ int fold_circle_into_line(cudaStream_t st, CPlanes src, uint32_t log_n, qm31 alp
 // quotients.cu
 // vec: every column pointer and output plane is 16-byte aligned (4 rows per
 // thread with vector loads).
+// d_bsum (optional): b_sum as 4 words in device memory, written by an earlier
+// kernel of the stream (quot_line_coeffs); the b_sum argument is then unused.
 int accumulate_numerators(cudaStream_t st, const void* d_entries, uint32_t n_entries, qm31 b_sum, uint32_t log_size,
-                          Planes out, bool vec = false);
+                          Planes out, bool vec = false, const uint32_t* d_bsum = nullptr);
 int compute_quotients_and_combine(cudaStream_t st, const void* d_accs, uint32_t n_accs, const DomainTables& dt,
                                   Planes out);
 int lift_and_accumulate(cudaStream_t st, const void* d_cols, uint32_t n_cols, uint32_t log_size, Planes out);
@@ -272,6 +274,21 @@ struct QuotAcc {
   cm31 prx, pry, pix, piy;
 };
 struct LiftCol { const uint32_t* p[4]; uint32_t log_size; uint32_t pad; };
+// One term of the DEEP quotients: a column's value at a sample point.
+// val: word offset of the value (4 words) in the sampled values; point: its
+// sample point; k: the power of the random coefficient it takes.
+struct LineTerm { uint32_t val, point, k, pad; };
+constexpr uint32_t QUOT_MAX_BATCHES = 32, QUOT_MAX_POINTS = 16;
+// The line coefficients of every term (complex_conjugate_line_coeffs with
+// alpha^k, core/constraints.rs:119-134), in one block: c into entries[i] (the
+// entries of batch b are [batch_first[b], batch_first[b + 1])), the batch's
+// sum of b into d_bsums[4b, 4b + 4), and per sample point the sum of a over
+// its batches (batch_point[b]) into accs[point].first_linear. d_scratch: 8
+// words per term. points: ptq per sample point.
+int quot_line_coeffs(cudaStream_t st, const LineTerm* d_terms, uint32_t n_terms, const uint32_t* d_vals,
+                     const ptq* d_points, qm31 alpha, NumEntry* d_entries, const uint32_t* d_batch_first,
+                     const uint32_t* d_batch_point, uint32_t n_batches, uint32_t* d_bsums, QuotAcc* d_accs,
+                     uint32_t n_points, uint32_t* d_scratch);
 
 // eval_at_point.cu
 size_t eval_at_point_scratch_bytes(uint32_t n_polys, uint32_t log_n, uint32_t chunk_log = 12);
