@@ -235,7 +235,14 @@ __global__ void __launch_bounds__(TH, TH >= 256 ? 4 : 8)
     u = next_u;
     in_log = out_log;
   }
-  if (state && tid == 0) channel_mix_root_draw_dev(state, layers.p[0], root_copy, felt);
+  if (tid == 0) {
+    if (state) {
+      channel_mix_root_draw_dev(state, layers.p[0], root_copy, felt);
+    } else if (root_copy) {
+#pragma unroll
+      for (int j = 0; j < 8; j++) root_copy[j] = layers.p[0][j];
+    }
+  }
 }
 
 int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters,
@@ -244,15 +251,31 @@ int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layer
   return commit_node_layers_ch(st, top_log, layers, d_counters, nullptr, nullptr, nullptr);
 }
 
+static bool merkle_legacy() {
+  static const bool legacy = [] {
+    const char* e = getenv("GS_MERKLE_LEGACY");
+    return e && e[0] == '1';
+  }();
+  return legacy;
+}
+
+int commit_node_layers_to(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters,
+                          uint32_t* root_out) {
+  GS_REQUIRE(root_out != nullptr, "null root output");
+  if (top_log == 0 || merkle_legacy()) {  // no tree kernel writes the root
+    GS_TRY(commit_node_layers(st, top_log, layers, d_counters));
+    GS_CUDA_TRY(cudaMemcpyAsync(root_out, layers[0], 32, cudaMemcpyDefault, st));
+    return OK;
+  }
+  return commit_node_layers_ch(st, top_log, layers, d_counters, nullptr, root_out, nullptr);
+}
+
 // A tree of top_log <= TREE_MAX_LOG uses at most 2^(27 - 2U) + 2^(27 - 3U) + 1
 // ticket counters for units of 2^U children (checked against TREE_COUNTERS).
 int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters,
                           uint32_t* d_state, uint32_t* d_root_copy, uint32_t* d_felt) {
   GS_REQUIRE(top_log <= 30, "layer log size out of range");
-  static const bool legacy = [] {
-    const char* e = getenv("GS_MERKLE_LEGACY");
-    return e && e[0] == '1';
-  }();
+  const bool legacy = merkle_legacy();
   if (!legacy) {
     uint32_t top = top_log;
     while (top > TREE_MAX_LOG) {  // layers above 2^27 nodes: one launch each

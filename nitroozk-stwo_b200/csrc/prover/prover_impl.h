@@ -125,6 +125,10 @@ struct Prover {
                                            (uint8_t*)t.layers[L]));
     } else {
       GS_TRY(commit_on_layer(st, t.eval_log, nullptr, tab, t.n_cols, t.layers[t.eval_log]));
+      if (ctx.d_mail) {  // the tree kernel writes the root into mailbox slot 0 itself
+        GS_TRY(commit_node_layers_to(st, t.eval_log, t.layers.data(), ctx.tree_counters, (uint32_t*)ctx.d_mail));
+        return ctx.mail_record(0);
+      }
       GS_TRY(commit_node_layers(st, t.eval_log, t.layers.data(), ctx.tree_counters));
     }
     // the root comes back through mailbox slot 0; commit_coeffs waits for it

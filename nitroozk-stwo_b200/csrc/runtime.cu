@@ -96,6 +96,15 @@ int Context::init(void* user_stream) {
   GS_CUDA_TRY(cudaMalloc((void**)&d_small, small_cap));
   GS_CUDA_TRY(cudaMallocHost((void**)&h_small, small_cap + MAIL_SLOTS * MAIL_BYTES));
   h_mail = h_small + small_cap;
+  {
+    void* dm = nullptr;
+    if (cudaHostGetDevicePointer(&dm, h_mail, 0) == cudaSuccess) {
+      d_mail = (uint8_t*)dm;
+    } else {
+      cudaGetLastError();
+      d_mail = nullptr;
+    }
+  }
   for (int i = 0; i < MAIL_SLOTS; i++) GS_CUDA_TRY(cudaEventCreateWithFlags(&mail_ev[i], cudaEventDisableTiming));
   GS_CUDA_TRY(cudaMalloc((void**)&tree_counters, 4 * TREE_COUNTERS));
   GS_CUDA_TRY(cudaMemsetAsync(tree_counters, 0, 4 * TREE_COUNTERS, stream));
@@ -141,6 +150,7 @@ void Context::destroy() {
     mail_ev[i] = nullptr;
   }
   h_mail = nullptr;
+  d_mail = nullptr;
   if (h_read) cudaFreeHost(h_read);
   h_read = nullptr;
   read_cap = 0;
@@ -256,6 +266,12 @@ int Context::read_back(const void* d_src, size_t bytes, void* host_dst) {
 int Context::mail_start(int slot, const void* d_src, size_t bytes) {
   GS_REQUIRE(slot >= 0 && slot < MAIL_SLOTS && bytes <= MAIL_BYTES, "mailbox read out of range");
   GS_CUDA_TRY(cudaMemcpyAsync(h_mail + slot * MAIL_BYTES, d_src, bytes, cudaMemcpyDeviceToHost, stream));
+  GS_CUDA_TRY(cudaEventRecord(mail_ev[slot], stream));
+  return OK;
+}
+
+int Context::mail_record(int slot) {
+  GS_REQUIRE(slot >= 0 && slot < MAIL_SLOTS, "mailbox slot out of range");
   GS_CUDA_TRY(cudaEventRecord(mail_ev[slot], stream));
   return OK;
 }

@@ -148,8 +148,13 @@ struct Context {
   static constexpr int MAIL_SLOTS = 4;
   static constexpr size_t MAIL_BYTES = 256;
   uint8_t* h_mail = nullptr;
+  // The slots' device alias (the area is mapped pinned memory), or null: a
+  // kernel that writes its result there directly needs no copy, only
+  // mail_record(slot) after it.
+  uint8_t* d_mail = nullptr;
   cudaEvent_t mail_ev[MAIL_SLOTS] = {nullptr};
   int mail_start(int slot, const void* d_src, size_t bytes);
+  int mail_record(int slot);
   int mail_wait(int slot, const void** host);
   // growable pinned host buffer for read-backs (decommitment values)
   uint8_t* h_read = nullptr;
@@ -208,6 +213,11 @@ int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, 
 constexpr uint32_t TREE_MAX_LOG = 27;
 constexpr uint32_t TREE_COUNTERS = 1024;
 int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters);
+// The same, with the root also written to root_out (8 words, e.g. mapped
+// host memory) by the launch that computes it (or copied there when no tree
+// kernel runs).
+int commit_node_layers_to(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters,
+                          uint32_t* root_out);
 // The same, followed by the Fiat-Shamir channel step on the root in the same
 // launch (the FRI commit phase).
 int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters,
