@@ -3,7 +3,8 @@ allocation the pool cannot satisfy maps to GS_ERR_OOM and leaves the context
 usable; the proof-of-work search bound maps to GS_ERR_TIMEOUT (the bound set
 low with the GS_GRIND_MAX_HI switch, in a child process); proof-server jobs
 are validated at submission like direct proofs; a server destroyed with
-queued jobs drains them within its HBM budget."""
+queued jobs drains them within its HBM budget; the legacy Merkle path (in a
+child process) gives the oracle's proofs."""
 import ctypes as C
 import hashlib
 import os
@@ -67,6 +68,29 @@ def test_grind_search_bound_is_timeout():
     assert f"status {GS_ERR_TIMEOUT}" in out.stdout and "search bound" in out.stdout, out.stdout
     nonce = int(out.stdout.split("after:")[1])
     assert O.verify_pow(digest, 4, nonce)
+
+
+LEGACY_CHILD = r"""
+import sys
+sys.path[:0] = [{pkg!r}, {oracle!r}]
+from gpustark import prove as G
+import pyoracle as O
+ok = all(G.prove_wide_fibonacci(n, 9, seed=4, input_mode=1) == O.prove("wide_fibonacci", n, n_cols=9, seed=4,
+                                                                        input_mode=1) for n in (5, 9))
+print("match" if ok else "differ")
+"""
+
+
+def test_legacy_merkle_path_proofs_match():
+    """GS_MERKLE_LEGACY=1 (per-layer launches and a cluster tail instead of
+    the one-launch tree kernel; read once per process, hence a child): the
+    roots reach the host by a copy into the mailbox, and the proofs equal
+    the oracle's."""
+    env = dict(os.environ, GS_MERKLE_LEGACY="1")
+    code = LEGACY_CHILD.format(pkg=os.path.join(ROOT, "nitroozk-stwo_b200"), oracle=os.path.join(ROOT, "oracle"))
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert "match" in out.stdout, out.stdout
 
 
 def test_server_validates_jobs_at_submission(G):

@@ -40,7 +40,11 @@ def test_poseidon_reference_split_is_rejected_like_the_reference(G):
         O.prove("poseidon", 6, split_log=1)
 
 
-@pytest.mark.parametrize("blowup,queries,pow_bits,last", [(2, 20, 4, 0), (1, 3, 10, 0), (3, 9, 0, 1)])
+# last layers of 2^(last + blowup) values: up to 2^5 with a degree bound of at
+# most 2^3 take the device's last-layer step (one to three Blake2s blocks in
+# its mix), larger ones the host's
+@pytest.mark.parametrize("blowup,queries,pow_bits,last", [(2, 20, 4, 0), (1, 3, 10, 0), (3, 9, 0, 1), (1, 5, 8, 3),
+                                                          (2, 7, 3, 4), (1, 6, 5, 4)])
 def test_pcs_configs(G, blowup, queries, pow_bits, last):
     cfg = G.pcs_config(pow_bits=pow_bits, log_blowup=blowup, n_queries=queries, log_last_layer=last)
     got = G.prove_wide_fibonacci(9, 20, seed=3, input_mode=1, config=cfg)
