@@ -309,26 +309,39 @@ static int last_layer_coeffs(Prover& pv, const uint32_t* h, uint32_t log, std::v
 }
 
 // compute_decommitment_positions_and_witness_evals (prover/fri.rs:301-330),
-// fold step 1: positions are both members of each queried pair; the witness
-// values are the pair members that were not queried.
-void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::vector<uint8_t>& is_witness) {
-  // q is sorted and unique: a pair holds one or two queries
+// fold step 1: the decommitted positions are both members of each queried
+// pair; the witness values are the pair members that were not queried. Fills
+// `wit` with the witness positions (and `pos`, when given, with every
+// decommitted position) and returns the number of decommitted positions.
+size_t fri_witness_positions(const std::vector<size_t>& q, std::vector<size_t>& wit, std::vector<size_t>* pos) {
+  // q is sorted and unique. A query starts a pair unless its left neighbour
+  // is in the same pair; the witness of a pair is the member that was not
+  // queried: q ^ 1 after a starting query, unless q is even and q + 1 follows
+  // (both members queried). The flags are computed as integers: for random
+  // queries a branch on them mispredicts half the time.
   const size_t n = q.size();
-  pos.resize(2 * n);
-  is_witness.resize(2 * n);
-  size_t o = 0;
-  for (size_t i = 0; i < n;) {
-    const size_t start = q[i] & ~(size_t)1;
-    const bool both = i + 1 < n && q[i + 1] == start + 1;
-    pos[o] = start;
-    pos[o + 1] = start + 1;
-    is_witness[o] = q[i] != start;
-    is_witness[o + 1] = !both && q[i] == start;
-    o += 2;
-    i += both ? 2 : 1;
+  wit.resize(n);
+  size_t n_pos = 0, nw = 0;
+  for (size_t i = 0; i < n; i++) {
+    const size_t v = q[i];
+    const size_t left = i > 0 ? q[i - 1] : ~(size_t)0;
+    const size_t right = i + 1 < n ? q[i + 1] : ~(size_t)0;
+    const size_t starts = (size_t)(((left ^ v) >> 1) != 0);
+    const size_t both = ((v & 1) ^ 1) & (size_t)(right == v + 1);
+    wit[nw] = v ^ 1;
+    nw += starts & (both ^ 1);
+    n_pos += starts << 1;
   }
-  pos.resize(o);
-  is_witness.resize(o);
+  wit.resize(nw);
+  if (pos) {
+    pos->clear();
+    for (size_t i = 0; i < n; i++)
+      if (i == 0 || ((q[i - 1] ^ q[i]) >> 1) != 0) {
+        pos->push_back(q[i] & ~(size_t)1);
+        pos->push_back(q[i] | 1);
+      }
+  }
+  return n_pos;
 }
 
 int validate_request(const ProveRequest& r) {

@@ -11,7 +11,7 @@ namespace prover {
 int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& first, std::vector<FriLayerDev>& inner,
                std::vector<qm31>& last_coeffs, const std::function<void()>& while_busy, uint64_t* nonce,
                bool* have_nonce, std::function<int()>* replay);
-void fri_positions(const std::vector<size_t>& q, std::vector<size_t>& pos, std::vector<uint8_t>& is_witness);
+size_t fri_witness_positions(const std::vector<size_t>& q, std::vector<size_t>& wit, std::vector<size_t>* pos);
 
 int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_bytes, ProveStats* stats,
                uint8_t* out_buf, size_t out_cap) {
@@ -372,9 +372,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   static thread_local GatherPlan g;
   g.clear();
   struct FriPlan {
-    std::vector<size_t> pos;
-    std::vector<uint8_t> wit;  // 1: the position is a witness value
-    std::vector<size_t> wpos;  // the witness positions: only their values are gathered
+    size_t n_wit = 0;  // witness values (only theirs are gathered)
     size_t val_base = 0;
     MerkleDecommitPlan merkle;
   };
@@ -383,31 +381,30 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   static thread_local SharedWitness sw;
   sw.build(g, queries, lifting);
   // FRI layer i (the first layer is i = 0) is queried at S_i, its leaves
-  // decommitted as the pairs of S_i
+  // decommitted as the pairs of S_i. The position lists are scratch of this
+  // thread, reused from layer to layer: planning never waits, and a plan
+  // keeps only counts and offsets.
+  static thread_local std::vector<size_t> s_pos, s_wpos, s_lq, s_f;
+  static const std::vector<const uint32_t*> no_cols;
   auto plan_fri = [&](FriLayerDev& L, const std::vector<size_t>& q, size_t i, FriPlan& fp) -> int {
-    fri_positions(q, fp.pos, fp.wit);
-    fp.wpos.clear();
-    fp.wpos.reserve(fp.pos.size());
-    for (size_t k = 0; k < fp.pos.size(); k++)
-      if (fp.wit[k]) fp.wpos.push_back(fp.pos[k]);
-    std::vector<const uint32_t*> cols = {L.planes[0], L.planes[1], L.planes[2], L.planes[3]};
-    GS_TRY(g.add_cols(cols, fp.wpos, &fp.val_base));
-    if (L.layers.size() == (size_t)lifting - i + 1)
-      return fp.merkle.plan_shared(g, L.layers, cols, fp.pos, sw, (int)L.layers.size() - 3, i + 1, false);
-    return fp.merkle.plan(g, L.layers, cols, fp.pos, false);
+    const bool shared = L.layers.size() == (size_t)lifting - i + 1;
+    const size_t n_pos = fri_witness_positions(q, s_wpos, shared ? nullptr : &s_pos);
+    fp.n_wit = s_wpos.size();
+    const uint32_t* cols[4] = {L.planes[0], L.planes[1], L.planes[2], L.planes[3]};
+    GS_TRY(g.add_cols(cols, 4, s_wpos, &fp.val_base));
+    if (shared) return fp.merkle.plan_shared_hashes(g, L.layers, n_pos, sw, (int)L.layers.size() - 3, i + 1);
+    return fp.merkle.plan(g, L.layers, no_cols, s_pos, false);
   };
   FriPlan first_plan;
   GS_TRY(plan_fri(first, queries, 0, first_plan));
   std::vector<FriPlan> inner_plans(inner.size());
-  std::vector<size_t> lq = queries;
-  std::vector<size_t> f;
+  s_lq.assign(queries.begin(), queries.end());
   for (size_t i = 0; i < inner.size(); i++) {
-    f.clear();
-    f.reserve(lq.size());
-    for (size_t q : lq)
-      if (f.empty() || f.back() != (q >> 1)) f.push_back(q >> 1);
-    lq.swap(f);
-    GS_TRY(plan_fri(inner[i], lq, i + 1, inner_plans[i]));
+    s_f.clear();
+    for (size_t q : s_lq)
+      if (s_f.empty() || s_f.back() != (q >> 1)) s_f.push_back(q >> 1);
+    s_lq.swap(s_f);
+    GS_TRY(plan_fri(inner[i], s_lq, i + 1, inner_plans[i]));
   }
   pv.mark("fri_plans");
   std::vector<MerkleDecommitPlan> tree_plans(n_trees);
@@ -433,8 +430,8 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
   while ((1u << last_layer_log) < last.size()) last_layer_log++;
   auto fri_layer = [&](host::Writer& w, const FriPlan& fp, const FriLayerDev& L) {
     // the witness values (4 coordinates each), consecutive in the gather
-    w.u64(fp.wpos.size());
-    w.put_gathered(w.gathered ? go.word_out + fp.val_base : nullptr, 16 * fp.wpos.size());
+    w.u64(fp.n_wit);
+    w.put_gathered(w.gathered ? go.word_out + fp.val_base : nullptr, 16 * fp.n_wit);
     fp.merkle.write_decommitment(w, go);
     w.hash(L.root);
   };

@@ -156,8 +156,11 @@ struct GatherPlan {
   // Values of `cols` at `pos`, position-major; returns the first output word.
   // More than 4 columns must be equally spaced (one tree's columns are).
   int add_cols(const std::vector<const uint32_t*>& cols, const std::vector<size_t>& pos, size_t* first) {
+    return add_cols(cols.data(), cols.size(), pos, first);
+  }
+  int add_cols(const uint32_t* const* cols, size_t n_cols, const std::vector<size_t>& pos, size_t* first) {
     ColGather b{};
-    b.n_cols = (uint32_t)cols.size();
+    b.n_cols = (uint32_t)n_cols;
     b.n_pos = (uint32_t)pos.size();
     b.pos_off = positions.size();
     b.out_off = n_words;
@@ -268,7 +271,11 @@ struct MerkleDecommitPlan {
       size_t nw = 0, nn = 0, last_parent = ~(size_t)0;
       for (size_t i = 0; i < n; i++) {
         const size_t q = prev[i];
-        const bool sib = (q & 1) ? (i > 0 && prev[i - 1] == q - 1) : (i + 1 < n && prev[i + 1] == q + 1);
+        // the sibling q ^ 1 can only be the left (odd q) or the right (even q)
+        // neighbour in the sorted list: compare both, without a branch
+        const size_t left = i > 0 ? prev[i - 1] : ~(size_t)0;
+        const size_t right = i + 1 < n ? prev[i + 1] : ~(size_t)0;
+        const bool sib = (left == (q ^ 1)) | (right == (q ^ 1));
         w[nw] = (uint32_t)(q ^ 1);
         nw += sib ? 0 : 1;
         const size_t par = q >> 1;
@@ -292,6 +299,9 @@ struct MerkleDecommitPlan {
   int plan_shared(GatherPlan& g, const std::vector<uint32_t*>& layers, const std::vector<const uint32_t*>& cols,
                   const std::vector<size_t>& pos, const SharedWitness& sw, int top_L, size_t m0,
                   bool with_values = true);
+  // The hash witnesses alone, for n_positions leaf positions.
+  int plan_shared_hashes(GatherPlan& g, const std::vector<uint32_t*>& layers, size_t n_positions,
+                         const SharedWitness& sw, int top_L, size_t m0);
   // Serialised MerkleDecommitment (hash witnesses, no column witness) and
   // the queried values: gathered bytes, written by the writer's gathered pass.
   void write_decommitment(host::Writer& w, const GatherOut& g) const {
@@ -330,7 +340,11 @@ struct SharedWitness {
       size_t nw = 0, nn = 0, last_parent = ~(size_t)0;
       for (size_t i = 0; i < n; i++) {
         const size_t q = prev[i];
-        const bool sib = (q & 1) ? (i > 0 && prev[i - 1] == q - 1) : (i + 1 < n && prev[i + 1] == q + 1);
+        // the sibling q ^ 1 can only be the left (odd q) or the right (even q)
+        // neighbour in the sorted list: compare both, without a branch
+        const size_t left = i > 0 ? prev[i - 1] : ~(size_t)0;
+        const size_t right = i + 1 < n ? prev[i + 1] : ~(size_t)0;
+        const bool sib = (left == (q ^ 1)) | (right == (q ^ 1));
         w[nw] = (uint32_t)(q ^ 1);
         nw += sib ? 0 : 1;
         const size_t par = q >> 1;
@@ -350,11 +364,18 @@ struct SharedWitness {
 inline int MerkleDecommitPlan::plan_shared(GatherPlan& g, const std::vector<uint32_t*>& layers,
                                            const std::vector<const uint32_t*>& cols, const std::vector<size_t>& pos,
                                            const SharedWitness& sw, int top_L, size_t m0, bool with_values) {
+  if (with_values) GS_TRY(g.add_cols(cols, pos, &value_base));
+  GS_TRY(plan_shared_hashes(g, layers, pos.size(), sw, top_L, m0));
+  n_cols = with_values ? cols.size() : 0;
+  return OK;
+}
+
+inline int MerkleDecommitPlan::plan_shared_hashes(GatherPlan& g, const std::vector<uint32_t*>& layers,
+                                                  size_t n_pos, const SharedWitness& sw, int top_L, size_t m0) {
   GS_REQUIRE(top_L < (int)layers.size() - 1 && m0 + (size_t)(top_L + 1) <= sw.first.size(),
              "shared witness lists too short for the tree");
-  n_positions = pos.size();
-  n_cols = with_values ? cols.size() : 0;
-  if (with_values) GS_TRY(g.add_cols(cols, pos, &value_base));
+  n_positions = n_pos;
+  n_cols = 0;
   hash_begin = g.n_hashes();
   size_t m = m0;
   for (int L = top_L; L >= 0; L--, m++)
