@@ -211,7 +211,7 @@ int fri_commit(Prover& pv, uint32_t* quot[4], uint32_t lifting, FriLayerDev& fir
   if (dev_pow) GS_TRY(fri_last_layer_pow(st, d_last, cur.log, pv.cfg.log_last_layer, pv.cfg.pow_bits, ctl, ctl + pow_off));
   std::vector<uint32_t> hc(ctl_used);
   if (while_busy) while_busy();
-  GS_TRY(pv.ctx.read_back(ctl, hc.size() * 4, hc.data()));
+  GS_TRY(pv.ctx.read_back_published(ctl, hc.size() * 4, hc.data()));
   std::vector<uint32_t> h(hc.begin() + 16 + 16 * (size_t)n_roots, hc.begin() + pow_off);
   GS_REQUIRE(hc[9] == 0, "device channel: no challenge within the draw bound");
   if (dev_pow) {

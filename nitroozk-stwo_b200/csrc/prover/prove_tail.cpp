@@ -271,7 +271,7 @@ int prove_tail(Prover& pv, AirHost& air, uint32_t split, std::string* proof_byte
     d_qpoints = (const ptq*)d;
     d_qaccs = (QuotAcc*)((uint8_t*)d + o_acc);
     GS_TRY(pv.ctx.join_side());
-    GS_TRY(pv.ctx.read_back(d_vals, h.size() * 4, h.data()));
+    GS_TRY(pv.ctx.read_back_published(d_vals, h.size() * 4, h.data()));
   }
   // mixed tree by tree, column by column, point by point
   std::vector<qm31> flat;

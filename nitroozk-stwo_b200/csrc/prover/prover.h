@@ -226,9 +226,8 @@ struct GatherPlan {
                        d_out));
     GS_TRY(gather_hash_runs(st, (const HashRun*)(d_in + o_runs), (uint32_t)runs.size(),
                             (const uint32_t*)(d_in + o_idx), d_out + hbase));
-    void* hr = nullptr;
-    GS_TRY(ctx.read_buffer(out_words * 4, &hr));
-    if (out_words) GS_CUDA_TRY(cudaMemcpyAsync(hr, d_out, out_words * 4, cudaMemcpyDeviceToHost, st));
+    const void* hr = nullptr;
+    GS_TRY(ctx.publish(d_out, out_words * 4, &hr));
     out->word_out = (const uint32_t*)hr;
     out->hash_out = out->word_out + hbase;
     return OK;

@@ -153,6 +153,7 @@ void Context::destroy() {
   d_mail = nullptr;
   if (h_read) cudaFreeHost(h_read);
   h_read = nullptr;
+  d_read = nullptr;
   read_cap = 0;
   if (pool) cudaMemPoolDestroy(pool);  // released once its last allocation is freed
   pool = nullptr;
@@ -294,8 +295,52 @@ int Context::read_buffer(size_t bytes, void** out) {
     size_t cap = bytes < (1u << 20) ? (1u << 20) : bytes + bytes / 2;
     GS_CUDA_TRY(cudaMallocHost((void**)&h_read, cap));
     read_cap = cap;
+    d_read = nullptr;
+    void* dm = nullptr;
+    if (cudaHostGetDevicePointer(&dm, h_read, 0) == cudaSuccess) d_read = dm;
+    else cudaGetLastError();
   }
   *out = h_read;
+  return OK;
+}
+
+// Device words into mapped pinned memory: 16-byte stores where source and
+// destination allow, single words for the rest.
+__global__ void publish_kernel(const uint32_t* __restrict__ src, uint32_t* dst, size_t n_words) {
+  const size_t n16 = n_words / 4;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (size_t i = t0; i < n16; i += stride)
+    reinterpret_cast<uint4*>(dst)[i] = __ldg(reinterpret_cast<const uint4*>(src) + i);
+  for (size_t i = 4 * n16 + t0; i < n_words; i += stride) dst[i] = src[i];
+}
+
+int Context::publish(const void* d_src, size_t bytes, const void** host) {
+  GS_REQUIRE(bytes % 4 == 0, "published reads are whole words");
+  void* h = nullptr;
+  GS_TRY(read_buffer(bytes ? bytes : 4, &h));
+  if (bytes && d_read && ((uintptr_t)d_src & 15) == 0) {
+    const size_t n16 = bytes / 16;
+    size_t blocks = (n16 + 255) / 256;
+    const size_t cap = (size_t)num_sms() * 4;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    publish_kernel<<<(unsigned)blocks, 256, 0, stream>>>((const uint32_t*)d_src, (uint32_t*)d_read, bytes / 4);
+    note_launch();
+    GS_CUDA_TRY(cudaGetLastError());
+  } else if (bytes) {
+    GS_CUDA_TRY(cudaMemcpyAsync(h, d_src, bytes, cudaMemcpyDeviceToHost, stream));
+  }
+  *host = h;
+  return OK;
+}
+
+int Context::read_back_published(const void* d_src, size_t bytes, void* host_dst) {
+  if (bytes == 0) return OK;
+  const void* h = nullptr;
+  GS_TRY(publish(d_src, bytes, &h));
+  GS_TRY(stream_sync(stream));
+  memcpy(host_dst, h, bytes);
   return OK;
 }
 

@@ -156,10 +156,20 @@ struct Context {
   int mail_start(int slot, const void* d_src, size_t bytes);
   int mail_record(int slot);
   int mail_wait(int slot, const void** host);
-  // growable pinned host buffer for read-backs (decommitment values)
+  // growable pinned host buffer for read-backs (decommitment values), and
+  // its device alias (mapped pinned memory), or null
   uint8_t* h_read = nullptr;
+  void* d_read = nullptr;
   size_t read_cap = 0;
   int read_buffer(size_t bytes, void** out);
+  // Stores `bytes` (a multiple of 4) from device memory into the read
+  // buffer with a kernel on the context's stream (no copy-engine step
+  // between the producing kernels and the host), or with a copy where the
+  // buffer has no device alias; *host points to them once the stream has
+  // reached this point.
+  int publish(const void* d_src, size_t bytes, const void** host);
+  // read_back through publish: the same result.
+  int read_back_published(const void* d_src, size_t bytes, void* host_dst);
   // growable device scratch (stream ordered)
   void* scratch = nullptr;
   size_t scratch_cap = 0;
