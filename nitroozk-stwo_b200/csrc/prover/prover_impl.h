@@ -37,8 +37,11 @@ struct PhaseLog {
   std::vector<cudaEvent_t> ev;
   std::vector<std::chrono::steady_clock::time_point> host;
   void init(cudaStream_t s) {
-    const char* e = getenv("GS_PHASE_LOG");
-    on = e && e[0] == '1';
+    static const bool enabled = [] {  // read once per process
+      const char* e = getenv("GS_PHASE_LOG");
+      return e && e[0] == '1';
+    }();
+    on = enabled;
     st = s;
   }
   void mark(const char* name) {
