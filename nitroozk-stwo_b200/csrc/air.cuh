@@ -75,5 +75,10 @@ struct ColGather {
 };
 int gather_cols(cudaStream_t st, const ColGather* d_blocks, uint32_t n_blocks, uint32_t max_items,
                 const uint32_t* d_positions, uint32_t* d_out);
+// Both gathers in one launch: the column values to d_words, the hashes to
+// d_hashes (16-byte aligned). The outputs may be mapped host memory.
+int gather_all(cudaStream_t st, const ColGather* d_blocks, uint32_t n_blocks, uint32_t max_items,
+               const uint32_t* d_positions, uint32_t* d_words, const HashRun* d_runs, uint32_t n_runs,
+               const uint32_t* d_idx, uint32_t* d_hashes);
 
 }  // namespace gs

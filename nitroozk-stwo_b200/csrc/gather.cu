@@ -52,6 +52,48 @@ int gather_hash_runs(cudaStream_t st, const HashRun* d_runs, uint32_t n_runs, co
   return OK;
 }
 
+// The two gathers above in one grid: blocks [0, n_blocks * X) take the
+// column descriptors (X blocks each), the rest one hash run each.
+__global__ void __launch_bounds__(256) gather_all_kernel(const ColGather* __restrict__ blocks, uint32_t n_blocks,
+                                                         uint32_t X, const uint32_t* __restrict__ positions,
+                                                         uint32_t* words, const HashRun* __restrict__ runs,
+                                                         const uint32_t* __restrict__ idx, uint32_t* hashes) {
+  const uint32_t bid = blockIdx.x;
+  if (bid < n_blocks * X) {
+    const ColGather b = blocks[bid / X];
+    const uint32_t n = b.n_pos * b.n_cols;
+    for (uint32_t t = (bid % X) * blockDim.x + threadIdx.x; t < n; t += X * blockDim.x) {
+      const uint32_t p = t / b.n_cols, c = t - p * b.n_cols;
+      const uint32_t* src = b.n_cols <= 4 ? b.cols[c] : b.base + c * b.stride;
+      words[b.out_off + t] = __ldg(src + positions[b.pos_off + p]);
+    }
+    return;
+  }
+  const HashRun r = runs[bid - n_blocks * X];
+  for (uint32_t k = threadIdx.x; k < r.count; k += blockDim.x) {
+    const uint4* s = reinterpret_cast<const uint4*>(r.src + 8 * (size_t)__ldg(idx + (size_t)r.first + k));
+    uint4* o = reinterpret_cast<uint4*>(hashes + 8 * ((size_t)r.out + k));
+    o[0] = __ldg(s);
+    o[1] = __ldg(s + 1);
+  }
+}
+
+int gather_all(cudaStream_t st, const ColGather* d_blocks, uint32_t n_blocks, uint32_t max_items,
+               const uint32_t* d_positions, uint32_t* d_words, const HashRun* d_runs, uint32_t n_runs,
+               const uint32_t* d_idx, uint32_t* d_hashes) {
+  if (max_items == 0) n_blocks = 0;
+  const uint32_t X = n_blocks ? ((max_items + 255) / 256 < 64 ? (max_items + 255) / 256 : 64) : 0;
+  const uint64_t grid = (uint64_t)n_blocks * X + n_runs;
+  if (grid == 0) return OK;
+  GS_REQUIRE(grid <= 0x7fffffffu, "too many gather blocks");
+  GS_REQUIRE(n_runs == 0 || ((uintptr_t)d_hashes & 15) == 0, "hash gather output must be 16-byte aligned");
+  gather_all_kernel<<<(unsigned)grid, 256, 0, st>>>(d_blocks, n_blocks, X, d_positions, d_words, d_runs, d_idx,
+                                                    d_hashes);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  return OK;
+}
+
 // Column::batch_at_multi (crates/stwo/src/prover/backend/mod.rs:73-89):
 // out[i * n_cols + c] = cols[c][idx[i]], row-major over the indices.
 __global__ void gather_multi_kernel(const uint32_t* const* __restrict__ cols, uint32_t n_cols,

@@ -426,7 +426,10 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
   // kernel's upper levels, the interaction phase, the host's draws); the
   // composition joins it.
   const uint32_t n_trace = air.n_trace_cols();
-  GS_TRY(pv.commit_evals(trace, n_trace, T, nullptr, [&](Tree& t) { return pv.extend(t, E, n_trace, true); }));
+  // Wide-Fibonacci: the composition's preparation fills the trace root's wait
+  const std::function<int(Tree&)> prep = [&](Tree&) { return pv.prepare_composition(air); };
+  GS_TRY(pv.commit_evals(trace, n_trace, T, air.kind == AirKind::WideFibonacci ? prep : nullptr,
+                         [&](Tree& t) { return pv.extend(t, E, n_trace, true); }));
   pv.mark("trace_commit");
   if (air.kind == AirKind::Poseidon) {
     auto z = pv.ch.draw_felts(2);
@@ -446,7 +449,7 @@ int prove_component(Context& ctx, const ProveRequest& req, std::string* proof_by
     GS_TRY(poseidon_interaction(st, trace, T, air.lookup, inter, scratch, nullptr));
     GS_TRY(pv.ctx.mail_start(1, logup_claimed_sum_ptr(scratch, T), 16));
     pv.mark("interaction");
-    GS_TRY(pv.commit_evals(inter, 4, T, nullptr, [&](Tree& t) { return pv.extend(t, E, t.n_cols, true); }));
+    GS_TRY(pv.commit_evals(inter, 4, T, prep, [&](Tree& t) { return pv.extend(t, E, t.n_cols, true); }));
     const void* h = nullptr;
     GS_TRY(pv.ctx.mail_wait(1, &h));
     const uint32_t* cs = (const uint32_t*)h;

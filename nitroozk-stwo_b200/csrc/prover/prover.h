@@ -220,14 +220,20 @@ struct GatherPlan {
     // multiple of 4 words
     const size_t hbase = (n_words + 3) & ~(size_t)3;
     const size_t out_words = hbase + 8 * n_hash_out;
-    uint32_t* d_out = nullptr;
-    GS_TRY(A.alloc_n(out_words + 4, &d_out));
-    GS_TRY(gather_cols(st, (const ColGather*)d_in, (uint32_t)blocks.size(), max_items, (const uint32_t*)(d_in + o_pos),
-                       d_out));
-    GS_TRY(gather_hash_runs(st, (const HashRun*)(d_in + o_runs), (uint32_t)runs.size(),
-                            (const uint32_t*)(d_in + o_idx), d_out + hbase));
-    const void* hr = nullptr;
-    GS_TRY(ctx.publish(d_out, out_words * 4, &hr));
+    // one launch writes both gathers straight into the mapped read buffer
+    // (or into device memory, published after, where it has no alias)
+    void* hr = nullptr;
+    GS_TRY(ctx.read_buffer(out_words * 4 + 16, &hr));
+    uint32_t* d_out = (uint32_t*)ctx.d_read;
+    if (!d_out) GS_TRY(A.alloc_n(out_words + 4, &d_out));
+    GS_TRY(gather_all(st, (const ColGather*)d_in, (uint32_t)blocks.size(), max_items, (const uint32_t*)(d_in + o_pos),
+                      d_out, (const HashRun*)(d_in + o_runs), (uint32_t)runs.size(), (const uint32_t*)(d_in + o_idx),
+                      d_out + hbase));
+    if (!ctx.d_read) {
+      const void* h = nullptr;
+      GS_TRY(ctx.publish(d_out, out_words * 4, &h));
+      hr = (void*)h;
+    }
     out->word_out = (const uint32_t*)hr;
     out->hash_out = out->word_out + hbase;
     return OK;

@@ -227,28 +227,21 @@ struct Prover {
     return OK;
   }
 
-  // Composition polynomial coefficients (4 planes of 2^eval_log) for the component.
-  int composition(const AirHost& air, qm31 random_coeff, uint32_t* comp[4]) {
-    const uint32_t E = air.max_constraint_log(), T = air.log_n;
-    // trace columns on the evaluation domain
-    std::vector<const uint32_t*> on_domain(trees.size(), nullptr);
-    for (size_t t = 1; t < trees.size(); t++) {
-      Tree& tr = trees[t];
-      if (tr.eval_log == E) { on_domain[t] = tr.evals; continue; }
-      GS_TRY(extend(tr, E, tr.n_cols));  // the columns not extended earlier
-      on_domain[t] = tr.ext;
-    }
-    GS_TRY(ctx.join_side());
+  // What the composition needs before its random coefficient is drawn: the
+  // constraint denominators, the output planes and their pointer table.
+  // Called while the last trace root is read back; composition() calls it
+  // itself when nothing did.
+  struct CompositionPrep {
+    bool ready = false;
     ConstraintParams prm;
+    uint32_t* comp[4] = {nullptr, nullptr, nullptr, nullptr};
+    const uint32_t* const* ctab = nullptr;
+  } cprep;
+  int prepare_composition(const AirHost& air) {
+    if (cprep.ready) return OK;
+    const uint32_t E = air.max_constraint_log(), T = air.log_n;
+    ConstraintParams& prm = cprep.prm;
     memset(&prm, 0, sizeof(prm));
-    const uint32_t nc = air.n_constraints();
-    GS_REQUIRE(nc <= (uint32_t)MAX_CONSTRAINTS, "too many constraints");
-    qm31 pw = qm_one();
-    for (uint32_t k = 0; k < nc; k++) {  // constraint k gets alpha^(nc-1-k)
-      uint32_t* p = prm.powers + 4 * (nc - 1 - k);
-      p[0] = pw.x.a; p[1] = pw.x.b; p[2] = pw.y.a; p[3] = pw.y.b;
-      pw = qm_mul(pw, random_coeff);
-    }
     // denominators 1 / vanishing(CanonicCoset(T), eval_domain.at(i)), bit-reversed
     const uint32_t log_expand = E - T;
     GS_REQUIRE(log_expand <= 3, "constraint blowup above 8");
@@ -260,7 +253,36 @@ struct Prover {
       dn[i] = inv(host::canonic_vanishing_m31(T, host::index_point(idx)));
     }
     for (uint32_t i = 0; i < dn.size(); i++) prm.denom_inv[host::bitrev(i, log_expand)] = dn[i];
-    for (int c = 0; c < 4; c++) GS_TRY(A.alloc_n((size_t)1 << E, &comp[c]));
+    for (int c = 0; c < 4; c++) GS_TRY(A.alloc_n((size_t)1 << E, &cprep.comp[c]));
+    std::vector<const uint32_t*> cp = {cprep.comp[0], cprep.comp[1], cprep.comp[2], cprep.comp[3]};
+    GS_TRY(table(cp, &cprep.ctab));
+    cprep.ready = true;
+    return OK;
+  }
+
+  // Composition polynomial coefficients (4 planes of 2^eval_log) for the component.
+  int composition(const AirHost& air, qm31 random_coeff, uint32_t* comp[4]) {
+    const uint32_t E = air.max_constraint_log(), T = air.log_n;
+    GS_TRY(prepare_composition(air));
+    // trace columns on the evaluation domain
+    std::vector<const uint32_t*> on_domain(trees.size(), nullptr);
+    for (size_t t = 1; t < trees.size(); t++) {
+      Tree& tr = trees[t];
+      if (tr.eval_log == E) { on_domain[t] = tr.evals; continue; }
+      GS_TRY(extend(tr, E, tr.n_cols));  // the columns not extended earlier
+      on_domain[t] = tr.ext;
+    }
+    GS_TRY(ctx.join_side());
+    ConstraintParams& prm = cprep.prm;
+    const uint32_t nc = air.n_constraints();
+    GS_REQUIRE(nc <= (uint32_t)MAX_CONSTRAINTS, "too many constraints");
+    qm31 pw = qm_one();
+    for (uint32_t k = 0; k < nc; k++) {  // constraint k gets alpha^(nc-1-k)
+      uint32_t* p = prm.powers + 4 * (nc - 1 - k);
+      p[0] = pw.x.a; p[1] = pw.x.b; p[2] = pw.y.a; p[3] = pw.y.b;
+      pw = qm_mul(pw, random_coeff);
+    }
+    for (int c = 0; c < 4; c++) comp[c] = cprep.comp[c];
     Planes out{{comp[0], comp[1], comp[2], comp[3]}};
     if (air.kind == AirKind::WideFibonacci) {
       GS_TRY(wf_constraints(st, on_domain[1], air.n_cols, E, T, prm, out));
@@ -269,9 +291,7 @@ struct Prover {
       GS_TRY(poseidon_constraints(st, on_domain[1], on_domain[2], E, T, prm, air.lookup, shift, out));
     }
     // finalize: interpolate the 4 coordinates on CanonicCoset(E)
-    std::vector<const uint32_t*> cp = {comp[0], comp[1], comp[2], comp[3]};
-    const uint32_t* const* ctab = nullptr;
-    GS_TRY(table(cp, &ctab));
+    const uint32_t* const* ctab = cprep.ctab;
     GS_TRY(interpolate_columns(st, (uint32_t* const*)ctab, 4, E, itw, tw_log));
     return OK;
   }
