@@ -31,27 +31,31 @@ def pcs_config(pow_bits=10, log_blowup=1, log_last_layer=0, n_queries=70, line_f
     return L.PcsConfig(pow_bits, log_blowup, log_last_layer, n_queries, line_fold_step)
 
 
+_DEFAULT_CONFIG = pcs_config()  # read-only for the prover; shared by calls without a config
+
+
 _tls = threading.local()
 
 
 def _buffer(capacity):
     """Per-thread output buffer, reused across proofs (a fresh multi-MB buffer
-    per call would cost its page faults every time)."""
+    per call would cost its page faults every time), with its address."""
     buf = getattr(_tls, "buf", None)
     if buf is None or len(buf) < capacity:
         buf = (C.c_uint8 * capacity)()
         _tls.buf = buf
-    return buf
+        _tls.addr = C.addressof(buf)
+    return buf, _tls.addr
 
 
 def _run(fn, args, ctx, capacity):
     n = C.c_size_t()
-    buf = _buffer(capacity)
+    buf, addr = _buffer(capacity)
     capacity = len(buf)
-    st = fn(*args, C.cast(buf, C.c_void_p), capacity, C.byref(n))
+    st = fn(*args, addr, capacity, C.byref(n))
     if st == 1 and n.value > capacity:  # retry with the exact size
-        buf = _buffer(n.value)
-        st = fn(*args, C.cast(buf, C.c_void_p), len(buf), C.byref(n))
+        buf, addr = _buffer(n.value)
+        st = fn(*args, addr, len(buf), C.byref(n))
     if st == GS_ERR_PROOF:
         raise ConstraintsNotSatisfied(L.lib().gs_last_error().decode())
     L.check(st, fn.__name__)
@@ -77,7 +81,7 @@ def prove_wide_fibonacci(log_n_rows, n_columns=100, seed=0, input_mode=INPUT_REF
     merkle_channel: 'blake2s' (Blake2sMerkleChannel) or 'poseidon252'."""
     ctx = ctx or default_context()
     keep, ptr = _inputs(host_inputs)
-    cfg = config or pcs_config()
+    cfg = config or _DEFAULT_CONFIG
     return _run(_entry("gs_prove_wide_fibonacci", merkle_channel),
                 (ctx.handle, log_n_rows, n_columns, seed, input_mode, ptr, C.byref(cfg)), ctx, capacity)
 
@@ -88,7 +92,7 @@ def prove_poseidon(log_n_instances, seed=0, input_mode=INPUT_REFERENCE, host_inp
     merkle_channel: 'blake2s' (Blake2sMerkleChannel) or 'poseidon252'."""
     ctx = ctx or default_context()
     keep, ptr = _inputs(host_inputs)
-    cfg = config or pcs_config()
+    cfg = config or _DEFAULT_CONFIG
     return _run(_entry("gs_prove_poseidon", merkle_channel),
                 (ctx.handle, log_n_instances, seed, input_mode, ptr, composition_log_split, C.byref(cfg)), ctx,
                 capacity)
