@@ -954,6 +954,94 @@ def proof_timeline(air, log_n, reps):
                     "kernels_per_proof": round(sum(r[3] for r in rows) / n, 1)}))
 
 
+def fft_worklist_case(n_items, min_log, max_log, args):
+    """Many FFTs of uneven sizes: n_items columns of log sizes uniform in
+    [min_log, max_log], half interpolated in place, half evaluated with blowup
+    1 (coefficients of log - 1), timed three ways on one stream with CUDA
+    events (device time of the whole sequence, host launch costs included):
+    one gs_fft_worklist call; one gs_interpolate_columns / gs_evaluate_columns
+    call per size group; one call per column. Prints one JSON line."""
+    import torch
+    from gpustark import lib as gslib
+    from gpustark.backend import GpuBackend as B, Context
+    rng = np.random.default_rng(11)
+    ctx = Context(torch.cuda.current_stream())
+    tw = B.precompute_twiddles(max_log, ctx=ctx)
+    items = []
+    for k in range(n_items):
+        log = int(rng.integers(min_log, max_log + 1))
+        if k % 2 == 0:
+            x = torch.from_numpy(rng.integers(0, P, 1 << log, dtype=np.int64).astype(np.int32)).cuda()
+            items.append(("interpolate", x, x))
+        else:
+            c = torch.from_numpy(rng.integers(0, P, 1 << (log - 1), dtype=np.int64).astype(np.int32)).cuda()
+            items.append(("evaluate", c, torch.empty(1 << log, dtype=torch.int32, device="cuda")))
+    groups = {}
+    for kind, s, d in items:
+        groups.setdefault((kind, s.numel(), d.numel()), []).append((s, d))
+    # every argument array is built once, outside the timed loops: the three
+    # forms differ in their launches, not in Python-side preparation
+    import ctypes as C
+    from gpustark import _lib as L
+    lib = gslib()
+    arr = (L.FftItem * n_items)()
+    for k, (kind, s, d) in enumerate(items):
+        arr[k].src, arr[k].dst = s.data_ptr(), d.data_ptr()
+        arr[k].log_size = d.numel().bit_length() - 1
+        arr[k].coeffs_log_size = s.numel().bit_length() - 1
+        arr[k].inverse = 1 if kind == "interpolate" else 0
+    twp, itwp = C.c_void_p(tw.twiddles.data_ptr()), C.c_void_p(tw.itwiddles.data_ptr())
+    calls_group = []
+    for (kind, ns, nd), cols in groups.items():
+        dp, kd = L.ptr_array([d.data_ptr() for _, d in cols])
+        if kind == "interpolate":
+            calls_group.append((lib.gs_interpolate_columns, (ctx.handle, dp, len(cols), nd.bit_length() - 1, itwp,
+                                                             tw.root_log), kd))
+        else:
+            sp, ks = L.ptr_array([s.data_ptr() for s, _ in cols])
+            calls_group.append((lib.gs_evaluate_columns, (ctx.handle, sp, ns.bit_length() - 1, dp, len(cols),
+                                                          nd.bit_length() - 1, twp, tw.root_log), (kd, ks)))
+    calls_col = []
+    for kind, s, d in items:
+        dp, kd = L.ptr_array([d.data_ptr()])
+        if kind == "interpolate":
+            calls_col.append((lib.gs_interpolate_columns, (ctx.handle, dp, 1, d.numel().bit_length() - 1, itwp,
+                                                           tw.root_log), kd))
+        else:
+            sp, ks = L.ptr_array([s.data_ptr()])
+            calls_col.append((lib.gs_evaluate_columns, (ctx.handle, sp, s.numel().bit_length() - 1, dp, 1,
+                                                        d.numel().bit_length() - 1, twp, tw.root_log), (kd, ks)))
+
+    def worklist():
+        L.check(lib.gs_fft_worklist(ctx.handle, arr, n_items, twp, itwp, tw.root_log), "fft_worklist")
+
+    def per_size():
+        for f, a, _ in calls_group:
+            L.check(f(*a), "fft")
+
+    def per_column():
+        for f, a, _ in calls_col:
+            L.check(f(*a), "fft")
+
+    res = {}
+    for name, fn in (("worklist", worklist), ("per_size_group", per_size), ("per_column", per_column)):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        l0 = gslib().gs_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        res[name] = {"us": round(1e3 * e0.elapsed_time(e1) / args.steps, 1),
+                     "launches": (gslib().gs_launch_count() - l0) // args.steps}
+    words = sum(d.numel() for _, _, d in items)
+    print(json.dumps({"case": "fft_worklist", "items": n_items, "logs": [min_log, max_log],
+                      "size_groups": len(groups), "output_words": words, **res}))
+
+
 def run_case(args):
     """One op on a small case, for ncu captures: `--case fft:26`, `--case lde:18:162:2` (extension
     of 162 columns from 2^18 to 2^20), `--case merkle:20:64`, `--case fold:22`, `--case p252:18:8`
@@ -964,6 +1052,9 @@ def run_case(args):
     kind, *params = args.case.split(":")
     if kind == "timeline":
         proof_timeline(params[0], int(params[1]), max(2, args.steps))
+        return
+    if kind == "fftwl":
+        fft_worklist_case(int(params[0]), int(params[1]), int(params[2]), args)
         return
     rng = np.random.default_rng(7)
     ctx = Context(torch.cuda.current_stream())
@@ -1026,7 +1117,9 @@ def main():
     ap.add_argument("--fft-autotune", default="on", choices=["on", "off"],
                     help="time the FFT pass splits per log size before warm-up and install the fastest")
     ap.add_argument("--case", default=None,
-                    help="profiling case: fft:<log>, lde:<log>:<cols>[:<ext>], merkle:<log>:<cols>, fold:<log> (one op, no JSON contract)")
+                    help="profiling case: fft:<log>, lde:<log>:<cols>[:<ext>], merkle:<log>:<cols>, fold:<log> (one op, "
+                         "no JSON contract); fftwl:<items>:<min_log>:<max_log> times the FFT work-list against "
+                         "per-size and per-column calls")
     args = ap.parse_args()
     if args.case:
         run_case(args)

@@ -94,6 +94,26 @@ int gs_interpolate_columns(gs_ctx* ctx, uint32_t* const* cols, uint32_t n_cols, 
  * evals (distinct buffers of 2^log_size words). */
 int gs_evaluate_columns(gs_ctx* ctx, const uint32_t* const* coeffs, uint32_t coeffs_log_size, uint32_t* const* evals,
                         uint32_t n_cols, uint32_t log_size, const uint32_t* twiddles, uint32_t twiddles_log_size);
+/* Batched FFTs of uneven sizes (the reference launches ntt_b2n_column /
+ * ntt_n2b_columns once per size group, cuda/poly.rs:179-294, 409-552; this
+ * entry has no single reference counterpart): item k interpolates
+ * (inverse = 1) the 2^log_size bit-reversed evaluations at src into
+ * coefficients at dst (src == dst: in place), or evaluates (inverse = 0) the
+ * 2^coeffs_log_size coefficients at src on CanonicCoset(log_size) into dst
+ * (distinct buffers). Every item of log size 3..13 runs in ONE launch of a
+ * persistent grid that walks the list, largest first, each FFT whole in
+ * shared memory; other sizes take the per-size path of gs_interpolate_columns
+ * / gs_evaluate_columns. Results equal those entries' bit for bit. Items must
+ * not overlap one another. itwiddles / twiddles: the trees of
+ * half_odds(twiddles_log_size), twiddles_log_size + 1 >= every log_size (a
+ * tree may be NULL when no item needs it). */
+typedef struct {
+  const uint32_t* src;
+  uint32_t* dst;
+  uint32_t log_size, coeffs_log_size, inverse, reserved;
+} gs_fft_item;
+int gs_fft_worklist(gs_ctx* ctx, const gs_fft_item* items, uint32_t n_items, const uint32_t* twiddles,
+                    const uint32_t* itwiddles, uint32_t twiddles_log_size);
 
 /* FFT pass-split tuning. No counterpart in the reference, whose CUDA FFT
  * (ntt.cu) has one fixed geometry. An FFT that computes n layers runs in

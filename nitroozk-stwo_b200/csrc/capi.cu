@@ -144,6 +144,26 @@ int gs_interpolate_columns(gs_ctx* ctx, uint32_t* const* cols, uint32_t n_cols, 
   return interpolate_columns(ctx->c.stream, (uint32_t* const*)d, n_cols, log_size, itwiddles, twiddles_log_size);
 }
 
+int gs_fft_worklist(gs_ctx* ctx, const gs_fft_item* items, uint32_t n_items, const uint32_t* twiddles,
+                    const uint32_t* itwiddles, uint32_t twiddles_log_size) {
+  CTX_REQUIRED(ctx);
+  if (n_items == 0) return OK;
+  GS_REQUIRE(items != nullptr, "null item list");
+  static_assert(sizeof(gs_fft_item) == sizeof(FftItem) && offsetof(gs_fft_item, log_size) == offsetof(FftItem, log) &&
+                    offsetof(gs_fft_item, inverse) == offsetof(FftItem, inverse),
+                "gs_fft_item and FftItem differ");
+  bool aligned = true;  // the per-size path's vector access, for the items that take it
+  for (uint32_t k = 0; k < n_items; k++) {
+    const gs_fft_item& x = items[k];
+    GS_REQUIRE(x.inverse <= 1, "inverse must be 0 or 1");
+    GS_REQUIRE(x.inverse || x.src != x.dst, "an evaluation needs distinct source and destination");
+    aligned = aligned && (((uintptr_t)x.src & 15) == 0) && (((uintptr_t)x.dst & 15) == 0);
+  }
+  fft_set_columns_aligned(aligned);
+  // the same fields in the same order (checked above)
+  return fft_worklist(ctx->c, reinterpret_cast<const FftItem*>(items), n_items, twiddles, itwiddles, twiddles_log_size);
+}
+
 int gs_evaluate_columns(gs_ctx* ctx, const uint32_t* const* coeffs, uint32_t coeffs_log_size, uint32_t* const* evals,
                         uint32_t n_cols, uint32_t log_size, const uint32_t* twiddles, uint32_t twiddles_log_size) {
   CTX_REQUIRED(ctx);

@@ -28,6 +28,7 @@
 // are computed — no zero-extension pass.
 #include "runtime.cuh"
 #include <algorithm>
+#include <vector>
 #include <iterator>
 #include <cstdlib>
 
@@ -596,6 +597,131 @@ int evaluate_columns(cudaStream_t st, const uint32_t* const* d_src, uint32_t coe
   if (log_n <= 2) return launch_small(st, d_src, d_dst, n_cols, log_n, false, src_mask);
   GS_REQUIRE(tw_log + 1 >= log_n, "twiddle tree too small for the domain");
   return run_passes<false>(st, d_src, d_dst, n_cols, log_n, coeff_log, src_mask, d_twiddles, 1u << tw_log);
+}
+
+// ------------------------------------------------------------- work-list
+// Device form of an item: the host adds the 1/2^log scale of an
+// interpolation.
+struct FftWlItem {
+  const uint32_t* src;
+  uint32_t* dst;
+  uint32_t log, coeff_log, inverse, scale;
+};
+
+// Persistent grid: block b takes items b, b + gridDim.x, ... of a list sorted
+// by decreasing size, so the large items start first. Each item runs whole in
+// shared memory: load (an evaluation replicates its 2^coeff_log
+// coefficients over the domain, the top layers of the zero-padded FFT being
+// copies), the layers with the twiddle rule of the pass kernels (line layer
+// i >= 1: tw[tw_len - 2^(log - i) + h]; circle layer 0: circle_twiddle), one
+// block barrier per layer, then the store (scaled for an interpolation).
+__global__ void __launch_bounds__(256) fft_worklist_kernel(const FftWlItem* __restrict__ items, uint32_t n_items,
+                                                           const uint32_t* __restrict__ tw,
+                                                           const uint32_t* __restrict__ itw, uint32_t tw_len) {
+  extern __shared__ uint32_t sm[];
+  for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const FftWlItem w = items[it];
+    const uint32_t n = w.log, N = 1u << n;
+    const uint32_t cmask = w.inverse ? N - 1u : (1u << w.coeff_log) - 1u;
+    for (uint32_t v = threadIdx.x; v < N; v += blockDim.x) sm[v] = __ldg(w.src + (v & cmask));
+    __syncthreads();
+    const uint32_t* t = w.inverse ? itw : tw;
+    const uint32_t layers = w.inverse ? n : w.coeff_log;
+    for (uint32_t k = 0; k < layers; k++) {
+      const uint32_t i = w.inverse ? k : layers - 1 - k;
+      for (uint32_t j = threadIdx.x; j < N / 2; j += blockDim.x) {
+        const uint32_t h = j >> i;
+        const uint32_t v = (h << (i + 1)) | (j & ((1u << i) - 1u));
+        const uint32_t u = v + (1u << i);
+        const uint32_t tw_h = i == 0 ? circle_twiddle(t, tw_len, n, h) : __ldg(t + tw_len - (1u << (n - i)) + h);
+        const uint32_t a = sm[v], b = sm[u];
+        if (w.inverse) {
+          sm[v] = add(a, b);
+          sm[u] = mul(sub(a, b), tw_h);
+        } else {
+          const uint32_t p = mul(b, tw_h);
+          sm[v] = add(a, p);
+          sm[u] = sub(a, p);
+        }
+      }
+      __syncthreads();
+    }
+    for (uint32_t v = threadIdx.x; v < N; v += blockDim.x) w.dst[v] = w.inverse ? mul(sm[v], w.scale) : sm[v];
+    __syncthreads();  // the next item reuses the shared buffer
+  }
+}
+
+int fft_worklist(Context& ctx, const FftItem* items, uint32_t n_items, const uint32_t* d_twiddles,
+                 const uint32_t* d_itwiddles, uint32_t tw_log) {
+  if (n_items == 0) return OK;
+  GS_REQUIRE(items != nullptr, "null item list");
+  GS_REQUIRE(tw_log <= 30, "twiddle log size out of range");
+  cudaStream_t st = ctx.stream;
+  // 1/2^log for every log, once; the items bucketed by size, largest first
+  static const std::vector<uint32_t> inv_pow2 = [] {
+    std::vector<uint32_t> t(31);
+    for (uint32_t k = 0; k <= 30; k++) t[k] = inv(1u << k);
+    return t;
+  }();
+  uint32_t count[FFT_WL_MAX_LOG + 1] = {0};
+  for (uint32_t k = 0; k < n_items; k++) {
+    const FftItem& x = items[k];
+    GS_REQUIRE(x.src && x.dst, "null column in a work-list item");
+    GS_REQUIRE(x.log >= 1 && x.log <= 30 && tw_log + 1 >= x.log, "work-list item size out of range");
+    GS_REQUIRE(x.inverse || (x.coeff_log >= 1 && x.coeff_log <= x.log), "coefficient log size must be in [1, log]");
+    GS_REQUIRE(x.inverse ? d_itwiddles != nullptr : d_twiddles != nullptr, "null twiddle tree");
+    if (x.log >= FFT_WL_MIN_LOG && x.log <= FFT_WL_MAX_LOG) count[x.log]++;
+  }
+  uint32_t first[FFT_WL_MAX_LOG + 2] = {0}, total = 0;
+  for (int lg = (int)FFT_WL_MAX_LOG; lg >= (int)FFT_WL_MIN_LOG; lg--) {
+    first[lg] = total;
+    total += count[lg];
+  }
+  std::vector<FftWlItem> wl(total);
+  for (uint32_t k = 0; k < n_items; k++) {
+    const FftItem& x = items[k];
+    if (x.log < FFT_WL_MIN_LOG || x.log > FFT_WL_MAX_LOG) continue;
+    wl[first[x.log]++] = FftWlItem{x.src, x.dst, x.log, x.inverse ? x.log : x.coeff_log, x.inverse ? 1u : 0u,
+                                   x.inverse ? inv_pow2[x.log] : 1u};
+  }
+  // the items outside the shared-memory range, one call each
+  for (uint32_t k = 0; k < n_items; k++) {
+    const FftItem& x = items[k];
+    if (x.log >= FFT_WL_MIN_LOG && x.log <= FFT_WL_MAX_LOG) continue;
+    const void* const* ts = nullptr;
+    const void* const* td = nullptr;
+    GS_TRY(ctx.stage_ptrs((const void* const*)&x.src, 1, &ts));
+    GS_TRY(ctx.stage_ptrs((const void* const*)&x.dst, 1, &td));
+    if (x.inverse)
+      GS_TRY(interpolate_columns_to(st, (const uint32_t* const*)ts, (uint32_t* const*)td, 1, x.log, d_itwiddles,
+                                    tw_log));
+    else
+      GS_TRY(evaluate_columns(st, (const uint32_t* const*)ts, x.coeff_log, (uint32_t* const*)td, 1, x.log,
+                              d_twiddles, tw_log));
+  }
+  if (wl.empty()) return OK;
+  const void* d = nullptr;
+  void* owned = nullptr;  // a list too long for the staging ring: a buffer of its own
+  const size_t bytes = wl.size() * sizeof(FftWlItem);
+  if (bytes <= ctx.ring_cap / 2) {
+    GS_TRY(ctx.stage_bytes(wl.data(), bytes, &d));
+  } else {
+    GS_TRY(ctx.alloc_async(bytes, &owned));
+    GS_CUDA_TRY(cudaMemcpyAsync(owned, wl.data(), bytes, cudaMemcpyHostToDevice, st));
+    d = owned;
+  }
+  const size_t smem = (size_t)4 << wl.front().log;
+  static const cudaError_t attr = cudaFuncSetAttribute(fft_worklist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       4 << FFT_WL_MAX_LOG);
+  GS_CUDA_TRY(attr);
+  const uint32_t per_sm = (uint32_t)std::min<size_t>(8, (200u << 10) / smem);
+  const uint32_t grid = (uint32_t)std::min<size_t>(wl.size(), (size_t)num_sms() * (per_sm ? per_sm : 1));
+  fft_worklist_kernel<<<grid, 256, smem, st>>>((const FftWlItem*)d, (uint32_t)wl.size(), d_twiddles, d_itwiddles,
+                                               1u << tw_log);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  if (owned) GS_CUDA_TRY(cudaFreeAsync(owned, st));  // stream-ordered: after the kernel
+  return OK;
 }
 
 // Installs the tuning for FFTs computing `layers` layers (0: every size) on

@@ -203,6 +203,22 @@ int batch_inverse(cudaStream_t st, const uint32_t* d_in, uint32_t* d_out, size_t
 // fft.cu (columns given by a device table of pointers)
 int interpolate_columns(cudaStream_t st, uint32_t* const* d_cols, uint32_t n_cols, uint32_t log_n,
                         const uint32_t* d_itwiddles, uint32_t tw_log);
+// One FFT of a work-list: interpolate (inverse != 0) 2^log evaluations, or
+// evaluate 2^coeff_log coefficients on the domain of 2^log; src and dst are
+// device columns (the same column for an in-place interpolation).
+struct FftItem {
+  const uint32_t* src;
+  uint32_t* dst;
+  uint32_t log, coeff_log, inverse, pad;
+};
+constexpr uint32_t FFT_WL_MIN_LOG = 3, FFT_WL_MAX_LOG = 13;
+// Many FFTs of uneven sizes: every item of log size in [FFT_WL_MIN_LOG,
+// FFT_WL_MAX_LOG] in one launch of a persistent grid whose blocks walk the
+// list (largest first), each item whole in shared memory; the others through
+// interpolate_columns / evaluate_columns, one call each. Twiddle trees as for
+// those (tw_log + 1 >= every log).
+int fft_worklist(Context& ctx, const FftItem* items, uint32_t n_items, const uint32_t* d_twiddles,
+                 const uint32_t* d_itwiddles, uint32_t tw_log);
 int evaluate_columns(cudaStream_t st, const uint32_t* const* d_src, uint32_t coeff_log, uint32_t* const* d_dst,
                      uint32_t n_cols, uint32_t log_n, const uint32_t* d_twiddles, uint32_t tw_log);
 int bit_reverse(cudaStream_t st, uint32_t* d, uint32_t log_n);

@@ -32,6 +32,12 @@ class PcsConfig(C.Structure):
                 ("line_fold_step", C.c_uint32)]
 
 
+class FftItem(C.Structure):
+    """gs_fft_item: one FFT of a work-list (include/gpustark.h)."""
+    _fields_ = [("src", C.c_void_p), ("dst", C.c_void_p), ("log_size", C.c_uint32), ("coeffs_log_size", C.c_uint32),
+                ("inverse", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class GpuStarkError(RuntimeError):
     pass
 
@@ -55,6 +61,7 @@ _PROTOS = {
     "gs_precompute_twiddles": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p],
     "gs_interpolate_columns": [C.c_void_p, VPP, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32],
     "gs_evaluate_columns": [C.c_void_p, VPP, C.c_uint32, VPP, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32],
+    "gs_fft_worklist": [C.c_void_p, C.POINTER(FftItem), C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32],
     "gs_fft_autotune": [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, U32P, U32P],
     "gs_fft_set_tuning": [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32],
     "gs_fft_get_tuning": [C.c_uint32, C.c_uint32, U32P, U32P],

@@ -133,6 +133,25 @@ class GpuBackend:
                                             _p(twiddles.twiddles), twiddles.root_log), "evaluate_polynomials")
         return out
 
+    @staticmethod
+    def fft_worklist(items, twiddles: TwiddleTree, ctx=None):
+        """Many FFTs of uneven sizes in one launch (gs_fft_worklist). items:
+        tuples ("interpolate", src, dst) with src and dst 2^log-word tensors
+        (src is dst: in place) or ("evaluate", coeffs, dst) with dst of
+        2^log words; returns the dst tensors."""
+        ctx = ctx or default_context()
+        arr = (L.FftItem * max(len(items), 1))()
+        for k, (kind, src, dst) in enumerate(items):
+            if kind not in ("interpolate", "evaluate"):
+                raise ValueError(f"unknown work-list item kind {kind!r}")
+            arr[k].src, arr[k].dst = src.data_ptr(), dst.data_ptr()
+            arr[k].log_size = dst.numel().bit_length() - 1
+            arr[k].coeffs_log_size = src.numel().bit_length() - 1
+            arr[k].inverse = 1 if kind == "interpolate" else 0
+        L.check(L.lib().gs_fft_worklist(ctx.handle, arr, len(items), _p(twiddles.twiddles), _p(twiddles.itwiddles),
+                                        twiddles.root_log), "fft_worklist")
+        return [dst for _, _, dst in items]
+
     ALL_EXTENSIONS = 0xFFFFFFFF
 
     @staticmethod
