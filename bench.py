@@ -1042,6 +1042,60 @@ def fft_worklist_case(n_items, min_log, max_log, args):
                       "size_groups": len(groups), "output_words": words, **res}))
 
 
+def merkle_worklist_case(n_trees, min_log, max_log, n_cols, args):
+    """Many small Merkle trees: n_trees trees of n_cols columns, log sizes
+    uniform in [min_log, max_log], built (leaves and every node layer) by one
+    gs_merkle_worklist call, against one gs_commit_on_layer +
+    gs_commit_node_layers pair per tree (the per-tree path). CUDA events
+    around the whole sequence, argument arrays built outside the timed loop;
+    one JSON line."""
+    import ctypes as C
+    import torch
+    from gpustark import lib as gslib
+    from gpustark import _lib as L
+    from gpustark.backend import Context
+    rng = np.random.default_rng(13)
+    ctx = Context(torch.cuda.current_stream())
+    lib = gslib()
+    arr = (L.MerkleItem * n_trees)()
+    keep, per_tree = [], []
+    for k in range(n_trees):
+        log = int(rng.integers(min_log, max_log + 1))
+        cols = torch.from_numpy(rng.integers(0, P, (n_cols, 1 << log), dtype=np.int64).astype(np.int32)).cuda()
+        layers = [torch.empty((1 << lg) * 8, dtype=torch.int32, device="cuda") for lg in range(log + 1)]
+        cp, kc = L.ptr_array([cols[i].data_ptr() for i in range(n_cols)])
+        lp, kl = L.ptr_array([t.data_ptr() for t in layers])
+        keep += [cols, layers, kc, kl]
+        arr[k].cols, arr[k].n_cols, arr[k].log_size, arr[k].layers = cp, n_cols, log, lp
+        per_tree.append((log, cp, C.c_void_p(layers[log].data_ptr()), lp))
+
+    def worklist():
+        L.check(lib.gs_merkle_worklist(ctx.handle, arr, n_trees), "merkle_worklist")
+
+    def per_tree_calls():
+        for log, cp, leaf, lp in per_tree:
+            L.check(lib.gs_commit_on_layer(ctx.handle, log, None, n_cols, cp, leaf), "commit_on_layer")
+            if log:
+                L.check(lib.gs_commit_node_layers(ctx.handle, log, lp), "commit_node_layers")
+
+    res = {}
+    for name, fn in (("worklist", worklist), ("per_tree", per_tree_calls)):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        l0 = lib.gs_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        res[name] = {"us": round(1e3 * e0.elapsed_time(e1) / args.steps, 1),
+                     "launches": (lib.gs_launch_count() - l0) // args.steps}
+    print(json.dumps({"case": "merkle_worklist", "trees": n_trees, "logs": [min_log, max_log], "columns": n_cols,
+                      **res}))
+
+
 def run_case(args):
     """One op on a small case, for ncu captures: `--case fft:26`, `--case lde:18:162:2` (extension
     of 162 columns from 2^18 to 2^20), `--case merkle:20:64`, `--case fold:22`, `--case p252:18:8`
@@ -1055,6 +1109,9 @@ def run_case(args):
         return
     if kind == "fftwl":
         fft_worklist_case(int(params[0]), int(params[1]), int(params[2]), args)
+        return
+    if kind == "merklewl":
+        merkle_worklist_case(int(params[0]), int(params[1]), int(params[2]), int(params[3]), args)
         return
     rng = np.random.default_rng(7)
     ctx = Context(torch.cuda.current_stream())
@@ -1119,7 +1176,8 @@ def main():
     ap.add_argument("--case", default=None,
                     help="profiling case: fft:<log>, lde:<log>:<cols>[:<ext>], merkle:<log>:<cols>, fold:<log> (one op, "
                          "no JSON contract); fftwl:<items>:<min_log>:<max_log> times the FFT work-list against "
-                         "per-size and per-column calls")
+                         "per-size and per-column calls; merklewl:<trees>:<min_log>:<max_log>:<cols> the Merkle "
+                         "work-list against per-tree calls")
     args = ap.parse_args()
     if args.case:
         run_case(args)

@@ -171,6 +171,23 @@ int gs_poseidon252_grind(gs_ctx* ctx, const uint8_t digest[32], uint32_t pow_bit
  * host array of top_log + 1 device buffers, layers[L] holding 2^L hashes;
  * layers[top_log] is the input, all smaller layers are written. */
 int gs_commit_node_layers(gs_ctx* ctx, uint32_t top_log, uint32_t* const* layers);
+/* Whole Merkle trees of uneven sizes, many at once (the reference commits one
+ * tree at a time through commit_on_first_layer / commit_on_layer_with_previous,
+ * bindings.rs:262-275, driven by MerkleProver::commit, prover/vcs/prover.rs:
+ * 39-48; this entry has no single reference counterpart). Tree k hashes its
+ * n_cols >= 1 columns of 2^log_size words into the leaf layer and every node
+ * layer above it: cols and layers are host arrays of device pointers,
+ * layers[L] holding 2^L hashes (16-byte aligned) for L = 0..log_size. Every
+ * tree of log size <= 10 is built in ONE launch of a persistent grid that
+ * walks the list, largest first, each tree in one block through shared
+ * memory; larger trees take gs_commit_on_layer + gs_commit_node_layers.
+ * Results equal those entries' byte for byte. Trees must not share layers. */
+typedef struct {
+  const uint32_t* const* cols;
+  uint32_t n_cols, log_size;
+  uint32_t* const* layers;
+} gs_merkle_item;
+int gs_merkle_worklist(gs_ctx* ctx, const gs_merkle_item* items, uint32_t n_items);
 
 /* MerkleOpsLifted::build_leaves (prover/vcs_lifted/ops.rs:8-18; CPU
  * prover/backend/cpu/merkle_lifted.rs:12-77; reference CUDA blake2s.cu:

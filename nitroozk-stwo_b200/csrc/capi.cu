@@ -218,6 +218,16 @@ int gs_commit_on_layer(gs_ctx* ctx, uint32_t log_size, const uint32_t* prev_laye
   return commit_on_layer(ctx->c.stream, log_size, prev_layer, (const uint32_t* const*)d, n_cols, out);
 }
 
+int gs_merkle_worklist(gs_ctx* ctx, const gs_merkle_item* items, uint32_t n_items) {
+  CTX_REQUIRED(ctx);
+  if (n_items == 0) return OK;
+  GS_REQUIRE(items != nullptr, "null tree list");
+  static_assert(sizeof(gs_merkle_item) == sizeof(MerkleItem) && offsetof(gs_merkle_item, n_cols) == offsetof(MerkleItem, n_cols) &&
+                    offsetof(gs_merkle_item, layers) == offsetof(MerkleItem, layers),
+                "gs_merkle_item and MerkleItem differ");
+  return merkle_worklist(ctx->c, reinterpret_cast<const MerkleItem*>(items), n_items);
+}
+
 int gs_commit_node_layers(gs_ctx* ctx, uint32_t top_log, uint32_t* const* layers) {
   CTX_REQUIRED(ctx);
   GS_REQUIRE(layers != nullptr, "null layer list");

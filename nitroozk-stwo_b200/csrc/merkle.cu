@@ -15,6 +15,9 @@
 #include "merkle_tail.cuh"
 #include "channel.cuh"
 #include <cstdlib>
+#include <cstring>
+#include <vector>
+#include <algorithm>
 
 namespace gs {
 
@@ -247,6 +250,141 @@ __global__ void __launch_bounds__(TH, TH >= 256 ? 4 : 8)
 
 int commit_node_layers_ch(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters,
                           uint32_t* d_state, uint32_t* d_root_copy, uint32_t* d_felt);
+
+// ------------------------------------------------------------- work-list
+// A tree of the work-list on the device: its columns and layers as offsets
+// into one pointer pool.
+struct MerkleWlItem {
+  uint32_t col_off, n_cols, layer_off, log;
+};
+
+// Persistent grid: block b takes trees b, b + gridDim.x, ... of a list
+// bucketed by decreasing size. Leaf i hashes the columns' values at row i
+// (commit_on_layer without a previous layer: 16 column words per message
+// block, the last block final); each node layer hashes pairs of the layer
+// below from shared memory (two buffers: 2^log and 2^(log-1) hashes), every
+// layer also stored to its global buffer.
+__global__ void __launch_bounds__(256) merkle_worklist_kernel(const MerkleWlItem* __restrict__ items, uint32_t n_items,
+                                                              void* const* __restrict__ pool, uint32_t max_log) {
+  extern __shared__ uint4 sb[];
+  uint4* const buf0 = sb;
+  uint4* const buf1 = sb + 2 * (1u << max_log);
+  for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const MerkleWlItem w = items[it];
+    const uint32_t* const* cols = reinterpret_cast<const uint32_t* const*>(pool + w.col_off);
+    uint32_t* const* layers = reinterpret_cast<uint32_t* const*>(pool + w.layer_off);
+    const uint32_t n = 1u << w.log;
+    const uint32_t total_bytes = 4u * w.n_cols;
+    const uint32_t n_blocks = (w.n_cols + 15u) / 16u;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+      uint32_t h[8], m[16];
+      blake2s_init(h);
+      for (uint32_t blk = 0; blk < n_blocks; blk++) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const uint32_t c = 16 * blk + j;
+          m[j] = c < w.n_cols ? __ldg(cols[c] + i) : 0u;
+        }
+        uint32_t t = 64u * (blk + 1);
+        if (t > total_bytes) t = total_bytes;
+        blake2s_compress(h, m, t, blk + 1 == n_blocks);
+      }
+      store_hash(layers[w.log], i, h);
+      buf0[2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
+      buf0[2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+    }
+    __syncthreads();
+    bool in0 = true;  // the layer below sits in buf0
+    for (int L = (int)w.log - 1; L >= 0; L--) {
+      const uint4* in = in0 ? buf0 : buf1;
+      uint4* out = in0 ? buf1 : buf0;
+      for (uint32_t j = threadIdx.x; j < (1u << L); j += blockDim.x) {
+        uint4 c[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) c[q] = in[4 * j + q];
+        uint32_t h[8];
+        hash_children16(c, h);
+        store_hash(layers[L], j, h);
+        out[2 * j] = make_uint4(h[0], h[1], h[2], h[3]);
+        out[2 * j + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+      }
+      __syncthreads();
+      in0 = !in0;
+    }
+    __syncthreads();  // the next tree reuses the buffers
+  }
+}
+
+int merkle_worklist(Context& ctx, const MerkleItem* items, uint32_t n_items) {
+  if (n_items == 0) return OK;
+  GS_REQUIRE(items != nullptr, "null tree list");
+  cudaStream_t st = ctx.stream;
+  uint32_t count[MERKLE_WL_MAX_LOG + 1] = {0};
+  for (uint32_t k = 0; k < n_items; k++) {
+    const MerkleItem& x = items[k];
+    GS_REQUIRE(x.cols && x.layers && x.n_cols >= 1, "a work-list tree needs columns and layers");
+    GS_REQUIRE(x.log <= 30, "tree log size out of range");
+    for (uint32_t c = 0; c < x.n_cols; c++) GS_REQUIRE(x.cols[c] != nullptr, "null column");
+    for (uint32_t L = 0; L <= x.log; L++)
+      GS_REQUIRE(x.layers[L] && ((uintptr_t)x.layers[L] & 15) == 0, "layer buffers must be 16-byte aligned");
+    if (x.log <= MERKLE_WL_MAX_LOG) count[x.log]++;
+  }
+  // larger trees: the per-tree path
+  for (uint32_t k = 0; k < n_items; k++) {
+    const MerkleItem& x = items[k];
+    if (x.log <= MERKLE_WL_MAX_LOG) continue;
+    const void* const* d = nullptr;
+    GS_TRY(ctx.stage_ptrs((const void* const*)x.cols, x.n_cols, &d));
+    GS_TRY(commit_on_layer(st, x.log, nullptr, (const uint32_t* const*)d, x.n_cols, x.layers[x.log]));
+    GS_TRY(commit_node_layers(st, x.log, x.layers, ctx.tree_counters));
+  }
+  uint32_t first[MERKLE_WL_MAX_LOG + 1] = {0}, total = 0, max_log = 0;
+  for (int lg = (int)MERKLE_WL_MAX_LOG; lg >= 0; lg--) {
+    first[lg] = total;
+    total += count[lg];
+    if (count[lg] && max_log == 0) max_log = (uint32_t)lg;
+  }
+  if (total == 0) return OK;
+  // one upload: the items, then the pointer pool (columns and layers)
+  std::vector<MerkleWlItem> wl(total);
+  std::vector<void*> pool;  // column pointers are only read
+  for (uint32_t k = 0; k < n_items; k++) {
+    const MerkleItem& x = items[k];
+    if (x.log > MERKLE_WL_MAX_LOG) continue;
+    MerkleWlItem w{(uint32_t)pool.size(), x.n_cols, 0, x.log};
+    for (uint32_t c = 0; c < x.n_cols; c++) pool.push_back(const_cast<uint32_t*>(x.cols[c]));
+    w.layer_off = (uint32_t)pool.size();
+    for (uint32_t L = 0; L <= x.log; L++) pool.push_back(x.layers[L]);
+    wl[first[x.log]++] = w;
+  }
+  const size_t o_pool = (wl.size() * sizeof(MerkleWlItem) + 15) & ~(size_t)15;
+  const size_t bytes = o_pool + pool.size() * sizeof(void*);
+  std::vector<uint8_t> up(bytes);
+  memcpy(up.data(), wl.data(), wl.size() * sizeof(MerkleWlItem));
+  memcpy(up.data() + o_pool, pool.data(), pool.size() * sizeof(void*));
+  const void* d = nullptr;
+  void* owned = nullptr;
+  if (bytes <= ctx.ring_cap / 2) {
+    GS_TRY(ctx.stage_bytes(up.data(), bytes, &d));
+  } else {
+    GS_TRY(ctx.alloc_async(bytes, &owned));
+    GS_CUDA_TRY(cudaMemcpyAsync(owned, up.data(), bytes, cudaMemcpyHostToDevice, st));
+    d = owned;
+  }
+  const size_t smem = (size_t)3 * 16 << max_log;  // 2^max_log + 2^(max_log - 1) hashes, reserved as 3 * 2^max_log uint4
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      merkle_worklist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(((size_t)3 * 16) << MERKLE_WL_MAX_LOG));
+  GS_CUDA_TRY(attr);
+  const uint32_t per_sm = (uint32_t)std::min<size_t>(8, ((size_t)200 << 10) / smem);
+  const uint32_t grid = (uint32_t)std::min<size_t>(wl.size(), (size_t)num_sms() * (per_sm ? per_sm : 1));
+  merkle_worklist_kernel<<<grid, 256, smem, st>>>((const MerkleWlItem*)d, (uint32_t)wl.size(),
+                                                  (void* const*)((const uint8_t*)d + o_pool), max_log);
+  note_launch();
+  GS_CUDA_TRY(cudaGetLastError());
+  if (owned) GS_CUDA_TRY(cudaFreeAsync(owned, st));  // stream-ordered: after the kernel
+  return OK;
+}
+
 int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters) {
   return commit_node_layers_ch(st, top_log, layers, d_counters, nullptr, nullptr, nullptr);
 }

@@ -239,6 +239,20 @@ int commit_on_layer(cudaStream_t st, uint32_t log_size, const uint32_t* d_prev, 
 constexpr uint32_t TREE_MAX_LOG = 27;
 constexpr uint32_t TREE_COUNTERS = 1024;
 int commit_node_layers(cudaStream_t st, uint32_t top_log, uint32_t* const* layers, uint32_t* d_counters);
+// One tree of a Merkle work-list: n_cols >= 1 device columns of 2^log words
+// (host array of pointers) and log + 1 device layers (host array; layers[L]
+// holds 2^L hashes, 16-byte aligned), the leaves hashing the columns.
+struct MerkleItem {
+  const uint32_t* const* cols;
+  uint32_t n_cols, log;
+  uint32_t* const* layers;
+};
+constexpr uint32_t MERKLE_WL_MAX_LOG = 10;
+// Many trees: every tree of log <= MERKLE_WL_MAX_LOG whole (leaves and every
+// node layer) in one launch of a persistent grid walking the list, largest
+// first, each tree in one block through shared memory; larger trees through
+// commit_on_layer + commit_node_layers, one tree at a time.
+int merkle_worklist(Context& ctx, const MerkleItem* items, uint32_t n_items);
 // The same, with the root also written to root_out (8 words, e.g. mapped
 // host memory) by the launch that computes it (or copied there when no tree
 // kernel runs).

@@ -38,6 +38,11 @@ class FftItem(C.Structure):
                 ("inverse", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class MerkleItem(C.Structure):
+    """gs_merkle_item: one tree of a Merkle work-list (include/gpustark.h)."""
+    _fields_ = [("cols", VPP), ("n_cols", C.c_uint32), ("log_size", C.c_uint32), ("layers", VPP)]
+
+
 class GpuStarkError(RuntimeError):
     pass
 
@@ -67,6 +72,7 @@ _PROTOS = {
     "gs_fft_get_tuning": [C.c_uint32, C.c_uint32, U32P, U32P],
     "gs_commit_on_layer": [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, VPP, C.c_void_p],
     "gs_commit_node_layers": [C.c_void_p, C.c_uint32, VPP],
+    "gs_merkle_worklist": [C.c_void_p, C.POINTER(MerkleItem), C.c_uint32],
     "gs_poseidon252_commit_on_layer": [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, VPP, C.c_void_p],
     "gs_poseidon252_permute": [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p],
     "gs_poseidon252_grind": [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64)],

@@ -213,6 +213,25 @@ class GpuBackend:
         return layers
 
     @staticmethod
+    def merkle_worklist(trees, ctx=None):
+        """Whole Blake2s Merkle trees of uneven sizes at once (gs_merkle_worklist).
+        trees: lists of columns (tensors of 2^log words each, at least one per
+        tree); returns per tree its layers, layers[L] of 2^L x 8 words."""
+        ctx = ctx or default_context()
+        arr = (L.MerkleItem * max(len(trees), 1))()
+        keep, out = [], []
+        for k, cols in enumerate(trees):
+            log = cols[0].numel().bit_length() - 1
+            layers = [torch.empty((1 << lg) * 8, dtype=torch.int32, device="cuda") for lg in range(log + 1)]
+            cp, kc = L.ptr_array([c.data_ptr() for c in cols])
+            lp, kl = L.ptr_array([t.data_ptr() for t in layers])
+            keep += [kc, kl]
+            arr[k].cols, arr[k].n_cols, arr[k].log_size, arr[k].layers = cp, len(cols), log, lp
+            out.append(layers)
+        L.check(L.lib().gs_merkle_worklist(ctx.handle, arr, len(trees)), "merkle_worklist")
+        return out
+
+    @staticmethod
     def poseidon252_commit_on_layer(log_size, prev_layer, columns, ctx=None, out=None):
         """MerkleOps<Poseidon252MerkleHasher>::commit_on_layer (prover/backend/
         cuda/poseidon252.rs:21-42): 2^log_size felt252 hashes as a uint8 tensor

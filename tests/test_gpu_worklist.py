@@ -1,9 +1,13 @@
-"""Batched FFTs of uneven sizes (gs_fft_worklist): every item equals the
+"""Work-lists of uneven sizes. FFTs (gs_fft_worklist): every item equals the
 oracle's interpolation or evaluation on the same twiddle tree, and the
 per-size entries gs_interpolate_columns / gs_evaluate_columns, bit for bit;
 items inside the work-list range (log 3..13, one launch) and outside it
 (the per-size path) mixed in one call; in-place interpolations; errors for
-bad items."""
+bad items. Merkle trees (gs_merkle_worklist): every layer of every tree
+equals gs_commit_on_layer + gs_commit_node_layers and the oracle's layers,
+trees of log 0..10 in one launch and larger ones on the per-tree path."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -114,3 +118,60 @@ def test_worklist_longer_than_the_staging_ring(B):
     got = host(flat).reshape(n, 1 << log)
     for k in rng.choice(n, 60, replace=False):
         assert np.array_equal(got[k], O.interpolate(data[k], log, root_log=ROOT_LOG))
+
+
+# ----------------------------------------------------------- Merkle trees
+def tree_reference(B, cols):
+    """The per-tree path: gs_commit_on_layer for the leaves, then
+    gs_commit_node_layers."""
+    log = cols[0].numel().bit_length() - 1
+    layers = [torch.empty((1 << lg) * 8, dtype=torch.int32, device="cuda") for lg in range(log + 1)]
+    B.commit_on_layer(log, None, cols, out=layers[log])
+    if log:
+        B.commit_node_layers(layers)
+    return layers
+
+
+@pytest.mark.parametrize("seed,n_trees,logs,max_cols", [(5, 30, list(range(0, 13)), 40), (6, 200, list(range(2, 11)), 20),
+                                                         (7, 3, [11, 12], 17)])
+def test_merkle_worklist_matches_oracle_and_per_tree_path(B, seed, n_trees, logs, max_cols):
+    rng = np.random.default_rng(seed)
+    host_trees, trees = [], []
+    for _ in range(n_trees):
+        log, k = int(rng.choice(logs)), int(rng.integers(1, max_cols + 1))
+        h = [rand_m31(rng, 1 << log) for _ in range(k)]
+        host_trees.append(h)
+        trees.append([dev(c) for c in h])
+    got = B.merkle_worklist(trees)
+    torch.cuda.synchronize()
+    for h, cols, layers in zip(host_trees, trees, got):
+        ref = tree_reference(B, cols)
+        for a, b in zip(layers, ref):
+            assert np.array_equal(host(a), host(b))
+        log = len(layers) - 1
+        if log <= 8:  # the oracle, layer by layer
+            exp = O.commit_on_layer(log, None, h)
+            assert np.array_equal(host(layers[log]).view(np.uint8), exp.reshape(-1))
+            for lg in range(log - 1, -1, -1):
+                exp = O.commit_on_layer(lg, exp, [])
+                assert np.array_equal(host(layers[lg]).view(np.uint8), exp.reshape(-1))
+
+
+def test_merkle_worklist_rejects_bad_trees(B):
+    """A tree without columns, and a misaligned layer, are refused before any launch."""
+    from gpustark import GpuStarkError
+    from gpustark import _lib as L
+    from gpustark.backend import default_context
+    ctx = default_context()
+    col = torch.zeros(1 << 4, dtype=torch.int32, device="cuda")
+    layers = [torch.zeros(((1 << lg) * 8) + 4, dtype=torch.int32, device="cuda") for lg in range(5)]
+    cp, kc = L.ptr_array([col.data_ptr()])
+    item = L.MerkleItem()
+    lp, kl = L.ptr_array([t.data_ptr() for t in layers])
+    item.cols, item.n_cols, item.log_size, item.layers = cp, 0, 4, lp
+    assert L.lib().gs_merkle_worklist(ctx.handle, C.byref(item), 1) != 0
+    assert b"columns and layers" in L.lib().gs_last_error()
+    lp2, kl2 = L.ptr_array([t.data_ptr() + (4 if lg == 2 else 0) for lg, t in enumerate(layers)])
+    item.n_cols, item.layers = 1, lp2
+    assert L.lib().gs_merkle_worklist(ctx.handle, C.byref(item), 1) != 0
+    assert b"16-byte aligned" in L.lib().gs_last_error()
