@@ -105,8 +105,9 @@ int gs_evaluate_columns(gs_ctx* ctx, const uint32_t* const* coeffs, uint32_t coe
  * shared memory; other sizes take the per-size path of gs_interpolate_columns
  * / gs_evaluate_columns. Results equal those entries' bit for bit. Items must
  * not overlap one another. itwiddles / twiddles: the trees of
- * half_odds(twiddles_log_size), twiddles_log_size + 1 >= every log_size (a
- * tree may be NULL when no item needs it). */
+ * half_odds(twiddles_log_size), twiddles_log_size + 1 >= every log_size;
+ * itwiddles may be NULL when no item interpolates, twiddles when no item
+ * evaluates. */
 typedef struct {
   const uint32_t* src;
   uint32_t* dst;
